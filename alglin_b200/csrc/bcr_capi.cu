@@ -1,0 +1,914 @@
+// C ABI of the B200 BorderedCR solver (declarations and reference citations in
+// include/alglin_b200.h).  The handle owns a host copy of the loaded matrix in
+// the reference layout and the device buffers of the factorization; every
+// numerical step runs on the GPU through bcr_kernels.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "alglin_b200.h"
+#include "bcr_device.h"
+
+using bcr::Dims;
+
+namespace {
+
+std::string fmt(const char* f, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, f);
+  vsnprintf(buf, sizeof buf, f, ap);
+  va_end(ap);
+  return buf;
+}
+
+const char* kInternalName[] = {"CyclicReduction+LU", "CyclicReduction+QR", "CyclicReduction+QRP"};
+const char* kLastName[] = {"LastBlock LU", "LastBlock LUPQ", "LastBlock QR", "LastBlock QRP",
+                           "LastBlock SVD", "LastBlock LSS", "LastBlock LSY", "LastBlock PINV"};
+const char* kLast2Name[] = {"LastBlock NONE", "LastBlock SVD", "LastBlock LSS", "LastBlock LSY",
+                            "LastBlock PINV"};
+
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+template <typename T>
+cudaError_t dalloc(T*& p, size_t count) {
+  dfree(p);
+  return cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(count, 1) * sizeof(T));
+}
+
+void gecopy(int m, int n, const double* A, int lda, double* B, int ldb) {
+  for (int j = 0; j < n; ++j) std::memcpy(B + (size_t)j * ldb, A + (size_t)j * lda, sizeof(double) * m);
+}
+
+void geadd(int m, int n, const double* A, int lda, double* B, int ldb) {
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < m; ++i) B[(size_t)j * ldb + i] += A[(size_t)j * lda + i];
+}
+
+}  // namespace
+
+struct bcr_handle_s {
+  // construction / partition (kept for info(), hxx:373-423, cc:139-158)
+  int nthreads = 0;
+  int max_parallel_block = 1;
+  int used_parallel_block = 1;
+  // sizes
+  Dims d{};
+  bool allocated = false;
+  // selections and flags
+  int sel = 0, sel_last = 0, sel_last2 = 0;
+  bool fthread = true, sthread = true, debug = false;
+  int precision = BCR_PRECISION_FP64;
+  std::string err = "no error";
+  std::string info_buf;
+  // host copy of the loaded matrix (reference layout)
+  std::vector<double> hD, hE, hB, hC, hCq, hF, hH;
+  // device
+  bool dev_ready = false, dirty = true, factorized = false;
+  bcr::DevState s{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  double* dX = nullptr;
+  size_t dX_cap = 0;
+  double* dY = nullptr;
+  size_t dY_cap = 0;
+  std::vector<void*> pinned;
+
+  int fail(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+  int L() const { return std::max(nrows(), ncols()); }
+  int nrows() const { return d.n * (d.nblock + 1) + d.qr + d.nr; }
+  int ncols() const { return d.n * (d.nblock + 1) + d.qx + d.nx; }
+
+  void partition() {
+    // cc:139-158: each chunk keeps at least two block rows
+    int NBLK = std::max(1, max_parallel_block);
+    int used = NBLK, red = 2 * NBLK;
+    while (red > d.nblock) { red -= 2; --used; }
+    used_parallel_block = used <= 1 ? 1 : used;
+  }
+  int thread_count() const { return nthreads > 0 ? nthreads : 1; }
+
+  void release_device() {
+    if (!dev_ready) return;
+    cudaDeviceSynchronize();
+    for (void* p : pinned) cudaHostUnregister(p);
+    pinned.clear();
+    bcr::DevState& z = s;
+    dfree(z.D0); dfree(z.E0); dfree(z.B0); dfree(z.C0); dfree(z.Cq); dfree(z.F0); dfree(z.H);
+    dfree(z.D); dfree(z.E); dfree(z.B); dfree(z.C); dfree(z.T); dfree(z.P);
+    dfree(z.Rbuf); dfree(z.Fbuf); dfree(z.XB); dfree(z.part); dfree(z.Ffin); dfree(z.Hl);
+    dfree(z.tau_l); dfree(z.piv_l); dfree(z.st); dfree(z.mv_part);
+    dfree(dX); dfree(dY);
+    dX_cap = dY_cap = 0;
+    if (own_stream && stream) cudaStreamDestroy(stream);
+    if (own_stream) stream = nullptr;
+    own_stream = false;
+    dev_ready = false;
+    dirty = true;
+    factorized = false;
+  }
+
+  int cuda_fail(cudaError_t e, const char* where) {
+    return fail(BCR_CUDA_ERROR, fmt("alglin_b200: CUDA error in %s: %s\n", where, cudaGetErrorString(e)));
+  }
+
+  int ensure_device() {
+    if (dev_ready) return BCR_OK;
+    if (!allocated) return fail(BCR_BAD_ARGUMENT, "BorderedCR: allocate() must be called first\n");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+      return fail(BCR_CUDA_ERROR, "alglin_b200: no CUDA device is available (the solver has no CPU path)\n");
+    if (bcr::panel_smem_per_warp(d, 8) > 227 * 1024)
+      return fail(BCR_BAD_ARGUMENT,
+                  fmt("alglin_b200: block size n=%d with nr=%d, nx=%d exceeds the shared-memory panel "
+                      "of the FP64 device path\n", d.n, d.nr, d.nx));
+    if (!stream) {
+      e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+      own_stream = true;
+    }
+    const size_t nb = d.nblock, n = d.n, nr = d.nr, nx = d.nx, qx = d.qx, qr = d.qr;
+    const size_t Lmax = std::max(d.Nr, d.Nc);
+    bcr::DevState& z = s;
+    z.d = d;
+    cudaError_t r = cudaSuccess;
+    auto A = [&](cudaError_t x) { if (r == cudaSuccess) r = x; };
+    A(dalloc(z.D0, nb * n * n)); A(dalloc(z.E0, nb * n * n)); A(dalloc(z.B0, nb * n * nx));
+    A(dalloc(z.C0, (nb + 1) * nr * n)); A(dalloc(z.Cq, nr * qx)); A(dalloc(z.F0, nr * nx));
+    A(dalloc(z.H, (n + qr) * d.Nc));
+    A(dalloc(z.D, nb * n * n)); A(dalloc(z.E, nb * n * n)); A(dalloc(z.B, nb * n * nx));
+    A(dalloc(z.C, (nb + 1) * nr * n)); A(dalloc(z.T, nb * (2 * n * n + n))); A(dalloc(z.P, nb * n));
+    A(dalloc(z.Rbuf, nb * nr * n)); A(dalloc(z.Fbuf, nb * nr * nx));
+    z.xb_cap = 16;
+    A(dalloc(z.XB, nb * nr * 16));
+    const size_t parts = (nb + 1 + 63) / 64 + 1;
+    z.part_cap = (int)(parts * std::max<size_t>({nr * nx, nr * 16, nr, 1}));
+    A(dalloc(z.part, (size_t)z.part_cap));
+    A(dalloc(z.Ffin, std::max<size_t>(nr * nx, 1)));
+    A(dalloc(z.Hl, (size_t)d.Nr * d.Nc)); A(dalloc(z.tau_l, Lmax)); A(dalloc(z.piv_l, Lmax));
+    A(dalloc(z.st, 1)); A(dalloc(z.mv_part, (nb + 2) * nr));
+    if (r != cudaSuccess) {
+      dev_ready = true;
+      release_device();
+      return cuda_fail(r, "device allocation");
+    }
+    // pin the host copy so the per-factorize upload runs at full PCIe rate
+    for (std::vector<double>* v : {&hD, &hE, &hB, &hC, &hCq, &hF, &hH})
+      if (!v->empty() && cudaHostRegister(v->data(), v->size() * 8, cudaHostRegisterDefault) == cudaSuccess)
+        pinned.push_back(v->data());
+    cudaGetLastError();
+    dev_ready = true;
+    dirty = true;
+    return BCR_OK;
+  }
+
+  int upload() {
+    int rc = ensure_device();
+    if (rc) return rc;
+    bcr::DevState& z = s;
+    auto up = [&](double* dst, const std::vector<double>& v) {
+      if (!v.empty()) cudaMemcpyAsync(dst, v.data(), v.size() * 8, cudaMemcpyHostToDevice, stream);
+    };
+    up(z.D0, hD); up(z.E0, hE); up(z.B0, hB); up(z.C0, hC); up(z.Cq, hCq); up(z.F0, hF); up(z.H, hH);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "upload");
+    dirty = false;
+    return BCR_OK;
+  }
+
+  int ensure_buffer(double*& p, size_t& cap, size_t count) {
+    if (cap >= count) return BCR_OK;
+    cudaStreamSynchronize(stream);
+    cudaError_t e = dalloc(p, count);
+    if (e != cudaSuccess) { cap = 0; return cuda_fail(e, "scratch allocation"); }
+    cap = count;
+    return BCR_OK;
+  }
+
+  int read_status(bcr::StatusWords& st) {
+    cudaError_t e = cudaMemcpyAsync(&st, s.st, sizeof st, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(e, "factorize");
+    return BCR_OK;
+  }
+
+  int factorize_device() {
+    factorized = false;
+    if (sel_last != bcr::LAST_LU && sel_last != bcr::LAST_QR)
+      return fail(BCR_NUMERICAL,
+                  fmt("BorderedCR<t_Value>::load_and_factorize_last failed\n"
+                      "(last block solver '%s' is not available on the device)\n", kLastName[sel_last]));
+    s.sel = sel;
+    s.sel_last = sel_last;
+    bcr::launch_factorize(s, stream);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "factorize launch");
+    bcr::StatusWords st{};
+    int rc = read_status(st);
+    if (rc) return rc;
+    if (st.code == bcr::DEV_ZERO_PIVOT) {
+      const int n = d.n;
+      if (sel == bcr::SEL_LU)
+        return fail(BCR_NUMERICAL, fmt("BorderedCR::buildT [LU] getrf(M=%d,N=%d,A,LDA=%d,iperm)::INFO = %d\n",
+                                       2 * n, n, 2 * n, st.info));
+      return fail(BCR_NUMERICAL, fmt("BorderedCR::buildT [%s] singular R factor at block %d (column %d)\n",
+                                     sel == bcr::SEL_QR ? "QR" : "QRP", st.block, st.info));
+    }
+    if (st.code == bcr::DEV_LAST_SINGULAR || st.code == bcr::DEV_BAD_SHAPE) {
+      if (sel_last2 != 0)
+        return fail(BCR_NUMERICAL,
+                    fmt("BorderedCR<t_Value>::load_and_factorize_last failed\n"
+                        "(fallback solver '%s' is not available on the device)\n", kLast2Name[sel_last2]));
+      return fail(BCR_NUMERICAL, "BorderedCR<t_Value>::load_and_factorize_last failed\n");
+    }
+    factorized = true;
+    return BCR_OK;
+  }
+
+  int solve_device(int nrhs, double* dx, int ld) {
+    if (!factorized) return fail(BCR_NUMERICAL, "BorderedCR::solve: the matrix is not factorized\n");
+    if (nrhs < 0 || ld < L()) return fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::solve: bad ldRhs = %d\n", ld));
+    if (nrhs == 0) return BCR_OK;
+    bcr::launch_solve(s, dx, ld, nrhs, stream);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "solve launch");
+    return BCR_OK;
+  }
+
+  int solve_host(int nrhs, double* x, int ld) {
+    if (!factorized) return fail(BCR_NUMERICAL, "BorderedCR::solve: the matrix is not factorized\n");
+    if (nrhs < 0 || ld < L()) return fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::solve: bad ldRhs = %d\n", ld));
+    if (nrhs == 0) return BCR_OK;
+    const size_t Lx = (size_t)L();
+    int rc = ensure_buffer(dX, dX_cap, Lx * nrhs);
+    if (rc) return rc;
+    cudaMemcpy2DAsync(dX, Lx * 8, x, (size_t)ld * 8, Lx * 8, nrhs, cudaMemcpyHostToDevice, stream);
+    rc = solve_device(nrhs, dX, (int)Lx);
+    if (rc) return rc;
+    cudaMemcpy2DAsync(x, (size_t)ld * 8, dX, Lx * 8, Lx * 8, nrhs, cudaMemcpyDeviceToHost, stream);
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(e, "solve");
+    return BCR_OK;
+  }
+
+  // --------------------------------------------------------------- check ---
+  int check_matrix() {
+    // cc:2538-2659
+    const int n = d.n, nb = d.nblock;
+    auto scan = [&](const std::vector<double>& v, int NR, int NC, int nblk, const char* name,
+                    bool blocked) -> int {
+      const size_t SB = (size_t)NR * NC;
+      for (size_t i = 0; i < SB * nblk; ++i)
+        if (!std::isfinite(v[i])) {
+          const size_t b = i / SB, w = i - b * SB;
+          if (blocked)
+            return fail(BCR_BAD_ARGUMENT,
+                        fmt("BorderedCR::check_matrix, found %g at block %zu position (%zu,%zu) of %dx%d matrix %s\n",
+                            v[i], b, w % NR, w / NR, NR, NC, name));
+          return fail(BCR_BAD_ARGUMENT,
+                      fmt("BorderedCR::check_matrix, found %g at position (%zu,%zu) of %dx%d matrix %s\n",
+                          v[i], w % NR, w / NR, NR, NC, name));
+        }
+      return BCR_OK;
+    };
+    int rc;
+    if ((rc = scan(hH, n + d.qr, d.Nc, 1, "H0Hqp", false))) return rc;
+    if ((rc = scan(hB, n, d.nx, nb, "B", true))) return rc;
+    if ((rc = scan(hC, d.nr, n, nb + 1, "C", true))) return rc;
+    if ((rc = scan(hCq, d.nr, d.qx, 1, "Cq", false))) return rc;
+    if ((rc = scan(hD, n, n, nb, "D", true))) return rc;
+    if ((rc = scan(hE, n, n, nb, "E", true))) return rc;
+    if ((rc = scan(hF, d.nr, d.nx, 1, "F", false))) return rc;
+    return BCR_OK;
+  }
+};
+
+#define H_CHECK(h)                                    \
+  do {                                                \
+    if (!(h)) return BCR_BAD_ARGUMENT;                \
+  } while (0)
+#define H_ALLOC(h)                                                                   \
+  do {                                                                               \
+    H_CHECK(h);                                                                      \
+    if (!(h)->allocated) return (h)->fail(BCR_BAD_ARGUMENT, "BorderedCR: allocate() must be called first\n"); \
+  } while (0)
+#define NBL_CHECK(h, nbl, hi, what)                                                            \
+  do {                                                                                         \
+    if ((nbl) < 0 || (nbl) > (hi))                                                             \
+      return (h)->fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::%s( %d, ...) block index out of range\n", what, nbl)); \
+  } while (0)
+#define LD_CHECK(h, ld, rows, what)                                                                    \
+  do {                                                                                                 \
+    if ((ld) < (rows))                                                                                 \
+      return (h)->fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::%s, bad leading dimension %d < %d\n", what, ld, rows)); \
+  } while (0)
+
+extern "C" {
+
+int bcr_create(bcr_handle* out, int num_threads, int num_parallel_block) {
+  if (!out) return BCR_BAD_ARGUMENT;
+  auto* h = new bcr_handle_s;
+  h->nthreads = num_threads > 0 ? num_threads : 0;
+  if (h->nthreads > 0)
+    h->max_parallel_block = num_parallel_block == 0 ? h->nthreads : std::min(h->nthreads, num_parallel_block);
+  else
+    h->max_parallel_block = 1;
+  *out = h;
+  return BCR_OK;
+}
+
+int bcr_destroy(bcr_handle h) {
+  if (!h) return BCR_OK;
+  h->release_device();
+  delete h;
+  return BCR_OK;
+}
+
+int bcr_allocate(bcr_handle h, int nblock, int n, int qr, int qx, int nr, int nx) {
+  H_CHECK(h);
+  if (nblock < 1 || n < 1 || qr < 0 || qx < 0 || nr < 0 || nx < 0)
+    return h->fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::allocate( nblock=%d, n=%d, qr=%d, qx=%d, nr=%d, nx=%d ) bad sizes\n",
+                                         nblock, n, qr, qx, nr, nx));
+  if (h->allocated && h->d.nblock == nblock && h->d.n == n && h->d.qr == qr && h->d.qx == qx &&
+      h->d.nr == nr && h->d.nx == nx) {
+    h->partition();
+    return BCR_OK;  // cc:55-61
+  }
+  h->release_device();
+  Dims d{};
+  d.nblock = nblock; d.n = n; d.qr = qr; d.qx = qx; d.nr = nr; d.nx = nx;
+  d.Nr = 2 * n + nr + qr;
+  d.Nc = 2 * n + nx + qx;
+  h->d = d;
+  const size_t nb = nblock;
+  h->hD.assign(nb * n * n, 0.0);
+  h->hE.assign(nb * n * n, 0.0);
+  h->hB.assign(nb * n * nx, 0.0);
+  h->hC.assign((nb + 1) * nr * n, 0.0);
+  h->hCq.assign((size_t)nr * qx, 0.0);
+  h->hF.assign((size_t)nr * nx, 0.0);
+  h->hH.assign((size_t)(n + qr) * d.Nc, 0.0);
+  h->allocated = true;
+  h->dirty = true;
+  h->factorized = false;
+  h->partition();
+  return BCR_OK;
+}
+
+int bcr_dup(bcr_handle dst, bcr_handle src) {
+  H_CHECK(dst);
+  H_ALLOC(src);
+  dst->max_parallel_block = src->max_parallel_block;
+  int rc = bcr_allocate(dst, src->d.nblock, src->d.n, src->d.qr, src->d.qx, src->d.nr, src->d.nx);
+  if (rc) return rc;
+  dst->hD = src->hD; dst->hE = src->hE; dst->hB = src->hB; dst->hC = src->hC;
+  dst->hCq = src->hCq; dst->hF = src->hF; dst->hH = src->hH;
+  if (dst->dev_ready) dst->release_device();  // host vectors were replaced: re-pin lazily
+  dst->nthreads = 0;  // cc:197: the copy runs on the inline pool
+  dst->dirty = true;
+  dst->factorized = false;
+  return BCR_OK;
+}
+
+int bcr_nrows(bcr_handle h) { return h ? h->nrows() : 0; }
+int bcr_ncols(bcr_handle h) { return h ? h->ncols() : 0; }
+int bcr_number_of_blocks(bcr_handle h) { return h ? h->d.nblock : 0; }
+int bcr_block_size(bcr_handle h) { return h ? h->d.n : 0; }
+int bcr_dim_qr(bcr_handle h) { return h ? h->d.qr : 0; }
+int bcr_dim_qx(bcr_handle h) { return h ? h->d.qx : 0; }
+int bcr_dim_nr(bcr_handle h) { return h ? h->d.nr : 0; }
+int bcr_dim_nx(bcr_handle h) { return h ? h->d.nx : 0; }
+int bcr_Nr(bcr_handle h) { return h ? h->d.Nr : 0; }
+int bcr_Nc(bcr_handle h) { return h ? h->d.Nc : 0; }
+
+#define ZERO_FN(name, vec)                                 \
+  int name(bcr_handle h) {                                 \
+    H_ALLOC(h);                                            \
+    std::fill(h->vec.begin(), h->vec.end(), 0.0);          \
+    h->dirty = true;                                       \
+    return BCR_OK;                                         \
+  }
+ZERO_FN(bcr_zero_B, hB)
+ZERO_FN(bcr_zero_C, hC)
+ZERO_FN(bcr_zero_Cq, hCq)
+ZERO_FN(bcr_zero_D, hD)
+ZERO_FN(bcr_zero_E, hE)
+ZERO_FN(bcr_zero_F, hF)
+ZERO_FN(bcr_zero_H, hH)
+#undef ZERO_FN
+
+int bcr_fill_zero(bcr_handle h) {
+  H_ALLOC(h);
+  bcr_zero_B(h); bcr_zero_C(h); bcr_zero_Cq(h); bcr_zero_D(h); bcr_zero_E(h); bcr_zero_F(h); bcr_zero_H(h);
+  return BCR_OK;
+}
+
+int bcr_load_B(bcr_handle h, int nbl, const double* B, int ldB) {
+  H_ALLOC(h);
+  NBL_CHECK(h, nbl, h->d.nblock - 1, "load_B");
+  LD_CHECK(h, ldB, h->d.n, "load_B");
+  const int n = h->d.n, nx = h->d.nx;
+  gecopy(n, nx, B, ldB, h->hB.data() + (size_t)nbl * n * nx, n);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_add_to_B(bcr_handle h, int nbl, const double* B, int ldB) {
+  H_ALLOC(h);
+  NBL_CHECK(h, nbl, h->d.nblock - 1, "add_to_B");
+  LD_CHECK(h, ldB, h->d.n, "add_to_B");
+  const int n = h->d.n, nx = h->d.nx;
+  geadd(n, nx, B, ldB, h->hB.data() + (size_t)nbl * n * nx, n);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_load_C(bcr_handle h, int nbl, const double* C, int ldC) {
+  H_ALLOC(h);
+  NBL_CHECK(h, nbl, h->d.nblock, "load_C");
+  LD_CHECK(h, ldC, h->d.nr, "load_C");
+  const int n = h->d.n, nr = h->d.nr;
+  gecopy(nr, n, C, ldC, h->hC.data() + (size_t)nbl * nr * n, nr);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_add_to_C(bcr_handle h, int nbl, const double* C, int ldC) {
+  H_ALLOC(h);
+  NBL_CHECK(h, nbl, h->d.nblock, "add_to_C");
+  if (ldC < h->d.nr) return h->fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::add_to_C( %d, C, ldC = %d ) bad ldC\n", nbl, ldC));
+  const int n = h->d.n, nr = h->d.nr;
+  geadd(nr, n, C, ldC, h->hC.data() + (size_t)nbl * nr * n, nr);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_add_to_C2(bcr_handle h, int nbl, const double* C, int ldC) {
+  H_ALLOC(h);
+  NBL_CHECK(h, nbl, h->d.nblock - 1, "add_to_C2");
+  if (ldC < h->d.nr) return h->fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::add_to_C2( %d, C, ldC = %d ) bad ldC\n", nbl, ldC));
+  const int n = h->d.n, nr = h->d.nr;
+  geadd(nr, 2 * n, C, ldC, h->hC.data() + (size_t)nbl * nr * n, nr);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_add_to_C2F(bcr_handle h, int nbl, const double* C2F, int ldC) {
+  H_ALLOC(h);
+  NBL_CHECK(h, nbl, h->d.nblock - 1, "add_to_C2F");
+  if (ldC < h->d.nr) return h->fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::add_to_C2F( %d, C2F, ldC = %d ) bad ldC\n", nbl, ldC));
+  const int n = h->d.n, nr = h->d.nr, nx = h->d.nx;
+  geadd(nr, 2 * n, C2F, ldC, h->hC.data() + (size_t)nbl * nr * n, nr);
+  geadd(nr, nx, C2F + (size_t)ldC * 2 * n, ldC, h->hF.data(), nr);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_load_D(bcr_handle h, int nbl, const double* D, int ldD) {
+  H_ALLOC(h);
+  NBL_CHECK(h, nbl, h->d.nblock - 1, "load_D");
+  LD_CHECK(h, ldD, h->d.n, "load_D");
+  const int n = h->d.n;
+  gecopy(n, n, D, ldD, h->hD.data() + (size_t)nbl * n * n, n);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_load_E(bcr_handle h, int nbl, const double* E, int ldE) {
+  H_ALLOC(h);
+  NBL_CHECK(h, nbl, h->d.nblock - 1, "load_E");
+  LD_CHECK(h, ldE, h->d.n, "load_E");
+  const int n = h->d.n;
+  gecopy(n, n, E, ldE, h->hE.data() + (size_t)nbl * n * n, n);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_load_DE(bcr_handle h, int nbl, const double* DE, int ldDE) {
+  H_ALLOC(h);
+  NBL_CHECK(h, nbl, h->d.nblock - 1, "load_DE");
+  LD_CHECK(h, ldDE, h->d.n, "load_DE");
+  const int n = h->d.n;
+  gecopy(n, n, DE, ldDE, h->hD.data() + (size_t)nbl * n * n, n);
+  gecopy(n, n, DE + (size_t)n * ldDE, ldDE, h->hE.data() + (size_t)nbl * n * n, n);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_load_DEB(bcr_handle h, int nbl, const double* DEB, int ldDEB) {
+  H_ALLOC(h);
+  NBL_CHECK(h, nbl, h->d.nblock - 1, "load_DEB");
+  LD_CHECK(h, ldDEB, h->d.n, "load_DEB");
+  const int n = h->d.n, nx = h->d.nx;
+  gecopy(n, n, DEB, ldDEB, h->hD.data() + (size_t)nbl * n * n, n);
+  gecopy(n, n, DEB + (size_t)n * ldDEB, ldDEB, h->hE.data() + (size_t)nbl * n * n, n);
+  gecopy(n, nx, DEB + (size_t)2 * n * ldDEB, ldDEB, h->hB.data() + (size_t)nbl * n * nx, n);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_load_F(bcr_handle h, const double* F, int ldF) {
+  H_ALLOC(h);
+  LD_CHECK(h, ldF, h->d.nr, "load_F");
+  gecopy(h->d.nr, h->d.nx, F, ldF, h->hF.data(), h->d.nr);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_add_to_F(bcr_handle h, const double* F, int ldF) {
+  H_ALLOC(h);
+  LD_CHECK(h, ldF, h->d.nr, "add_to_F");
+  geadd(h->d.nr, h->d.nx, F, ldF, h->hF.data(), h->d.nr);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_load_Cq(bcr_handle h, const double* Cq, int ldC) {
+  H_ALLOC(h);
+  LD_CHECK(h, ldC, h->d.nr, "load_Cq");
+  gecopy(h->d.nr, h->d.qx, Cq, ldC, h->hCq.data(), h->d.nr);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_load_CqF(bcr_handle h, const double* CqF, int ldCF) {
+  H_ALLOC(h);
+  LD_CHECK(h, ldCF, h->d.nr, "load_CqF");
+  const int nr = h->d.nr, qx = h->d.qx, nx = h->d.nx;
+  gecopy(nr, qx, CqF, ldCF, h->hCq.data(), nr);
+  gecopy(nr, nx, CqF + (size_t)qx * ldCF, ldCF, h->hF.data(), nr);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_load_bottom(bcr_handle h, const double* H0, int ld0, const double* HN, int ldN,
+                    const double* Hq, int ldQ, const double* Hp, int ldP) {
+  H_ALLOC(h);
+  const int n = h->d.n, m = n + h->d.qr;
+  LD_CHECK(h, ld0, m, "load_bottom");
+  LD_CHECK(h, ldN, m, "load_bottom");
+  if (h->d.qx) LD_CHECK(h, ldQ, m, "load_bottom");
+  if (h->d.nx) LD_CHECK(h, ldP, m, "load_bottom");
+  double* H = h->hH.data();
+  gecopy(m, n, H0, ld0, H, m); H += (size_t)m * n;
+  gecopy(m, n, HN, ldN, H, m); H += (size_t)m * n;
+  gecopy(m, h->d.qx, Hq, ldQ, H, m); H += (size_t)m * h->d.qx;
+  gecopy(m, h->d.nx, Hp, ldP, H, m);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_load_bottom_H(bcr_handle h, const double* Hm, int ldH) {
+  H_ALLOC(h);
+  const int m = h->d.n + h->d.qr;
+  LD_CHECK(h, ldH, m, "load_bottom");
+  gecopy(m, h->d.Nc, Hm, ldH, h->hH.data(), m);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_load_bottom2(bcr_handle h, const double* C0, int ld0, const double* CN, int ldN,
+                     const double* Cq, int ldCq, const double* F, int ldF) {
+  H_ALLOC(h);
+  const int n = h->d.n, nr = h->d.nr;
+  if (nr == 0) return BCR_OK;
+  LD_CHECK(h, ld0, nr, "load_bottom2");
+  LD_CHECK(h, ldN, nr, "load_bottom2");
+  gecopy(nr, n, C0, ld0, h->hC.data(), nr);
+  gecopy(nr, n, CN, ldN, h->hC.data() + (size_t)h->d.nblock * nr * n, nr);
+  if (h->d.qx) { LD_CHECK(h, ldCq, nr, "load_bottom2"); gecopy(nr, h->d.qx, Cq, ldCq, h->hCq.data(), nr); }
+  if (h->d.nx) { LD_CHECK(h, ldF, nr, "load_bottom2"); gecopy(nr, h->d.nx, F, ldF, h->hF.data(), nr); }
+  h->dirty = true;
+  return BCR_OK;
+}
+
+int bcr_load_bottom2_H(bcr_handle h, const double* P, int ld) {
+  H_ALLOC(h);
+  const int n = h->d.n, nr = h->d.nr;
+  if (nr == 0) return BCR_OK;
+  LD_CHECK(h, ld, nr, "load_bottom2");
+  gecopy(nr, n, P, ld, h->hC.data(), nr); P += (size_t)ld * n;
+  gecopy(nr, n, P, ld, h->hC.data() + (size_t)h->d.nblock * nr * n, nr); P += (size_t)ld * n;
+  gecopy(nr, h->d.qx, P, ld, h->hCq.data(), nr); P += (size_t)ld * h->d.qx;
+  gecopy(nr, h->d.nx, P, ld, h->hF.data(), nr);
+  h->dirty = true;
+  return BCR_OK;
+}
+
+double* bcr_block_data(bcr_handle h, char which, int nbl) {
+  if (!h || !h->allocated) return nullptr;
+  const Dims& d = h->d;
+  h->dirty = true;  // the caller may write through the pointer
+  switch (which) {
+    case 'B': return nbl >= 0 && nbl < d.nblock ? h->hB.data() + (size_t)nbl * d.n * d.nx : nullptr;
+    case 'C': return nbl >= 0 && nbl <= d.nblock ? h->hC.data() + (size_t)nbl * d.nr * d.n : nullptr;
+    case 'D': return nbl >= 0 && nbl < d.nblock ? h->hD.data() + (size_t)nbl * d.n * d.n : nullptr;
+    case 'E': return nbl >= 0 && nbl < d.nblock ? h->hE.data() + (size_t)nbl * d.n * d.n : nullptr;
+    case 'F': return h->hF.data();
+    case 'Q': return h->hCq.data();
+    case 'H': return h->hH.data();
+    default: return nullptr;
+  }
+}
+
+int bcr_select(bcr_handle h, const char* c) {
+  H_CHECK(h);
+  std::string s = c ? c : "";
+  if (s == "LU") h->sel = 0;
+  else if (s == "QR") h->sel = 1;
+  else if (s == "QRP") h->sel = 2;
+  else
+    return h->fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::select( choice='%s' )\nunknown/unsupported factorization type ('LU','QR','QRP')", s.c_str()));
+  h->factorized = false;
+  return BCR_OK;
+}
+
+int bcr_select_last(bcr_handle h, const char* c) {
+  H_CHECK(h);
+  std::string s = c ? c : "";
+  static const char* names[] = {"LU", "LUPQ", "QR", "QRP", "SVD", "LSS", "LSY", "PINV"};
+  for (int i = 0; i < 8; ++i)
+    if (s == names[i]) { h->sel_last = i; h->factorized = false; return BCR_OK; }
+  return h->fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::select_last( choice='%s' )\nunknown/unsupported factorization type ('LU','LUPQ','QR','QRP','SVD','LSS','LSY','PINV')", s.c_str()));
+}
+
+int bcr_select_last2(bcr_handle h, const char* c) {
+  H_CHECK(h);
+  std::string s = c ? c : "";
+  static const char* names[] = {"NONE", "SVD", "LSS", "LSY", "PINV"};
+  for (int i = 0; i < 5; ++i)
+    if (s == names[i]) { h->sel_last2 = i; h->factorized = false; return BCR_OK; }
+  return h->fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::select_last2( choice='%s' )\nunknown/unsupported factorization type ('NONE','SVD','LSS','LSY','PINV')", s.c_str()));
+}
+
+int bcr_selected(bcr_handle h, int* internal, int* last, int* last2) {
+  H_CHECK(h);
+  if (internal) *internal = h->sel;
+  if (last) *last = h->sel_last;
+  if (last2) *last2 = h->sel_last2;
+  return BCR_OK;
+}
+
+int bcr_set_factorize_use_thread(bcr_handle h, int yes) { H_CHECK(h); h->fthread = yes != 0; return BCR_OK; }
+int bcr_set_solve_use_thread(bcr_handle h, int yes) { H_CHECK(h); h->sthread = yes != 0; return BCR_OK; }
+int bcr_factorize_use_thread(bcr_handle h) { return h && h->fthread ? 1 : 0; }
+int bcr_solve_use_thread(bcr_handle h) { return h && h->sthread ? 1 : 0; }
+
+int bcr_set_num_parallel_block(bcr_handle h, int npb) {
+  H_CHECK(h);
+  h->max_parallel_block = std::max(1, std::min(h->thread_count(), npb));  // hxx:407-423
+  h->partition();
+  return BCR_OK;
+}
+
+int bcr_set_precision(bcr_handle h, int p) {
+  H_CHECK(h);
+  if (p != BCR_PRECISION_FP64 && p != BCR_PRECISION_MIXED)
+    return h->fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::set_precision( %d ) unknown precision\n", p));
+  h->precision = p;
+  h->factorized = false;
+  return BCR_OK;
+}
+
+const char* bcr_info(bcr_handle h, const char* indent) {
+  if (!h) return "";
+  const char* in = indent ? indent : "";
+  h->info_buf = fmt(
+      "%srows   = %d\n%scols   = %d\n%snblock = %d\n%sn      = %d\n%sqr     = %d\n%sqx     = %d\n"
+      "%snr     = %d\n%snx     = %d\n%streads = %d/nblk:%d/factorize:%s/solve:%s\n"
+      "%sintern = %s\n%slast   = %s\n%slast2  = %s\n",
+      in, h->nrows(), in, h->ncols(), in, h->d.nblock, in, h->d.n, in, h->d.qr, in, h->d.qx, in,
+      h->d.nr, in, h->d.nx, in, h->thread_count(), h->used_parallel_block, h->fthread ? "true" : "false",
+      h->sthread ? "true" : "false", in, kInternalName[h->sel], in, kLastName[h->sel_last], in,
+      kLast2Name[h->sel_last2]);
+  return h->info_buf.c_str();
+}
+
+const char* bcr_last_error(bcr_handle h) { return h ? h->err.c_str() : "invalid handle"; }
+
+int bcr_set_debug(bcr_handle h, int yes) { H_CHECK(h); h->debug = yes != 0; return BCR_OK; }
+
+int bcr_check_matrix(bcr_handle h) {
+  H_ALLOC(h);
+  return h->check_matrix();
+}
+
+int bcr_factorize(bcr_handle h) {
+  H_ALLOC(h);
+  if (h->debug) {
+    int rc = h->check_matrix();
+    if (rc) return rc;
+  }
+  int rc = h->upload();
+  if (rc) return rc;
+  return h->factorize_device();
+}
+
+int bcr_solve(bcr_handle h, double* x) {
+  H_ALLOC(h);
+  return h->solve_host(1, x, h->L());
+}
+
+int bcr_solve_n(bcr_handle h, int nrhs, double* rhs, int ldRhs) {
+  H_ALLOC(h);
+  return h->solve_host(nrhs, rhs, ldRhs);
+}
+
+int bcr_t_solve(bcr_handle h, double*) {
+  H_CHECK(h);
+  return h->fail(BCR_BAD_ARGUMENT, "BorderedCR::t_solve() not defined\n");
+}
+
+int bcr_t_solve_n(bcr_handle h, int, double*, int) {
+  H_CHECK(h);
+  return h->fail(BCR_BAD_ARGUMENT, "BorderedCR::t_solve() not defined\n");
+}
+
+static int mv_host(bcr_handle h, double alpha, const double* x, double beta, double* res) {
+  int rc = h->ensure_device();
+  if (rc) return rc;
+  if (h->dirty && (rc = h->upload())) return rc;
+  const size_t nc = h->ncols(), nrw = h->nrows();
+  if ((rc = h->ensure_buffer(h->dX, h->dX_cap, std::max(nc, (size_t)1)))) return rc;
+  if ((rc = h->ensure_buffer(h->dY, h->dY_cap, std::max(nrw, (size_t)1)))) return rc;
+  cudaMemcpyAsync(h->dX, x, nc * 8, cudaMemcpyHostToDevice, h->stream);
+  if (beta != 0.0) cudaMemcpyAsync(h->dY, res, nrw * 8, cudaMemcpyHostToDevice, h->stream);
+  bcr::launch_mv(h->s, alpha, h->dX, beta, h->dY, h->stream);
+  cudaMemcpyAsync(res, h->dY, nrw * 8, cudaMemcpyDeviceToHost, h->stream);
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "Mv");
+  return BCR_OK;
+}
+
+int bcr_mv(bcr_handle h, const double* x, double* res) {
+  H_ALLOC(h);
+  return mv_host(h, 1.0, x, 0.0, res);
+}
+
+int bcr_add_mv(bcr_handle h, double alpha, const double* x, double* res) {
+  H_ALLOC(h);
+  return mv_host(h, alpha, x, 1.0, res);
+}
+
+// ----------------------------------------------------------------- sparse ---
+int bcr_sparse_nnz(bcr_handle h) {
+  if (!h) return 0;
+  const Dims& d = h->d;
+  return d.n * d.nblock * (2 * d.n + d.nx + d.nr) + d.nr * (d.n + d.qx + d.nx) + (d.n + d.qr) * (2 * d.n + d.qx + d.nx);
+}
+
+int bcr_sparse_pattern(bcr_handle h, int* I, int* J, int offs) {
+  H_ALLOC(h);
+  const Dims& d = h->d;
+  const int n = d.n, nb = d.nblock, nr = d.nr, nx = d.nx, qr = d.qr, qx = d.qx;
+  int k = 0;
+  for (int nbl = 0; nbl < nb; ++nbl) {
+    for (int ij = 0; ij < n * n; ++ij) { I[k] = nbl * n + offs + ij % n; J[k] = nbl * n + offs + ij / n; ++k; }
+    for (int ij = 0; ij < n * n; ++ij) { I[k] = nbl * n + offs + ij % n; J[k] = (nbl + 1) * n + offs + ij / n; ++k; }
+    for (int ij = 0; ij < n * nx; ++ij) { I[k] = nbl * n + offs + ij % n; J[k] = (nb + 1) * n + qx + offs + ij / n; ++k; }
+  }
+  const int nqr = n + qr;
+  for (int ij = 0; ij < nqr * d.Nc; ++ij) {
+    int i = ij % nqr, j = ij / nqr;
+    I[k] = nb * n + i + offs;
+    if (j >= n) j += nb * n - n;
+    J[k] = j + offs;
+    ++k;
+  }
+  for (int nbl = 0; nbl <= nb; ++nbl)
+    for (int ij = 0; ij < nr * n; ++ij) { I[k] = (nb + 1) * n + qr + offs + ij % nr; J[k] = nbl * n + offs + ij / nr; ++k; }
+  for (int ij = 0; ij < nr * qx; ++ij) { I[k] = (nb + 1) * n + qr + offs + ij % nr; J[k] = (nb + 1) * n + offs + ij / nr; ++k; }
+  for (int ij = 0; ij < nr * nx; ++ij) { I[k] = (nb + 1) * n + qr + offs + ij % nr; J[k] = (nb + 1) * n + qx + offs + ij / nr; ++k; }
+  if (k != bcr_sparse_nnz(h))
+    return h->fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::sparse_pattern( I, J, offs ), inserted %d values, expected %d\n", k, bcr_sparse_nnz(h)));
+  return BCR_OK;
+}
+
+int bcr_sparse_values(bcr_handle h, double* V) {
+  H_ALLOC(h);
+  const Dims& d = h->d;
+  const size_t n = d.n, nx = d.nx, nr = d.nr;
+  size_t k = 0;
+  for (int nbl = 0; nbl < d.nblock; ++nbl) {
+    std::memcpy(V + k, h->hD.data() + nbl * n * n, n * n * 8); k += n * n;
+    std::memcpy(V + k, h->hE.data() + nbl * n * n, n * n * 8); k += n * n;
+    std::memcpy(V + k, h->hB.data() + nbl * n * nx, n * nx * 8); k += n * nx;
+  }
+  std::memcpy(V + k, h->hH.data(), h->hH.size() * 8); k += h->hH.size();
+  std::memcpy(V + k, h->hC.data(), h->hC.size() * 8); k += h->hC.size();
+  std::memcpy(V + k, h->hCq.data(), h->hCq.size() * 8); k += h->hCq.size();
+  std::memcpy(V + k, h->hF.data(), nr * nx * 8); k += nr * nx;
+  return BCR_OK;
+}
+
+int bcr_sparse_load(bcr_handle h, const double* V, const int* I, int r_offs, const int* J, int c_offs,
+                    int nnz, int do_error) {
+  H_ALLOC(h);
+  // cc:2419-2482
+  const Dims& d = h->d;
+  const int n = d.n, nb = d.nblock;
+  const int rH = n * nb, rC = rH + n + d.qr, nrow = rC + d.nr;
+  const int cCq = rH + n, cF = cCq + d.qx, ncol = cF + d.nx;
+  bcr_fill_zero(h);
+  int status = BCR_OK;
+  for (int kk = 0; kk < nnz; ++kk) {
+    const int i = I[kk] - r_offs, j = J[kk] - c_offs;
+    const double v = V[kk];
+    const int ib = i / n, jb = j / n;
+    bool ok = true;
+    if (i < 0 || j < 0) ok = false;
+    else if (i < rH) {
+      if (j < cCq) {
+        if (ib == jb) h->hD[(size_t)ib * n * n + (i % n) + (size_t)(j % n) * n] = v;
+        else if (ib + 1 == jb) h->hE[(size_t)ib * n * n + (i % n) + (size_t)(j % n) * n] = v;
+        else ok = false;
+      } else if (j < cF) ok = false;
+      else if (j < ncol) h->hB[(size_t)ib * n * d.nx + (i % n) + (size_t)(j - cF) * n] = v;
+      else ok = false;
+    } else if (i < rC) {
+      const int m = n + d.qr;
+      if (j < n) h->hH[(i - rH) + (size_t)j * m] = v;
+      else if (j < rH) ok = false;
+      else if (j < ncol) h->hH[(i - rH) + (size_t)(j - rH + n) * m] = v;
+      else ok = false;
+    } else if (i < nrow) {
+      if (j < cCq) h->hC[(size_t)jb * d.nr * n + (i - rC) + (size_t)(j % n) * d.nr] = v;
+      else if (j < cF) h->hCq[(i - rC) + (size_t)(j - cCq) * d.nr] = v;
+      else if (j < ncol) h->hF[(i - rC) + (size_t)(j - cF) * d.nr] = v;
+      else ok = false;
+    } else ok = false;
+    if (!ok) {
+      h->err = fmt("in BorderedCR<t_Value>::sparse_load, indices (i,j) = ( %d, %d) out of pattern!\n", I[kk], J[kk]);
+      if (do_error) return BCR_BAD_ARGUMENT;
+      status = BCR_OK;
+    }
+  }
+  h->dirty = true;
+  return status;
+}
+
+// ------------------------------------------------------- device-resident ---
+int bcr_set_stream(bcr_handle h, void* stream) {
+  H_CHECK(h);
+  if (h->own_stream && h->stream) {
+    cudaStreamSynchronize(h->stream);
+    cudaStreamDestroy(h->stream);
+  }
+  h->own_stream = false;
+  h->stream = static_cast<cudaStream_t>(stream);
+  return BCR_OK;
+}
+
+int bcr_upload(bcr_handle h) {
+  H_ALLOC(h);
+  int rc = h->upload();
+  if (rc) return rc;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  return e == cudaSuccess ? BCR_OK : h->cuda_fail(e, "upload");
+}
+
+int bcr_factorize_device(bcr_handle h) {
+  H_ALLOC(h);
+  int rc = h->ensure_device();
+  if (rc) return rc;
+  if (h->dirty && (rc = h->upload())) return rc;
+  return h->factorize_device();
+}
+
+int bcr_solve_device(bcr_handle h, int nrhs, double* d_x, int ld) {
+  H_ALLOC(h);
+  return h->solve_device(nrhs, d_x, ld);
+}
+
+int bcr_mv_device(bcr_handle h, double alpha, const double* d_x, double beta, double* d_res) {
+  H_ALLOC(h);
+  int rc = h->ensure_device();
+  if (rc) return rc;
+  if (h->dirty && (rc = h->upload())) return rc;
+  bcr::launch_mv(h->s, alpha, d_x, beta, d_res, h->stream);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? BCR_OK : h->cuda_fail(e, "Mv launch");
+}
+
+int bcr_synchronize(bcr_handle h) {
+  H_CHECK(h);
+  if (!h->stream) return BCR_OK;
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  return e == cudaSuccess ? BCR_OK : h->cuda_fail(e, "synchronize");
+}
+
+}  // extern "C"

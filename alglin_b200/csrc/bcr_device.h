@@ -1,0 +1,44 @@
+// Host-side launchers for the BorderedCR device kernels (internal interface
+// between the C-ABI layer and the CUDA translation units).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "bcr_common.cuh"
+
+namespace bcr {
+
+// device buffers of one factorization, FP64 path
+struct DevState {
+  Dims d;
+  int sel;        // Internal
+  int sel_last;   // LastKind actually used (after fallback)
+  // loaded matrix (reference layout), never modified on the device
+  double *D0, *E0, *B0, *C0, *Cq, *F0, *H;
+  // working blocks / factors
+  double *D, *E, *B, *C, *T;
+  int* P;
+  // scratch: border contributions per eliminated block
+  double *Rbuf, *Fbuf, *XB;
+  int xb_cap;           // nrhs capacity of XB
+  double *part;         // reduction partials
+  int part_cap;         // doubles
+  double *Ffin;         // F + sum of Schur updates (nr x nx)
+  double *Hl;           // last block Nr x Nc
+  double *tau_l;        // last block Householder scalars
+  int* piv_l;           // last block pivots
+  StatusWords* st;      // device status
+  double* mv_part;      // Mv border partials ((nblock+1) x nr)
+};
+
+// factorization of every cyclic-reduction level plus the last block
+void launch_factorize(DevState& s, cudaStream_t st);
+// x: device, column-major (ldx x nrhs); in place, reference semantics
+void launch_solve(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st);
+// res = alpha * A * x + beta * res with the loaded (unfactored) matrix
+void launch_mv(DevState& s, double alpha, const double* x, double beta, double* res,
+               cudaStream_t st);
+
+// smem bytes needed by one warp of the panel kernel; 0 if it does not fit
+size_t panel_smem_per_warp(const Dims& d, int elem_bytes);
+
+}  // namespace bcr

@@ -1,0 +1,350 @@
+"""Benchmark of the B200 BorderedCR solver on the headline BABD workload.
+
+Workload (one "step" = factorize + solve of one system):
+  trapezoid-collocation BABD, n=16, nblock=100000, qr=qx=2, nr=nx=4, one
+  right-hand side, FP64, internal LU, last block LU (seeded synthetic data).
+  unknowns = ncols = 16*100001 + 2 + 4 = 1,600,022.
+
+  value : ncols / (device time of factorize + solve), matrix resident in HBM
+  e2e   : the same metric through the C ABI with host buffers
+          (bcr_factorize uploads the matrix from pinned host memory,
+           bcr_solve copies the right-hand side in and the solution out)
+
+The matrix (0.65 GB) is larger than L2 (126 MB), so no L2 flush is needed
+between steps.  Multi-GPU: one process per GPU, each solving its own system
+(independent replicas, weak scaling, no collective on the data path).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BABD factor+solve unknowns/s at rel. residual ≤1e-12: mixed vs plain FP64 GPU"
+CFG = dict(nblock=100000, n=16, qr=2, qx=2, nr=4, nx=4)
+
+
+def workload_config(extra=None):
+    c = {"workload": "trapezoid-collocation BABD n=16 nblock=100000 qr=qx=2 nr=nx=4, 1 rhs, "
+                     "internal LU + last-block LU (FP64)",
+         "nblock": CFG["nblock"], "n": CFG["n"], "qr": CFG["qr"], "qx": CFG["qx"],
+         "nr": CFG["nr"], "nx": CFG["nx"], "nrhs": 1,
+         "l2": "inputs (0.65 GB matrix) larger than L2; no flush needed"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for _, _, f in rows:
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(r[0] for r in rows),
+                "sm_max_mhz": max(r[1] for r in rows), "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def algorithmic_bytes(d, nrhs=1):
+    """Minimum HBM traffic per block (FP64): factorize reads D,E,B,C once and
+    writes the factors T (2n^2), U-row D',E',B',C' once plus int32 pivots;
+    solve reads the factors and reads/writes x in both sweeps."""
+    n, nr, nx = d["n"], d["nr"], d["nx"]
+    fact = 8 * ((2 * n * n + n * nx + nr * n) + (4 * n * n + n * nx + nr * n)) + 4 * n
+    solve = 8 * (4 * n * n + n * nx + nr * n) + 4 * n + 8 * 4 * n * nrhs
+    return fact * d["nblock"], solve * d["nblock"]
+
+
+def launches_per_step(nblock, nr, nx):
+    levels = 0
+    k = 1
+    while k < nblock:
+        levels += 1
+        k *= 2
+    fact = levels * (2 if nr else 1) + (2 if nr * nx else 0) + 2
+    solve = levels * 2 + (2 if nr else 0) + 1
+    return fact + solve
+
+
+def cpu_reference_run(s, b, steps, warmup, threads):
+    """The reference's own BorderedCR (oracle/_ref) on the host cores."""
+    from oracle import pyoracle as po
+    src = po.RefBCR(s, "LU", "LU", "NONE", nthreads=threads, npb=threads)
+    work = po.RefBCR(s, "LU", "LU", "NONE", nthreads=threads, npb=threads)
+    work.set_threads(True, True)
+    times = []
+    x = None
+    for i in range(warmup + steps):
+        t, x = work.time_factor_solve(src, b)
+        if i >= warmup:
+            times.append(t)
+    return times, x
+
+
+def rel_residual_host(h, s, x, b):
+    r = h.mv(x[:s.ncols])[:s.nrows] - b[:s.nrows]
+    from tests._util import block_norm_inf
+    return float(np.abs(r).max() / (block_norm_inf(s) * np.abs(x[:s.ncols]).max() + np.abs(b[:s.nrows]).max()))
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from alglin_b200 import synth
+    from oracle import pyoracle as po
+    if not po.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libbcr_ref.so was not built"}))
+        return 0
+    s = synth.collocation(**CFG, seed=0)
+    b = synth.rhs(s, 1, seed=1)[0]
+    threads = os.cpu_count() or 1
+    steps = max(1, min(args.steps, 5))
+    warm = max(1, min(args.warmup, 1))
+    times, x = cpu_reference_run(s, b, steps, warm, threads)
+    t = statistics.median(times)
+    v = s.ncols / t
+    line = {"metric": METRIC, "value": v, "unit": "unknowns/s", "n_gpus": args.gpus, "steps": steps,
+            "warmup": warm, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": workload_config({"threads": threads}),
+            "cpu_baseline": {"value": v, "unit": "unknowns/s", "cores": threads, "kind": "reference",
+                             "sample": "full workload, median of %d factorize+solve runs" % steps},
+            "e2e": {"value": v, "unit": "unknowns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA GPU")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from alglin_b200 import bcr, synth
+
+    s = synth.collocation(**CFG, seed=rank)
+    b = synth.rhs(s, 1, seed=1 + rank)[0]
+    L = max(s.nrows, s.ncols)
+    h = bcr.BorderedCR()
+    h.load_system(s)
+    h.select("LU")
+    h.select_last("LU")
+    stream = torch.cuda.current_stream()
+    h.set_stream(stream.cuda_stream)
+    h.upload()
+    b_dev = torch.from_numpy(b).cuda()
+    x_dev = torch.empty_like(b_dev)
+
+    def step():
+        ok = h.factorize_device()
+        x_dev.copy_(b_dev)
+        ok = ok and h.solve_device(1, x_dev.data_ptr(), L)
+        return ok
+
+    for _ in range(args.warmup):
+        assert step(), h.last_error()
+    torch.cuda.synchronize()
+    # device-resident timing: factorize and solve phases measured separately
+    ef = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    es = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record()
+        for i in range(args.steps):
+            ef[i].record()
+            assert h.factorize_device(), h.last_error()
+            x_dev.copy_(b_dev)
+            es[i].record()
+            assert h.solve_device(1, x_dev.data_ptr(), L), h.last_error()
+        ef[args.steps].record()
+        t_end.record()
+        torch.cuda.synchronize()
+    clocks = clk.summary()
+    total_ms = t_start.elapsed_time(t_end)
+    fact_ms = statistics.mean(ef[i].elapsed_time(es[i]) for i in range(args.steps))
+    solve_ms = statistics.mean(es[i].elapsed_time(ef[i + 1]) for i in range(args.steps))
+    ms = total_ms / args.steps
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * s.ncols / (ms * 1e-3)
+
+    # accuracy of the timed result
+    x = x_dev.cpu().numpy()
+    relres = rel_residual_host(h, s, x, b)
+
+    # end to end through the C ABI with host buffers
+    xh = b.copy()
+    for _ in range(2):
+        assert h.factorize() and h.solve(xh), h.last_error()
+        xh[:] = b
+    nbytes_mat = sum(getattr(s, k).nbytes for k in ("D", "E", "B", "C", "Cq", "F", "H"))
+    te = []
+    for _ in range(max(3, min(args.steps, 10))):
+        xh[:] = b
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        assert h.factorize(), h.last_error()
+        assert h.solve(xh), h.last_error()
+        te.append(time.perf_counter() - t0)
+    e2e_t = statistics.median(te)
+    if dist:
+        t = torch.tensor([e2e_t], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+
+    fact_b, solve_b = algorithmic_bytes(CFG)
+    peak, peak_kind = load_peaks()
+    achieved = fact_b / (fact_ms * 1e-3) / 1e9
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            cpu = cpu_baseline(s, b)
+        line = {
+            "metric": METRIC, "value": value, "unit": "unknowns/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "ours",
+            "config": workload_config({"parallelism": f"replicas x{world}"}),
+            "phases_ms": {"factorize": fact_ms, "solve": solve_ms},
+            "rel_residual": relres,
+            "roofline": {"bound": "hbm", "kernel": "factorize (all CR level launches)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "algorithmic_bytes": fact_b},
+            "e2e": {"value": world * s.ncols / e2e_t, "unit": "unknowns/s",
+                    "h2d_bytes_per_step": nbytes_mat + 8 * L, "d2h_bytes_per_step": 8 * L},
+            "gpu_launches": launches_per_step(CFG["nblock"], CFG["nr"], CFG["nx"]) * args.steps,
+            "clocks": clocks,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def cpu_baseline(s, b):
+    from oracle import pyoracle as po
+    threads = os.cpu_count() or 1
+    if po.ref_available():
+        times, _ = cpu_reference_run(s, b, 3, 1, threads)
+        t = statistics.median(times)
+        return {"value": s.ncols / t, "unit": "unknowns/s", "cores": threads, "kind": "reference",
+                "sample": "full workload, median of 3 factorize+solve runs of the reference "
+                          "BorderedCR with its own thread pool"}
+    o = po.Oracle(s, "LU", "LU")
+    t0 = time.perf_counter()
+    o.factorize()
+    o.solve(b)
+    t = time.perf_counter() - t0
+    return {"value": s.ncols / t, "unit": "unknowns/s", "cores": 1, "kind": "port",
+            "sample": "full workload, one factorize+solve of the C oracle"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

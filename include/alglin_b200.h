@@ -1,0 +1,155 @@
+/*
+ * alglin_b200 -- C ABI of the B200 BorderedCR solver for bordered
+ * block-almost-bidiagonal (BABD) linear systems.
+ *
+ * Each entry point replaces one member of the reference C++ class
+ * alglin::BorderedCR<double> (ebertolazzi/alglin, src/Alglin/BABD_BorderedCR.hxx,
+ * src/BABD_BorderedCR.cc); the citation beside each declaration names it.
+ * The reference's historic C interface header (Alglin/BABD_C_interface.h,
+ * included by src_tests/test8-Cinterface.c:20 and test9-Cinterface.c:20) is
+ * absent from the reference tree, so this ABI follows the C++ method names.
+ *
+ * Conventions
+ *   - plain pointers and sizes only; matrices are column-major with a leading
+ *     dimension, exactly as the reference loaders take them;
+ *   - every call returns an int status:
+ *       BCR_OK (0), BCR_NUMERICAL (1: factorize/solve returned false in the
+ *       reference), BCR_BAD_ARGUMENT (2: the reference throws
+ *       Utils::Runtime_Error), BCR_CUDA_ERROR (3), BCR_DEVICE_TIMEOUT (4);
+ *     bcr_last_error() returns the message of the last failure, in the
+ *     reference's wording where the reference has one;
+ *   - the handle keeps a host copy of the loaded matrix; factorize() copies it
+ *     to the GPU once and leaves it untouched (the reference overwrites it),
+ *     so bcr_mv() after bcr_factorize() still multiplies by the loaded matrix;
+ *   - all compute runs on the current CUDA device; there is no CPU fallback:
+ *     without a usable GPU the compute calls return BCR_CUDA_ERROR.
+ */
+#ifndef ALGLIN_B200_H
+#define ALGLIN_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BCR_OK 0
+#define BCR_NUMERICAL 1
+#define BCR_BAD_ARGUMENT 2
+#define BCR_CUDA_ERROR 3
+#define BCR_DEVICE_TIMEOUT 4
+
+/* working precision of the device factorization (extension: set_precision) */
+#define BCR_PRECISION_FP64 0
+#define BCR_PRECISION_MIXED 1
+
+typedef struct bcr_handle_s *bcr_handle;
+
+/* --- life cycle ----------------------------------------------------------- */
+/* BorderedCR(Utils::ThreadPoolBase* TP, integer npb)  hxx:373-384.
+ * num_threads stands for TP->thread_count() (0: no pool); it only feeds info() */
+int bcr_create(bcr_handle *h, int num_threads, int num_parallel_block);
+int bcr_destroy(bcr_handle h);                                    /* ~BorderedCR hxx:386 */
+int bcr_allocate(bcr_handle h, int nblock, int n, int qr, int qx,
+                 int nr, int nx);                                 /* allocate cc:42-170 */
+int bcr_dup(bcr_handle dst, bcr_handle src);                      /* dup cc:181-198 */
+
+/* --- sizes (hxx:617-650) -------------------------------------------------- */
+int bcr_nrows(bcr_handle h);
+int bcr_ncols(bcr_handle h);
+int bcr_number_of_blocks(bcr_handle h);
+int bcr_block_size(bcr_handle h);
+int bcr_dim_qr(bcr_handle h);
+int bcr_dim_qx(bcr_handle h);
+int bcr_dim_nr(bcr_handle h);
+int bcr_dim_nx(bcr_handle h);
+int bcr_Nr(bcr_handle h);
+int bcr_Nc(bcr_handle h);
+
+/* --- zeroing (hxx:658-682, cc:237-279) ------------------------------------ */
+int bcr_zero_B(bcr_handle h);
+int bcr_zero_C(bcr_handle h);
+int bcr_zero_Cq(bcr_handle h);
+int bcr_zero_D(bcr_handle h);
+int bcr_zero_E(bcr_handle h);
+int bcr_zero_F(bcr_handle h);
+int bcr_zero_H(bcr_handle h);
+int bcr_fill_zero(bcr_handle h);
+
+/* --- loaders (cc:289-793) --------------------------------------------------- */
+int bcr_load_B(bcr_handle h, int nbl, const double *B, int ldB);      /* cc:453 */
+int bcr_add_to_B(bcr_handle h, int nbl, const double *B, int ldB);    /* cc:479 */
+int bcr_load_C(bcr_handle h, int nbl, const double *C, int ldC);      /* cc:507 */
+int bcr_add_to_C(bcr_handle h, int nbl, const double *C, int ldC);    /* cc:534 */
+int bcr_add_to_C2(bcr_handle h, int nbl, const double *C, int ldC);   /* cc:567 */
+int bcr_add_to_C2F(bcr_handle h, int nbl, const double *C2F, int ldC);/* cc:765 */
+int bcr_load_D(bcr_handle h, int nbl, const double *D, int ldD);      /* cc:598 */
+int bcr_load_E(bcr_handle h, int nbl, const double *E, int ldE);      /* cc:625 */
+int bcr_load_DE(bcr_handle h, int nbl, const double *DE, int ldDE);   /* cc:654 */
+int bcr_load_DEB(bcr_handle h, int nbl, const double *DEB, int ldDEB);/* cc:666 */
+int bcr_load_F(bcr_handle h, const double *F, int ldF);               /* cc:681 */
+int bcr_add_to_F(bcr_handle h, const double *F, int ldF);             /* cc:705 */
+int bcr_load_Cq(bcr_handle h, const double *Cq, int ldC);             /* cc:729 */
+int bcr_load_CqF(bcr_handle h, const double *CqF, int ldCF);          /* cc:753 */
+int bcr_load_bottom(bcr_handle h, const double *H0, int ld0, const double *HN, int ldN,
+                    const double *Hq, int ldQ, const double *Hp, int ldP);  /* cc:291 */
+int bcr_load_bottom_H(bcr_handle h, const double *H, int ldH);        /* cc:358 */
+int bcr_load_bottom2(bcr_handle h, const double *C0, int ld0, const double *CN, int ldN,
+                     const double *Cq, int ldCq, const double *F, int ldF); /* cc:382 */
+/* [C0 | CN | Cq | F] as one nr x Nc matrix: load_bottom2(MatW)  cc:430-447 */
+int bcr_load_bottom2_H(bcr_handle h, const double *CCqF, int ld);
+
+/* host copy of a block for element access (accessors hxx:972-998):
+ * which = 'B','C','D','E' (block nbl), 'F', 'Q' (Cq), 'H' (nbl ignored);
+ * column-major with the reference leading dimensions; NULL if out of range */
+double *bcr_block_data(bcr_handle h, char which, int nbl);
+
+/* --- algorithm selection (hxx:459-540) ------------------------------------ */
+int bcr_select(bcr_handle h, const char *choice);        /* "LU" "QR" "QRP" */
+int bcr_select_last(bcr_handle h, const char *choice);   /* "LU" "LUPQ" "QR" "QRP" "SVD" "LSS" "LSY" "PINV" */
+int bcr_select_last2(bcr_handle h, const char *choice);  /* "NONE" "SVD" "LSS" "LSY" "PINV" */
+int bcr_selected(bcr_handle h, int *internal, int *last, int *last2);
+int bcr_set_factorize_use_thread(bcr_handle h, int yes); /* hxx:391 (kept for info()) */
+int bcr_set_solve_use_thread(bcr_handle h, int yes);     /* hxx:393 */
+int bcr_factorize_use_thread(bcr_handle h);              /* hxx:396 */
+int bcr_solve_use_thread(bcr_handle h);                  /* hxx:398 */
+int bcr_set_num_parallel_block(bcr_handle h, int npb);   /* hxx:407-423 */
+int bcr_set_precision(bcr_handle h, int precision);      /* extension: FP64 / mixed */
+/* info(indent) cc:208-235; the returned string lives until the next call */
+const char *bcr_info(bcr_handle h, const char *indent);
+const char *bcr_last_error(bcr_handle h);                /* hxx:445 */
+int bcr_set_debug(bcr_handle h, int yes);                /* hxx:1172 */
+int bcr_check_matrix(bcr_handle h);                      /* cc:2538-2659 */
+
+/* --- factorize / solve (hxx:1029-1038) ------------------------------------- */
+int bcr_factorize(bcr_handle h);                         /* factorize cc:803-839 */
+/* x: length >= max(nrows, ncols); in place: rhs in, solution out (cc:1489) */
+int bcr_solve(bcr_handle h, double *x);
+/* rhs: ldRhs x nrhs, ldRhs >= max(nrows, ncols)  (cc:1546-1605) */
+int bcr_solve_n(bcr_handle h, int nrhs, double *rhs, int ldRhs);
+int bcr_t_solve(bcr_handle h, double *x);                /* cc:2089: not defined */
+int bcr_t_solve_n(bcr_handle h, int nrhs, double *rhs, int ldRhs); /* cc:2096 */
+
+/* --- products (cc:2111-2166) ---------------------------------------------- */
+int bcr_mv(bcr_handle h, const double *x, double *res);
+int bcr_add_mv(bcr_handle h, double alpha, const double *x, double *res);
+
+/* --- sparse export / import (hxx:1079-1115, cc:2342-2482) ------------------ */
+int bcr_sparse_nnz(bcr_handle h);
+int bcr_sparse_pattern(bcr_handle h, int *I, int *J, int offs);
+int bcr_sparse_values(bcr_handle h, double *V);
+int bcr_sparse_load(bcr_handle h, const double *V, const int *I, int r_offs,
+                    const int *J, int c_offs, int nnz, int do_error);
+
+/* --- device-resident variants (extension for callers whose data is on the GPU) */
+/* stream: a cudaStream_t (NULL = the handle's own stream) */
+int bcr_set_stream(bcr_handle h, void *stream);
+int bcr_upload(bcr_handle h);          /* host copy of the matrix -> device */
+int bcr_factorize_device(bcr_handle h);/* factorize the device-resident matrix */
+/* d_x: device pointer, ld x nrhs column-major; stream-ordered, asynchronous */
+int bcr_solve_device(bcr_handle h, int nrhs, double *d_x, int ld);
+int bcr_mv_device(bcr_handle h, double alpha, const double *d_x, double beta, double *d_res);
+int bcr_synchronize(bcr_handle h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,169 @@
+"""GPU parity tests: the CUDA BorderedCR path, called through the C ABI, against
+the reference's own results (golden fixtures) and the CPU oracle.
+
+Tolerances (floating point): forward error against the reference/oracle
+solution <= 1e-10 on these well-conditioned systems, and relative residual
+||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= 1e-13 for the FP64 path.
+"""
+import numpy as np
+import pytest
+
+from alglin_b200 import bcr as B
+from alglin_b200 import synth
+from oracle import pyoracle as po
+from tests._util import GOLDEN_CASES, block_norm_inf, fwd_err, load_golden
+
+pytestmark = pytest.mark.gpu
+
+DEVICE_LAST = ("LU", "QR")   # last-block solvers implemented on the device
+
+
+def gpu_solver(s, internal="LU", last="LU", last2="NONE"):
+    h = B.BorderedCR()
+    h.load_system(s)
+    h.select(internal)
+    h.select_last(last)
+    h.select_last2(last2)
+    return h
+
+
+def gpu_solve(h, b):
+    X = np.array(b, dtype=np.float64, order="C", copy=True)
+    if X.ndim == 1:
+        assert h.solve(X), h.last_error()
+    else:
+        assert h.solve_n(X.shape[0], X, X.shape[1]), h.last_error()
+    return X
+
+
+def relres(o, s, x, b):
+    r = b[:s.nrows] - o.mv(x[:s.ncols])
+    return np.abs(r).max() / (block_norm_inf(s) * np.abs(x[:s.ncols]).max() + np.abs(b[:s.nrows]).max())
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_gpu_matches_reference_golden(name):
+    s, b, X, tags = load_golden(name)
+    ran = 0
+    for (internal, last, last2), xg in zip(tags, X):
+        if last not in DEVICE_LAST:
+            continue
+        h = gpu_solver(s, internal, last, last2)
+        assert h.factorize(), h.last_error()
+        x = gpu_solve(h, b)
+        for c in range(b.shape[0]):
+            assert fwd_err(x[c, :s.ncols], xg[c, :s.ncols]) < 1e-10, (name, internal, last, c)
+        ran += 1
+    assert ran > 0
+
+
+SHAPES = [
+    (1, 1, 0, 0, 0, 0), (1, 2, 0, 0, 1, 1), (2, 1, 0, 0, 1, 1), (3, 2, 1, 1, 1, 1),
+    (5, 3, 0, 2, 2, 0), (8, 4, 2, 2, 3, 3), (33, 5, 1, 0, 0, 2), (100, 8, 0, 0, 2, 2),
+    (127, 16, 2, 2, 4, 4), (64, 32, 0, 0, 8, 8), (257, 7, 3, 1, 2, 5), (1000, 2, 0, 0, 0, 0),
+]
+
+
+@pytest.mark.parametrize("dims", SHAPES)
+@pytest.mark.parametrize("internal", ["LU", "QR", "QRP"])
+def test_gpu_matches_oracle_random(dims, internal):
+    s = synth.collocation(*dims, seed=sum(dims)) if dims[1] > 1 else synth.dominant(*dims, seed=1)
+    b = synth.rhs(s, nrhs=2, seed=7)
+    last = "LU" if s.Nr == s.Nc else "QR"
+    if s.Nr < s.Nc:
+        pytest.skip("under-determined last block needs the SVD family")
+    o = po.Oracle(s, internal, last)
+    assert o.factorize(), o.last_error()
+    xo = o.solve(b)
+    h = gpu_solver(s, internal, last)
+    assert h.factorize(), h.last_error()
+    xg = gpu_solve(h, b)
+    for c in range(2):
+        assert fwd_err(xg[c, :s.ncols], xo[c, :s.ncols]) < 1e-10, (dims, internal, c)
+        assert relres(o, s, xg[c], b[c]) < 1e-13
+    # single right-hand side entry point
+    x1 = gpu_solve(h, b[0])
+    assert fwd_err(x1[:s.ncols], xo[0, :s.ncols]) < 1e-10
+
+
+def test_gpu_many_rhs_chunks():
+    s = synth.collocation(77, 6, 1, 1, 2, 2, seed=9)
+    b = synth.rhs(s, nrhs=37, seed=3)
+    o = po.Oracle(s, "LU", "LU"); assert o.factorize()
+    h = gpu_solver(s); assert h.factorize(), h.last_error()
+    xg = gpu_solve(h, b)
+    xo = o.solve(b)
+    assert fwd_err(xg[:, :s.ncols], xo[:, :s.ncols]) < 1e-10
+
+
+def test_gpu_mv_matches_oracle():
+    s = synth.collocation(513, 8, 2, 2, 3, 3, seed=4)
+    x = np.random.default_rng(0).standard_normal(s.ncols)
+    o = po.Oracle(s)
+    h = gpu_solver(s)
+    y = h.mv(x)
+    yo = o.mv(x)
+    assert np.abs(y[:s.nrows] - yo).max() < 1e-12 * np.abs(yo).max()
+    r = np.ones(s.nrows)
+    h.add_mv(-2.0, x, r)
+    assert np.abs(r - (1 - 2 * yo)).max() < 1e-12 * np.abs(yo).max()
+
+
+def test_gpu_manufactured_test7_style():
+    """src_tests/test7-BorderedCR.cc:120-288 sizes and checks."""
+    s = synth.dominant(10000, 8, 4, 4, 1, 1, seed=2)
+    xref = 1.0 + (np.arange(s.ncols) % 100)
+    h = gpu_solver(s)
+    rhs = np.zeros(max(s.nrows, s.ncols))
+    rhs[:s.nrows] = h.mv(xref)
+    assert h.factorize(), h.last_error()
+    x = rhs.copy()
+    assert h.solve(x)
+    assert np.abs(x[:s.ncols] - xref).max() < 1e-8
+    assert np.abs(x[:s.ncols] - xref).sum() / s.ncols < 1e-8
+    X = np.stack([rhs, rhs])
+    assert h.solve_n(2, X, X.shape[1])
+    assert np.abs(X[:, :s.ncols] - xref).max() < 1e-8
+    res = h.mv(x[:s.ncols]) - rhs[:s.nrows]
+    assert np.linalg.norm(res) < 1e-6 and np.abs(res).sum() < 1e-6
+
+
+def test_gpu_singular_panel_fails_like_reference():
+    s = synth.dominant(4, 3, 0, 0, 0, 0, seed=1)
+    s.D[1] = 0.0
+    s.E[0] = 0.0
+    h = gpu_solver(s)
+    assert not h.factorize()
+    assert "getrf(M=6,N=3,A,LDA=6,iperm)::INFO = 1" in h.last_error()
+
+
+def test_gpu_singular_last_block_without_fallback():
+    s = synth._zeros(1, 1, 0, 0, 1, 1)
+    s.D[0, 0, 0] = 1; s.H[1, 0] = 1; s.C[0, 0, 0] = 1; s.C[1, 0, 0] = 1
+    h = gpu_solver(s, "LU", "LU", "NONE")
+    assert not h.factorize()
+    assert "load_and_factorize_last" in h.last_error()
+
+
+def test_gpu_deterministic():
+    s = synth.collocation(999, 16, 2, 2, 4, 4, seed=1)
+    b = synth.rhs(s, 1, seed=2)[0]
+    h = gpu_solver(s)
+    assert h.factorize()
+    x1 = gpu_solve(h, b)
+    assert h.factorize()
+    x2 = gpu_solve(h, b)
+    assert np.array_equal(x1, x2)
+
+
+@pytest.mark.parametrize("internal", ["LU", "QR"])
+def test_gpu_full_size_config_B_residual(internal):
+    """n=16, nblock=100000, qr=qx=2, nr=nx=4: FP64 bar rel. residual <= 1e-13."""
+    s = synth.collocation(**synth.CONFIGS["B"], seed=0)
+    b = synth.rhs(s, nrhs=1, seed=1)[0]
+    h = gpu_solver(s, internal, "LU")
+    assert h.factorize(), h.last_error()
+    x = gpu_solve(h, b)
+    r = h.mv(x[:s.ncols]) - b[:s.nrows]
+    rel = np.abs(r).max() / (block_norm_inf(s) * np.abs(x[:s.ncols]).max() + np.abs(b[:s.nrows]).max())
+    assert rel < 1e-13, rel
