@@ -87,10 +87,17 @@ _SIGS = [
     ("bcr_set_stream", [_H, ct.c_void_p], ct.c_int),
     ("bcr_upload", [_H], ct.c_int),
     ("bcr_factorize_device", [_H], ct.c_int),
+    ("bcr_factorize_async", [_H], ct.c_int),
+    ("bcr_factorize_status", [_H], ct.c_int),
     ("bcr_solve_device", [_H, ct.c_int, ct.c_void_p, ct.c_int], ct.c_int),
     ("bcr_mv_device", [_H, ct.c_double, ct.c_void_p, ct.c_double, ct.c_void_p], ct.c_int),
     ("bcr_synchronize", [_H], ct.c_int),
+    ("bcr_get_stream", [_H], ct.c_void_p),
+    ("bcr_graph_capture", [_H, ct.c_int, ct.c_int, ct.c_void_p, ct.c_int, ct.c_void_p], ct.c_int),
+    ("bcr_graph_launch", [_H, ct.c_int], ct.c_int),
 ]
+
+GRAPH_FACTORIZE, GRAPH_SOLVE, GRAPH_STEP = 1, 2, 3
 
 _lib = None
 
@@ -347,6 +354,13 @@ class BorderedCR:
     def factorize_device(self) -> bool:
         return self._check(self.L.bcr_factorize_device(self.h), numerical_ok=True)
 
+    def factorize_async(self):
+        """Enqueue the factorization (graph-capturable); see factorize_status()."""
+        self._check(self.L.bcr_factorize_async(self.h))
+
+    def factorize_status(self) -> bool:
+        return self._check(self.L.bcr_factorize_status(self.h), numerical_ok=True)
+
     def solve_device(self, nrhs: int, d_x_ptr: int, ld: int) -> bool:
         return self._check(self.L.bcr_solve_device(self.h, nrhs, d_x_ptr, ld), numerical_ok=True)
 
@@ -354,3 +368,13 @@ class BorderedCR:
         self._check(self.L.bcr_mv_device(self.h, alpha, d_x_ptr, beta, d_res_ptr))
 
     def synchronize(self): self._check(self.L.bcr_synchronize(self.h))
+
+    def stream(self) -> int:
+        """cudaStream_t (as an int) the handle enqueues on."""
+        return self.L.bcr_get_stream(self.h) or 0
+
+    def graph_capture(self, what: int, nrhs: int = 0, d_x_ptr: int = 0, ld: int = 0, d_rhs_ptr: int = 0):
+        self._check(self.L.bcr_graph_capture(self.h, what, nrhs, d_x_ptr or None, ld, d_rhs_ptr or None))
+
+    def graph_launch(self, what: int):
+        self._check(self.L.bcr_graph_launch(self.h, what))

@@ -69,12 +69,13 @@ struct bcr_handle_s {
   int sel = 0, sel_last = 0, sel_last2 = 0;
   bool fthread = true, sthread = true, debug = false;
   int precision = BCR_PRECISION_FP64;
+  int use_tc = 1;  // FP64 tensor-core pair kernel where it applies
   std::string err = "no error";
   std::string info_buf;
   // host copy of the loaded matrix (reference layout)
   std::vector<double> hD, hE, hB, hC, hCq, hF, hH;
   // device
-  bool dev_ready = false, dirty = true, factorized = false;
+  bool dev_ready = false, dirty = true, factorized = false, pending_status = false;
   bcr::DevState s{};
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -83,6 +84,12 @@ struct bcr_handle_s {
   double* dY = nullptr;
   size_t dY_cap = 0;
   std::vector<void*> pinned;
+  cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
+
+  void drop_graphs() {
+    for (auto& g : graphs)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  }
 
   int fail(int code, const std::string& m) {
     err = m;
@@ -104,6 +111,7 @@ struct bcr_handle_s {
   void release_device() {
     if (!dev_ready) return;
     cudaDeviceSynchronize();
+    drop_graphs();
     for (void* p : pinned) cudaHostUnregister(p);
     pinned.clear();
     bcr::DevState& z = s;
@@ -151,12 +159,12 @@ struct bcr_handle_s {
     A(dalloc(z.C0, (nb + 1) * nr * n)); A(dalloc(z.Cq, nr * qx)); A(dalloc(z.F0, nr * nx));
     A(dalloc(z.H, (n + qr) * d.Nc));
     A(dalloc(z.D, nb * n * n)); A(dalloc(z.E, nb * n * n)); A(dalloc(z.B, nb * n * nx));
-    A(dalloc(z.C, (nb + 1) * nr * n)); A(dalloc(z.T, nb * (2 * n * n + n))); A(dalloc(z.P, nb * n));
+    A(dalloc(z.C, (nb + 1) * nr * n)); A(dalloc(z.T, nb * (2 * n * n + n))); A(dalloc(z.P, nb * 3 * n));
     A(dalloc(z.Rbuf, nb * nr * n)); A(dalloc(z.Fbuf, nb * nr * nx));
     z.xb_cap = 16;
     A(dalloc(z.XB, nb * nr * 16));
-    const size_t parts = (nb + 1 + 63) / 64 + 1;
-    z.part_cap = (int)(parts * std::max<size_t>({nr * nx, nr * 16, nr, 1}));
+    const size_t parts = (nb + 1 + 1023) / 1024 + 1;
+    z.part_cap = (int)(parts * 256);
     A(dalloc(z.part, (size_t)z.part_cap));
     A(dalloc(z.Ffin, std::max<size_t>(nr * nx, 1)));
     A(dalloc(z.Hl, (size_t)d.Nr * d.Nc)); A(dalloc(z.tau_l, Lmax)); A(dalloc(z.piv_l, Lmax));
@@ -206,7 +214,7 @@ struct bcr_handle_s {
     return BCR_OK;
   }
 
-  int factorize_device() {
+  int factorize_launch() {
     factorized = false;
     if (sel_last != bcr::LAST_LU && sel_last != bcr::LAST_QR)
       return fail(BCR_NUMERICAL,
@@ -214,12 +222,22 @@ struct bcr_handle_s {
                       "(last block solver '%s' is not available on the device)\n", kLastName[sel_last]));
     s.sel = sel;
     s.sel_last = sel_last;
+    s.use_tc = use_tc;
     bcr::launch_factorize(s, stream);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "factorize launch");
+    pending_status = true;
+    factorized = true;  // provisional until the status word is read
+    return BCR_OK;
+  }
+
+  int factorize_status() {
+    if (!pending_status) return factorized ? BCR_OK : fail(BCR_NUMERICAL, err);
+    pending_status = false;
     bcr::StatusWords st{};
     int rc = read_status(st);
-    if (rc) return rc;
+    if (rc) { factorized = false; return rc; }
+    factorized = false;
     if (st.code == bcr::DEV_ZERO_PIVOT) {
       const int n = d.n;
       if (sel == bcr::SEL_LU)
@@ -239,6 +257,12 @@ struct bcr_handle_s {
     return BCR_OK;
   }
 
+  int factorize_device() {
+    int rc = factorize_launch();
+    if (rc) return rc;
+    return factorize_status();
+  }
+
   int solve_device(int nrhs, double* dx, int ld) {
     if (!factorized) return fail(BCR_NUMERICAL, "BorderedCR::solve: the matrix is not factorized\n");
     if (nrhs < 0 || ld < L()) return fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::solve: bad ldRhs = %d\n", ld));
@@ -250,6 +274,10 @@ struct bcr_handle_s {
   }
 
   int solve_host(int nrhs, double* x, int ld) {
+    if (pending_status) {
+      int rc = factorize_status();
+      if (rc) return rc;
+    }
     if (!factorized) return fail(BCR_NUMERICAL, "BorderedCR::solve: the matrix is not factorized\n");
     if (nrhs < 0 || ld < L()) return fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::solve: bad ldRhs = %d\n", ld));
     if (nrhs == 0) return BCR_OK;
@@ -349,7 +377,7 @@ int bcr_allocate(bcr_handle h, int nblock, int n, int qr, int qx, int nr, int nx
     return BCR_OK;  // cc:55-61
   }
   h->release_device();
-  Dims d{};
+  Dims d{};  // (release_device also drops captured graphs)
   d.nblock = nblock; d.n = n; d.qr = qr; d.qx = qx; d.nr = nr; d.nx = nx;
   d.Nr = 2 * n + nr + qr;
   d.Nc = 2 * n + nx + qx;
@@ -889,6 +917,19 @@ int bcr_factorize_device(bcr_handle h) {
   return h->factorize_device();
 }
 
+int bcr_factorize_async(bcr_handle h) {
+  H_ALLOC(h);
+  int rc = h->ensure_device();
+  if (rc) return rc;
+  if (h->dirty && (rc = h->upload())) return rc;
+  return h->factorize_launch();
+}
+
+int bcr_factorize_status(bcr_handle h) {
+  H_ALLOC(h);
+  return h->factorize_status();
+}
+
 int bcr_solve_device(bcr_handle h, int nrhs, double* d_x, int ld) {
   H_ALLOC(h);
   return h->solve_device(nrhs, d_x, ld);
@@ -902,6 +943,63 @@ int bcr_mv_device(bcr_handle h, double alpha, const double* d_x, double beta, do
   bcr::launch_mv(h->s, alpha, d_x, beta, d_res, h->stream);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? BCR_OK : h->cuda_fail(e, "Mv launch");
+}
+
+void* bcr_get_stream(bcr_handle h) {
+  if (!h || !h->allocated) return nullptr;
+  if (h->ensure_device()) return nullptr;
+  return h->stream;
+}
+
+int bcr_graph_capture(bcr_handle h, int what, int nrhs, double* d_x, int ld, const double* d_rhs) {
+  H_ALLOC(h);
+  if (what < BCR_GRAPH_FACTORIZE || what > BCR_GRAPH_STEP)
+    return h->fail(BCR_BAD_ARGUMENT, fmt("bcr_graph_capture: unknown graph kind %d\n", what));
+  int rc = h->ensure_device();
+  if (rc) return rc;
+  if (h->dirty && (rc = h->upload())) return rc;
+  if ((what & BCR_GRAPH_SOLVE) && (nrhs < 1 || ld < h->L() || !d_x))
+    return h->fail(BCR_BAD_ARGUMENT, "bcr_graph_capture: bad right-hand-side buffer\n");
+  // one eager run first: it validates the selection and sets kernel attributes
+  if (what & BCR_GRAPH_FACTORIZE) {
+    if ((rc = h->factorize_device())) return rc;
+  } else if (!h->factorized) {
+    return h->fail(BCR_NUMERICAL, "bcr_graph_capture: factorize before capturing a solve\n");
+  }
+  if (what & BCR_GRAPH_SOLVE) {
+    if (d_rhs) cudaMemcpyAsync(d_x, d_rhs, (size_t)ld * nrhs * 8, cudaMemcpyDeviceToDevice, h->stream);
+    if ((rc = h->solve_device(nrhs, d_x, ld))) return rc;
+  }
+  cudaError_t e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "graph warm-up");
+  if (h->graphs[what]) { cudaGraphExecDestroy(h->graphs[what]); h->graphs[what] = nullptr; }
+  e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) return h->cuda_fail(e, "cudaStreamBeginCapture");
+  if (what & BCR_GRAPH_FACTORIZE) {
+    h->s.sel = h->sel; h->s.sel_last = h->sel_last; h->s.use_tc = h->use_tc;
+    bcr::launch_factorize(h->s, h->stream);
+  }
+  if (what & BCR_GRAPH_SOLVE) {
+    if (d_rhs) cudaMemcpyAsync(d_x, d_rhs, (size_t)ld * nrhs * 8, cudaMemcpyDeviceToDevice, h->stream);
+    bcr::launch_solve(h->s, d_x, ld, nrhs, h->stream);
+  }
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(h->stream, &graph);
+  if (e != cudaSuccess) { cudaGetLastError(); return h->cuda_fail(e, "cudaStreamEndCapture"); }
+  e = cudaGraphInstantiate(&h->graphs[what], graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) { h->graphs[what] = nullptr; return h->cuda_fail(e, "cudaGraphInstantiate"); }
+  return BCR_OK;
+}
+
+int bcr_graph_launch(bcr_handle h, int what) {
+  H_ALLOC(h);
+  if (what < BCR_GRAPH_FACTORIZE || what > BCR_GRAPH_STEP || !h->graphs[what])
+    return h->fail(BCR_BAD_ARGUMENT, "bcr_graph_launch: graph not captured\n");
+  cudaError_t e = cudaGraphLaunch(h->graphs[what], h->stream);
+  if (e != cudaSuccess) return h->cuda_fail(e, "cudaGraphLaunch");
+  if (what & BCR_GRAPH_FACTORIZE) { h->pending_status = true; h->factorized = true; }
+  return BCR_OK;
 }
 
 int bcr_synchronize(bcr_handle h) {

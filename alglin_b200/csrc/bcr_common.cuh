@@ -6,7 +6,9 @@
 //   B     [nblock][n*nx]       column-major n x nx
 //   C     [nblock+1][nr*n]     column-major nr x n
 //   T     [nblock][2n*n + n]   panel factors (2n x n, ld 2n) + tau
-//   P     [nblock][n]          0-based row pivots (LU) or column swaps (QRP)
+//   P     [nblock][3n] (uint8)  row map: position -> original panel row (2n
+//                               entries, getrf's final row order), then the
+//                               column map of QRP (n entries, y index -> x index)
 // Each array lives in its own device allocation; a cyclic-reduction level
 // touches whole blocks, so every block read or written is one contiguous run.
 #pragma once
@@ -34,6 +36,7 @@ struct Dims {
 };
 
 __host__ __device__ inline size_t szT(const Dims& d) { return 2 * (size_t)d.n * d.n + d.n; }
+__host__ __device__ inline size_t szP(const Dims& d) { return 3 * (size_t)d.n; }
 
 // number of pairs (j-k, j) eliminated at the level with stride k
 __host__ __device__ inline long pairs_at_level(int nblock, int k) {

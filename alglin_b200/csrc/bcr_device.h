@@ -12,11 +12,12 @@ struct DevState {
   Dims d;
   int sel;        // Internal
   int sel_last;   // LastKind actually used (after fallback)
+  int use_tc;     // allow the FP64 tensor-core pair kernel
   // loaded matrix (reference layout), never modified on the device
   double *D0, *E0, *B0, *C0, *Cq, *F0, *H;
   // working blocks / factors
   double *D, *E, *B, *C, *T;
-  int* P;
+  unsigned char* P;   // row / column maps, szP bytes per block
   // scratch: border contributions per eliminated block
   double *Rbuf, *Fbuf, *XB;
   int xb_cap;           // nrhs capacity of XB

@@ -36,7 +36,7 @@ struct FactorArgs {
   const double *D0, *E0, *B0, *C0;  // loaded matrix, read at the first level
   T *D, *E, *B, *C;                  // working blocks
   T* Tm;
-  int* P;
+  unsigned char* P;
   T *Rbuf, *Fbuf;
   StatusWords* st;
   int k, first, ldw;
@@ -235,7 +235,24 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_factor_level(FactorArgs<T>
       }
       if (SEL != SEL_LU)
         for (int i = lane; i < n; i += 32) Tj[2 * nn + i] = tau[i];
-      for (int i = lane; i < n; i += 32) a.P[(size_t)j * n + i] = ipiv[i];
+      __syncwarp();
+      // row map (getrf row order) and column map (QRP) from the swap sequence,
+      // built in the tau scratch (already stored)
+      unsigned char* Pj = a.P + (size_t)j * szP(d);
+      unsigned char* mp = reinterpret_cast<unsigned char*>(tau);
+      if (lane == 0) {
+        if (SEL == SEL_LU) {
+          for (int r = 0; r < n2; ++r) mp[r] = (unsigned char)r;
+          for (int i = 0; i < n; ++i) { unsigned char t = mp[i]; mp[i] = mp[ipiv[i]]; mp[ipiv[i]] = t; }
+        } else {
+          for (int r = 0; r < n2; ++r) mp[r] = (unsigned char)r;
+          for (int i = 0; i < n; ++i) mp[n2 + i] = (unsigned char)i;
+          if (SEL == SEL_QRP)
+            for (int i = 0; i < n; ++i) { unsigned char t = mp[n2 + i]; mp[n2 + i] = mp[n2 + ipiv[i]]; mp[n2 + ipiv[i]] = t; }
+        }
+      }
+      __syncwarp();
+      for (int i = lane; i < (SEL == SEL_LU ? n2 : 3 * n); i += 32) Pj[i] = mp[i];
       const size_t oj = (size_t)j * nn, ojp = (size_t)jp * nn;
       for (int idx = lane; idx < (int)nn; idx += 32) {
         const int i = idx % n, c = idx / n;
@@ -266,6 +283,467 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_factor_level(FactorArgs<T>
   }
 }
 
+// ---------------------------------------------------------------------------
+// register-resident LU pair elimination for n <= N <= 16 (lane = panel row)
+//
+// Lane l < 2n holds row l of the work matrix [panel | x_jp | x_jpp | xb] in
+// registers.  Row interchanges are not performed physically: every lane keeps
+// the LAPACK row position of its row (mypos), and the swap of positions i and
+// p at step i (getrf's ipiv) is replayed on those positions, so the final
+// positions reproduce the row order of getrf exactly.  The pivot row of each
+// step is broadcast through shared memory; the nr border rows are spread over
+// the lanes by column (lane c holds column c, and c+32) and are eliminated with
+// the same pivot rows, which yields C_j U^-1 and the C/F Schur updates.
+// ---------------------------------------------------------------------------
+template <int N, int NXM, int NRM>
+__global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<double> a) {
+  constexpr int NC = 3 * N + NXM;
+  constexpr int NCP = (NC + 1) & ~1;
+  constexpr int SLOTS = (NC + 31) / 32;
+  constexpr unsigned FULL = 0xffffffffu;
+  __shared__ __align__(16) double ubuf[4][NCP];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const Dims d = a.d;
+  const int n = d.n, nr = d.nr, nx = d.nx, nb = d.nblock, n2 = 2 * n;
+  const size_t nn = (size_t)n * n, nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
+  double* ub = ubuf[warp];
+  const int k = a.k;
+  const long np = pairs_at_level(nb, k);
+  const bool first = a.first != 0;
+  const bool act = lane < n2, top = lane < n;
+  const int ri = top ? lane : lane - n;
+  const double* srcD = first ? a.D0 : a.D;
+  const double* srcE = first ? a.E0 : a.E;
+  const double* srcB = first ? a.B0 : a.B;
+  const double* srcC = first ? a.C0 : a.C;
+
+  for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
+    const int j = k + (int)(2L * k * q), jp = j - k;
+    double row[NC];
+    {
+      const double* Pm = top ? srcE + (size_t)jp * nn : srcD + (size_t)j * nn;
+      const double* Xm = top ? srcD + (size_t)jp * nn : srcE + (size_t)j * nn;
+      const double* Bm = srcB + (size_t)(top ? jp : j) * nnx;
+#pragma unroll
+      for (int c = 0; c < N; ++c) {
+        double pv = 0.0, xv = 0.0;
+        if (act && c < n) { pv = Pm[(size_t)c * n + ri]; xv = Xm[(size_t)c * n + ri]; }
+        row[c] = pv;
+        row[N + c] = top ? xv : 0.0;
+        row[2 * N + c] = top ? 0.0 : xv;
+      }
+#pragma unroll
+      for (int c = 0; c < NXM; ++c) row[3 * N + c] = (act && c < nx) ? Bm[(size_t)c * n + ri] : 0.0;
+    }
+    double cr[NRM][SLOTS];
+#pragma unroll
+    for (int r = 0; r < NRM; ++r)
+#pragma unroll
+      for (int sl = 0; sl < SLOTS; ++sl) cr[r][sl] = 0.0;
+    if (lane < n) {
+      const double* Cj = srcC + (size_t)j * nrn + (size_t)lane * nr;
+#pragma unroll
+      for (int r = 0; r < NRM; ++r)
+        if (r < nr) cr[r][0] = Cj[r];
+    }
+
+    int mypos = lane, mykey = 0, info = 0;
+    bool done = !act;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      if (i < n) {
+        double v = done ? -1.0 : fabs(row[i]);
+        if (v != v) v = -0.5;  // NaN never wins against a number
+        int key = done ? 0x7fffffff : mypos;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ov = __shfl_xor_sync(FULL, v, o);
+          const int ok = __shfl_xor_sync(FULL, key, o);
+          if (ov > v || (ov == v && ok < key)) { v = ov; key = ok; }
+        }
+        const unsigned m = __ballot_sync(FULL, !done && mypos == key);
+        const int p = __ffs(m) - 1;
+        if (lane == i) mykey = key;
+        if (!done && mypos == i && lane != p) mypos = key;
+        if (lane == p) {
+          mypos = i;
+#pragma unroll
+          for (int c = (i & ~1); c < NCP; c += 2)
+            *reinterpret_cast<double2*>(&ub[c]) = make_double2(row[c], c + 1 < NC ? row[c + 1] : 0.0);
+        }
+        __syncwarp();
+        const double piv = ub[i];
+        if (piv == 0.0 && info == 0) info = i + 1;
+        const double rinv = piv != 0.0 ? 1.0 / piv : 0.0;
+        if (!done && lane != p) {
+          const double l = row[i] * rinv;
+          row[i] = l;
+#pragma unroll
+          for (int c = i + 1; c < NC; ++c) row[c] = fma(-l, ub[c], row[c]);
+        }
+        if (lane == p) done = true;
+#pragma unroll
+        for (int r = 0; r < NRM; ++r) {
+          if (r < nr) {
+            const double mr = __shfl_sync(FULL, cr[r][0], i) * rinv;
+            if (lane == i) cr[r][0] = mr;
+            else if (lane > i && lane < NC) cr[r][0] = fma(-mr, ub[lane], cr[r][0]);
+#pragma unroll
+            for (int sl = 1; sl < SLOTS; ++sl)
+              if (lane + 32 * sl < NC) cr[r][sl] = fma(-mr, ub[lane + 32 * sl], cr[r][sl]);
+          }
+        }
+        __syncwarp();
+      }
+    }
+    if (info != 0) {
+      if (lane == 0) report(a.st, DEV_ZERO_PIVOT, j, info, k);
+      continue;
+    }
+    // ---------------------------------------------------------------- store
+    if (act) {
+      double* Tj = a.Tm + (size_t)j * szT(d);
+      const bool urow = mypos < n;
+      const int rr = urow ? mypos : mypos - n;
+      const size_t blk = urow ? (size_t)j : (size_t)jp;
+      double* Dd = a.D + blk * nn + rr;
+      double* Ed = a.E + blk * nn + rr;
+      double* Bd = a.B + blk * nnx + rr;
+#pragma unroll
+      for (int c = 0; c < N; ++c)
+        if (c < n) {
+          Tj[(size_t)mypos + (size_t)c * n2] = row[c];
+          Dd[(size_t)c * n] = row[N + c];
+          Ed[(size_t)c * n] = row[2 * N + c];
+        }
+#pragma unroll
+      for (int c = 0; c < NXM; ++c)
+        if (c < nx) Bd[(size_t)c * n] = row[3 * N + c];
+    }
+    if (act) a.P[(size_t)j * szP(d) + mypos] = (unsigned char)lane;
+#pragma unroll
+    for (int sl = 0; sl < SLOTS; ++sl) {
+      const int col = lane + 32 * sl;
+      if (col >= NC) continue;
+#pragma unroll
+      for (int r = 0; r < NRM; ++r) {
+        if (r >= nr) continue;
+        const double v = cr[r][sl];
+        if (col < N) {
+          if (col < n) a.C[(size_t)j * nrn + (size_t)col * nr + r] = v;
+        } else if (col < 2 * N) {
+          const int c = col - N;
+          if (c < n) {
+            const size_t o = (size_t)jp * nrn + (size_t)c * nr + r;
+            a.C[o] = srcC[o] + v;
+          }
+        } else if (col < 3 * N) {
+          const int c = col - 2 * N;
+          if (c < n) a.Rbuf[(size_t)j * nrn + (size_t)c * nr + r] = v;
+        } else {
+          const int c = col - 3 * N;
+          if (c < nx) a.Fbuf[(size_t)j * nrnx + (size_t)c * nr + r] = v;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-core LU pair elimination for n == N (N = 8 or 16), nr <= 8, nx <= 8.
+//
+//   phase 1 (SIMT, lane = panel row): partial-pivot LU of the 2N x N panel
+//     [E_jp; D_j] in registers, with getrf's row order replayed on positions
+//     (mypos) and the pivot chosen by exact integer reductions on the bits of
+//     |a| (largest |a|, then smallest position: the idamax rule).  The nr
+//     border rows ride along as a second register row of lanes 0..nr-1 and
+//     come out as C_j U^-1.
+//   phase 2 (SIMT): the elimination operator on the trailing columns,
+//       G = [ L^-1 ; -M L^-1 ; -(C_j U^-1) L^-1 ]      ((2N+8) x N)
+//     by a right triangular solve X L = [I; -M; -C'] per lane.
+//   phase 3 (FP64 tensor cores, mma.sync m8n8k4): one GEMM
+//       [U-row | reduced row | border update] = G (PW)_top + [0; (PW)_bot; 0]
+//     over the 2N + nx trailing columns [x_jp | x_jpp | xb].
+// The results are staged in shared memory and written with coalesced stores.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+template <int N>
+struct TcShape {
+  static constexpr int MT = 2 * N + 8;             // GEMM rows: U-row, reduced row, border (padded)
+  static constexpr int NTILES = (2 * N + 8 + 7) / 8;  // trailing columns 2N + nx, nx <= 8
+  static constexpr int NTP = NTILES * 8;
+  static constexpr int LDW = NTP + 1;               // work / output rows (odd: conflict-light)
+  static constexpr int LDG = N + 4;                 // operator rows (16B aligned, conflict-free A loads)
+  static constexpr int KSTEPS = N / 4;
+  static constexpr int MTILES = MT / 8;
+  static constexpr int WS = MT * LDW;               // doubles
+  static constexpr int GS = MT * LDG;
+  static constexpr size_t BYTES = (size_t)(WS + GS + N) * 8 + 2 * N * sizeof(int);
+};
+
+size_t tc_smem_per_warp(int n) {
+  return n == 16 ? TcShape<16>::BYTES : n == 8 ? TcShape<8>::BYTES : 0;
+}
+
+template <int N>
+__global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a) {
+  using S = TcShape<N>;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  double* Wt = reinterpret_cast<double*>(smem_raw + (size_t)warp * S::BYTES);
+  double* Gs = Wt + S::WS;
+  double* bc = Gs + S::GS;
+  int* rowof = reinterpret_cast<int*>(bc + N);
+  const Dims d = a.d;
+  const int nr = d.nr, nx = d.nx, nb = d.nblock;
+  constexpr int n = N, n2 = 2 * N;
+  constexpr size_t nn = (size_t)N * N;
+  const size_t nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
+  const int NT = n2 + nx;  // live trailing columns
+  const int k = a.k;
+  const long np = pairs_at_level(nb, k);
+  const bool first = a.first != 0;
+  const double* srcD = first ? a.D0 : a.D;
+  const double* srcE = first ? a.E0 : a.E;
+  const double* srcB = first ? a.B0 : a.B;
+  const double* srcC = first ? a.C0 : a.C;
+  const bool act = lane < n2, top = lane < n;
+  const int ri = top ? lane : lane - n;
+  const int g = lane >> 2, t = lane & 3;
+
+  for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
+    const int j = k + (int)(2L * k * q), jp = j - k;
+    // ------------------------------------------------------------ load
+    double rowA[N], rowC[N];
+    {
+      const double* Pm = top ? srcE + (size_t)jp * nn : srcD + (size_t)j * nn;
+#pragma unroll
+      for (int c = 0; c < N; ++c) rowA[c] = act ? Pm[(size_t)c * n + ri] : 0.0;
+#pragma unroll
+      for (int c = 0; c < N; ++c) rowC[c] = 0.0;
+      if (lane < nr) {
+        const double* Cj = srcC + (size_t)j * nrn + lane;
+#pragma unroll
+        for (int c = 0; c < N; ++c) rowC[c] = Cj[(size_t)c * nr];
+      }
+      // trailing columns in the original row order: TOP [D_jp 0 B_jp], BOTTOM [0 E_j B_j]
+      // compile-time trip counts: every load of the pair is issued before the
+      // first one is consumed, so a lone pair pays one memory latency
+      const double* Djp = srcD + (size_t)jp * nn;
+      const double* Ej = srcE + (size_t)j * nn;
+#pragma unroll
+      for (int it = 0; it < (int)(nn / 32); ++it) {
+        const int idx = lane + 32 * it;
+        const int r = idx % n, c = idx / n;
+        Wt[r * S::LDW + c] = Djp[idx];
+        Wt[r * S::LDW + n + c] = 0.0;
+        Wt[(n + r) * S::LDW + c] = 0.0;
+        Wt[(n + r) * S::LDW + n + c] = Ej[idx];
+      }
+      const double* Bjp = srcB + (size_t)jp * nnx;
+      const double* Bj = srcB + (size_t)j * nnx;
+#pragma unroll
+      for (int it = 0; it < (8 * N + 31) / 32; ++it) {
+        const int idx = lane + 32 * it;
+        if (idx < (int)nnx) {
+          const int r = idx % n, c = idx / n;
+          Wt[r * S::LDW + n2 + c] = Bjp[idx];
+          Wt[(n + r) * S::LDW + n2 + c] = Bj[idx];
+        }
+      }
+      // zero the padding columns of the live rows (they feed padding outputs only,
+      // but keep them finite)
+      for (int idx = lane; idx < n2 * (S::NTP - NT); idx += 32) {
+        const int r = idx % n2, c = NT + idx / n2;
+        Wt[r * S::LDW + c] = 0.0;
+      }
+    }
+    // --------------------------------------------------- phase 1: panel LU
+    int mypos = lane, mykey = 0, info = 0;
+    bool done = !act;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      // pivot: max |a| over rows not yet used, ties to the smaller position
+      const double av = fabs(rowA[i]);
+      const unsigned long long bits = (unsigned long long)__double_as_longlong(av);
+      unsigned hi = (unsigned)(bits >> 32) + 1u;
+      if (done) hi = 0u;
+      else if (av != av) hi = 1u;  // NaN loses against every number
+      const unsigned hmax = __reduce_max_sync(FULL, hi);
+      const unsigned lo = (hi == hmax) ? (unsigned)bits : 0u;
+      const unsigned lmax = __reduce_max_sync(FULL, lo);
+      const bool cand = (hi == hmax) && (lo == lmax) && !done;
+      const unsigned pmin = __reduce_min_sync(FULL, cand ? (unsigned)mypos : 0xffffffffu);
+      const unsigned m = __ballot_sync(FULL, cand && (unsigned)mypos == pmin);
+      const int p = __ffs(m) - 1;
+      if (lane == i) mykey = (int)pmin;
+      if (!done && mypos == i && lane != p) mypos = (int)pmin;
+      if (lane == p) {
+        mypos = i;
+#pragma unroll
+        for (int c = (i & ~1); c < N; c += 2)
+          *reinterpret_cast<double2*>(&bc[c]) = make_double2(rowA[c], rowA[c + 1]);
+      }
+      __syncwarp();
+      const double piv = bc[i];
+      if (piv == 0.0 && info == 0) info = i + 1;
+      const double rinv = piv != 0.0 ? 1.0 / piv : 0.0;
+      if (!done && lane != p) {
+        const double l = rowA[i] * rinv;
+        rowA[i] = l;
+#pragma unroll
+        for (int c = i + 1; c < N; ++c) rowA[c] = fma(-l, bc[c], rowA[c]);
+      }
+      if (lane < nr) {
+        const double l = rowC[i] * rinv;
+        rowC[i] = l;
+#pragma unroll
+        for (int c = i + 1; c < N; ++c) rowC[c] = fma(-l, bc[c], rowC[c]);
+      }
+      if (lane == p) done = true;
+      __syncwarp();
+    }
+    if (info != 0) {
+      if (lane == 0) report(a.st, DEV_ZERO_PIVOT, j, info, k);
+      continue;
+    }
+    // panel factors T_j (L\U and M in getrf row order), pivots, C_j U^-1
+    {
+      double* Tj = a.Tm + (size_t)j * szT(d);
+      if (act) {
+#pragma unroll
+        for (int c = 0; c < N; ++c) Tj[(size_t)mypos + (size_t)c * n2] = rowA[c];
+        rowof[mypos] = lane;
+      }
+      if (act) a.P[(size_t)j * szP(d) + mypos] = (unsigned char)lane;
+      if (lane < nr) {
+        double* Cj = a.C + (size_t)j * nrn + lane;
+#pragma unroll
+        for (int c = 0; c < N; ++c) Cj[(size_t)c * nr] = rowC[c];
+      }
+      // L^T rows (column c of L, contiguous in m) for the triangular solve
+      if (act && mypos < n) {
+#pragma unroll
+        for (int c = 0; c < N; ++c) Gs[c * S::LDG + mypos] = rowA[c];
+      }
+    }
+    __syncwarp();
+    // ------------------------------------ phase 2: operator G (X L = R)
+    // R rows: identity for U-row positions, -M for reduced positions, -C' for border rows
+    {
+      double x[N];
+#pragma unroll
+      for (int c = 0; c < N; ++c) x[c] = (mypos < n) ? (c == mypos ? 1.0 : 0.0) : -rowA[c];
+#pragma unroll
+      for (int c = 0; c < N; ++c) rowC[c] = -rowC[c];
+#pragma unroll
+      for (int c = N - 1; c >= 0; --c) {
+        double s = x[c], sc = rowC[c];
+#pragma unroll
+        for (int mm = c + 1; mm < N; ++mm) {
+          const double l = Gs[c * S::LDG + mm];  // L(mm, c)
+          s = fma(-x[mm], l, s);
+          sc = fma(-rowC[mm], l, sc);
+        }
+        x[c] = s;
+        rowC[c] = sc;
+      }
+      __syncwarp();
+      if (act) {
+#pragma unroll
+        for (int c = 0; c < N; c += 2)
+          *reinterpret_cast<double2*>(&Gs[mypos * S::LDG + c]) = make_double2(x[c], x[c + 1]);
+      }
+      if (lane < 8) {  // border rows (zero when lane >= nr)
+#pragma unroll
+        for (int c = 0; c < N; c += 2) {
+          const bool live = lane < nr;
+          *reinterpret_cast<double2*>(&Gs[(n2 + lane) * S::LDG + c]) =
+              make_double2(live ? rowC[c] : 0.0, live ? rowC[c + 1] : 0.0);
+        }
+      }
+    }
+    __syncwarp();
+    // ----------------------------------------- phase 3: tensor-core GEMM
+    double acc[S::MTILES][S::NTILES][2];
+#pragma unroll
+    for (int mt = 0; mt < S::MTILES; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < S::NTILES; ++nt) {
+        const int row = mt * 8 + g;
+        double c0 = 0.0, c1 = 0.0;
+        if (row >= n && row < n2) {  // (PW)_bot
+          const double* w = Wt + rowof[row] * S::LDW + nt * 8 + 2 * t;
+          c0 = w[0];
+          c1 = w[1];
+        }
+        acc[mt][nt][0] = c0;
+        acc[mt][nt][1] = c1;
+      }
+#pragma unroll
+    for (int ks = 0; ks < S::KSTEPS; ++ks) {
+      double bfr[S::NTILES];
+      const double* wrow = Wt + rowof[ks * 4 + t] * S::LDW + g;
+#pragma unroll
+      for (int nt = 0; nt < S::NTILES; ++nt) bfr[nt] = wrow[nt * 8];
+#pragma unroll
+      for (int mt = 0; mt < S::MTILES; ++mt) {
+        const double afr = Gs[(mt * 8 + g) * S::LDG + ks * 4 + t];
+#pragma unroll
+        for (int nt = 0; nt < S::NTILES; ++nt) dmma_8x8x4(acc[mt][nt][0], acc[mt][nt][1], afr, bfr[nt]);
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int mt = 0; mt < S::MTILES; ++mt)
+#pragma unroll
+      for (int nt = 0; nt < S::NTILES; ++nt) {
+        double* o = Wt + (mt * 8 + g) * S::LDW + nt * 8 + 2 * t;
+        o[0] = acc[mt][nt][0];
+        o[1] = acc[mt][nt][1];
+      }
+    __syncwarp();
+    // ------------------------------------------------------------ store
+    {
+      double* Dj = a.D + (size_t)j * nn;
+      double* Ejo = a.E + (size_t)j * nn;
+      double* Djp = a.D + (size_t)jp * nn;
+      double* Ejp = a.E + (size_t)jp * nn;
+      for (int idx = lane; idx < (int)nn; idx += 32) {
+        const int r = idx % n, c = idx / n;
+        Dj[idx] = Wt[r * S::LDW + c];
+        Ejo[idx] = Wt[r * S::LDW + n + c];
+        Djp[idx] = Wt[(n + r) * S::LDW + c];
+        Ejp[idx] = Wt[(n + r) * S::LDW + n + c];
+      }
+      double* Bj = a.B + (size_t)j * nnx;
+      double* Bjp = a.B + (size_t)jp * nnx;
+      for (int idx = lane; idx < (int)nnx; idx += 32) {
+        const int r = idx % n, c = idx / n;
+        Bj[idx] = Wt[r * S::LDW + n2 + c];
+        Bjp[idx] = Wt[(n + r) * S::LDW + n2 + c];
+      }
+      for (int idx = lane; idx < (int)nrn; idx += 32) {
+        const int r = idx % nr, c = idx / nr;
+        const size_t o = (size_t)jp * nrn + idx;
+        a.C[o] = srcC[o] + Wt[(n2 + r) * S::LDW + c];
+        a.Rbuf[(size_t)j * nrn + idx] = Wt[(n2 + r) * S::LDW + n + c];
+      }
+      for (int idx = lane; idx < (int)nrnx; idx += 32) {
+        const int r = idx % nr, c = idx / nr;
+        a.Fbuf[(size_t)j * nrnx + idx] = Wt[(n2 + r) * S::LDW + n2 + c];
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // C_jpp += dC_jpp for every pair of the level (one writer per target block)
 template <typename T>
 __global__ void k_border_fix(Dims d, T* C, const T* Rbuf, int k) {
@@ -282,30 +760,45 @@ __global__ void k_border_fix(Dims d, T* C, const T* Rbuf, int k) {
 }
 
 // ---------------------------------------------------------------------------
-// deterministic sums over blocks 1..nblock-1 of per-block m-vectors
-//   stage 1: CTA g sums a fixed chunk of blocks in order
-//   stage 2: one CTA sums the chunk partials in order and adds to out
+// deterministic sums of per-block m-vectors (m <= 256) over blocks
+// [first, first+count): CTA g reduces a fixed chunk of blocks with a fixed
+// thread-to-block map and a fixed shared-memory tree, so the result does not
+// depend on timing.  With out == nullptr the CTA writes its partial to
+// part[g]; otherwise (one CTA) it writes out = base + sum (column height h).
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_reduce_stage1(const T* buf, long first, long count, int m, long chunk, T* part) {
+__global__ void __launch_bounds__(256) k_reduce_tree(const T* buf, int stride, long first, long count,
+                                                     int m, long chunk, T* part, const T* base, int h,
+                                                     int ldb, T* out, int ldo) {
+  __shared__ T red[256];
+  const int tid = threadIdx.x;
+  const int S = 256 / m;  // items reduced in parallel per element
+  const int e = tid % m, g = tid / m;
   const long b0 = first + (long)blockIdx.x * chunk;
   const long b1 = min(first + count, b0 + chunk);
-  for (int e = threadIdx.x; e < m; e += blockDim.x) {
-    T s = T(0);
-    for (long b = b0; b < b1; ++b) s += buf[(size_t)b * m + e];
-    part[(size_t)blockIdx.x * m + e] = s;
+  T a0 = T(0), a1 = T(0);
+  if (g < S) {
+    long b = b0 + g;
+    for (; b + S < b1; b += 2 * S) {
+      a0 += buf[(size_t)b * stride + e];
+      a1 += buf[(size_t)(b + S) * stride + e];
+    }
+    if (b < b1) a0 += buf[(size_t)b * stride + e];
   }
-}
-
-// out[e] (stride ld per column of height h) = base[e] + sum of partials
-template <typename T>
-__global__ void k_reduce_stage2(const T* part, int nparts, int m, int h, const T* base, int ldb,
-                                T* out, int ldo) {
-  for (int e = threadIdx.x; e < m; e += blockDim.x) {
-    T s = T(0);
-    for (int g = 0; g < nparts; ++g) s += part[(size_t)g * m + e];
-    const int r = e % h, c = e / h;
-    out[(size_t)c * ldo + r] = (base ? base[(size_t)c * ldb + r] : T(0)) + s;
+  red[tid] = a0 + a1;
+  __syncthreads();
+  for (int w = 1; w < S; w *= 2) {
+    if (g < S && g % (2 * w) == 0 && g + w < S) red[tid] += red[tid + w * m];
+    __syncthreads();
+  }
+  if (g == 0) {
+    const T s = red[e];
+    if (out) {
+      const int r = e % h, c = e / h;
+      out[(size_t)c * ldo + r] = (base ? base[(size_t)c * ldb + r] : T(0)) + s;
+    } else {
+      part[(size_t)blockIdx.x * m + e] = s;
+    }
   }
 }
 
@@ -316,7 +809,7 @@ template <typename T>
 struct SweepArgs {
   Dims d;
   const T *D, *E, *B, *C, *Tm;
-  const int* P;
+  const unsigned char* P;
   T* x;
   int ldx, nrhs;
   T* XB;
@@ -334,24 +827,15 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_forward_level(SweepArgs<T>
   for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
     const int j = k + (int)(2L * k * q), jp = j - k;
     const T* Tj = a.Tm + (size_t)j * szT(d);
-    for (int idx = lane; idx < n * nrhs; idx += 32) {
-      const int i = idx % n, c = idx / n;
-      W[(size_t)c * ldw + i] = a.x[(size_t)c * a.ldx + (size_t)jp * n + i];
-      W[(size_t)c * ldw + n + i] = a.x[(size_t)c * a.ldx + (size_t)j * n + i];
+    const unsigned char* Pj = a.P + (size_t)j * szP(d);
+    for (int idx = lane; idx < n2 * nrhs; idx += 32) {
+      const int pos = idx % n2, c = idx / n2;
+      const int r = a.sel == SEL_LU ? Pj[pos] : pos;  // original row at this position
+      const size_t o = (size_t)c * a.ldx + (r < n ? (size_t)jp * n + r : (size_t)j * n + (r - n));
+      W[(size_t)c * ldw + pos] = a.x[o];
     }
     __syncwarp();
     if (a.sel == SEL_LU) {
-      const int* Pj = a.P + (size_t)j * n;
-      for (int i = 0; i < n; ++i) {
-        const int p = Pj[i];
-        if (p != i)
-          for (int c = lane; c < nrhs; c += 32) {
-            T t = W[(size_t)c * ldw + i];
-            W[(size_t)c * ldw + i] = W[(size_t)c * ldw + p];
-            W[(size_t)c * ldw + p] = t;
-          }
-        __syncwarp();
-      }
       for (int i = 0; i < n; ++i) {
         for (int r = i + 1 + lane; r < n2; r += 32) {
           const T l = Tj[(size_t)i * n2 + r];
@@ -427,16 +911,142 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_backward_level(SweepArgs<T
         for (int r = lane; r < i; r += 32) Y[r] -= Tj[(size_t)i * n2 + r] * xi;
         __syncwarp();
       }
-      if (a.sel == SEL_QRP && lane == 0) {
-        const int* Pj = a.P + (size_t)j * n;
-        for (int i = n - 1; i >= 0; --i) {
-          const int p = Pj[i];
-          if (p != i) { T t = Y[i]; Y[i] = Y[p]; Y[p] = t; }
+      const unsigned char* cmap = a.P + (size_t)j * szP(d) + 2 * n;
+      for (int i = lane; i < n; i += 32) xc[(size_t)j * n + (a.sel == SEL_QRP ? cmap[i] : i)] = Y[i];
+      __syncwarp();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// register-resident sweeps for n <= N <= 16: one warp per pair.
+//
+// forward (forward, cc:1615-1719): lane = position r < 2n of the stacked
+//   [x_jp; x_j]; the row map gathers the original row with one shuffle, the
+//   unit-lower L and M are applied by n broadcast steps (LU) or the n
+//   Householder reflectors by warp reductions (QR/QRP); xb partial -C'_j x_j.
+// backward (backward, cc:1805-2075): lanes 0..15 form D'_j x_jp, lanes
+//   16..31 E'_j x_jpp for row i = lane & 15; the halves are combined, the B'_j
+//   xb term added and U solved by n broadcast steps (QRP: column-map scatter).
+// All loads of a pair are issued before the first use.
+// ---------------------------------------------------------------------------
+template <int N, int NRM>
+__global__ void __launch_bounds__(256) k_forward_rows(SweepArgs<double> a) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const Dims d = a.d;
+  const int n = d.n, nr = d.nr, nb = d.nblock, n2 = 2 * n, nrhs = a.nrhs, k = a.k;
+  const bool act = lane < n2;
+  const bool lu = a.sel == SEL_LU;
+  const long np = pairs_at_level(nb, k);
+  for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
+    const int j = k + (int)(2L * k * q), jp = j - k;
+    const double* Tj = a.Tm + (size_t)j * szT(d);
+    double t[N];
+#pragma unroll
+    for (int c = 0; c < N; ++c) t[c] = (act && c < n) ? Tj[(size_t)c * n2 + lane] : 0.0;
+    double tau[N];
+#pragma unroll
+    for (int c = 0; c < N; ++c) tau[c] = (!lu && c < n) ? Tj[2 * (size_t)n * n + c] : 0.0;
+    const int src = (act && lu) ? (int)a.P[(size_t)j * szP(d) + lane] : lane;
+    double cp[NRM];
+    const double* Cj = a.C + (size_t)j * nr * n;
+#pragma unroll
+    for (int r = 0; r < NRM; ++r) cp[r] = (lane < n && r < nr) ? Cj[(size_t)lane * nr + r] : 0.0;
+    for (int col = 0; col < nrhs; ++col) {
+      double* xc = a.x + (size_t)col * a.ldx;
+      const double orig = act ? (lane < n ? xc[(size_t)jp * n + lane] : xc[(size_t)j * n + lane - n]) : 0.0;
+      double w = __shfl_sync(FULL, orig, src);
+      if (lu) {
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+          if (i < n) {
+            const double wi = __shfl_sync(FULL, w, i);
+            if (lane > i && act) w = fma(-t[i], wi, w);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) {
+          if (i < n) {
+            const double v = (lane > i && act) ? t[i] : (lane == i ? 1.0 : 0.0);
+            double sdot = warp_sum(v * w);
+            w = fma(-tau[i] * sdot, v, w);
+          }
         }
       }
-      __syncwarp();
-      for (int i = lane; i < n; i += 32) xc[(size_t)j * n + i] = Y[i];
-      __syncwarp();
+      if (act) {
+        if (lane < n) xc[(size_t)j * n + lane] = w;
+        else xc[(size_t)jp * n + lane - n] = w;
+      }
+      const double wt = lane < n ? w : 0.0;
+#pragma unroll
+      for (int r = 0; r < NRM; ++r) {
+        if (r < nr) {
+          const double sr = warp_sum(cp[r] * wt);
+          if (lane == 0) a.XB[(size_t)j * nr * nrhs + (size_t)col * nr + r] = -sr;
+        }
+      }
+    }
+  }
+}
+
+template <int N, int NXM>
+__global__ void __launch_bounds__(256) k_backward_rows(SweepArgs<double> a) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const Dims d = a.d;
+  const int n = d.n, nx = d.nx, nb = d.nblock, n2 = 2 * n, nrhs = a.nrhs, k = a.k;
+  const int i = lane & 15;
+  const bool hi = lane >= 16, rowok = i < n;
+  const bool qrp = a.sel == SEL_QRP;
+  const long np = pairs_at_level(nb, k);
+  const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
+  for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
+    const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
+    const double* Mt = (hi ? a.E : a.D) + (size_t)j * n * n;
+    const double* Tj = a.Tm + (size_t)j * szT(d);
+    const double* Bj = a.B + (size_t)j * n * nx;
+    double m[N], u[N], bb[NXM];
+#pragma unroll
+    for (int c = 0; c < N; ++c) m[c] = (rowok && c < n) ? Mt[(size_t)c * n + i] : 0.0;
+#pragma unroll
+    for (int c = 0; c < N; ++c) u[c] = (!hi && rowok && c < n) ? Tj[(size_t)c * n2 + i] : 0.0;
+#pragma unroll
+    for (int c = 0; c < NXM; ++c) bb[c] = (!hi && rowok && c < nx) ? Bj[(size_t)c * n + i] : 0.0;
+    double rdi = 0.0;  // 1 / U(i,i)
+#pragma unroll
+    for (int c = 0; c < N; ++c)
+      if (c == i) rdi = (!hi && rowok) ? 1.0 / u[c] : 0.0;
+    const int dst = (qrp && !hi && rowok) ? (int)a.P[(size_t)j * szP(d) + n2 + i] : i;
+    for (int col = 0; col < nrhs; ++col) {
+      double* xc = a.x + (size_t)col * a.ldx;
+      const double xv = rowok ? (hi ? xc[(size_t)jpp * n + i] : xc[(size_t)jp * n + i]) : 0.0;
+      const double xj = (!hi && rowok) ? xc[(size_t)j * n + i] : 0.0;
+      double xbv[NXM];
+#pragma unroll
+      for (int c = 0; c < NXM; ++c) xbv[c] = c < nx ? xc[xb_off + c] : 0.0;
+      double s = 0.0;
+#pragma unroll
+      for (int c = 0; c < N; ++c) {
+        if (c < n) {
+          const double xcv = __shfl_sync(FULL, xv, (lane & 16) | c);
+          s = fma(m[c], xcv, s);
+        }
+      }
+      s += __shfl_xor_sync(FULL, s, 16);
+#pragma unroll
+      for (int c = 0; c < NXM; ++c) s = fma(bb[c], xbv[c], s);
+      double y = xj - s;
+#pragma unroll
+      for (int ii = N - 1; ii >= 0; --ii) {
+        if (ii < n) {
+          const double xi = __shfl_sync(FULL, y * rdi, ii);
+          if (i == ii) y = xi;
+          else if (i < ii) y = fma(-u[ii], xi, y);
+        }
+      }
+      if (!hi && rowok) xc[(size_t)j * n + dst] = y;
     }
   }
 }
@@ -691,6 +1301,23 @@ __global__ void k_mv_tail(Dims d, const double* H, const double* Cq, const doubl
 // ---------------------------------------------------------------------------
 // host orchestration
 // ---------------------------------------------------------------------------
+// Raise a kernel's dynamic shared-memory limit once per process and kernel;
+// later calls (for instance inside a CUDA graph capture) only launch.
+template <typename K>
+static void smem_limit_once(K* kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return;
+  static const void* keys[64];
+  static size_t done[64];
+  static int used = 0;
+  const void* key = reinterpret_cast<const void*>(kernel);
+  int slot = 0;
+  while (slot < used && keys[slot] != key) ++slot;
+  if (slot < used && done[slot] >= bytes) return;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (slot == used && used < 64) { keys[used] = key; ++used; }
+  if (slot < 64) done[slot] = bytes;
+}
+
 static int grid_for(long work_items, int per_cta, int cap) {
   long g = (work_items + per_cta - 1) / per_cta;
   if (g < 1) g = 1;
@@ -705,17 +1332,31 @@ static void check_launch(const char* what) {
   }
 }
 
+// sums of per-block m-vectors, m = h x cols (column-major, height h <= 256);
+// column groups of at most 256 elements are reduced one after the other
 static void reduce_blocks(DevState& s, const double* buf, long first, long count, int m, int h,
                           const double* base, int ldb, double* out, int ldo, cudaStream_t st) {
-  if (m <= 0) return;
-  const long chunk = 64;
-  int nparts = count > 0 ? (int)((count + chunk - 1) / chunk) : 0;
-  if (nparts > 0) {
-    k_reduce_stage1<double><<<nparts, 128, 0, st>>>(buf, first, count, m, chunk, s.part);
-    check_launch("k_reduce_stage1");
+  if (m <= 0 || h <= 0) return;
+  const int cols = m / h, cw = h <= 256 ? 256 / h : 1;
+  const long chunk = 1024;
+  const int nparts = count > 0 ? (int)((count + chunk - 1) / chunk) : 0;
+  for (int c0 = 0; c0 < cols; c0 += cw) {
+    const int cn = cols - c0 < cw ? cols - c0 : cw, mm = cn * h;
+    const double* bb = buf + (size_t)c0 * h;
+    const double* ba = base ? base + (size_t)c0 * ldb : nullptr;
+    double* oo = out + (size_t)c0 * ldo;
+    if (nparts > 1) {
+      k_reduce_tree<double><<<nparts, 256, 0, st>>>(bb, m, first, count, mm, chunk, s.part, nullptr, h,
+                                                    0, nullptr, 0);
+      check_launch("k_reduce_tree");
+      k_reduce_tree<double><<<1, 256, 0, st>>>(s.part, mm, 0, nparts, mm, nparts, nullptr, ba, h, ldb,
+                                               oo, ldo);
+    } else {
+      k_reduce_tree<double><<<1, 256, 0, st>>>(bb, m, first, count, mm, chunk, nullptr, ba, h, ldb, oo,
+                                               ldo);
+    }
+    check_launch("k_reduce_tree");
   }
-  k_reduce_stage2<double><<<1, 256, 0, st>>>(s.part, nparts, m, h, base, ldb, out, ldo);
-  check_launch("k_reduce_stage2");
 }
 
 void launch_factorize(DevState& s, cudaStream_t st) {
@@ -745,20 +1386,32 @@ void launch_factorize(DevState& s, cudaStream_t st) {
   if (wpb > WARPS_PANEL) wpb = WARPS_PANEL;
   if (wpb < 1) wpb = 1;  // callers reject sizes whose single warp does not fit
   const size_t smem = per_warp * wpb;
-  if (smem > 48 * 1024) {
-    if (s.sel == SEL_LU)
-      cudaFuncSetAttribute(k_factor_level<double, SEL_LU>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX);
-    else if (s.sel == SEL_QR)
-      cudaFuncSetAttribute(k_factor_level<double, SEL_QR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX);
-    else
-      cudaFuncSetAttribute(k_factor_level<double, SEL_QRP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_MAX);
+  if (s.sel == SEL_LU) smem_limit_once(k_factor_level<double, SEL_LU>, smem);
+  else if (s.sel == SEL_QR) smem_limit_once(k_factor_level<double, SEL_QR>, smem);
+  else smem_limit_once(k_factor_level<double, SEL_QRP>, smem);
+  // tensor-core LU kernel for n = 8, 16; register-resident LU kernel when the
+  // pair fits one warp's registers; shared-memory kernel otherwise
+  void (*tc_kernel)(FactorArgs<double>) = nullptr;
+  size_t tc_smem = 0;
+  if (s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 && (n == 16 || n == 8) && s.use_tc) {
+    tc_smem = tc_smem_per_warp(n) * 4;
+    if (n == 16) { tc_kernel = k_factor_lu_tc<16>; smem_limit_once(k_factor_lu_tc<16>, tc_smem); }
+    else { tc_kernel = k_factor_lu_tc<8>; smem_limit_once(k_factor_lu_tc<8>, tc_smem); }
+  }
+  void (*rows_kernel)(FactorArgs<double>) = nullptr;
+  if (!tc_kernel && s.sel == SEL_LU && d.nr <= 4 && d.nx <= 4) {
+    if (n <= 4) rows_kernel = k_factor_lu_rows<4, 4, 4>;
+    else if (n <= 8) rows_kernel = k_factor_lu_rows<8, 4, 4>;
+    else if (n <= 16) rows_kernel = k_factor_lu_rows<16, 4, 4>;
   }
   for (int k = 1; k < nb; k *= 2) {
     a.k = k;
     a.first = (k == 1);
     const long np = pairs_at_level(nb, k);
     const int grid = grid_for(np, wpb, 148 * 16);
-    if (s.sel == SEL_LU) k_factor_level<double, SEL_LU><<<grid, wpb * 32, smem, st>>>(a);
+    if (tc_kernel) tc_kernel<<<grid_for(np, 4, 148 * 16), 128, tc_smem, st>>>(a);
+    else if (rows_kernel) rows_kernel<<<grid_for(np, 4, 148 * 16), 128, 0, st>>>(a);
+    else if (s.sel == SEL_LU) k_factor_level<double, SEL_LU><<<grid, wpb * 32, smem, st>>>(a);
     else if (s.sel == SEL_QR) k_factor_level<double, SEL_QR><<<grid, wpb * 32, smem, st>>>(a);
     else k_factor_level<double, SEL_QRP><<<grid, wpb * 32, smem, st>>>(a);
     check_launch("k_factor_level");
@@ -795,13 +1448,21 @@ static void solve_chunk(DevState& s, double* x, int ldx, int nrhs, cudaStream_t 
   a.x = x; a.ldx = ldx; a.nrhs = nrhs; a.XB = s.XB; a.sel = s.sel;
   a.ldw = odd_ld(2 * n);
   const size_t smem_f = (size_t)a.ldw * nrhs * 8 * WARPS_PANEL;
-  if (smem_f > 48 * 1024)
-    cudaFuncSetAttribute(k_forward_level<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  smem_limit_once(k_forward_level<double>, smem_f);
+  // register-resident sweeps for n <= 16
+  void (*fwd_rows)(SweepArgs<double>) = nullptr;
+  void (*bwd_rows)(SweepArgs<double>) = nullptr;
+  if (d.nr <= 8 && d.nx <= 8) {
+    if (n <= 4) { fwd_rows = k_forward_rows<4, 8>; bwd_rows = k_backward_rows<4, 8>; }
+    else if (n <= 8) { fwd_rows = k_forward_rows<8, 8>; bwd_rows = k_backward_rows<8, 8>; }
+    else if (n <= 16) { fwd_rows = k_forward_rows<16, 8>; bwd_rows = k_backward_rows<16, 8>; }
+  }
   int K = 1;
   for (; K < nb; K *= 2) {
     a.k = K;
     const long np = pairs_at_level(nb, K);
-    k_forward_level<double><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_f, st>>>(a);
+    if (fwd_rows) fwd_rows<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a);
+    else k_forward_level<double><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_f, st>>>(a);
     check_launch("k_forward_level");
   }
   if (d.nr > 0) {
@@ -816,7 +1477,8 @@ static void solve_chunk(DevState& s, double* x, int ldx, int nrhs, cudaStream_t 
   for (int k = K; (k /= 2) > 0;) {
     a.k = k;
     const long np = pairs_at_level(nb, k);
-    k_backward_level<double><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_b, st>>>(a);
+    if (bwd_rows) bwd_rows<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a);
+    else k_backward_level<double><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_b, st>>>(a);
     check_launch("k_backward_level");
   }
 }

@@ -64,6 +64,17 @@ class BABD:
         return dataclasses.replace(
             self, **{k: getattr(self, k).copy() for k in ("D", "E", "B", "C", "Cq", "F", "H")})
 
+    def norm_inf(self) -> float:
+        """||A||_inf (largest absolute row sum) from the blocks."""
+        rows = np.abs(self.D).sum(axis=1) + np.abs(self.E).sum(axis=1) + np.abs(self.B).sum(axis=1)
+        m = float(rows.max()) if rows.size else 0.0
+        if self.H.size:
+            m = max(m, float(np.abs(self.H).sum(axis=0).max()))
+        if self.nr:
+            c = np.abs(self.C).sum(axis=(0, 1)) + np.abs(self.Cq).sum(axis=0) + np.abs(self.F).sum(axis=0)
+            m = max(m, float(c.max()))
+        return m
+
     def to_dense(self) -> np.ndarray:
         """Dense matrix (row-major numpy) for small cross-checks."""
         nb, n, qr, qx, nr, nx = self.dims()

@@ -144,10 +144,29 @@ int bcr_sparse_load(bcr_handle h, const double *V, const int *I, int r_offs,
 int bcr_set_stream(bcr_handle h, void *stream);
 int bcr_upload(bcr_handle h);          /* host copy of the matrix -> device */
 int bcr_factorize_device(bcr_handle h);/* factorize the device-resident matrix */
+/* enqueue the factorization on the handle's stream and return at once (no
+ * host synchronisation, so it can be captured in a CUDA graph); the outcome is
+ * read by bcr_factorize_status(), which synchronises the stream */
+int bcr_factorize_async(bcr_handle h);
+int bcr_factorize_status(bcr_handle h);
 /* d_x: device pointer, ld x nrhs column-major; stream-ordered, asynchronous */
 int bcr_solve_device(bcr_handle h, int nrhs, double *d_x, int ld);
 int bcr_mv_device(bcr_handle h, double alpha, const double *d_x, double beta, double *d_res);
 int bcr_synchronize(bcr_handle h);
+/* the cudaStream_t the handle enqueues on (its own non-blocking stream unless
+ * bcr_set_stream chose another); NULL without a device */
+void *bcr_get_stream(bcr_handle h);
+
+/* CUDA graphs of the device-resident path: capture once, replay many times.
+ * what = BCR_GRAPH_FACTORIZE, BCR_GRAPH_SOLVE or BCR_GRAPH_STEP (both).  The
+ * solve part works in place on d_x (ld x nrhs); when d_rhs is not NULL it
+ * first copies d_rhs into d_x.  The factorization status of a replay is read
+ * with bcr_factorize_status(). */
+#define BCR_GRAPH_FACTORIZE 1
+#define BCR_GRAPH_SOLVE 2
+#define BCR_GRAPH_STEP 3
+int bcr_graph_capture(bcr_handle h, int what, int nrhs, double *d_x, int ld, const double *d_rhs);
+int bcr_graph_launch(bcr_handle h, int what);
 
 #ifdef __cplusplus
 }

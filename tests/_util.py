@@ -30,14 +30,7 @@ def dense_norm_inf(s):
 
 def block_norm_inf(s):
     """||A||_inf from the block arrays (no dense matrix)."""
-    rows = np.abs(s.D).sum(axis=1) + np.abs(s.E).sum(axis=1) + np.abs(s.B).sum(axis=1)
-    m = rows.max() if rows.size else 0.0
-    Hm = np.abs(s.H).sum(axis=0)
-    m = max(m, Hm.max() if Hm.size else 0.0)
-    if s.nr:
-        c = np.abs(s.C).sum(axis=(0, 1)) + np.abs(s.Cq).sum(axis=0) + np.abs(s.F).sum(axis=0)
-        m = max(m, c.max())
-    return m
+    return s.norm_inf()
 
 
 def fwd_err(x, xref):
