@@ -95,6 +95,9 @@ _SIGS = [
     ("bcr_get_stream", [_H], ct.c_void_p),
     ("bcr_graph_capture", [_H, ct.c_int, ct.c_int, ct.c_void_p, ct.c_int, ct.c_void_p], ct.c_int),
     ("bcr_graph_launch", [_H, ct.c_int], ct.c_int),
+    ("bcr_mv_noalloc", [ct.c_int] * 6 + [ct.c_void_p] * 7 + [ct.c_double, ct.c_void_p, ct.c_double,
+                                                               ct.c_void_p, ct.c_void_p, ct.c_char_p,
+                                                               ct.c_int], ct.c_int),
 ]
 
 GRAPH_FACTORIZE, GRAPH_SOLVE, GRAPH_STEP = 1, 2, 3
@@ -115,6 +118,17 @@ def lib():
             f.restype = res
         _lib = L
     return _lib
+
+
+def mv_noalloc(dims, D, E, B, C, Cq, F, H, alpha, x, beta, res, stream=0):
+    """Allocation-free res = alpha*A*x + beta*res on caller-owned device memory
+    (every array argument is a device pointer, as an int).  Returns
+    (status, message)."""
+    buf = ct.create_string_buffer(256)
+    rc = lib().bcr_mv_noalloc(*dims, D or None, E or None, B or None, C or None, Cq or None,
+                              F or None, H or None, alpha, x or None, beta, res or None,
+                              stream or None, buf, 256)
+    return rc, buf.value.decode()
 
 
 def exported_symbols():
