@@ -76,6 +76,8 @@ _SIGS = [
     ("bcr_factorize", [_H], ct.c_int),
     ("bcr_solve", [_H, _dp], ct.c_int),
     ("bcr_solve_n", [_H, ct.c_int, _dp, ct.c_int], ct.c_int),
+    ("bcr_factorize_solve", [_H, ct.c_int, _dp, ct.c_int], ct.c_int),
+    ("bcr_factorize_solve_device", [_H, ct.c_int, ct.c_void_p, ct.c_int], ct.c_int),
     ("bcr_t_solve", [_H, _dp], ct.c_int),
     ("bcr_t_solve_n", [_H, ct.c_int, _dp, ct.c_int], ct.c_int),
     ("bcr_mv", [_H, _dp, _dp], ct.c_int),
@@ -324,6 +326,14 @@ class BorderedCR:
         """In place on a float64 buffer holding nrhs columns of stride ld."""
         assert X.dtype == np.float64 and X.flags.c_contiguous and X.size >= nrhs * ld
         return self._check(self.L.bcr_solve_n(self.h, nrhs, _p(X), ld), numerical_ok=True)
+
+    def factorize_solve(self, nrhs: int, X: np.ndarray, ld: int) -> bool:
+        """factorize() then solve_n(nrhs, X, ld) in one pass (in place on X)."""
+        assert X.dtype == np.float64 and X.flags.c_contiguous and X.size >= nrhs * ld
+        return self._check(self.L.bcr_factorize_solve(self.h, nrhs, _p(X), ld), numerical_ok=True)
+
+    def factorize_solve_device(self, nrhs: int, d_x_ptr: int, ld: int):
+        self._check(self.L.bcr_factorize_solve_device(self.h, nrhs, d_x_ptr, ld))
 
     def t_solve(self, x):
         return self._check(self.L.bcr_t_solve(self.h, _p(np.asarray(x, dtype=np.float64))))

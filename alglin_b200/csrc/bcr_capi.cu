@@ -231,6 +231,25 @@ struct bcr_handle_s {
     return BCR_OK;
   }
 
+  int factorize_solve_launch(int nrhs, double* dx, int ld) {
+    factorized = false;
+    if (sel_last != bcr::LAST_LU && sel_last != bcr::LAST_QR)
+      return fail(BCR_NUMERICAL,
+                  fmt("BorderedCR<t_Value>::load_and_factorize_last failed\n"
+                      "(last block solver '%s' is not available on the device)\n", kLastName[sel_last]));
+    if (nrhs < 0 || ld < L()) return fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::solve: bad ldRhs = %d\n", ld));
+    s.sel = sel;
+    s.sel_last = sel_last;
+    s.use_tc = use_tc;
+    if (nrhs == 0) bcr::launch_factorize(s, stream);
+    else bcr::launch_factorize_solve(s, dx, ld, nrhs, stream);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "factorize_solve launch");
+    pending_status = true;
+    factorized = true;
+    return BCR_OK;
+  }
+
   int factorize_status() {
     if (!pending_status) return factorized ? BCR_OK : fail(BCR_NUMERICAL, err);
     pending_status = false;
@@ -930,6 +949,34 @@ int bcr_factorize_status(bcr_handle h) {
   return h->factorize_status();
 }
 
+int bcr_factorize_solve(bcr_handle h, int nrhs, double* rhs, int ldRhs) {
+  H_ALLOC(h);
+  if (h->debug) {
+    int rc = h->check_matrix();
+    if (rc) return rc;
+  }
+  int rc = h->upload();
+  if (rc) return rc;
+  if (nrhs < 0 || ldRhs < h->L()) return h->fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::solve: bad ldRhs = %d\n", ldRhs));
+  const size_t Lx = (size_t)h->L();
+  if (nrhs > 0) {
+    if ((rc = h->ensure_buffer(h->dX, h->dX_cap, Lx * nrhs))) return rc;
+    cudaMemcpy2DAsync(h->dX, Lx * 8, rhs, (size_t)ldRhs * 8, Lx * 8, nrhs, cudaMemcpyHostToDevice, h->stream);
+  }
+  if ((rc = h->factorize_solve_launch(nrhs, h->dX, (int)Lx))) return rc;
+  if (nrhs > 0)
+    cudaMemcpy2DAsync(rhs, (size_t)ldRhs * 8, h->dX, Lx * 8, Lx * 8, nrhs, cudaMemcpyDeviceToHost, h->stream);
+  return h->factorize_status();
+}
+
+int bcr_factorize_solve_device(bcr_handle h, int nrhs, double* d_x, int ld) {
+  H_ALLOC(h);
+  int rc = h->ensure_device();
+  if (rc) return rc;
+  if (h->dirty && (rc = h->upload())) return rc;
+  return h->factorize_solve_launch(nrhs, d_x, ld);
+}
+
 int bcr_solve_device(bcr_handle h, int nrhs, double* d_x, int ld) {
   H_ALLOC(h);
   return h->solve_device(nrhs, d_x, ld);
@@ -975,11 +1022,13 @@ int bcr_graph_capture(bcr_handle h, int what, int nrhs, double* d_x, int ld, con
   if (h->graphs[what]) { cudaGraphExecDestroy(h->graphs[what]); h->graphs[what] = nullptr; }
   e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed);
   if (e != cudaSuccess) return h->cuda_fail(e, "cudaStreamBeginCapture");
-  if (what & BCR_GRAPH_FACTORIZE) {
-    h->s.sel = h->sel; h->s.sel_last = h->sel_last; h->s.use_tc = h->use_tc;
+  h->s.sel = h->sel; h->s.sel_last = h->sel_last; h->s.use_tc = h->use_tc;
+  if (what == BCR_GRAPH_STEP) {
+    if (d_rhs) cudaMemcpyAsync(d_x, d_rhs, (size_t)ld * nrhs * 8, cudaMemcpyDeviceToDevice, h->stream);
+    bcr::launch_factorize_solve(h->s, d_x, ld, nrhs, h->stream);
+  } else if (what == BCR_GRAPH_FACTORIZE) {
     bcr::launch_factorize(h->s, h->stream);
-  }
-  if (what & BCR_GRAPH_SOLVE) {
+  } else {
     if (d_rhs) cudaMemcpyAsync(d_x, d_rhs, (size_t)ld * nrhs * 8, cudaMemcpyDeviceToDevice, h->stream);
     bcr::launch_solve(h->s, d_x, ld, nrhs, h->stream);
   }

@@ -35,6 +35,11 @@ struct DevState {
 void launch_factorize(DevState& s, cudaStream_t st);
 // x: device, column-major (ldx x nrhs); in place, reference semantics
 void launch_solve(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st);
+// factorize, then solve x in place (ldx x nrhs); the forward elimination of
+// the right-hand sides is fused into the factorization when the pair kernel
+// can carry them
+void launch_factorize_solve(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st);
+bool factorize_solve_fuses(const DevState& s, int nrhs);
 // res = alpha * A * x + beta * res with the loaded (unfactored) matrix
 void launch_mv(DevState& s, double alpha, const double* x, double beta, double* res,
                cudaStream_t st);

@@ -40,6 +40,11 @@ struct FactorArgs {
   T *Rbuf, *Fbuf;
   StatusWords* st;
   int k, first, ldw;
+  // right-hand sides eliminated together with the factorization (forward
+  // sweep fused into the pair kernel); nrf == 0 when not fused
+  T* x;
+  int ldx, nrf;
+  T* XB;
 };
 
 __host__ __device__ inline int odd_ld(int r) { return r | 1; }
@@ -477,13 +482,13 @@ struct TcShape {
   static constexpr int MT = 2 * N + 8;             // GEMM rows: U-row, reduced row, border (padded)
   static constexpr int NTILES = (2 * N + 8 + 7) / 8;  // trailing columns 2N + nx, nx <= 8
   static constexpr int NTP = NTILES * 8;
-  static constexpr int LDW = NTP + 1;               // work / output rows (odd: conflict-light)
+  static constexpr int LDW = NTP + 1;               // trailing rows (odd: conflict-light)
   static constexpr int LDG = N + 4;                 // operator rows (16B aligned, conflict-free A loads)
   static constexpr int KSTEPS = N / 4;
   static constexpr int MTILES = MT / 8;
-  static constexpr int WS = MT * LDW;               // doubles
+  static constexpr int WS = 2 * N * LDW;            // doubles: the 2N panel rows' trailing part
   static constexpr int GS = MT * LDG;
-  static constexpr size_t BYTES = (size_t)(WS + GS + N) * 8 + 2 * N * sizeof(int);
+  static constexpr size_t BYTES = (size_t)(WS + GS + N + 2) * 8 + 2 * N * sizeof(int);
 };
 
 size_t tc_smem_per_warp(int n) {
@@ -498,14 +503,15 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   double* Wt = reinterpret_cast<double*>(smem_raw + (size_t)warp * S::BYTES);
   double* Gs = Wt + S::WS;
-  double* bc = Gs + S::GS;
-  int* rowof = reinterpret_cast<int*>(bc + N);
+  double* bc = Gs + S::GS;                        // pivot row + its reciprocal
+  int* rowof = reinterpret_cast<int*>(bc + N + 2);
   const Dims d = a.d;
   const int nr = d.nr, nx = d.nx, nb = d.nblock;
   constexpr int n = N, n2 = 2 * N;
   constexpr size_t nn = (size_t)N * N;
   const size_t nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
-  const int NT = n2 + nx;  // live trailing columns
+  const int nrf = a.nrf;             // fused right-hand sides
+  const int NT = n2 + nx + nrf;      // live trailing columns
   const int k = a.k;
   const long np = pairs_at_level(nb, k);
   const bool first = a.first != 0;
@@ -557,6 +563,12 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a) {
           Wt[(n + r) * S::LDW + n2 + c] = Bj[idx];
         }
       }
+      // fused right-hand sides: TOP rows hold x_jp, BOTTOM rows x_j
+      for (int idx = lane; idx < n2 * nrf; idx += 32) {
+        const int r = idx % n2, c = idx / n2;
+        const double* xc = a.x + (size_t)c * a.ldx;
+        Wt[r * S::LDW + n2 + nx + c] = r < n ? xc[(size_t)jp * n + r] : xc[(size_t)j * n + r - n];
+      }
       // zero the padding columns of the live rows (they feed padding outputs only,
       // but keep them finite)
       for (int idx = lane; idx < n2 * (S::NTP - NT); idx += 32) {
@@ -569,6 +581,9 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a) {
     bool done = !act;
 #pragma unroll
     for (int i = 0; i < N; ++i) {
+      // every lane forms the reciprocal of its own candidate while the pivot is
+      // searched; the pivot lane publishes its value with the pivot row
+      const double rc = __drcp_rn(rowA[i]);
       // pivot: max |a| over rows not yet used, ties to the smaller position
       const double av = fabs(rowA[i]);
       const unsigned long long bits = (unsigned long long)__double_as_longlong(av);
@@ -576,11 +591,17 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a) {
       if (done) hi = 0u;
       else if (av != av) hi = 1u;  // NaN loses against every number
       const unsigned hmax = __reduce_max_sync(FULL, hi);
-      const unsigned lo = (hi == hmax) ? (unsigned)bits : 0u;
-      const unsigned lmax = __reduce_max_sync(FULL, lo);
-      const bool cand = (hi == hmax) && (lo == lmax) && !done;
-      const unsigned pmin = __reduce_min_sync(FULL, cand ? (unsigned)mypos : 0xffffffffu);
-      const unsigned m = __ballot_sync(FULL, cand && (unsigned)mypos == pmin);
+      unsigned m = __ballot_sync(FULL, hi == hmax && !done);
+      unsigned pmin;
+      if (__popc(m) == 1) {  // unique maximum in the upper word: the usual case
+        pmin = (unsigned)__shfl_sync(FULL, mypos, __ffs(m) - 1);
+      } else {               // exact tie handling: lower word, then smallest position
+        const unsigned lo = (hi == hmax) ? (unsigned)bits : 0u;
+        const unsigned lmax = __reduce_max_sync(FULL, lo);
+        const bool cand = (hi == hmax) && (lo == lmax) && !done;
+        pmin = __reduce_min_sync(FULL, cand ? (unsigned)mypos : 0xffffffffu);
+        m = __ballot_sync(FULL, cand && (unsigned)mypos == pmin);
+      }
       const int p = __ffs(m) - 1;
       if (lane == i) mykey = (int)pmin;
       if (!done && mypos == i && lane != p) mypos = (int)pmin;
@@ -589,22 +610,30 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a) {
 #pragma unroll
         for (int c = (i & ~1); c < N; c += 2)
           *reinterpret_cast<double2*>(&bc[c]) = make_double2(rowA[c], rowA[c + 1]);
+        bc[N] = rc;
       }
       __syncwarp();
       const double piv = bc[i];
       if (piv == 0.0 && info == 0) info = i + 1;
-      const double rinv = piv != 0.0 ? 1.0 / piv : 0.0;
+      const double rinv = piv != 0.0 ? bc[N] : 0.0;
+      double u[N];
+#pragma unroll
+      for (int c = (i + 1) & ~1; c < N; c += 2) {
+        const double2 v2 = *reinterpret_cast<const double2*>(&bc[c]);
+        u[c] = v2.x;
+        u[c + 1] = v2.y;
+      }
       if (!done && lane != p) {
         const double l = rowA[i] * rinv;
         rowA[i] = l;
 #pragma unroll
-        for (int c = i + 1; c < N; ++c) rowA[c] = fma(-l, bc[c], rowA[c]);
+        for (int c = i + 1; c < N; ++c) rowA[c] = fma(-l, u[c], rowA[c]);
       }
       if (lane < nr) {
         const double l = rowC[i] * rinv;
         rowC[i] = l;
 #pragma unroll
-        for (int c = i + 1; c < N; ++c) rowC[c] = fma(-l, bc[c], rowC[c]);
+        for (int c = i + 1; c < N; ++c) rowC[c] = fma(-l, u[c], rowC[c]);
       }
       if (lane == p) done = true;
       __syncwarp();
@@ -627,10 +656,11 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a) {
 #pragma unroll
         for (int c = 0; c < N; ++c) Cj[(size_t)c * nr] = rowC[c];
       }
-      // L^T rows (column c of L, contiguous in m) for the triangular solve
+      // rows of L (row m contiguous) for the triangular solve
       if (act && mypos < n) {
 #pragma unroll
-        for (int c = 0; c < N; ++c) Gs[c * S::LDG + mypos] = rowA[c];
+        for (int c = 0; c < N; c += 2)
+          *reinterpret_cast<double2*>(&Gs[mypos * S::LDG + c]) = make_double2(rowA[c], rowA[c + 1]);
       }
     }
     __syncwarp();
@@ -642,17 +672,22 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a) {
       for (int c = 0; c < N; ++c) x[c] = (mypos < n) ? (c == mypos ? 1.0 : 0.0) : -rowA[c];
 #pragma unroll
       for (int c = 0; c < N; ++c) rowC[c] = -rowC[c];
+      // right-looking: once x[mm] is final, update every x[c], c < mm (the
+      // updates of one step are independent, so the dependent chain is N long)
 #pragma unroll
-      for (int c = N - 1; c >= 0; --c) {
-        double s = x[c], sc = rowC[c];
+      for (int mm = N - 1; mm > 0; --mm) {
+        const double xm = x[mm], cm = rowC[mm];
+        const double* Lrow = Gs + mm * S::LDG;  // L(mm, 0..mm-1)
 #pragma unroll
-        for (int mm = c + 1; mm < N; ++mm) {
-          const double l = Gs[c * S::LDG + mm];  // L(mm, c)
-          s = fma(-x[mm], l, s);
-          sc = fma(-rowC[mm], l, sc);
+        for (int c = 0; c < mm; c += 2) {
+          const double2 l2 = *reinterpret_cast<const double2*>(&Lrow[c]);
+          x[c] = fma(-xm, l2.x, x[c]);
+          rowC[c] = fma(-cm, l2.x, rowC[c]);
+          if (c + 1 < mm) {
+            x[c + 1] = fma(-xm, l2.y, x[c + 1]);
+            rowC[c + 1] = fma(-cm, l2.y, rowC[c + 1]);
+          }
         }
-        x[c] = s;
-        rowC[c] = sc;
       }
       __syncwarp();
       if (act) {
@@ -699,45 +734,44 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a) {
         for (int nt = 0; nt < S::NTILES; ++nt) dmma_8x8x4(acc[mt][nt][0], acc[mt][nt][1], afr, bfr[nt]);
       }
     }
-    __syncwarp();
-#pragma unroll
-    for (int mt = 0; mt < S::MTILES; ++mt)
-#pragma unroll
-      for (int nt = 0; nt < S::NTILES; ++nt) {
-        double* o = Wt + (mt * 8 + g) * S::LDW + nt * 8 + 2 * t;
-        o[0] = acc[mt][nt][0];
-        o[1] = acc[mt][nt][1];
-      }
-    __syncwarp();
     // ------------------------------------------------------------ store
+    // accumulator element (row 8mt+g, column 8nt+2t+h) straight to its block:
+    // rows [0,N) U-row, [N,2N) reduced row, [2N, 2N+nr) border updates;
+    // columns [0,N) x_jp, [N,2N) x_jpp, [2N, 2N+nx) xb
     {
-      double* Dj = a.D + (size_t)j * nn;
-      double* Ejo = a.E + (size_t)j * nn;
-      double* Djp = a.D + (size_t)jp * nn;
-      double* Ejp = a.E + (size_t)jp * nn;
-      for (int idx = lane; idx < (int)nn; idx += 32) {
-        const int r = idx % n, c = idx / n;
-        Dj[idx] = Wt[r * S::LDW + c];
-        Ejo[idx] = Wt[r * S::LDW + n + c];
-        Djp[idx] = Wt[(n + r) * S::LDW + c];
-        Ejp[idx] = Wt[(n + r) * S::LDW + n + c];
-      }
-      double* Bj = a.B + (size_t)j * nnx;
-      double* Bjp = a.B + (size_t)jp * nnx;
-      for (int idx = lane; idx < (int)nnx; idx += 32) {
-        const int r = idx % n, c = idx / n;
-        Bj[idx] = Wt[r * S::LDW + n2 + c];
-        Bjp[idx] = Wt[(n + r) * S::LDW + n2 + c];
-      }
-      for (int idx = lane; idx < (int)nrn; idx += 32) {
-        const int r = idx % nr, c = idx / nr;
-        const size_t o = (size_t)jp * nrn + idx;
-        a.C[o] = srcC[o] + Wt[(n2 + r) * S::LDW + c];
-        a.Rbuf[(size_t)j * nrn + idx] = Wt[(n2 + r) * S::LDW + n + c];
-      }
-      for (int idx = lane; idx < (int)nrnx; idx += 32) {
-        const int r = idx % nr, c = idx / nr;
-        a.Fbuf[(size_t)j * nrnx + idx] = Wt[(n2 + r) * S::LDW + n2 + c];
+#pragma unroll
+      for (int mt = 0; mt < S::MTILES; ++mt) {
+        const int row = mt * 8 + g;
+#pragma unroll
+        for (int nt = 0; nt < S::NTILES; ++nt)
+#pragma unroll
+          for (int hh = 0; hh < 2; ++hh) {
+            const int col = nt * 8 + 2 * t + hh;
+            const double v = acc[mt][nt][hh];
+            if (mt * 8 < n2) {  // panel rows (compile-time per mt)
+              const bool ur = row < n;
+              const int rr = ur ? row : row - n;
+              const size_t blk = ur ? (size_t)j : (size_t)jp;
+              if (col < n) a.D[blk * nn + (size_t)col * n + rr] = v;
+              else if (col < n2) a.E[blk * nn + (size_t)(col - n) * n + rr] = v;
+              else if (col < n2 + nx) a.B[blk * nnx + (size_t)(col - n2) * n + rr] = v;
+              else if (col < NT) a.x[(size_t)(col - n2 - nx) * a.ldx + blk * n + rr] = v;
+            } else {
+              const int rr = row - n2;
+              if (rr < nr) {
+                if (col < n) {
+                  const size_t o = (size_t)jp * nrn + (size_t)col * nr + rr;
+                  a.C[o] = srcC[o] + v;
+                } else if (col < n2) {
+                  a.Rbuf[(size_t)j * nrn + (size_t)(col - n) * nr + rr] = v;
+                } else if (col < n2 + nx) {
+                  a.Fbuf[(size_t)j * nrnx + (size_t)(col - n2) * nr + rr] = v;
+                } else if (col < NT) {
+                  a.XB[(size_t)j * nr * nrf + (size_t)(col - n2 - nx) * nr + rr] = v;
+                }
+              }
+            }
+          }
       }
     }
     __syncwarp();
@@ -930,14 +964,14 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_backward_level(SweepArgs<T
 //   xb term added and U solved by n broadcast steps (QRP: column-map scatter).
 // All loads of a pair are issued before the first use.
 // ---------------------------------------------------------------------------
-template <int N, int NRM>
-__global__ void __launch_bounds__(256) k_forward_rows(SweepArgs<double> a) {
+template <int N, int NRM, bool LU>
+__global__ void __launch_bounds__(256, 2) k_forward_rows(SweepArgs<double> a) {
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   const Dims d = a.d;
   const int n = d.n, nr = d.nr, nb = d.nblock, n2 = 2 * n, nrhs = a.nrhs, k = a.k;
   const bool act = lane < n2;
-  const bool lu = a.sel == SEL_LU;
+  constexpr bool lu = LU;
   const long np = pairs_at_level(nb, k);
   for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
     const int j = k + (int)(2L * k * q), jp = j - k;
@@ -945,9 +979,9 @@ __global__ void __launch_bounds__(256) k_forward_rows(SweepArgs<double> a) {
     double t[N];
 #pragma unroll
     for (int c = 0; c < N; ++c) t[c] = (act && c < n) ? Tj[(size_t)c * n2 + lane] : 0.0;
-    double tau[N];
+    double tau[LU ? 1 : N];
 #pragma unroll
-    for (int c = 0; c < N; ++c) tau[c] = (!lu && c < n) ? Tj[2 * (size_t)n * n + c] : 0.0;
+    for (int c = 0; c < (LU ? 1 : N); ++c) tau[c] = (!lu && c < n) ? Tj[2 * (size_t)n * n + c] : 0.0;
     const int src = (act && lu) ? (int)a.P[(size_t)j * szP(d) + lane] : lane;
     double cp[NRM];
     const double* Cj = a.C + (size_t)j * nr * n;
@@ -971,7 +1005,7 @@ __global__ void __launch_bounds__(256) k_forward_rows(SweepArgs<double> a) {
           if (i < n) {
             const double v = (lane > i && act) ? t[i] : (lane == i ? 1.0 : 0.0);
             double sdot = warp_sum(v * w);
-            w = fma(-tau[i] * sdot, v, w);
+            w = fma(-tau[LU ? 0 : i] * sdot, v, w);
           }
         }
       }
@@ -992,7 +1026,7 @@ __global__ void __launch_bounds__(256) k_forward_rows(SweepArgs<double> a) {
 }
 
 template <int N, int NXM>
-__global__ void __launch_bounds__(256) k_backward_rows(SweepArgs<double> a) {
+__global__ void __launch_bounds__(256, 2) k_backward_rows(SweepArgs<double> a) {
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   const Dims d = a.d;
@@ -1359,7 +1393,51 @@ static void reduce_blocks(DevState& s, const double* buf, long first, long count
   }
 }
 
-void launch_factorize(DevState& s, cudaStream_t st) {
+// ---------------------------------------------------------------------------
+// pair-kernel choice for the factorization
+// ---------------------------------------------------------------------------
+struct FactorPlan {
+  void (*tc)(FactorArgs<double>) = nullptr;    // tensor-core LU (n = 8, 16)
+  size_t tc_smem = 0;
+  void (*rows)(FactorArgs<double>) = nullptr;  // register LU (n <= 16)
+  size_t smem = 0;                             // shared-memory kernel
+  int wpb = 1;
+  int tc_cols = 0;                             // trailing-column capacity of tc
+};
+
+static FactorPlan plan_factor(const DevState& s) {
+  const Dims d = s.d;
+  const int n = d.n;
+  FactorPlan p;
+  const size_t per_warp = panel_smem_per_warp(d, 8);
+  p.wpb = (int)(SMEM_MAX / per_warp);
+  if (p.wpb > WARPS_PANEL) p.wpb = WARPS_PANEL;
+  if (p.wpb < 1) p.wpb = 1;
+  p.smem = per_warp * p.wpb;
+  if (s.sel == SEL_LU) smem_limit_once(k_factor_level<double, SEL_LU>, p.smem);
+  else if (s.sel == SEL_QR) smem_limit_once(k_factor_level<double, SEL_QR>, p.smem);
+  else smem_limit_once(k_factor_level<double, SEL_QRP>, p.smem);
+  if (s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 && (n == 16 || n == 8) && s.use_tc) {
+    p.tc_smem = tc_smem_per_warp(n) * 4;
+    if (n == 16) { p.tc = k_factor_lu_tc<16>; smem_limit_once(k_factor_lu_tc<16>, p.tc_smem); p.tc_cols = TcShape<16>::NTP; }
+    else { p.tc = k_factor_lu_tc<8>; smem_limit_once(k_factor_lu_tc<8>, p.tc_smem); p.tc_cols = TcShape<8>::NTP; }
+  }
+  if (!p.tc && s.sel == SEL_LU && d.nr <= 4 && d.nx <= 4) {
+    if (n <= 4) p.rows = k_factor_lu_rows<4, 4, 4>;
+    else if (n <= 8) p.rows = k_factor_lu_rows<8, 4, 4>;
+    else if (n <= 16) p.rows = k_factor_lu_rows<16, 4, 4>;
+  }
+  return p;
+}
+
+// number of right-hand sides the factorization can carry (0: none)
+static int fusable_rhs(const DevState& s, const FactorPlan& p, int nrhs) {
+  if (!p.tc || nrhs < 1 || nrhs > 16) return 0;
+  return 2 * s.d.n + s.d.nx + nrhs <= p.tc_cols ? nrhs : 0;
+}
+
+// every CR level: pair eliminations and the C_jpp border fix-up
+static void factor_levels(DevState& s, const FactorPlan& p, double* x, int ldx, int nrf, cudaStream_t st) {
   const Dims d = s.d;
   const int n = d.n, nb = d.nblock;
   const size_t nn = (size_t)n * n, nnx = (size_t)n * d.nx, nrn = (size_t)d.nr * n;
@@ -1381,39 +1459,17 @@ void launch_factorize(DevState& s, cudaStream_t st) {
   a.D = s.D; a.E = s.E; a.B = s.B; a.C = s.C;
   a.Tm = s.T; a.P = s.P; a.Rbuf = s.Rbuf; a.Fbuf = s.Fbuf; a.st = s.st;
   a.ldw = odd_ld(2 * n + d.nr);
-  const size_t per_warp = panel_smem_per_warp(d, 8);
-  int wpb = (int)(SMEM_MAX / per_warp);
-  if (wpb > WARPS_PANEL) wpb = WARPS_PANEL;
-  if (wpb < 1) wpb = 1;  // callers reject sizes whose single warp does not fit
-  const size_t smem = per_warp * wpb;
-  if (s.sel == SEL_LU) smem_limit_once(k_factor_level<double, SEL_LU>, smem);
-  else if (s.sel == SEL_QR) smem_limit_once(k_factor_level<double, SEL_QR>, smem);
-  else smem_limit_once(k_factor_level<double, SEL_QRP>, smem);
-  // tensor-core LU kernel for n = 8, 16; register-resident LU kernel when the
-  // pair fits one warp's registers; shared-memory kernel otherwise
-  void (*tc_kernel)(FactorArgs<double>) = nullptr;
-  size_t tc_smem = 0;
-  if (s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 && (n == 16 || n == 8) && s.use_tc) {
-    tc_smem = tc_smem_per_warp(n) * 4;
-    if (n == 16) { tc_kernel = k_factor_lu_tc<16>; smem_limit_once(k_factor_lu_tc<16>, tc_smem); }
-    else { tc_kernel = k_factor_lu_tc<8>; smem_limit_once(k_factor_lu_tc<8>, tc_smem); }
-  }
-  void (*rows_kernel)(FactorArgs<double>) = nullptr;
-  if (!tc_kernel && s.sel == SEL_LU && d.nr <= 4 && d.nx <= 4) {
-    if (n <= 4) rows_kernel = k_factor_lu_rows<4, 4, 4>;
-    else if (n <= 8) rows_kernel = k_factor_lu_rows<8, 4, 4>;
-    else if (n <= 16) rows_kernel = k_factor_lu_rows<16, 4, 4>;
-  }
+  a.x = x; a.ldx = ldx; a.nrf = nrf; a.XB = s.XB;
   for (int k = 1; k < nb; k *= 2) {
     a.k = k;
     a.first = (k == 1);
     const long np = pairs_at_level(nb, k);
-    const int grid = grid_for(np, wpb, 148 * 16);
-    if (tc_kernel) tc_kernel<<<grid_for(np, 4, 148 * 16), 128, tc_smem, st>>>(a);
-    else if (rows_kernel) rows_kernel<<<grid_for(np, 4, 148 * 16), 128, 0, st>>>(a);
-    else if (s.sel == SEL_LU) k_factor_level<double, SEL_LU><<<grid, wpb * 32, smem, st>>>(a);
-    else if (s.sel == SEL_QR) k_factor_level<double, SEL_QR><<<grid, wpb * 32, smem, st>>>(a);
-    else k_factor_level<double, SEL_QRP><<<grid, wpb * 32, smem, st>>>(a);
+    const int grid = grid_for(np, p.wpb, 148 * 16);
+    if (p.tc) p.tc<<<grid_for(np, 4, 148 * 16), 128, p.tc_smem, st>>>(a);
+    else if (p.rows) p.rows<<<grid_for(np, 4, 148 * 16), 128, 0, st>>>(a);
+    else if (s.sel == SEL_LU) k_factor_level<double, SEL_LU><<<grid, p.wpb * 32, p.smem, st>>>(a);
+    else if (s.sel == SEL_QR) k_factor_level<double, SEL_QR><<<grid, p.wpb * 32, p.smem, st>>>(a);
+    else k_factor_level<double, SEL_QRP><<<grid, p.wpb * 32, p.smem, st>>>(a);
     check_launch("k_factor_level");
     if (nrn) {
       const long tot = np * (long)nrn;
@@ -1421,9 +1477,14 @@ void launch_factorize(DevState& s, cudaStream_t st) {
       check_launch("k_border_fix");
     }
   }
+}
+
+// F = F0 + sum of the Schur updates; assemble and factor the last block
+static void factor_last(DevState& s, cudaStream_t st) {
+  const Dims d = s.d;
   const int nrnx = d.nr * d.nx;
   if (nrnx > 0)
-    reduce_blocks(s, s.Fbuf, 1, nb - 1, nrnx, d.nr, s.F0, d.nr, s.Ffin, d.nr, st);
+    reduce_blocks(s, s.Fbuf, 1, d.nblock - 1, nrnx, d.nr, s.F0, d.nr, s.Ffin, d.nr, st);
   k_last_assemble<double><<<grid_for((long)d.Nr * d.Nc, 256, 64), 256, 0, st>>>(
       d, s.D, s.E, s.B, s.C, s.H, s.Cq, s.Ffin, s.Hl);
   check_launch("k_last_assemble");
@@ -1431,56 +1492,122 @@ void launch_factorize(DevState& s, cudaStream_t st) {
   check_launch("k_last_factor");
 }
 
-static void solve_chunk(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st);
-
-// right-hand sides are independent: sweep them in chunks of at most 16 columns
-void launch_solve(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st) {
-  for (int c0 = 0; c0 < nrhs; c0 += 16)
-    solve_chunk(s, x + (size_t)c0 * ldx, ldx, nrhs - c0 < 16 ? nrhs - c0 : 16, st);
+void launch_factorize(DevState& s, cudaStream_t st) {
+  const FactorPlan p = plan_factor(s);
+  factor_levels(s, p, nullptr, 0, 0, st);
+  factor_last(s, st);
 }
 
-static void solve_chunk(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st) {
+// sweep kernels for one chunk of right-hand sides
+struct SweepPlan {
+  void (*fwd)(SweepArgs<double>) = nullptr;
+  void (*bwd)(SweepArgs<double>) = nullptr;
+};
+
+static SweepPlan plan_sweeps(const DevState& s) {
   const Dims d = s.d;
-  const int n = d.n, nb = d.nblock;
+  const int n = d.n;
+  SweepPlan p;
+  if (d.nr <= 8 && d.nx <= 8 && n <= 16) {
+    const bool lu = s.sel == SEL_LU, r4 = d.nr <= 4, x4 = d.nx <= 4;
+#define BCR_FWD(NN) (r4 ? (lu ? k_forward_rows<NN, 4, true> : k_forward_rows<NN, 4, false>) \
+                        : (lu ? k_forward_rows<NN, 8, true> : k_forward_rows<NN, 8, false>))
+#define BCR_BWD(NN) (x4 ? k_backward_rows<NN, 4> : k_backward_rows<NN, 8>)
+    if (n <= 4) { p.fwd = BCR_FWD(4); p.bwd = BCR_BWD(4); }
+    else if (n <= 8) { p.fwd = BCR_FWD(8); p.bwd = BCR_BWD(8); }
+    else { p.fwd = BCR_FWD(16); p.bwd = BCR_BWD(16); }
+#undef BCR_FWD
+#undef BCR_BWD
+  }
+  return p;
+}
+
+static SweepArgs<double> sweep_args(DevState& s, double* x, int ldx, int nrhs) {
   SweepArgs<double> a;
-  a.d = d;
+  a.d = s.d;
   a.D = s.D; a.E = s.E; a.B = s.B; a.C = s.C; a.Tm = s.T; a.P = s.P;
   a.x = x; a.ldx = ldx; a.nrhs = nrhs; a.XB = s.XB; a.sel = s.sel;
-  a.ldw = odd_ld(2 * n);
+  return a;
+}
+
+static int top_level(int nb) {
+  int K = 1;
+  while (K < nb) K *= 2;
+  return K;
+}
+
+// xb += sum of the per-block -C'_j x_j contributions
+static void reduce_xb(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st) {
+  const Dims d = s.d;
+  if (d.nr > 0) {
+    double* xb = x + (size_t)(d.nblock + 1) * d.n + d.qr;
+    reduce_blocks(s, s.XB, 1, d.nblock - 1, d.nr * nrhs, d.nr, xb, ldx, xb, ldx, st);
+  }
+}
+
+static void forward_levels(DevState& s, const SweepPlan& p, double* x, int ldx, int nrhs, cudaStream_t st) {
+  const Dims d = s.d;
+  SweepArgs<double> a = sweep_args(s, x, ldx, nrhs);
+  a.ldw = odd_ld(2 * d.n);
   const size_t smem_f = (size_t)a.ldw * nrhs * 8 * WARPS_PANEL;
   smem_limit_once(k_forward_level<double>, smem_f);
-  // register-resident sweeps for n <= 16
-  void (*fwd_rows)(SweepArgs<double>) = nullptr;
-  void (*bwd_rows)(SweepArgs<double>) = nullptr;
-  if (d.nr <= 8 && d.nx <= 8) {
-    if (n <= 4) { fwd_rows = k_forward_rows<4, 8>; bwd_rows = k_backward_rows<4, 8>; }
-    else if (n <= 8) { fwd_rows = k_forward_rows<8, 8>; bwd_rows = k_backward_rows<8, 8>; }
-    else if (n <= 16) { fwd_rows = k_forward_rows<16, 8>; bwd_rows = k_backward_rows<16, 8>; }
-  }
-  int K = 1;
-  for (; K < nb; K *= 2) {
+  for (int K = 1; K < d.nblock; K *= 2) {
     a.k = K;
-    const long np = pairs_at_level(nb, K);
-    if (fwd_rows) fwd_rows<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a);
+    const long np = pairs_at_level(d.nblock, K);
+    if (p.fwd) p.fwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a);
     else k_forward_level<double><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_f, st>>>(a);
     check_launch("k_forward_level");
   }
-  if (d.nr > 0) {
-    double* xb = x + (size_t)(nb + 1) * n + d.qr;
-    reduce_blocks(s, s.XB, 1, nb - 1, d.nr * nrhs, d.nr, xb, ldx, xb, ldx, st);
-  }
+  reduce_xb(s, x, ldx, nrhs, st);
+}
+
+static void last_and_backward(DevState& s, const SweepPlan& p, double* x, int ldx, int nrhs, cudaStream_t st) {
+  const Dims d = s.d;
   const size_t smem_l = (size_t)(d.Nr > d.Nc ? d.Nr : d.Nc) * 8;
   k_last_solve<double><<<1, 256, smem_l, st>>>(d, s.Hl, s.piv_l, s.tau_l, s.sel_last, x, ldx, nrhs);
   check_launch("k_last_solve");
-  a.ldw = n;
-  const size_t smem_b = (size_t)n * 8 * WARPS_PANEL;
-  for (int k = K; (k /= 2) > 0;) {
+  SweepArgs<double> a = sweep_args(s, x, ldx, nrhs);
+  a.ldw = d.n;
+  const size_t smem_b = (size_t)d.n * 8 * WARPS_PANEL;
+  for (int k = top_level(d.nblock); (k /= 2) > 0;) {
     a.k = k;
-    const long np = pairs_at_level(nb, k);
-    if (bwd_rows) bwd_rows<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a);
+    const long np = pairs_at_level(d.nblock, k);
+    if (p.bwd) p.bwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a);
     else k_backward_level<double><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_b, st>>>(a);
     check_launch("k_backward_level");
   }
+}
+
+// right-hand sides are independent: sweep them in chunks of at most 16 columns
+void launch_solve(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st) {
+  const SweepPlan p = plan_sweeps(s);
+  for (int c0 = 0; c0 < nrhs; c0 += 16) {
+    const int nc = nrhs - c0 < 16 ? nrhs - c0 : 16;
+    double* xc = x + (size_t)c0 * ldx;
+    forward_levels(s, p, xc, ldx, nc, st);
+    last_and_backward(s, p, xc, ldx, nc, st);
+  }
+}
+
+// factorize and solve in one pass: when the pair kernel can carry the right-
+// hand sides, their forward elimination rides in the factorization's GEMM and
+// the separate forward sweep disappears
+void launch_factorize_solve(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st) {
+  const FactorPlan fp = plan_factor(s);
+  const int nrf = fusable_rhs(s, fp, nrhs);
+  if (nrf == 0) {
+    launch_factorize(s, st);
+    launch_solve(s, x, ldx, nrhs, st);
+    return;
+  }
+  factor_levels(s, fp, x, ldx, nrf, st);
+  reduce_xb(s, x, ldx, nrf, st);
+  factor_last(s, st);
+  last_and_backward(s, plan_sweeps(s), x, ldx, nrf, st);
+}
+
+bool factorize_solve_fuses(const DevState& s, int nrhs) {
+  return fusable_rhs(s, plan_factor(s), nrhs) == nrhs;
 }
 
 void launch_mv(DevState& s, double alpha, const double* x, double beta, double* res,

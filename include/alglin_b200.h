@@ -125,6 +125,11 @@ int bcr_factorize(bcr_handle h);                         /* factorize cc:803-839
 int bcr_solve(bcr_handle h, double *x);
 /* rhs: ldRhs x nrhs, ldRhs >= max(nrows, ncols)  (cc:1546-1605) */
 int bcr_solve_n(bcr_handle h, int nrhs, double *rhs, int ldRhs);
+/* factorize() followed by solve(nrhs, rhs, ldRhs) in one pass (the Newton-step
+ * use of factorize + solve, BABD.hxx:271-313): the forward elimination of the
+ * right-hand sides rides in the factorization kernels where they fit; the
+ * factors are kept for later solve() calls */
+int bcr_factorize_solve(bcr_handle h, int nrhs, double *rhs, int ldRhs);
 int bcr_t_solve(bcr_handle h, double *x);                /* cc:2089: not defined */
 int bcr_t_solve_n(bcr_handle h, int nrhs, double *rhs, int ldRhs); /* cc:2096 */
 
@@ -151,6 +156,8 @@ int bcr_factorize_async(bcr_handle h);
 int bcr_factorize_status(bcr_handle h);
 /* d_x: device pointer, ld x nrhs column-major; stream-ordered, asynchronous */
 int bcr_solve_device(bcr_handle h, int nrhs, double *d_x, int ld);
+/* bcr_factorize_solve on device memory, asynchronous like bcr_factorize_async */
+int bcr_factorize_solve_device(bcr_handle h, int nrhs, double *d_x, int ld);
 int bcr_mv_device(bcr_handle h, double alpha, const double *d_x, double beta, double *d_res);
 int bcr_synchronize(bcr_handle h);
 /* the cudaStream_t the handle enqueues on (its own non-blocking stream unless

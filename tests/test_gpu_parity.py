@@ -167,3 +167,25 @@ def test_gpu_full_size_config_B_residual(internal):
     r = h.mv(x[:s.ncols]) - b[:s.nrows]
     rel = np.abs(r).max() / (block_norm_inf(s) * np.abs(x[:s.ncols]).max() + np.abs(b[:s.nrows]).max())
     assert rel < 1e-13, rel
+
+
+@pytest.mark.parametrize("dims,internal,nrhs", [
+    ((1000, 16, 2, 2, 4, 4), "LU", 1), ((1000, 16, 2, 2, 4, 4), "LU", 4),
+    ((777, 8, 0, 0, 2, 2), "LU", 3), ((300, 16, 2, 2, 4, 4), "LU", 6),
+    ((129, 16, 1, 1, 3, 2), "QR", 2), ((65, 5, 1, 1, 2, 2), "LU", 2)])
+def test_gpu_factorize_solve_fused(dims, internal, nrhs):
+    """factorize+solve in one pass (forward elimination fused into the pair
+    kernel where it fits) gives the oracle's answer, and the stored factors
+    still serve a later plain solve."""
+    s = synth.collocation(*dims, seed=21)
+    b = synth.rhs(s, nrhs=nrhs, seed=5)
+    last = "LU" if s.Nr == s.Nc else "QR"
+    o = po.Oracle(s, internal, last)
+    assert o.factorize(), o.last_error()
+    xo = o.solve(b)
+    h = gpu_solver(s, internal, last)
+    X = b.copy()
+    assert h.factorize_solve(nrhs, X, X.shape[1]), h.last_error()
+    assert fwd_err(X[:, :s.ncols], xo[:, :s.ncols]) < 1e-10
+    x2 = gpu_solve(h, b)
+    assert fwd_err(x2[:, :s.ncols], xo[:, :s.ncols]) < 1e-10
