@@ -118,7 +118,7 @@ struct bcr_handle_s {
     dfree(z.D0); dfree(z.E0); dfree(z.B0); dfree(z.C0); dfree(z.Cq); dfree(z.F0); dfree(z.H);
     dfree(z.D); dfree(z.E); dfree(z.B); dfree(z.C); dfree(z.T); dfree(z.P);
     dfree(z.Rbuf); dfree(z.Fbuf); dfree(z.XB); dfree(z.part); dfree(z.Ffin); dfree(z.Hl);
-    dfree(z.tau_l); dfree(z.piv_l); dfree(z.st); dfree(z.mv_part);
+    dfree(z.tau_l); dfree(z.piv_l); dfree(z.st); dfree(z.mv_part); dfree(z.slab);
     dfree(dX); dfree(dY);
     dX_cap = dY_cap = 0;
     if (own_stream && stream) cudaStreamDestroy(stream);
@@ -140,10 +140,9 @@ struct bcr_handle_s {
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev == 0)
       return fail(BCR_CUDA_ERROR, "alglin_b200: no CUDA device is available (the solver has no CPU path)\n");
-    if (bcr::panel_smem_per_warp(d, 8) > 227 * 1024)
+    if (d.n > 128)
       return fail(BCR_BAD_ARGUMENT,
-                  fmt("alglin_b200: block size n=%d with nr=%d, nx=%d exceeds the shared-memory panel "
-                      "of the FP64 device path\n", d.n, d.nr, d.nx));
+                  fmt("alglin_b200: block size n=%d exceeds the supported maximum of 128\n", d.n));
     if (!stream) {
       e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
       if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
@@ -169,6 +168,9 @@ struct bcr_handle_s {
     A(dalloc(z.Ffin, std::max<size_t>(nr * nx, 1)));
     A(dalloc(z.Hl, (size_t)d.Nr * d.Nc)); A(dalloc(z.tau_l, Lmax)); A(dalloc(z.piv_l, Lmax));
     A(dalloc(z.st, 1)); A(dalloc(z.mv_part, (nb + 2) * nr));
+    z.slab_elems = bcr::cta_slab_elems(d);
+    z.slab_ctas = bcr::use_cta_kernel(d) ? 148 * 2 : 0;
+    if (z.slab_ctas) A(dalloc(z.slab, z.slab_elems * z.slab_ctas));
     if (r != cudaSuccess) {
       dev_ready = true;
       release_device();

@@ -29,7 +29,14 @@ struct DevState {
   int* piv_l;           // last block pivots
   StatusWords* st;      // device status
   double* mv_part;      // Mv border partials ((nblock+1) x nr)
+  double* slab;         // CTA-per-pair work matrices (large n)
+  size_t slab_elems;    // doubles per CTA
+  int slab_ctas;        // CTAs that own a slab
 };
+
+// large blocks: one CTA per pair with the work matrix in a global slab
+bool use_cta_kernel(const Dims& d);
+size_t cta_slab_elems(const Dims& d);
 
 // factorization of every cyclic-reduction level plus the last block
 void launch_factorize(DevState& s, cudaStream_t st);

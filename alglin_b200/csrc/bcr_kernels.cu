@@ -29,6 +29,7 @@ namespace bcr {
 
 static constexpr int WARPS_PANEL = 4;
 static constexpr size_t SMEM_MAX = 227 * 1024;
+static constexpr int CTA_KERNEL_MIN_N = 24;  // n above this: one CTA per pair
 
 template <typename T>
 struct FactorArgs {
@@ -49,11 +50,21 @@ struct FactorArgs {
 
 __host__ __device__ inline int odd_ld(int r) { return r | 1; }
 
+// pairs of large blocks go to one CTA each (work matrix in a global slab)
+bool use_cta_kernel(const Dims& d) {
+  return d.n > CTA_KERNEL_MIN_N || panel_smem_per_warp(d, 8) > SMEM_MAX;
+}
+
+size_t cta_slab_elems(const Dims& d) { return (size_t)(2 * d.n + d.nr) * (3 * d.n + d.nx); }
+
 size_t panel_smem_per_warp(const Dims& d, int elem_bytes) {
   const int R = 2 * d.n + d.nr, NC = 3 * d.n + d.nx;
   size_t b = (size_t)odd_ld(R) * NC * elem_bytes + (size_t)d.n * (elem_bytes + sizeof(int));
   return b;
 }
+
+template <typename T> __device__ void block_argmax(T& v, int& idx, T* sv, int* si);
+template <typename T> __device__ T block_sum(T v, T* sv);
 
 // ---------------------------------------------------------------------------
 // warp-level elimination of x_j from the staged work matrix
@@ -778,6 +789,206 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Large blocks: one CTA eliminates one pair; the (2n+nr) x (3n+nx) work
+// matrix lives in a global scratch slab of the CTA (column-major, ld = R),
+// which stays in L2 while the CTA works on it.  Same elimination as the warp
+// kernels (getrf pivot rule, dlarfg reflectors, border rows eliminated by the
+// U rows), parallelised over the CTA's threads with block barriers.
+// ---------------------------------------------------------------------------
+template <typename T, int SEL>
+__global__ void __launch_bounds__(256) k_factor_cta(FactorArgs<T> a, T* slab, size_t slab_elems) {
+  __shared__ T sv[32];
+  __shared__ int si[32];
+  __shared__ T s_tau[256];
+  __shared__ int s_piv[256];
+  const int tid = threadIdx.x, bs = blockDim.x;
+  const Dims d = a.d;
+  const int n = d.n, nr = d.nr, nx = d.nx, nb = d.nblock;
+  const int n2 = 2 * n, R = n2 + nr, NC = 3 * n + nx;
+  const size_t nn = (size_t)n * n, nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
+  T* W = slab + (size_t)blockIdx.x * slab_elems;
+  const int k = a.k;
+  const long np = pairs_at_level(nb, k);
+  const bool first = a.first != 0;
+  for (long q = blockIdx.x; q < np; q += gridDim.x) {
+    const int j = k + (int)(2L * k * q), jp = j - k;
+    const size_t oj = (size_t)j * nn, ojp = (size_t)jp * nn;
+    // ------------------------------------------------------------ load
+    for (int idx = tid; idx < (int)nn; idx += bs) {
+      const int i = idx % n, c = idx / n;
+      T ejp, djp, dj, ej;
+      if (first) {
+        ejp = T(a.E0[ojp + idx]); djp = T(a.D0[ojp + idx]); dj = T(a.D0[oj + idx]); ej = T(a.E0[oj + idx]);
+      } else {
+        ejp = a.E[ojp + idx]; djp = a.D[ojp + idx]; dj = a.D[oj + idx]; ej = a.E[oj + idx];
+      }
+      W[(size_t)c * R + i] = ejp;
+      W[(size_t)(n + c) * R + i] = djp;
+      W[(size_t)(n2 + c) * R + i] = T(0);
+      W[(size_t)c * R + n + i] = dj;
+      W[(size_t)(n + c) * R + n + i] = T(0);
+      W[(size_t)(n2 + c) * R + n + i] = ej;
+    }
+    for (int idx = tid; idx < (int)nnx; idx += bs) {
+      const int i = idx % n, c = idx / n;
+      const size_t o1 = (size_t)jp * nnx + idx, o2 = (size_t)j * nnx + idx;
+      W[(size_t)(3 * n + c) * R + i] = first ? T(a.B0[o1]) : a.B[o1];
+      W[(size_t)(3 * n + c) * R + n + i] = first ? T(a.B0[o2]) : a.B[o2];
+    }
+    for (int idx = tid; idx < (int)nrn; idx += bs) {
+      const int r = idx % nr, c = idx / nr;
+      const size_t o = (size_t)j * nrn + idx;
+      W[(size_t)c * R + n2 + r] = first ? T(a.C0[o]) : a.C[o];
+      W[(size_t)(n + c) * R + n2 + r] = T(0);
+      W[(size_t)(n2 + c) * R + n2 + r] = T(0);
+    }
+    for (int idx = tid; idx < (int)nrnx; idx += bs) {
+      const int r = idx % nr, c = idx / nr;
+      W[(size_t)(3 * n + c) * R + n2 + r] = T(0);
+    }
+    __syncthreads();
+    // ----------------------------------------------------------- eliminate
+    int info = 0;
+    for (int i = 0; i < n && info == 0; ++i) {
+      T* ci = W + (size_t)i * R;
+      if (SEL == SEL_QRP) {
+        // column with the largest remaining 2-norm over the panel rows
+        T best = T(-1);
+        int bc = i;
+        for (int c = i + tid; c < n; c += bs) {
+          const T* col = W + (size_t)c * R;
+          T s2 = T(0);
+          for (int r = i; r < n2; ++r) s2 += col[r] * col[r];
+          if (s2 > best) { best = s2; bc = c; }
+        }
+        block_argmax(best, bc, sv, si);
+        if (tid == 0) s_piv[i] = bc;
+        if (bc != i)
+          for (int r = tid; r < R; r += bs) {
+            T t = ci[r]; ci[r] = W[(size_t)bc * R + r]; W[(size_t)bc * R + r] = t;
+          }
+        __syncthreads();
+      }
+      if (SEL == SEL_LU) {
+        T best = T(-1);
+        int bi = i;
+        for (int r = i + tid; r < n2; r += bs) {
+          T v = dev_abs(ci[r]);
+          if (v > best) { best = v; bi = r; }
+        }
+        block_argmax(best, bi, sv, si);
+        if (tid == 0) s_piv[i] = bi;
+        const T pv = ci[bi];
+        if (pv == T(0)) { info = i + 1; break; }
+        if (bi != i)
+          for (int c = tid; c < NC; c += bs) {
+            T* col = W + (size_t)c * R;
+            T t = col[i]; col[i] = col[bi]; col[bi] = t;
+          }
+        __syncthreads();
+        const T rinv = T(1) / pv;
+        for (int r = i + 1 + tid; r < R; r += bs) ci[r] *= rinv;
+        __syncthreads();
+      } else {
+        const T alpha = ci[i];
+        T s2 = T(0);
+        for (int r = i + 1 + tid; r < n2; r += bs) s2 += ci[r] * ci[r];
+        s2 = block_sum(s2, sv);
+        T tt = T(0), beta = alpha;
+        if (s2 != T(0)) {
+          const T nrm = sqrt(alpha * alpha + s2);
+          beta = alpha >= T(0) ? -nrm : nrm;
+          tt = (beta - alpha) / beta;
+          const T sc = T(1) / (alpha - beta);
+          for (int r = i + 1 + tid; r < n2; r += bs) ci[r] *= sc;
+        }
+        __syncthreads();
+        if (tid == 0) { ci[i] = beta; s_tau[i] = tt; if (SEL == SEL_QR) s_piv[i] = i; }
+        __syncthreads();
+        if (beta == T(0)) { info = i + 1; break; }
+        if (tt != T(0))
+          for (int c = i + 1 + tid; c < NC; c += bs) {
+            T* col = W + (size_t)c * R;
+            T w = col[i];
+            for (int r = i + 1; r < n2; ++r) w += ci[r] * col[r];
+            w *= tt;
+            col[i] -= w;
+            for (int r = i + 1; r < n2; ++r) col[r] -= w * ci[r];
+          }
+        __syncthreads();
+        if (R > n2) {
+          const T rb = T(1) / beta;
+          for (int r = n2 + tid; r < R; r += bs) ci[r] *= rb;
+          __syncthreads();
+        }
+      }
+      // rank-1 update of the rows below i (LU) or of the border rows (QR/QRP)
+      const int r0 = SEL == SEL_LU ? i + 1 : n2;
+      const int rows = R - r0, cols = NC - i - 1;
+      if (rows > 0 && cols > 0) {
+        const long tot = (long)rows * cols;
+        for (long e = tid; e < tot; e += bs) {
+          const int r = r0 + (int)(e % rows), c = i + 1 + (int)(e / rows);
+          T* col = W + (size_t)c * R;
+          col[r] -= ci[r] * col[i];
+        }
+      }
+      __syncthreads();
+    }
+    if (info != 0) {
+      if (tid == 0) report(a.st, DEV_ZERO_PIVOT, j, info, k);
+      __syncthreads();
+      continue;
+    }
+    // ---------------------------------------------------------------- store
+    T* Tj = a.Tm + (size_t)j * szT(d);
+    for (int idx = tid; idx < (int)(2 * nn); idx += bs) {
+      const int r = idx % n2, c = idx / n2;
+      Tj[idx] = W[(size_t)c * R + r];
+    }
+    if (SEL != SEL_LU)
+      for (int i = tid; i < n; i += bs) Tj[2 * nn + i] = s_tau[i];
+    unsigned char* Pj = a.P + (size_t)j * szP(d);
+    if (tid == 0) {
+      // row map (getrf order) or QRP column map from the swap sequence
+      unsigned char mp[768];
+      for (int r = 0; r < n2; ++r) mp[r] = (unsigned char)r;
+      for (int i = 0; i < n; ++i) mp[n2 + i] = (unsigned char)i;
+      if (SEL == SEL_LU)
+        for (int i = 0; i < n; ++i) { unsigned char t = mp[i]; mp[i] = mp[s_piv[i]]; mp[s_piv[i]] = t; }
+      if (SEL == SEL_QRP)
+        for (int i = 0; i < n; ++i) { unsigned char t = mp[n2 + i]; mp[n2 + i] = mp[n2 + s_piv[i]]; mp[n2 + s_piv[i]] = t; }
+      for (int r = 0; r < 3 * n; ++r) Pj[r] = mp[r];
+    }
+    for (int idx = tid; idx < (int)nn; idx += bs) {
+      const int i = idx % n, c = idx / n;
+      a.D[oj + idx] = W[(size_t)(n + c) * R + i];
+      a.E[oj + idx] = W[(size_t)(n2 + c) * R + i];
+      a.D[ojp + idx] = W[(size_t)(n + c) * R + n + i];
+      a.E[ojp + idx] = W[(size_t)(n2 + c) * R + n + i];
+    }
+    for (int idx = tid; idx < (int)nnx; idx += bs) {
+      const int i = idx % n, c = idx / n;
+      a.B[(size_t)j * nnx + idx] = W[(size_t)(3 * n + c) * R + i];
+      a.B[(size_t)jp * nnx + idx] = W[(size_t)(3 * n + c) * R + n + i];
+    }
+    for (int idx = tid; idx < (int)nrn; idx += bs) {
+      const int r = idx % nr, c = idx / nr;
+      const size_t oc = (size_t)jp * nrn + idx;
+      a.C[(size_t)j * nrn + idx] = W[(size_t)c * R + n2 + r];
+      const T cjp = first ? T(a.C0[oc]) : a.C[oc];
+      a.C[oc] = cjp + W[(size_t)(n + c) * R + n2 + r];
+      a.Rbuf[(size_t)j * nrn + idx] = W[(size_t)(n2 + c) * R + n2 + r];
+    }
+    for (int idx = tid; idx < (int)nrnx; idx += bs) {
+      const int r = idx % nr, c = idx / nr;
+      a.Fbuf[(size_t)j * nrnx + idx] = W[(size_t)(3 * n + c) * R + n2 + r];
+    }
+    __syncthreads();
+  }
+}
+
 // C_jpp += dC_jpp for every pair of the level (one writer per target block)
 template <typename T>
 __global__ void k_border_fix(Dims d, T* C, const T* Rbuf, int k) {
@@ -1397,6 +1608,7 @@ static void reduce_blocks(DevState& s, const double* buf, long first, long count
 // pair-kernel choice for the factorization
 // ---------------------------------------------------------------------------
 struct FactorPlan {
+  void (*cta)(FactorArgs<double>, double*, size_t) = nullptr;  // CTA per pair (large n)
   void (*tc)(FactorArgs<double>) = nullptr;    // tensor-core LU (n = 8, 16)
   size_t tc_smem = 0;
   void (*rows)(FactorArgs<double>) = nullptr;  // register LU (n <= 16)
@@ -1426,6 +1638,10 @@ static FactorPlan plan_factor(const DevState& s) {
     if (n <= 4) p.rows = k_factor_lu_rows<4, 4, 4>;
     else if (n <= 8) p.rows = k_factor_lu_rows<8, 4, 4>;
     else if (n <= 16) p.rows = k_factor_lu_rows<16, 4, 4>;
+  }
+  if (!p.tc && !p.rows && use_cta_kernel(d)) {
+    p.cta = s.sel == SEL_LU ? k_factor_cta<double, SEL_LU>
+          : s.sel == SEL_QR ? k_factor_cta<double, SEL_QR> : k_factor_cta<double, SEL_QRP>;
   }
   return p;
 }
@@ -1465,7 +1681,8 @@ static void factor_levels(DevState& s, const FactorPlan& p, double* x, int ldx, 
     a.first = (k == 1);
     const long np = pairs_at_level(nb, k);
     const int grid = grid_for(np, p.wpb, 148 * 16);
-    if (p.tc) p.tc<<<grid_for(np, 4, 148 * 16), 128, p.tc_smem, st>>>(a);
+    if (p.cta) p.cta<<<grid_for(np, 1, s.slab_ctas), 256, 0, st>>>(a, s.slab, s.slab_elems);
+    else if (p.tc) p.tc<<<grid_for(np, 4, 148 * 16), 128, p.tc_smem, st>>>(a);
     else if (p.rows) p.rows<<<grid_for(np, 4, 148 * 16), 128, 0, st>>>(a);
     else if (s.sel == SEL_LU) k_factor_level<double, SEL_LU><<<grid, p.wpb * 32, p.smem, st>>>(a);
     else if (s.sel == SEL_QR) k_factor_level<double, SEL_QR><<<grid, p.wpb * 32, p.smem, st>>>(a);

@@ -189,3 +189,24 @@ def test_gpu_factorize_solve_fused(dims, internal, nrhs):
     assert fwd_err(X[:, :s.ncols], xo[:, :s.ncols]) < 1e-10
     x2 = gpu_solve(h, b)
     assert fwd_err(x2[:, :s.ncols], xo[:, :s.ncols]) < 1e-10
+
+
+@pytest.mark.parametrize("dims", [(65, 32, 0, 0, 8, 8), (17, 48, 2, 3, 4, 1), (9, 64, 1, 1, 2, 2),
+                                  (5, 128, 4, 4, 16, 16)])
+@pytest.mark.parametrize("internal", ["LU", "QR", "QRP"])
+def test_gpu_large_blocks(dims, internal):
+    """n > 24 runs one CTA per pair with the work matrix in a global slab
+    (config C has n=32, config E n=128)."""
+    s = synth.collocation(*dims, seed=sum(dims))
+    b = synth.rhs(s, nrhs=2, seed=3)
+    last = "LU" if s.Nr == s.Nc else "QR"
+    o = po.Oracle(s, internal, last)
+    assert o.factorize(), o.last_error()
+    xo = o.solve(b)
+    h = gpu_solver(s, internal, last)
+    assert h.factorize(), h.last_error()
+    xg = gpu_solve(h, b)
+    for c in range(2):
+        assert fwd_err(xg[c, :s.ncols], xo[c, :s.ncols]) < 1e-9, (dims, internal, c)
+        if s.nrows == s.ncols:  # rectangular last blocks are least-squares solves
+            assert relres(o, s, xg[c], b[c]) < 1e-13
