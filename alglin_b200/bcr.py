@@ -69,6 +69,8 @@ _SIGS = [
     ("bcr_solve_use_thread", [_H], ct.c_int),
     ("bcr_set_num_parallel_block", [_H, ct.c_int], ct.c_int),
     ("bcr_set_precision", [_H, ct.c_int], ct.c_int),
+    ("bcr_set_refinement", [_H, ct.c_double, ct.c_int], ct.c_int),
+    ("bcr_refinement_info", [_H, ct.POINTER(ct.c_int), _dp], ct.c_int),
     ("bcr_info", [_H, ct.c_char_p], ct.c_char_p),
     ("bcr_last_error", [_H], ct.c_char_p),
     ("bcr_set_debug", [_H, ct.c_int], ct.c_int),
@@ -292,6 +294,17 @@ class BorderedCR:
     def solve_use_thread(self): return bool(self.L.bcr_solve_use_thread(self.h))
     def set_num_parallel_block(self, npb): self._check(self.L.bcr_set_num_parallel_block(self.h, npb))
     def set_precision(self, p): self._check(self.L.bcr_set_precision(self.h, p))
+
+    def set_refinement(self, tol: float = 1e-12, max_iter: int = 10):
+        """Stopping rule of the mixed path's iterative refinement."""
+        self._check(self.L.bcr_set_refinement(self.h, float(tol), int(max_iter)))
+
+    def refinement_info(self) -> tuple[int, float]:
+        """(corrections applied, final |b-Ax|/(|A||x|+|b|)) of the last mixed solve."""
+        it = ct.c_int(0)
+        rr = ct.c_double(0.0)
+        self._check(self.L.bcr_refinement_info(self.h, ct.byref(it), ct.byref(rr)))
+        return it.value, rr.value
     def set_debug(self, yes): self._check(self.L.bcr_set_debug(self.h, int(yes)))
     def check_matrix(self): self._check(self.L.bcr_check_matrix(self.h))
 

@@ -70,6 +70,13 @@ struct bcr_handle_s {
   bool fthread = true, sthread = true, debug = false;
   int precision = BCR_PRECISION_FP64;
   int use_tc = 1;  // FP64 tensor-core pair kernel where it applies
+  // iterative refinement of the mixed path (FP32 factors, FP64 residuals)
+  double ir_tol = 1e-12;
+  int ir_max = 10;
+  int ir_iters = 0;          // corrections applied by the last solve
+  double ir_relres = 0.0;    // max over columns of |b-Ax|/(|A||x|+|b|) after it
+  int ir_nrhs = 0;
+  bool ir_pending = false;   // the norms of the last solve are still on the device
   std::string err = "no error";
   std::string info_buf;
   // host copy of the loaded matrix (reference layout)
@@ -83,6 +90,15 @@ struct bcr_handle_s {
   size_t dX_cap = 0;
   double* dY = nullptr;
   size_t dY_cap = 0;
+  double* dB = nullptr;      // copy of the right-hand sides (refinement)
+  size_t dB_cap = 0;
+  double* dR = nullptr;      // residuals / corrections (refinement)
+  size_t dR_cap = 0;
+  double* dNorm = nullptr;   // [0] |A|_inf, then |r|,|x|,|b| per column (as u64 bits)
+  size_t dNorm_cap = 0;
+  double* dRow = nullptr;    // row sums of |A|
+  size_t dRow_cap = 0;
+  bool mixed_ready = false;
   std::vector<void*> pinned;
   cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
 
@@ -119,8 +135,11 @@ struct bcr_handle_s {
     dfree(z.D); dfree(z.E); dfree(z.B); dfree(z.C); dfree(z.T); dfree(z.P);
     dfree(z.Rbuf); dfree(z.Fbuf); dfree(z.XB); dfree(z.part); dfree(z.Ffin); dfree(z.Hl);
     dfree(z.tau_l); dfree(z.piv_l); dfree(z.st); dfree(z.mv_part); dfree(z.slab);
-    dfree(dX); dfree(dY);
-    dX_cap = dY_cap = 0;
+    dfree(z.Df); dfree(z.Ef); dfree(z.Bf); dfree(z.Cf); dfree(z.Tf); dfree(z.Rbuff);
+    dfree(dX); dfree(dY); dfree(dB); dfree(dR); dfree(dNorm); dfree(dRow);
+    dX_cap = dY_cap = dB_cap = dR_cap = dNorm_cap = dRow_cap = 0;
+    mixed_ready = false;
+    ir_pending = false;
     if (own_stream && stream) cudaStreamDestroy(stream);
     if (own_stream) stream = nullptr;
     own_stream = false;
@@ -170,7 +189,11 @@ struct bcr_handle_s {
     A(dalloc(z.st, 1)); A(dalloc(z.mv_part, (nb + 2) * nr));
     z.slab_elems = bcr::cta_slab_elems(d);
     z.slab_ctas = bcr::use_cta_kernel(d) ? 148 * 2 : 0;
-    if (z.slab_ctas) A(dalloc(z.slab, z.slab_elems * z.slab_ctas));
+    if (z.slab_ctas) {
+      double* slab = nullptr;
+      A(dalloc(slab, z.slab_elems * z.slab_ctas));
+      z.slab = slab;
+    }
     if (r != cudaSuccess) {
       dev_ready = true;
       release_device();
@@ -216,8 +239,34 @@ struct bcr_handle_s {
     return BCR_OK;
   }
 
-  int factorize_launch() {
-    factorized = false;
+  // FP32 working arrays of the mixed path, allocated on first use
+  int ensure_mixed() {
+    if (mixed_ready) return BCR_OK;
+    if (nrows() != ncols())
+      return fail(BCR_BAD_ARGUMENT,
+                  fmt("alglin_b200: the mixed-precision path needs a square system (rows %d, cols %d)\n",
+                      nrows(), ncols()));
+    const size_t nb = d.nblock, n = d.n, nr = d.nr, nx = d.nx;
+    bcr::DevState& z = s;
+    cudaStreamSynchronize(stream);
+    cudaError_t r = cudaSuccess;
+    auto A = [&](cudaError_t x) { if (r == cudaSuccess) r = x; };
+    A(dalloc(z.Df, nb * n * n)); A(dalloc(z.Ef, nb * n * n)); A(dalloc(z.Bf, nb * n * nx));
+    A(dalloc(z.Cf, (nb + 1) * nr * n)); A(dalloc(z.Tf, nb * (2 * n * n + n)));
+    A(dalloc(z.Rbuff, nb * nr * n));
+    A(dalloc(dRow, (size_t)std::max(nrows(), 1)));
+    dRow_cap = (size_t)std::max(nrows(), 1);
+    if (r != cudaSuccess) {
+      dfree(z.Df); dfree(z.Ef); dfree(z.Bf); dfree(z.Cf); dfree(z.Tf); dfree(z.Rbuff); dfree(dRow);
+      dRow_cap = 0;
+      return cuda_fail(r, "mixed-precision allocation");
+    }
+    mixed_ready = true;
+    return BCR_OK;
+  }
+
+  // selection state copied into the device state before any launch
+  int prepare_launch() {
     if (sel_last != bcr::LAST_LU && sel_last != bcr::LAST_QR)
       return fail(BCR_NUMERICAL,
                   fmt("BorderedCR<t_Value>::load_and_factorize_last failed\n"
@@ -225,7 +274,30 @@ struct bcr_handle_s {
     s.sel = sel;
     s.sel_last = sel_last;
     s.use_tc = use_tc;
+    s.mixed = precision == BCR_PRECISION_MIXED ? 1 : 0;
+    if (s.mixed) {
+      int rc = ensure_mixed();
+      if (rc) return rc;
+      if (dNorm_cap < 4) {
+        rc = ensure_buffer(dNorm, dNorm_cap, 4);
+        if (rc) return rc;
+      }
+    }
+    return BCR_OK;
+  }
+
+  // the factorization kernels; the mixed path also measures |A|_inf (FP64)
+  void enqueue_factorize() {
+    if (s.mixed)
+      bcr::launch_norm_A(s, dRow, reinterpret_cast<unsigned long long*>(dNorm), stream);
     bcr::launch_factorize(s, stream);
+  }
+
+  int factorize_launch() {
+    factorized = false;
+    int rc = prepare_launch();
+    if (rc) return rc;
+    enqueue_factorize();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "factorize launch");
     pending_status = true;
@@ -235,14 +307,19 @@ struct bcr_handle_s {
 
   int factorize_solve_launch(int nrhs, double* dx, int ld) {
     factorized = false;
-    if (sel_last != bcr::LAST_LU && sel_last != bcr::LAST_QR)
-      return fail(BCR_NUMERICAL,
-                  fmt("BorderedCR<t_Value>::load_and_factorize_last failed\n"
-                      "(last block solver '%s' is not available on the device)\n", kLastName[sel_last]));
     if (nrhs < 0 || ld < L()) return fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::solve: bad ldRhs = %d\n", ld));
-    s.sel = sel;
-    s.sel_last = sel_last;
-    s.use_tc = use_tc;
+    int rc = prepare_launch();
+    if (rc) return rc;
+    if (s.mixed) {
+      // adaptive refinement needs the factorization's status first
+      enqueue_factorize();
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(e, "factorize launch");
+      pending_status = true;
+      factorized = true;
+      if ((rc = factorize_status())) return rc;
+      return nrhs > 0 ? solve_mixed(nrhs, dx, ld, -1) : BCR_OK;
+    }
     if (nrhs == 0) bcr::launch_factorize(s, stream);
     else bcr::launch_factorize_solve(s, dx, ld, nrhs, stream);
     cudaError_t e = cudaGetLastError();
@@ -284,10 +361,74 @@ struct bcr_handle_s {
     return factorize_status();
   }
 
-  int solve_device(int nrhs, double* dx, int ld) {
+  // |b-Ax|/(|A||x|+|b|), max over the columns of the last mixed solve
+  int read_refinement() {
+    if (!ir_pending) return BCR_OK;
+    ir_pending = false;
+    std::vector<unsigned long long> w(1 + 3 * (size_t)ir_nrhs);
+    cudaError_t e = cudaMemcpyAsync(w.data(), dNorm, w.size() * 8, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(e, "refinement norms");
+    auto as_d = [](unsigned long long u) { double v; std::memcpy(&v, &u, 8); return v; };
+    const double nA = as_d(w[0]);
+    double worst = 0.0;
+    for (int c = 0; c < ir_nrhs; ++c) {
+      const double nr_ = as_d(w[1 + 3 * c]), nx_ = as_d(w[2 + 3 * c]), nb_ = as_d(w[3 + 3 * c]);
+      const double den = nA * nx_ + nb_;
+      double rr = den > 0 ? nr_ / den : (nr_ > 0 ? INFINITY : 0.0);
+      if (!(rr <= worst)) worst = rr;  // NaN wins
+    }
+    ir_relres = worst;
+    return BCR_OK;
+  }
+
+  // mixed path: x = A^-1 b with FP32 factors, then corrections d = A^-1 r from
+  // FP64 residuals r = b - Ax until |r|/(|A||x|+|b|) <= ir_tol (adaptive: the
+  // host reads the norms after every residual) or for exactly `fixed` steps
+  // (graph capture: no host synchronisation)
+  int solve_mixed(int nrhs, double* dx, int ld, int fixed) {
+    const size_t Lx = (size_t)L(), nrw = (size_t)nrows(), ncl = (size_t)ncols();
+    int rc;
+    if ((rc = ensure_buffer(dB, dB_cap, Lx * nrhs))) return rc;
+    if ((rc = ensure_buffer(dR, dR_cap, Lx * nrhs))) return rc;
+    if ((rc = ensure_buffer(dNorm, dNorm_cap, 1 + 3 * (size_t)nrhs))) return rc;
+    auto* norms = reinterpret_cast<unsigned long long*>(dNorm);
+    cudaMemcpy2DAsync(dB, Lx * 8, dx, (size_t)ld * 8, nrw * 8, nrhs, cudaMemcpyDeviceToDevice, stream);
+    bcr::launch_solve(s, dx, ld, nrhs, stream);
+    ir_nrhs = nrhs;
+    int it = 0;
+    for (;;) {
+      for (int c = 0; c < nrhs; ++c)
+        bcr::launch_residual(s, dB + c * Lx, dx + (size_t)c * ld, dR + c * Lx, norms + 1 + 3 * c, stream);
+      if (fixed < 0) {
+        ir_pending = true;
+        if ((rc = read_refinement())) return rc;
+        if (ir_relres <= ir_tol || it >= ir_max) break;
+      } else if (it >= fixed) {
+        ir_pending = true;
+        break;
+      }
+      bcr::launch_solve(s, dR, (int)Lx, nrhs, stream);
+      for (int c = 0; c < nrhs; ++c) bcr::launch_axpy(dx + (size_t)c * ld, dR + c * Lx, (long)ncl, stream);
+      ++it;
+    }
+    ir_iters = it;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "refinement launch");
+    return BCR_OK;
+  }
+
+  int solve_device(int nrhs, double* dx, int ld, int fixed = -1) {
     if (!factorized) return fail(BCR_NUMERICAL, "BorderedCR::solve: the matrix is not factorized\n");
     if (nrhs < 0 || ld < L()) return fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::solve: bad ldRhs = %d\n", ld));
     if (nrhs == 0) return BCR_OK;
+    if (s.mixed) {
+      if (pending_status) {
+        int rc = factorize_status();
+        if (rc) return rc;
+      }
+      return solve_mixed(nrhs, dx, ld, fixed);
+    }
     bcr::launch_solve(s, dx, ld, nrhs, stream);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "solve launch");
@@ -1019,24 +1160,34 @@ int bcr_graph_capture(bcr_handle h, int what, int nrhs, double* d_x, int ld, con
     if (d_rhs) cudaMemcpyAsync(d_x, d_rhs, (size_t)ld * nrhs * 8, cudaMemcpyDeviceToDevice, h->stream);
     if ((rc = h->solve_device(nrhs, d_x, ld))) return rc;
   }
+  // the mixed path's graph replays the refinement steps the eager run needed
+  const int ir_steps = h->ir_iters;
   cudaError_t e = cudaStreamSynchronize(h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "graph warm-up");
   if (h->graphs[what]) { cudaGraphExecDestroy(h->graphs[what]); h->graphs[what] = nullptr; }
   e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed);
   if (e != cudaSuccess) return h->cuda_fail(e, "cudaStreamBeginCapture");
-  h->s.sel = h->sel; h->s.sel_last = h->sel_last; h->s.use_tc = h->use_tc;
+  const bool mixed = h->s.mixed != 0;
   if (what == BCR_GRAPH_STEP) {
     if (d_rhs) cudaMemcpyAsync(d_x, d_rhs, (size_t)ld * nrhs * 8, cudaMemcpyDeviceToDevice, h->stream);
-    bcr::launch_factorize_solve(h->s, d_x, ld, nrhs, h->stream);
+    if (mixed) {
+      h->enqueue_factorize();
+      rc = h->solve_mixed(nrhs, d_x, ld, ir_steps);
+    } else {
+      bcr::launch_factorize_solve(h->s, d_x, ld, nrhs, h->stream);
+    }
   } else if (what == BCR_GRAPH_FACTORIZE) {
-    bcr::launch_factorize(h->s, h->stream);
+    h->enqueue_factorize();
   } else {
     if (d_rhs) cudaMemcpyAsync(d_x, d_rhs, (size_t)ld * nrhs * 8, cudaMemcpyDeviceToDevice, h->stream);
-    bcr::launch_solve(h->s, d_x, ld, nrhs, h->stream);
+    if (mixed) rc = h->solve_mixed(nrhs, d_x, ld, ir_steps);
+    else bcr::launch_solve(h->s, d_x, ld, nrhs, h->stream);
   }
+  h->ir_pending = false;
   cudaGraph_t graph = nullptr;
   e = cudaStreamEndCapture(h->stream, &graph);
   if (e != cudaSuccess) { cudaGetLastError(); return h->cuda_fail(e, "cudaStreamEndCapture"); }
+  if (rc) { cudaGraphDestroy(graph); return rc; }
   e = cudaGraphInstantiate(&h->graphs[what], graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) { h->graphs[what] = nullptr; return h->cuda_fail(e, "cudaGraphInstantiate"); }
@@ -1050,6 +1201,25 @@ int bcr_graph_launch(bcr_handle h, int what) {
   cudaError_t e = cudaGraphLaunch(h->graphs[what], h->stream);
   if (e != cudaSuccess) return h->cuda_fail(e, "cudaGraphLaunch");
   if (what & BCR_GRAPH_FACTORIZE) { h->pending_status = true; h->factorized = true; }
+  if ((what & BCR_GRAPH_SOLVE) && h->s.mixed) h->ir_pending = true;
+  return BCR_OK;
+}
+
+int bcr_set_refinement(bcr_handle h, double tol, int max_iter) {
+  H_CHECK(h);
+  if (!(tol >= 0.0) || max_iter < 0)
+    return h->fail(BCR_BAD_ARGUMENT, fmt("bcr_set_refinement: bad tolerance %g or iteration limit %d\n", tol, max_iter));
+  h->ir_tol = tol;
+  h->ir_max = max_iter;
+  return BCR_OK;
+}
+
+int bcr_refinement_info(bcr_handle h, int* iters, double* relres) {
+  H_CHECK(h);
+  int rc = h->read_refinement();
+  if (rc) return rc;
+  if (iters) *iters = h->s.mixed ? h->ir_iters : 0;
+  if (relres) *relres = h->s.mixed ? h->ir_relres : 0.0;
   return BCR_OK;
 }
 

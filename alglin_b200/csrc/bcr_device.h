@@ -29,7 +29,11 @@ struct DevState {
   int* piv_l;           // last block pivots
   StatusWords* st;      // device status
   double* mv_part;      // Mv border partials ((nblock+1) x nr)
-  double* slab;         // CTA-per-pair work matrices (large n)
+  // mixed precision: FP32 working blocks and factors (the loaded matrix, F,
+  // the last block, the vectors and the residual stay FP64)
+  int mixed;
+  float *Df, *Ef, *Bf, *Cf, *Tf, *Rbuff;
+  void* slab;           // CTA-per-pair work matrices (large n)
   size_t slab_elems;    // doubles per CTA
   int slab_ctas;        // CTAs that own a slab
 };
@@ -50,6 +54,13 @@ bool factorize_solve_fuses(const DevState& s, int nrhs);
 // res = alpha * A * x + beta * res with the loaded (unfactored) matrix
 void launch_mv(DevState& s, double alpha, const double* x, double beta, double* res,
                cudaStream_t st);
+
+// iterative-refinement helpers (FP64): ||A||_inf, r = b - A x with the norms
+// |r|, |x|, |b| (as non-negative doubles stored in unsigned 64-bit words), y += x
+void launch_norm_A(DevState& s, double* rowsum, unsigned long long* out, cudaStream_t st);
+void launch_residual(DevState& s, const double* b, const double* x, double* r, unsigned long long* out,
+                     cudaStream_t st);
+void launch_axpy(double* y, const double* x, long len, cudaStream_t st);
 
 // smem bytes needed by one warp of the panel kernel; 0 if it does not fit
 size_t panel_smem_per_warp(const Dims& d, int elem_bytes);

@@ -38,15 +38,29 @@ struct FactorArgs {
   T *D, *E, *B, *C;                  // working blocks
   T* Tm;
   unsigned char* P;
-  T *Rbuf, *Fbuf;
+  T* Rbuf;
+  double* Fbuf;  // the F Schur updates are accumulated in FP64 in every precision
   StatusWords* st;
   int k, first, ldw;
   // right-hand sides eliminated together with the factorization (forward
   // sweep fused into the pair kernel); nrf == 0 when not fused
-  T* x;
+  double* x;
   int ldx, nrf;
-  T* XB;
+  double* XB;
 };
+
+// element of a block: the loaded FP64 matrix at the first level, the working
+// copy (type T) afterwards
+template <typename T>
+__device__ __forceinline__ T ldsrc(bool first, const double* orig, const T* work, size_t i) {
+  return first ? T(orig[i]) : work[i];
+}
+
+template <typename T>
+__device__ __forceinline__ void store2(T* p, T a, T b) {
+  if constexpr (sizeof(T) == 8) *reinterpret_cast<double2*>(p) = make_double2(a, b);
+  else *reinterpret_cast<float2*>(p) = make_float2(a, b);
+}
 
 __host__ __device__ inline int odd_ld(int r) { return r | 1; }
 
@@ -311,56 +325,57 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_factor_level(FactorArgs<T>
 // the lanes by column (lane c holds column c, and c+32) and are eliminated with
 // the same pivot rows, which yields C_j U^-1 and the C/F Schur updates.
 // ---------------------------------------------------------------------------
-template <int N, int NXM, int NRM>
-__global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<double> a) {
+template <typename T, int N, int NXM, int NRM>
+__global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<T> a) {
   constexpr int NC = 3 * N + NXM;
   constexpr int NCP = (NC + 1) & ~1;
   constexpr int SLOTS = (NC + 31) / 32;
   constexpr unsigned FULL = 0xffffffffu;
-  __shared__ __align__(16) double ubuf[4][NCP];
+  __shared__ __align__(16) T ubuf[4][NCP];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   const Dims d = a.d;
   const int n = d.n, nr = d.nr, nx = d.nx, nb = d.nblock, n2 = 2 * n;
   const size_t nn = (size_t)n * n, nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
-  double* ub = ubuf[warp];
+  T* ub = ubuf[warp];
   const int k = a.k;
   const long np = pairs_at_level(nb, k);
   const bool first = a.first != 0;
   const bool act = lane < n2, top = lane < n;
   const int ri = top ? lane : lane - n;
-  const double* srcD = first ? a.D0 : a.D;
-  const double* srcE = first ? a.E0 : a.E;
-  const double* srcB = first ? a.B0 : a.B;
-  const double* srcC = first ? a.C0 : a.C;
 
   for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
     const int j = k + (int)(2L * k * q), jp = j - k;
-    double row[NC];
+    T row[NC];
     {
-      const double* Pm = top ? srcE + (size_t)jp * nn : srcD + (size_t)j * nn;
-      const double* Xm = top ? srcD + (size_t)jp * nn : srcE + (size_t)j * nn;
-      const double* Bm = srcB + (size_t)(top ? jp : j) * nnx;
+      // panel: E_jp (TOP) / D_j (BOTTOM); x_jp column: D_jp / 0; x_jpp: 0 / E_j
+      const size_t op = top ? (size_t)jp * nn : (size_t)j * nn;
+      const size_t ob = (size_t)(top ? jp : j) * nnx;
 #pragma unroll
       for (int c = 0; c < N; ++c) {
-        double pv = 0.0, xv = 0.0;
-        if (act && c < n) { pv = Pm[(size_t)c * n + ri]; xv = Xm[(size_t)c * n + ri]; }
+        T pv = T(0), xv = T(0);
+        if (act && c < n) {
+          const size_t o = op + (size_t)c * n + ri;
+          pv = top ? ldsrc(first, a.E0, a.E, o) : ldsrc(first, a.D0, a.D, o);
+          xv = top ? ldsrc(first, a.D0, a.D, o) : ldsrc(first, a.E0, a.E, o);
+        }
         row[c] = pv;
-        row[N + c] = top ? xv : 0.0;
-        row[2 * N + c] = top ? 0.0 : xv;
+        row[N + c] = top ? xv : T(0);
+        row[2 * N + c] = top ? T(0) : xv;
       }
 #pragma unroll
-      for (int c = 0; c < NXM; ++c) row[3 * N + c] = (act && c < nx) ? Bm[(size_t)c * n + ri] : 0.0;
+      for (int c = 0; c < NXM; ++c)
+        row[3 * N + c] = (act && c < nx) ? ldsrc(first, a.B0, a.B, ob + (size_t)c * n + ri) : T(0);
     }
-    double cr[NRM][SLOTS];
+    T cr[NRM][SLOTS];
 #pragma unroll
     for (int r = 0; r < NRM; ++r)
 #pragma unroll
-      for (int sl = 0; sl < SLOTS; ++sl) cr[r][sl] = 0.0;
+      for (int sl = 0; sl < SLOTS; ++sl) cr[r][sl] = T(0);
     if (lane < n) {
-      const double* Cj = srcC + (size_t)j * nrn + (size_t)lane * nr;
+      const size_t oc = (size_t)j * nrn + (size_t)lane * nr;
 #pragma unroll
       for (int r = 0; r < NRM; ++r)
-        if (r < nr) cr[r][0] = Cj[r];
+        if (r < nr) cr[r][0] = ldsrc(first, a.C0, a.C, oc + r);
     }
 
     int mypos = lane, mykey = 0, info = 0;
@@ -368,12 +383,12 @@ __global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<double> a) {
 #pragma unroll
     for (int i = 0; i < N; ++i) {
       if (i < n) {
-        double v = done ? -1.0 : fabs(row[i]);
-        if (v != v) v = -0.5;  // NaN never wins against a number
+        T v = done ? T(-1) : dev_abs(row[i]);
+        if (v != v) v = T(-0.5);  // NaN never wins against a number
         int key = done ? 0x7fffffff : mypos;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
-          const double ov = __shfl_xor_sync(FULL, v, o);
+          const T ov = __shfl_xor_sync(FULL, v, o);
           const int ok = __shfl_xor_sync(FULL, key, o);
           if (ov > v || (ov == v && ok < key)) { v = ov; key = ok; }
         }
@@ -385,14 +400,14 @@ __global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<double> a) {
           mypos = i;
 #pragma unroll
           for (int c = (i & ~1); c < NCP; c += 2)
-            *reinterpret_cast<double2*>(&ub[c]) = make_double2(row[c], c + 1 < NC ? row[c + 1] : 0.0);
+            store2(&ub[c], row[c], c + 1 < NC ? row[c + 1] : T(0));
         }
         __syncwarp();
-        const double piv = ub[i];
-        if (piv == 0.0 && info == 0) info = i + 1;
-        const double rinv = piv != 0.0 ? 1.0 / piv : 0.0;
+        const T piv = ub[i];
+        if (piv == T(0) && info == 0) info = i + 1;
+        const T rinv = piv != T(0) ? T(1) / piv : T(0);
         if (!done && lane != p) {
-          const double l = row[i] * rinv;
+          const T l = row[i] * rinv;
           row[i] = l;
 #pragma unroll
           for (int c = i + 1; c < NC; ++c) row[c] = fma(-l, ub[c], row[c]);
@@ -401,7 +416,7 @@ __global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<double> a) {
 #pragma unroll
         for (int r = 0; r < NRM; ++r) {
           if (r < nr) {
-            const double mr = __shfl_sync(FULL, cr[r][0], i) * rinv;
+            const T mr = __shfl_sync(FULL, cr[r][0], i) * rinv;
             if (lane == i) cr[r][0] = mr;
             else if (lane > i && lane < NC) cr[r][0] = fma(-mr, ub[lane], cr[r][0]);
 #pragma unroll
@@ -418,13 +433,13 @@ __global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<double> a) {
     }
     // ---------------------------------------------------------------- store
     if (act) {
-      double* Tj = a.Tm + (size_t)j * szT(d);
+      T* Tj = a.Tm + (size_t)j * szT(d);
       const bool urow = mypos < n;
       const int rr = urow ? mypos : mypos - n;
       const size_t blk = urow ? (size_t)j : (size_t)jp;
-      double* Dd = a.D + blk * nn + rr;
-      double* Ed = a.E + blk * nn + rr;
-      double* Bd = a.B + blk * nnx + rr;
+      T* Dd = a.D + blk * nn + rr;
+      T* Ed = a.E + blk * nn + rr;
+      T* Bd = a.B + blk * nnx + rr;
 #pragma unroll
       for (int c = 0; c < N; ++c)
         if (c < n) {
@@ -444,14 +459,14 @@ __global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<double> a) {
 #pragma unroll
       for (int r = 0; r < NRM; ++r) {
         if (r >= nr) continue;
-        const double v = cr[r][sl];
+        const T v = cr[r][sl];
         if (col < N) {
           if (col < n) a.C[(size_t)j * nrn + (size_t)col * nr + r] = v;
         } else if (col < 2 * N) {
           const int c = col - N;
           if (c < n) {
             const size_t o = (size_t)jp * nrn + (size_t)c * nr + r;
-            a.C[o] = srcC[o] + v;
+            a.C[o] = ldsrc(first, a.C0, a.C, o) + v;
           }
         } else if (col < 3 * N) {
           const int c = col - 2 * N;
@@ -989,6 +1004,13 @@ __global__ void __launch_bounds__(256) k_factor_cta(FactorArgs<T> a, T* slab, si
   }
 }
 
+// copy of loaded FP64 blocks into the working precision
+template <typename T>
+__global__ void k_convert_blocks(const double* src, T* dst, size_t count) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < count; e += (size_t)gridDim.x * blockDim.x)
+    dst[e] = T(src[e]);
+}
+
 // C_jpp += dC_jpp for every pair of the level (one writer per target block)
 template <typename T>
 __global__ void k_border_fix(Dims d, T* C, const T* Rbuf, int k) {
@@ -1050,14 +1072,15 @@ __global__ void __launch_bounds__(256) k_reduce_tree(const T* buf, int stride, l
 // ---------------------------------------------------------------------------
 // solve sweeps (forward, cc:1615-1795; backward, cc:1805-2075)
 // ---------------------------------------------------------------------------
+// factors of type T (FP64, or FP32 for the mixed path); vectors always FP64
 template <typename T>
 struct SweepArgs {
   Dims d;
   const T *D, *E, *B, *C, *Tm;
   const unsigned char* P;
-  T* x;
+  double* x;
   int ldx, nrhs;
-  T* XB;
+  double* XB;
   int k, ldw, sel;
 };
 
@@ -1067,7 +1090,7 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_forward_level(SweepArgs<T>
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   const Dims d = a.d;
   const int n = d.n, nr = d.nr, n2 = 2 * n, nrhs = a.nrhs, ldw = a.ldw, k = a.k;
-  T* W = reinterpret_cast<T*>(smem_raw) + (size_t)warp * ldw * nrhs;
+  double* W = reinterpret_cast<double*>(smem_raw) + (size_t)warp * ldw * nrhs;
   const long np = pairs_at_level(d.nblock, k);
   for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
     const int j = k + (int)(2L * k * q), jp = j - k;
@@ -1083,24 +1106,24 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_forward_level(SweepArgs<T>
     if (a.sel == SEL_LU) {
       for (int i = 0; i < n; ++i) {
         for (int r = i + 1 + lane; r < n2; r += 32) {
-          const T l = Tj[(size_t)i * n2 + r];
+          const double l = Tj[(size_t)i * n2 + r];
           for (int c = 0; c < nrhs; ++c) W[(size_t)c * ldw + r] -= l * W[(size_t)c * ldw + i];
         }
         __syncwarp();
       }
     } else {
       for (int i = 0; i < n; ++i) {
-        const T t = Tj[2 * (size_t)n * n + i];
+        const double t = Tj[2 * (size_t)n * n + i];
         const T* v = Tj + (size_t)i * n2;
         for (int c = 0; c < nrhs; ++c) {
-          T* w = W + (size_t)c * ldw;
-          T s = T(0);
-          for (int r = i + 1 + lane; r < n2; r += 32) s += v[r] * w[r];
+          double* w = W + (size_t)c * ldw;
+          double s = 0.0;
+          for (int r = i + 1 + lane; r < n2; r += 32) s += double(v[r]) * w[r];
           s = warp_sum(s);
           s = (s + w[i]) * t;
           __syncwarp();
           if (lane == 0) w[i] -= s;
-          for (int r = i + 1 + lane; r < n2; r += 32) w[r] -= s * v[r];
+          for (int r = i + 1 + lane; r < n2; r += 32) w[r] -= s * double(v[r]);
           __syncwarp();
         }
       }
@@ -1115,8 +1138,8 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_forward_level(SweepArgs<T>
       const T* Cj = a.C + (size_t)j * nr * n;
       for (int idx = lane; idx < nr * nrhs; idx += 32) {
         const int r = idx % nr, c = idx / nr;
-        T s = T(0);
-        for (int i = 0; i < n; ++i) s += Cj[(size_t)i * nr + r] * W[(size_t)c * ldw + i];
+        double s = 0.0;
+        for (int i = 0; i < n; ++i) s += double(Cj[(size_t)i * nr + r]) * W[(size_t)c * ldw + i];
         a.XB[(size_t)j * nr * nrhs + idx] = -s;
       }
     }
@@ -1130,7 +1153,7 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_backward_level(SweepArgs<T
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   const Dims d = a.d;
   const int n = d.n, nx = d.nx, n2 = 2 * n, nrhs = a.nrhs, k = a.k, nb = d.nblock;
-  T* Y = reinterpret_cast<T*>(smem_raw) + (size_t)warp * a.ldw;
+  double* Y = reinterpret_cast<double*>(smem_raw) + (size_t)warp * a.ldw;
   const long np = pairs_at_level(nb, k);
   const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
   for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
@@ -1140,9 +1163,9 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_backward_level(SweepArgs<T
     const T* Bj = a.B + (size_t)j * n * nx;
     const T* Tj = a.Tm + (size_t)j * szT(d);
     for (int c = 0; c < nrhs; ++c) {
-      T* xc = a.x + (size_t)c * a.ldx;
+      double* xc = a.x + (size_t)c * a.ldx;
       for (int i = lane; i < n; i += 32) {
-        T s = xc[(size_t)j * n + i];
+        double s = xc[(size_t)j * n + i];
         for (int m = 0; m < n; ++m) s -= Dj[(size_t)m * n + i] * xc[(size_t)jp * n + m];
         for (int m = 0; m < n; ++m) s -= Ej[(size_t)m * n + i] * xc[(size_t)jpp * n + m];
         for (int m = 0; m < nx; ++m) s -= Bj[(size_t)m * n + i] * xc[xb_off + m];
@@ -1150,7 +1173,7 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_backward_level(SweepArgs<T
       }
       __syncwarp();
       for (int i = n - 1; i >= 0; --i) {
-        const T xi = Y[i] / Tj[(size_t)i * n2 + i];
+        const double xi = Y[i] / double(Tj[(size_t)i * n2 + i]);
         __syncwarp();
         if (lane == 0) Y[i] = xi;
         for (int r = lane; r < i; r += 32) Y[r] -= Tj[(size_t)i * n2 + r] * xi;
@@ -1175,8 +1198,8 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_backward_level(SweepArgs<T
 //   xb term added and U solved by n broadcast steps (QRP: column-map scatter).
 // All loads of a pair are issued before the first use.
 // ---------------------------------------------------------------------------
-template <int N, int NRM, bool LU>
-__global__ void __launch_bounds__(256, 2) k_forward_rows(SweepArgs<double> a) {
+template <typename TF, int N, int NRM, bool LU>
+__global__ void __launch_bounds__(256, 2) k_forward_rows(SweepArgs<TF> a) {
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   const Dims d = a.d;
@@ -1186,16 +1209,16 @@ __global__ void __launch_bounds__(256, 2) k_forward_rows(SweepArgs<double> a) {
   const long np = pairs_at_level(nb, k);
   for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
     const int j = k + (int)(2L * k * q), jp = j - k;
-    const double* Tj = a.Tm + (size_t)j * szT(d);
+    const TF* Tj = a.Tm + (size_t)j * szT(d);
     double t[N];
 #pragma unroll
-    for (int c = 0; c < N; ++c) t[c] = (act && c < n) ? Tj[(size_t)c * n2 + lane] : 0.0;
+    for (int c = 0; c < N; ++c) t[c] = (act && c < n) ? double(Tj[(size_t)c * n2 + lane]) : 0.0;
     double tau[LU ? 1 : N];
 #pragma unroll
     for (int c = 0; c < (LU ? 1 : N); ++c) tau[c] = (!lu && c < n) ? Tj[2 * (size_t)n * n + c] : 0.0;
     const int src = (act && lu) ? (int)a.P[(size_t)j * szP(d) + lane] : lane;
     double cp[NRM];
-    const double* Cj = a.C + (size_t)j * nr * n;
+    const TF* Cj = a.C + (size_t)j * nr * n;
 #pragma unroll
     for (int r = 0; r < NRM; ++r) cp[r] = (lane < n && r < nr) ? Cj[(size_t)lane * nr + r] : 0.0;
     for (int col = 0; col < nrhs; ++col) {
@@ -1236,8 +1259,8 @@ __global__ void __launch_bounds__(256, 2) k_forward_rows(SweepArgs<double> a) {
   }
 }
 
-template <int N, int NXM>
-__global__ void __launch_bounds__(256, 2) k_backward_rows(SweepArgs<double> a) {
+template <typename TF, int N, int NXM>
+__global__ void __launch_bounds__(256, 2) k_backward_rows(SweepArgs<TF> a) {
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   const Dims d = a.d;
@@ -1249,9 +1272,9 @@ __global__ void __launch_bounds__(256, 2) k_backward_rows(SweepArgs<double> a) {
   const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
   for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
     const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
-    const double* Mt = (hi ? a.E : a.D) + (size_t)j * n * n;
-    const double* Tj = a.Tm + (size_t)j * szT(d);
-    const double* Bj = a.B + (size_t)j * n * nx;
+    const TF* Mt = (hi ? a.E : a.D) + (size_t)j * n * n;
+    const TF* Tj = a.Tm + (size_t)j * szT(d);
+    const TF* Bj = a.B + (size_t)j * n * nx;
     double m[N], u[N], bb[NXM];
 #pragma unroll
     for (int c = 0; c < N; ++c) m[c] = (rowok && c < n) ? Mt[(size_t)c * n + i] : 0.0;
@@ -1302,24 +1325,24 @@ __global__ void __launch_bounds__(256, 2) k_backward_rows(SweepArgs<double> a) {
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_last_assemble(Dims d, const T* D, const T* E, const T* B, const T* C,
-                                const double* H, const double* Cq, const T* Ffin, T* Hl) {
-  const int n = d.n, Nr = d.Nr, Nc = d.Nc, qx = d.qx, nx = d.nx, nr = d.nr, m = n + d.qr;
+                                const double* H, const double* Cq, const double* Ffin, double* Hl) {
+  const int n = d.n, Nr = d.Nr, Nc = d.Nc, qx = d.qx, nr = d.nr, m = n + d.qr;
   const int total = Nr * Nc;
   const T* CN = C + (size_t)d.nblock * nr * n;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
     const int r = e % Nr, c = e / Nr;
-    T v = T(0);
+    double v = 0.0;
     if (r < n) {
       if (c < n) v = D[(size_t)c * n + r];
       else if (c < 2 * n) v = E[(size_t)(c - n) * n + r];
       else if (c >= 2 * n + qx) v = B[(size_t)(c - 2 * n - qx) * n + r];
     } else if (r < n + m) {
-      v = T(H[(size_t)c * m + (r - n)]);
+      v = H[(size_t)c * m + (r - n)];
     } else {
       const int rr = r - n - m;
       if (c < n) v = C[(size_t)c * nr + rr];
       else if (c < 2 * n) v = CN[(size_t)(c - n) * nr + rr];
-      else if (c < 2 * n + qx) v = T(Cq[(size_t)(c - 2 * n) * nr + rr]);
+      else if (c < 2 * n + qx) v = Cq[(size_t)(c - 2 * n) * nr + rr];
       else v = Ffin[(size_t)(c - 2 * n - qx) * nr + rr];
     }
     Hl[e] = v;
@@ -1484,6 +1507,8 @@ __global__ void k_last_solve(Dims d, const T* A, const int* piv, const T* tau, i
 // ---------------------------------------------------------------------------
 // Mv with the loaded matrix (add_Mv, cc:2118-2166): res = alpha*A*x + beta*res
 // ---------------------------------------------------------------------------
+// ABS: |A| * 1 (row sums of absolute values, for ||A||_inf); x is not read
+template <bool ABS>
 __global__ void k_mv_rows(Dims d, const double* D, const double* E, const double* B, double alpha,
                           const double* x, double beta, double* res) {
   const int n = d.n, nx = d.nx;
@@ -1497,13 +1522,20 @@ __global__ void k_mv_rows(Dims d, const double* D, const double* E, const double
     const double* Ek = E + k * n * n;
     const double* Bk = B + k * n * nx;
     double s = 0;
-    for (int c = 0; c < n; ++c) s += Dk[(size_t)c * n + i] * x[k * n + c];
-    for (int c = 0; c < n; ++c) s += Ek[(size_t)c * n + i] * x[(k + 1) * n + c];
-    for (int c = 0; c < nx; ++c) s += Bk[(size_t)c * n + i] * x[xb_off + c];
-    res[e] = (beta == 0.0 ? 0.0 : beta * res[e]) + alpha * s;
+    if constexpr (ABS) {
+      for (int c = 0; c < n; ++c) s += fabs(Dk[(size_t)c * n + i]) + fabs(Ek[(size_t)c * n + i]);
+      for (int c = 0; c < nx; ++c) s += fabs(Bk[(size_t)c * n + i]);
+      res[e] = s;
+    } else {
+      for (int c = 0; c < n; ++c) s += Dk[(size_t)c * n + i] * x[k * n + c];
+      for (int c = 0; c < n; ++c) s += Ek[(size_t)c * n + i] * x[(k + 1) * n + c];
+      for (int c = 0; c < nx; ++c) s += Bk[(size_t)c * n + i] * x[xb_off + c];
+      res[e] = (beta == 0.0 ? 0.0 : beta * res[e]) + alpha * s;
+    }
   }
 }
 
+template <bool ABS>
 __global__ void k_mv_cpart(Dims d, const double* C, const double* x, double* part) {
   const int n = d.n, nr = d.nr;
   const size_t total = (size_t)(d.nblock + 1) * nr;
@@ -1513,12 +1545,13 @@ __global__ void k_mv_cpart(Dims d, const double* C, const double* x, double* par
     const int r = (int)(e % nr);
     const double* Ck = C + k * nr * n;
     double s = 0;
-    for (int c = 0; c < n; ++c) s += Ck[(size_t)c * nr + r] * x[k * n + c];
+    for (int c = 0; c < n; ++c) s += ABS ? fabs(Ck[(size_t)c * nr + r]) : Ck[(size_t)c * nr + r] * x[k * n + c];
     part[e] = s;
   }
 }
 
 // H rows and the nr border rows (Csum = sum_k C_k x_k precomputed)
+template <bool ABS>
 __global__ void k_mv_tail(Dims d, const double* H, const double* Cq, const double* F,
                           const double* Csum, double alpha, const double* x, double beta,
                           double* res) {
@@ -1530,16 +1563,16 @@ __global__ void k_mv_tail(Dims d, const double* H, const double* Cq, const doubl
     if (r < m) {
       for (int c = 0; c < Nc; ++c) {
         size_t xi = c < n ? (size_t)c : (c < 2 * n ? xN + (c - n) : xq + (c - 2 * n));
-        s += H[(size_t)c * m + r] * x[xi];
+        s += ABS ? fabs(H[(size_t)c * m + r]) : H[(size_t)c * m + r] * x[xi];
       }
     } else {
       const int rr = r - m;
       s = Csum[rr];
-      for (int c = 0; c < qx; ++c) s += Cq[(size_t)c * nr + rr] * x[xq + c];
-      for (int c = 0; c < nx; ++c) s += F[(size_t)c * nr + rr] * x[xb + c];
+      for (int c = 0; c < qx; ++c) s += ABS ? fabs(Cq[(size_t)c * nr + rr]) : Cq[(size_t)c * nr + rr] * x[xq + c];
+      for (int c = 0; c < nx; ++c) s += ABS ? fabs(F[(size_t)c * nr + rr]) : F[(size_t)c * nr + rr] * x[xb + c];
     }
     const size_t o = r0 + r;
-    res[o] = (beta == 0.0 ? 0.0 : beta * res[o]) + alpha * s;
+    res[o] = ABS ? s : (beta == 0.0 ? 0.0 : beta * res[o]) + alpha * s;
   }
 }
 
@@ -1605,55 +1638,79 @@ static void reduce_blocks(DevState& s, const double* buf, long first, long count
 }
 
 // ---------------------------------------------------------------------------
-// pair-kernel choice for the factorization
+// working arrays of one precision
 // ---------------------------------------------------------------------------
-struct FactorPlan {
-  void (*cta)(FactorArgs<double>, double*, size_t) = nullptr;  // CTA per pair (large n)
-  void (*tc)(FactorArgs<double>) = nullptr;    // tensor-core LU (n = 8, 16)
-  size_t tc_smem = 0;
-  void (*rows)(FactorArgs<double>) = nullptr;  // register LU (n <= 16)
-  size_t smem = 0;                             // shared-memory kernel
-  int wpb = 1;
-  int tc_cols = 0;                             // trailing-column capacity of tc
+template <typename T>
+struct WorkSet {
+  T *D, *E, *B, *C, *Tm, *Rbuf;
+  T* slab;
 };
 
-static FactorPlan plan_factor(const DevState& s) {
+static WorkSet<double> work_set(DevState& s, double*) {
+  return {s.D, s.E, s.B, s.C, s.T, s.Rbuf, reinterpret_cast<double*>(s.slab)};
+}
+static WorkSet<float> work_set(DevState& s, float*) {
+  return {s.Df, s.Ef, s.Bf, s.Cf, s.Tf, s.Rbuff, reinterpret_cast<float*>(s.slab)};
+}
+
+// ---------------------------------------------------------------------------
+// pair-kernel choice for the factorization
+// ---------------------------------------------------------------------------
+template <typename T>
+struct FactorPlan {
+  void (*cta)(FactorArgs<T>, T*, size_t) = nullptr;  // CTA per pair (large n)
+  void (*tc)(FactorArgs<T>) = nullptr;               // tensor-core LU (FP64, n = 8, 16)
+  size_t tc_smem = 0;
+  void (*rows)(FactorArgs<T>) = nullptr;             // register LU (n <= 16)
+  void (*smem_k)(FactorArgs<T>) = nullptr;           // shared-memory kernel
+  size_t smem = 0;
+  int wpb = 1;
+  int tc_cols = 0;                                   // trailing-column capacity of tc
+};
+
+template <typename T>
+static FactorPlan<T> plan_factor(const DevState& s) {
   const Dims d = s.d;
   const int n = d.n;
-  FactorPlan p;
-  const size_t per_warp = panel_smem_per_warp(d, 8);
+  FactorPlan<T> p;
+  const size_t per_warp = panel_smem_per_warp(d, (int)sizeof(T));
   p.wpb = (int)(SMEM_MAX / per_warp);
   if (p.wpb > WARPS_PANEL) p.wpb = WARPS_PANEL;
   if (p.wpb < 1) p.wpb = 1;
   p.smem = per_warp * p.wpb;
-  if (s.sel == SEL_LU) smem_limit_once(k_factor_level<double, SEL_LU>, p.smem);
-  else if (s.sel == SEL_QR) smem_limit_once(k_factor_level<double, SEL_QR>, p.smem);
-  else smem_limit_once(k_factor_level<double, SEL_QRP>, p.smem);
-  if (s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 && (n == 16 || n == 8) && s.use_tc) {
-    p.tc_smem = tc_smem_per_warp(n) * 4;
-    if (n == 16) { p.tc = k_factor_lu_tc<16>; smem_limit_once(k_factor_lu_tc<16>, p.tc_smem); p.tc_cols = TcShape<16>::NTP; }
-    else { p.tc = k_factor_lu_tc<8>; smem_limit_once(k_factor_lu_tc<8>, p.tc_smem); p.tc_cols = TcShape<8>::NTP; }
+  p.smem_k = s.sel == SEL_LU ? k_factor_level<T, SEL_LU>
+           : s.sel == SEL_QR ? k_factor_level<T, SEL_QR> : k_factor_level<T, SEL_QRP>;
+  smem_limit_once(p.smem_k, p.smem);
+  if constexpr (sizeof(T) == 8) {
+    if (s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 && (n == 16 || n == 8) && s.use_tc) {
+      p.tc_smem = tc_smem_per_warp(n) * 4;
+      if (n == 16) { p.tc = k_factor_lu_tc<16>; smem_limit_once(k_factor_lu_tc<16>, p.tc_smem); p.tc_cols = TcShape<16>::NTP; }
+      else { p.tc = k_factor_lu_tc<8>; smem_limit_once(k_factor_lu_tc<8>, p.tc_smem); p.tc_cols = TcShape<8>::NTP; }
+    }
   }
   if (!p.tc && s.sel == SEL_LU && d.nr <= 4 && d.nx <= 4) {
-    if (n <= 4) p.rows = k_factor_lu_rows<4, 4, 4>;
-    else if (n <= 8) p.rows = k_factor_lu_rows<8, 4, 4>;
-    else if (n <= 16) p.rows = k_factor_lu_rows<16, 4, 4>;
+    if (n <= 4) p.rows = k_factor_lu_rows<T, 4, 4, 4>;
+    else if (n <= 8) p.rows = k_factor_lu_rows<T, 8, 4, 4>;
+    else if (n <= 16) p.rows = k_factor_lu_rows<T, 16, 4, 4>;
   }
   if (!p.tc && !p.rows && use_cta_kernel(d)) {
-    p.cta = s.sel == SEL_LU ? k_factor_cta<double, SEL_LU>
-          : s.sel == SEL_QR ? k_factor_cta<double, SEL_QR> : k_factor_cta<double, SEL_QRP>;
+    p.cta = s.sel == SEL_LU ? k_factor_cta<T, SEL_LU>
+          : s.sel == SEL_QR ? k_factor_cta<T, SEL_QR> : k_factor_cta<T, SEL_QRP>;
   }
   return p;
 }
 
 // number of right-hand sides the factorization can carry (0: none)
-static int fusable_rhs(const DevState& s, const FactorPlan& p, int nrhs) {
+template <typename T>
+static int fusable_rhs(const DevState& s, const FactorPlan<T>& p, int nrhs) {
   if (!p.tc || nrhs < 1 || nrhs > 16) return 0;
   return 2 * s.d.n + s.d.nx + nrhs <= p.tc_cols ? nrhs : 0;
 }
 
 // every CR level: pair eliminations and the C_jpp border fix-up
-static void factor_levels(DevState& s, const FactorPlan& p, double* x, int ldx, int nrf, cudaStream_t st) {
+template <typename T>
+static void factor_levels(DevState& s, const FactorPlan<T>& p, const WorkSet<T>& w, double* x, int ldx,
+                          int nrf, cudaStream_t st) {
   const Dims d = s.d;
   const int n = d.n, nb = d.nblock;
   const size_t nn = (size_t)n * n, nnx = (size_t)n * d.nx, nrn = (size_t)d.nr * n;
@@ -1661,75 +1718,81 @@ static void factor_levels(DevState& s, const FactorPlan& p, double* x, int ldx, 
   // blocks not touched by the first level: the unpaired tail and C_nblock
   if (nb % 2 == 1) {
     const size_t t = (size_t)(nb - 1);
-    cudaMemcpyAsync(s.D + t * nn, s.D0 + t * nn, nn * 8, cudaMemcpyDeviceToDevice, st);
-    cudaMemcpyAsync(s.E + t * nn, s.E0 + t * nn, nn * 8, cudaMemcpyDeviceToDevice, st);
-    if (nnx) cudaMemcpyAsync(s.B + t * nnx, s.B0 + t * nnx, nnx * 8, cudaMemcpyDeviceToDevice, st);
-    if (nrn) cudaMemcpyAsync(s.C + t * nrn, s.C0 + t * nrn, nrn * 8, cudaMemcpyDeviceToDevice, st);
+    k_convert_blocks<T><<<1, 256, 0, st>>>(s.D0 + t * nn, w.D + t * nn, nn);
+    k_convert_blocks<T><<<1, 256, 0, st>>>(s.E0 + t * nn, w.E + t * nn, nn);
+    if (nnx) k_convert_blocks<T><<<1, 256, 0, st>>>(s.B0 + t * nnx, w.B + t * nnx, nnx);
+    if (nrn) k_convert_blocks<T><<<1, 256, 0, st>>>(s.C0 + t * nrn, w.C + t * nrn, nrn);
   }
-  if (nrn)
-    cudaMemcpyAsync(s.C + (size_t)nb * nrn, s.C0 + (size_t)nb * nrn, nrn * 8,
-                    cudaMemcpyDeviceToDevice, st);
-  FactorArgs<double> a;
+  if (nrn) k_convert_blocks<T><<<1, 256, 0, st>>>(s.C0 + (size_t)nb * nrn, w.C + (size_t)nb * nrn, nrn);
+  FactorArgs<T> a;
   a.d = d;
   a.D0 = s.D0; a.E0 = s.E0; a.B0 = s.B0; a.C0 = s.C0;
-  a.D = s.D; a.E = s.E; a.B = s.B; a.C = s.C;
-  a.Tm = s.T; a.P = s.P; a.Rbuf = s.Rbuf; a.Fbuf = s.Fbuf; a.st = s.st;
+  a.D = w.D; a.E = w.E; a.B = w.B; a.C = w.C;
+  a.Tm = w.Tm; a.P = s.P; a.Rbuf = w.Rbuf; a.Fbuf = s.Fbuf; a.st = s.st;
   a.ldw = odd_ld(2 * n + d.nr);
   a.x = x; a.ldx = ldx; a.nrf = nrf; a.XB = s.XB;
   for (int k = 1; k < nb; k *= 2) {
     a.k = k;
     a.first = (k == 1);
     const long np = pairs_at_level(nb, k);
-    const int grid = grid_for(np, p.wpb, 148 * 16);
-    if (p.cta) p.cta<<<grid_for(np, 1, s.slab_ctas), 256, 0, st>>>(a, s.slab, s.slab_elems);
+    if (p.cta) p.cta<<<grid_for(np, 1, s.slab_ctas), 256, 0, st>>>(a, w.slab, s.slab_elems);
     else if (p.tc) p.tc<<<grid_for(np, 4, 148 * 16), 128, p.tc_smem, st>>>(a);
     else if (p.rows) p.rows<<<grid_for(np, 4, 148 * 16), 128, 0, st>>>(a);
-    else if (s.sel == SEL_LU) k_factor_level<double, SEL_LU><<<grid, p.wpb * 32, p.smem, st>>>(a);
-    else if (s.sel == SEL_QR) k_factor_level<double, SEL_QR><<<grid, p.wpb * 32, p.smem, st>>>(a);
-    else k_factor_level<double, SEL_QRP><<<grid, p.wpb * 32, p.smem, st>>>(a);
+    else p.smem_k<<<grid_for(np, p.wpb, 148 * 16), p.wpb * 32, p.smem, st>>>(a);
     check_launch("k_factor_level");
     if (nrn) {
       const long tot = np * (long)nrn;
-      k_border_fix<double><<<grid_for(tot, 256, 148 * 8), 256, 0, st>>>(d, s.C, s.Rbuf, k);
+      k_border_fix<T><<<grid_for(tot, 256, 148 * 8), 256, 0, st>>>(d, w.C, w.Rbuf, k);
       check_launch("k_border_fix");
     }
   }
 }
 
-// F = F0 + sum of the Schur updates; assemble and factor the last block
-static void factor_last(DevState& s, cudaStream_t st) {
+// F = F0 + sum of the Schur updates (FP64); assemble and factor the last block (FP64)
+template <typename T>
+static void factor_last(DevState& s, const WorkSet<T>& w, cudaStream_t st) {
   const Dims d = s.d;
   const int nrnx = d.nr * d.nx;
   if (nrnx > 0)
     reduce_blocks(s, s.Fbuf, 1, d.nblock - 1, nrnx, d.nr, s.F0, d.nr, s.Ffin, d.nr, st);
-  k_last_assemble<double><<<grid_for((long)d.Nr * d.Nc, 256, 64), 256, 0, st>>>(
-      d, s.D, s.E, s.B, s.C, s.H, s.Cq, s.Ffin, s.Hl);
+  k_last_assemble<T><<<grid_for((long)d.Nr * d.Nc, 256, 64), 256, 0, st>>>(
+      d, w.D, w.E, w.B, w.C, s.H, s.Cq, s.Ffin, s.Hl);
   check_launch("k_last_assemble");
   k_last_factor<double><<<1, 512, 0, st>>>(d, s.Hl, s.piv_l, s.tau_l, s.sel_last, s.st);
   check_launch("k_last_factor");
 }
 
+template <typename T>
+static void factorize_t(DevState& s, cudaStream_t st) {
+  T* tag = nullptr;
+  const WorkSet<T> w = work_set(s, tag);
+  const FactorPlan<T> p = plan_factor<T>(s);
+  factor_levels(s, p, w, nullptr, 0, 0, st);
+  factor_last(s, w, st);
+}
+
 void launch_factorize(DevState& s, cudaStream_t st) {
-  const FactorPlan p = plan_factor(s);
-  factor_levels(s, p, nullptr, 0, 0, st);
-  factor_last(s, st);
+  if (s.mixed) factorize_t<float>(s, st);
+  else factorize_t<double>(s, st);
 }
 
 // sweep kernels for one chunk of right-hand sides
+template <typename T>
 struct SweepPlan {
-  void (*fwd)(SweepArgs<double>) = nullptr;
-  void (*bwd)(SweepArgs<double>) = nullptr;
+  void (*fwd)(SweepArgs<T>) = nullptr;
+  void (*bwd)(SweepArgs<T>) = nullptr;
 };
 
-static SweepPlan plan_sweeps(const DevState& s) {
+template <typename T>
+static SweepPlan<T> plan_sweeps(const DevState& s) {
   const Dims d = s.d;
   const int n = d.n;
-  SweepPlan p;
+  SweepPlan<T> p;
   if (d.nr <= 8 && d.nx <= 8 && n <= 16) {
     const bool lu = s.sel == SEL_LU, r4 = d.nr <= 4, x4 = d.nx <= 4;
-#define BCR_FWD(NN) (r4 ? (lu ? k_forward_rows<NN, 4, true> : k_forward_rows<NN, 4, false>) \
-                        : (lu ? k_forward_rows<NN, 8, true> : k_forward_rows<NN, 8, false>))
-#define BCR_BWD(NN) (x4 ? k_backward_rows<NN, 4> : k_backward_rows<NN, 8>)
+#define BCR_FWD(NN) (r4 ? (lu ? k_forward_rows<T, NN, 4, true> : k_forward_rows<T, NN, 4, false>) \
+                        : (lu ? k_forward_rows<T, NN, 8, true> : k_forward_rows<T, NN, 8, false>))
+#define BCR_BWD(NN) (x4 ? k_backward_rows<T, NN, 4> : k_backward_rows<T, NN, 8>)
     if (n <= 4) { p.fwd = BCR_FWD(4); p.bwd = BCR_BWD(4); }
     else if (n <= 8) { p.fwd = BCR_FWD(8); p.bwd = BCR_BWD(8); }
     else { p.fwd = BCR_FWD(16); p.bwd = BCR_BWD(16); }
@@ -1739,10 +1802,11 @@ static SweepPlan plan_sweeps(const DevState& s) {
   return p;
 }
 
-static SweepArgs<double> sweep_args(DevState& s, double* x, int ldx, int nrhs) {
-  SweepArgs<double> a;
+template <typename T>
+static SweepArgs<T> sweep_args(DevState& s, const WorkSet<T>& w, double* x, int ldx, int nrhs) {
+  SweepArgs<T> a;
   a.d = s.d;
-  a.D = s.D; a.E = s.E; a.B = s.B; a.C = s.C; a.Tm = s.T; a.P = s.P;
+  a.D = w.D; a.E = w.E; a.B = w.B; a.C = w.C; a.Tm = w.Tm; a.P = s.P;
   a.x = x; a.ldx = ldx; a.nrhs = nrhs; a.XB = s.XB; a.sel = s.sel;
   return a;
 }
@@ -1762,90 +1826,159 @@ static void reduce_xb(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st
   }
 }
 
-static void forward_levels(DevState& s, const SweepPlan& p, double* x, int ldx, int nrhs, cudaStream_t st) {
+template <typename T>
+static void forward_levels(DevState& s, const SweepPlan<T>& p, const WorkSet<T>& w, double* x, int ldx,
+                           int nrhs, cudaStream_t st) {
   const Dims d = s.d;
-  SweepArgs<double> a = sweep_args(s, x, ldx, nrhs);
+  SweepArgs<T> a = sweep_args(s, w, x, ldx, nrhs);
   a.ldw = odd_ld(2 * d.n);
   const size_t smem_f = (size_t)a.ldw * nrhs * 8 * WARPS_PANEL;
-  smem_limit_once(k_forward_level<double>, smem_f);
+  smem_limit_once(k_forward_level<T>, smem_f);
   for (int K = 1; K < d.nblock; K *= 2) {
     a.k = K;
     const long np = pairs_at_level(d.nblock, K);
     if (p.fwd) p.fwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a);
-    else k_forward_level<double><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_f, st>>>(a);
+    else k_forward_level<T><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_f, st>>>(a);
     check_launch("k_forward_level");
   }
   reduce_xb(s, x, ldx, nrhs, st);
 }
 
-static void last_and_backward(DevState& s, const SweepPlan& p, double* x, int ldx, int nrhs, cudaStream_t st) {
+template <typename T>
+static void last_and_backward(DevState& s, const SweepPlan<T>& p, const WorkSet<T>& w, double* x, int ldx,
+                              int nrhs, cudaStream_t st) {
   const Dims d = s.d;
   const size_t smem_l = (size_t)(d.Nr > d.Nc ? d.Nr : d.Nc) * 8;
   k_last_solve<double><<<1, 256, smem_l, st>>>(d, s.Hl, s.piv_l, s.tau_l, s.sel_last, x, ldx, nrhs);
   check_launch("k_last_solve");
-  SweepArgs<double> a = sweep_args(s, x, ldx, nrhs);
+  SweepArgs<T> a = sweep_args(s, w, x, ldx, nrhs);
   a.ldw = d.n;
   const size_t smem_b = (size_t)d.n * 8 * WARPS_PANEL;
   for (int k = top_level(d.nblock); (k /= 2) > 0;) {
     a.k = k;
     const long np = pairs_at_level(d.nblock, k);
     if (p.bwd) p.bwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a);
-    else k_backward_level<double><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_b, st>>>(a);
+    else k_backward_level<T><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_b, st>>>(a);
     check_launch("k_backward_level");
   }
 }
 
 // right-hand sides are independent: sweep them in chunks of at most 16 columns
-void launch_solve(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st) {
-  const SweepPlan p = plan_sweeps(s);
+template <typename T>
+static void solve_t(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st) {
+  T* tag = nullptr;
+  const WorkSet<T> w = work_set(s, tag);
+  const SweepPlan<T> p = plan_sweeps<T>(s);
   for (int c0 = 0; c0 < nrhs; c0 += 16) {
     const int nc = nrhs - c0 < 16 ? nrhs - c0 : 16;
     double* xc = x + (size_t)c0 * ldx;
-    forward_levels(s, p, xc, ldx, nc, st);
-    last_and_backward(s, p, xc, ldx, nc, st);
+    forward_levels(s, p, w, xc, ldx, nc, st);
+    last_and_backward(s, p, w, xc, ldx, nc, st);
   }
+}
+
+void launch_solve(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st) {
+  if (s.mixed) solve_t<float>(s, x, ldx, nrhs, st);
+  else solve_t<double>(s, x, ldx, nrhs, st);
 }
 
 // factorize and solve in one pass: when the pair kernel can carry the right-
 // hand sides, their forward elimination rides in the factorization's GEMM and
 // the separate forward sweep disappears
 void launch_factorize_solve(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st) {
-  const FactorPlan fp = plan_factor(s);
+  if (s.mixed) {
+    launch_factorize(s, st);
+    launch_solve(s, x, ldx, nrhs, st);
+    return;
+  }
+  double* tag = nullptr;
+  const WorkSet<double> w = work_set(s, tag);
+  const FactorPlan<double> fp = plan_factor<double>(s);
   const int nrf = fusable_rhs(s, fp, nrhs);
   if (nrf == 0) {
     launch_factorize(s, st);
     launch_solve(s, x, ldx, nrhs, st);
     return;
   }
-  factor_levels(s, fp, x, ldx, nrf, st);
+  factor_levels(s, fp, w, x, ldx, nrf, st);
   reduce_xb(s, x, ldx, nrf, st);
-  factor_last(s, st);
-  last_and_backward(s, plan_sweeps(s), x, ldx, nrf, st);
+  factor_last(s, w, st);
+  last_and_backward(s, plan_sweeps<double>(s), w, x, ldx, nrf, st);
 }
 
 bool factorize_solve_fuses(const DevState& s, int nrhs) {
-  return fusable_rhs(s, plan_factor(s), nrhs) == nrhs;
+  if (s.mixed) return false;
+  return fusable_rhs(s, plan_factor<double>(s), nrhs) == nrhs;
 }
 
-void launch_mv(DevState& s, double alpha, const double* x, double beta, double* res,
-               cudaStream_t st) {
+template <bool ABS>
+static void mv_t(DevState& s, double alpha, const double* x, double beta, double* res, cudaStream_t st) {
   const Dims d = s.d;
   const long rows = (long)d.nblock * d.n;
   if (rows > 0) {
-    k_mv_rows<<<grid_for(rows, 256, 148 * 8), 256, 0, st>>>(d, s.D0, s.E0, s.B0, alpha, x, beta, res);
+    k_mv_rows<ABS><<<grid_for(rows, 256, 148 * 8), 256, 0, st>>>(d, s.D0, s.E0, s.B0, alpha, x, beta, res);
     check_launch("k_mv_rows");
   }
   const int nr = d.nr;
-  double* Csum = s.Ffin;  // reuse the small nr x nx buffer only if large enough
+  double* Csum = s.Ffin;  // unused when nr == 0
   if (nr > 0) {
     const long tot = (long)(d.nblock + 1) * nr;
-    k_mv_cpart<<<grid_for(tot, 256, 148 * 8), 256, 0, st>>>(d, s.C0, x, s.mv_part);
+    k_mv_cpart<ABS><<<grid_for(tot, 256, 148 * 8), 256, 0, st>>>(d, s.C0, x, s.mv_part);
     check_launch("k_mv_cpart");
     Csum = s.mv_part + (size_t)(d.nblock + 1) * nr;
     reduce_blocks(s, s.mv_part, 0, d.nblock + 1, nr, nr, nullptr, nr, Csum, nr, st);
   }
-  k_mv_tail<<<1, 256, 0, st>>>(d, s.H, s.Cq, s.F0, Csum, alpha, x, beta, res);
+  k_mv_tail<ABS><<<1, 256, 0, st>>>(d, s.H, s.Cq, s.F0, Csum, alpha, x, beta, res);
   check_launch("k_mv_tail");
+}
+
+void launch_mv(DevState& s, double alpha, const double* x, double beta, double* res, cudaStream_t st) {
+  mv_t<false>(s, alpha, x, beta, res, st);
+}
+
+// out[slot] = max |v_i| over i < len (exact, order independent)
+__global__ void k_absmax(const double* v, long len, unsigned long long* out) {
+  double m = 0.0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long)gridDim.x * blockDim.x)
+    m = fmax(m, fabs(v[i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+__global__ void k_axpy(double* y, const double* x, long len) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long)gridDim.x * blockDim.x)
+    y[i] += x[i];
+}
+
+// ||A||_inf of the loaded matrix into norms[0]; scratch: ncols-long buffer
+void launch_norm_A(DevState& s, double* rowsum, unsigned long long* out, cudaStream_t st) {
+  const Dims d = s.d;
+  const long nrows = (long)d.n * (d.nblock + 1) + d.qr + d.nr;
+  mv_t<true>(s, 1.0, nullptr, 0.0, rowsum, st);
+  cudaMemsetAsync(out, 0, sizeof(unsigned long long), st);
+  k_absmax<<<grid_for(nrows, 256, 148 * 2), 256, 0, st>>>(rowsum, nrows, out);
+  check_launch("k_absmax");
+}
+
+// r = b - A x and the three inf-norms |r|, |x|, |b| into out[0..2]
+void launch_residual(DevState& s, const double* b, const double* x, double* r, unsigned long long* out,
+                     cudaStream_t st) {
+  const Dims d = s.d;
+  const long nrows = (long)d.n * (d.nblock + 1) + d.qr + d.nr;
+  const long ncols = (long)d.n * (d.nblock + 1) + d.qx + d.nx;
+  cudaMemcpyAsync(r, b, (size_t)nrows * 8, cudaMemcpyDeviceToDevice, st);
+  mv_t<false>(s, -1.0, x, 1.0, r, st);
+  cudaMemsetAsync(out, 0, 3 * sizeof(unsigned long long), st);
+  k_absmax<<<grid_for(nrows, 256, 148 * 2), 256, 0, st>>>(r, nrows, out);
+  k_absmax<<<grid_for(ncols, 256, 148 * 2), 256, 0, st>>>(x, ncols, out + 1);
+  k_absmax<<<grid_for(nrows, 256, 148 * 2), 256, 0, st>>>(b, nrows, out + 2);
+  check_launch("k_absmax");
+}
+
+void launch_axpy(double* y, const double* x, long len, cudaStream_t st) {
+  k_axpy<<<grid_for(len, 256, 148 * 4), 256, 0, st>>>(y, x, len);
+  check_launch("k_axpy");
 }
 
 }  // namespace bcr

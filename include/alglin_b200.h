@@ -113,6 +113,14 @@ int bcr_factorize_use_thread(bcr_handle h);              /* hxx:396 */
 int bcr_solve_use_thread(bcr_handle h);                  /* hxx:398 */
 int bcr_set_num_parallel_block(bcr_handle h, int npb);   /* hxx:407-423 */
 int bcr_set_precision(bcr_handle h, int precision);      /* extension: FP64 / mixed */
+/* Iterative refinement of the mixed path (extension, no reference counterpart):
+   corrections d = A^-1 r from FP64 residuals r = b - A x stop once
+   |r|_inf / (|A|_inf |x|_inf + |b|_inf) <= tol (default 1e-12) or after
+   max_iter corrections (default 10).  The mixed path needs a square system. */
+int bcr_set_refinement(bcr_handle h, double tol, int max_iter);
+/* corrections applied by the last mixed solve and its final relative residual
+   (max over right-hand sides); 0 and 0.0 on the FP64 path */
+int bcr_refinement_info(bcr_handle h, int* iters, double* relres);
 /* info(indent) cc:208-235; the returned string lives until the next call */
 const char *bcr_info(bcr_handle h, const char *indent);
 const char *bcr_last_error(bcr_handle h);                /* hxx:445 */

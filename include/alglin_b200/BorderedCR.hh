@@ -157,6 +157,15 @@ namespace alglin_b200 {
     void set_debug( bool yes ) { chk( bcr_set_debug( m_h, yes ) ); }
     void check_matrix() { chk( bcr_check_matrix( m_h ) ); }
 
+    // extensions: FP32 factors with FP64 iterative refinement
+    void set_precision_mixed( bool yes ) {
+      chk( bcr_set_precision( m_h, yes ? BCR_PRECISION_MIXED : BCR_PRECISION_FP64 ) );
+    }
+    void set_refinement( real_type tol, integer max_iter ) { chk( bcr_set_refinement( m_h, tol, max_iter ) ); }
+    void refinement_info( integer & iters, real_type & relres ) const {
+      chk( bcr_refinement_info( m_h, &iters, &relres ) );
+    }
+
     // -------------------------------------------------------------- sizes
     integer nrows() const            { return bcr_nrows( m_h ); }
     integer ncols() const            { return bcr_ncols( m_h ); }
