@@ -21,6 +21,7 @@ LIB_PATH = os.path.join(HERE, "libalglin_b200.so")
 
 BCR_OK, BCR_NUMERICAL, BCR_BAD_ARGUMENT, BCR_CUDA_ERROR, BCR_DEVICE_TIMEOUT = range(5)
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+PAIR_AUTO, PAIR_TC, PAIR_GRP, PAIR_ROWS, PAIR_CTA, PAIR_SMEM = range(6)
 
 _dp = ct.POINTER(ct.c_double)
 _ip = ct.POINTER(ct.c_int)
@@ -70,6 +71,7 @@ _SIGS = [
     ("bcr_set_num_parallel_block", [_H, ct.c_int], ct.c_int),
     ("bcr_set_precision", [_H, ct.c_int], ct.c_int),
     ("bcr_set_refinement", [_H, ct.c_double, ct.c_int], ct.c_int),
+    ("bcr_set_pair_kernel", [_H, ct.c_int], ct.c_int),
     ("bcr_refinement_info", [_H, ct.POINTER(ct.c_int), _dp], ct.c_int),
     ("bcr_info", [_H, ct.c_char_p], ct.c_char_p),
     ("bcr_last_error", [_H], ct.c_char_p),
@@ -164,9 +166,11 @@ class BorderedCR:
         self._check(self.L.bcr_create(ct.byref(self.h), num_threads, num_parallel_block))
 
     def __del__(self):
-        if getattr(self, "h", None) and self.h.value:
-            self.L.bcr_destroy(self.h)
-            self.h = _H()
+        h = getattr(self, "h", None)
+        if h is None or _H is None or not h.value:
+            return  # nothing to free, or the interpreter is shutting down
+        self.L.bcr_destroy(h)
+        self.h = _H()
 
     # ------------------------------------------------------------- errors ---
     def last_error(self) -> str:
@@ -294,6 +298,10 @@ class BorderedCR:
     def solve_use_thread(self): return bool(self.L.bcr_solve_use_thread(self.h))
     def set_num_parallel_block(self, npb): self._check(self.L.bcr_set_num_parallel_block(self.h, npb))
     def set_precision(self, p): self._check(self.L.bcr_set_precision(self.h, p))
+
+    def set_pair_kernel(self, choice: int):
+        """Force a pair-kernel family (PAIR_AUTO, PAIR_TC, PAIR_GRP, PAIR_ROWS, PAIR_CTA, PAIR_SMEM)."""
+        self._check(self.L.bcr_set_pair_kernel(self.h, int(choice)))
 
     def set_refinement(self, tol: float = 1e-12, max_iter: int = 10):
         """Stopping rule of the mixed path's iterative refinement."""

@@ -188,7 +188,7 @@ struct bcr_handle_s {
     A(dalloc(z.Hl, (size_t)d.Nr * d.Nc)); A(dalloc(z.tau_l, Lmax)); A(dalloc(z.piv_l, Lmax));
     A(dalloc(z.st, 1)); A(dalloc(z.mv_part, (nb + 2) * nr));
     z.slab_elems = bcr::cta_slab_elems(d);
-    z.slab_ctas = bcr::use_cta_kernel(d) ? 148 * 2 : 0;
+    z.slab_ctas = 148 * 2;  // the CTA-per-pair kernel may be chosen for any n
     if (z.slab_ctas) {
       double* slab = nullptr;
       A(dalloc(slab, z.slab_elems * z.slab_ctas));
@@ -1202,6 +1202,16 @@ int bcr_graph_launch(bcr_handle h, int what) {
   if (e != cudaSuccess) return h->cuda_fail(e, "cudaGraphLaunch");
   if (what & BCR_GRAPH_FACTORIZE) { h->pending_status = true; h->factorized = true; }
   if ((what & BCR_GRAPH_SOLVE) && h->s.mixed) h->ir_pending = true;
+  return BCR_OK;
+}
+
+int bcr_set_pair_kernel(bcr_handle h, int choice) {
+  H_CHECK(h);
+  if (choice < BCR_PAIR_AUTO || choice > BCR_PAIR_SMEM)
+    return h->fail(BCR_BAD_ARGUMENT, fmt("bcr_set_pair_kernel: unknown choice %d\n", choice));
+  h->s.pair_kernel = choice;
+  h->drop_graphs();
+  h->factorized = false;
   return BCR_OK;
 }
 

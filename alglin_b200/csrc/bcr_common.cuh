@@ -22,6 +22,9 @@ enum Internal : int { SEL_LU = 0, SEL_QR = 1, SEL_QRP = 2 };
 enum LastKind : int { LAST_LU = 0, LAST_LUPQ = 1, LAST_QR = 2, LAST_QRP = 3,
                       LAST_SVD = 4, LAST_LSS = 5, LAST_LSY = 6, LAST_PINV = 7 };
 
+// pair-kernel choice of the factorization (PAIR_AUTO picks by shape)
+enum PairKernel : int { PAIR_AUTO = 0, PAIR_TC = 1, PAIR_GRP = 2, PAIR_ROWS = 3, PAIR_CTA = 4, PAIR_SMEM = 5 };
+
 // error codes written by kernels into the device status word
 enum DevStatus : int {
   DEV_OK = 0,

@@ -13,6 +13,7 @@ struct DevState {
   int sel;        // Internal
   int sel_last;   // LastKind actually used (after fallback)
   int use_tc;     // allow the FP64 tensor-core pair kernel
+  int pair_kernel;  // PairKernel: AUTO, or a forced pair-kernel family
   // loaded matrix (reference layout), never modified on the device
   double *D0, *E0, *B0, *C0, *Cq, *F0, *H;
   // working blocks / factors

@@ -56,6 +56,27 @@ __device__ __forceinline__ T ldsrc(bool first, const double* orig, const T* work
   return first ? T(orig[i]) : work[i];
 }
 
+// the same through the read-only path; every load of a pair kernel's load
+// phase is independent of the shared-memory stores that follow it
+template <typename T>
+__device__ __forceinline__ T ldg_src(bool first, const double* orig, const T* work, size_t i) {
+  if constexpr (sizeof(T) == 8)
+    return __ldg(first ? orig + i : reinterpret_cast<const double*>(work) + i);
+  else
+    return first ? T(__ldg(orig + i)) : __ldg(work + i);
+}
+
+template <typename T>
+__device__ __forceinline__ void load2(const T* p, T& a, T& b) {
+  if constexpr (sizeof(T) == 8) {
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    a = v.x; b = v.y;
+  } else {
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    a = v.x; b = v.y;
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ void store2(T* p, T a, T b) {
   if constexpr (sizeof(T) == 8) *reinterpret_cast<double2*>(p) = make_double2(a, b);
@@ -97,6 +118,7 @@ __device__ int warp_eliminate_lu(T* W, int ldw, int n, int R, int NC, int* ipiv,
     warp_argmax(best, bi);
     if (lane == 0) ipiv[i] = bi;
     const T pv = ci[bi];
+    __syncwarp();  // every lane holds the pivot before column i is swapped
     if (pv == T(0)) return i + 1;  // LAPACK getrf INFO
     if (bi != i)
       for (int c = lane; c < NC; c += 32) {
@@ -805,6 +827,373 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a) {
 }
 
 // ---------------------------------------------------------------------------
+// LU pair kernel for n = 16 and n = 32 in either precision.  One CTA per
+// pair: 2n panel threads (one panel row each, in registers) plus one warp
+// whose first nr lanes hold the border rows C_j.  Three phases as in the
+// tensor-core kernel: register panel LU with the getrf pivot rule (the pivot
+// search spans the panel warps: each publishes its best candidate row and its
+// reciprocal, one barrier per column, double-buffered by column parity); the
+// operator G = [L^-1; -M L^-1; -C' L^-1]; one product G * (P W)_top, on the
+// FP64 tensor cores (DMMA 8x8x4) for double and on the FP32 pipe for float.
+// ---------------------------------------------------------------------------
+template <typename T> __device__ __forceinline__ T rcp_rn(T x);
+template <> __device__ __forceinline__ double rcp_rn<double>(double x) { return __drcp_rn(x); }
+template <> __device__ __forceinline__ float rcp_rn<float>(float x) { return __frcp_rn(x); }
+
+// total order of pivot candidates: (hi, lo) of |a|, NaN below every number,
+// finished rows below everything
+__device__ __forceinline__ void pivot_key(double av, bool done, unsigned& hi, unsigned& lo) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(av);
+  hi = done ? 0u : (av != av ? 1u : (unsigned)(b >> 32) + 1u);
+  lo = (done || av != av) ? 0u : (unsigned)b;
+}
+__device__ __forceinline__ void pivot_key(float av, bool done, unsigned& hi, unsigned& lo) {
+  hi = done ? 0u : (av != av ? 1u : (unsigned)__float_as_uint(av) + 1u);
+  lo = 0u;
+}
+
+template <typename T, int N>
+struct GrpShape {
+  static constexpr int TPP = 2 * N;        // panel threads, one per panel row
+  static constexpr int NTH = TPP + 32;     // + the border warp
+  static constexpr int NWP = TPP / 32;     // warps in the pivot search
+  static constexpr int NWA = NTH / 32;
+  static constexpr int MT = 2 * N + 8;     // product rows: U-row, reduced row, border (nr <= 8)
+  static constexpr int NTC = 2 * N + 8;    // trailing columns: x_jp, x_jpp, xb (nx <= 8)
+  static constexpr int LDW = NTC + 1;      // trailing rows (odd: conflict-light transposed stores)
+  static constexpr int LDG = N + 4;        // G rows (16-byte aligned rows, conflict-free fragments)
+  static constexpr int LDS = N + 2;
+  // FP64 product: DMMA tiles, warp w owns row tiles [w*RTW, (w+1)*RTW)
+  static constexpr int MTILES = MT / 8, NTILES = NTC / 8;
+  static constexpr int RTW = (MTILES + NWA - 1) / NWA;
+  static constexpr int PC = NTILES % 3 == 0 ? 3 : NTILES;  // column tiles per pass
+  // FP32 product: TR x TC thread grid, RPT x CPT elements per thread
+  static constexpr int TR = 8, TC = NTH / TR;
+  static constexpr int RPT = MT / TR, CPT = NTC / TC;
+  static constexpr size_t BYTES =
+      (size_t)(2 * N * LDW + MT * LDG + 2 * NWP * LDS) * sizeof(T) + (size_t)(2 * NWP * 4 + 2 * N) * sizeof(int);
+  static_assert(MT % TR == 0 && NTC % TC == 0 && NTILES % PC == 0, "product tiling");
+};
+
+// G * (P W)_top + [0; (P W)_bot; 0] -> the U-row of block j, the reduced row of
+// block jp and the border updates (C_jp, the C_jpp buffer, the F buffer)
+template <typename T, int N>
+struct GrpProduct;
+
+template <int N>
+struct GrpProduct<double, N> {
+  using S = GrpShape<double, N>;
+  template <typename Out>
+  __device__ static void run(const double* Wt, const double* Gs, const int* rowof, int t, Out out) {
+    const int w = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
+    const int mt0 = w * S::RTW;
+#pragma unroll
+    for (int pass = 0; pass < S::NTILES / S::PC; ++pass) {
+      double acc[S::RTW][S::PC][2];
+#pragma unroll
+      for (int mi = 0; mi < S::RTW; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < S::PC; ++ni) {
+          const int row = (mt0 + mi) * 8 + g, col = (pass * S::PC + ni) * 8 + 2 * q;
+          double c0 = 0.0, c1 = 0.0;
+          if (mt0 + mi < S::MTILES && row >= N && row < 2 * N) {
+            const double* wr = Wt + rowof[row] * S::LDW + col;
+            c0 = wr[0];
+            c1 = wr[1];
+          }
+          acc[mi][ni][0] = c0;
+          acc[mi][ni][1] = c1;
+        }
+#pragma unroll
+      for (int ks = 0; ks < N / 4; ++ks) {
+        double bfr[S::PC];
+        const double* wrow = Wt + rowof[ks * 4 + q] * S::LDW + pass * S::PC * 8 + g;
+#pragma unroll
+        for (int ni = 0; ni < S::PC; ++ni) bfr[ni] = wrow[ni * 8];
+#pragma unroll
+        for (int mi = 0; mi < S::RTW; ++mi) {
+          if (mt0 + mi < S::MTILES) {
+            const double afr = Gs[((mt0 + mi) * 8 + g) * S::LDG + ks * 4 + q];
+#pragma unroll
+            for (int ni = 0; ni < S::PC; ++ni) dmma_8x8x4(acc[mi][ni][0], acc[mi][ni][1], afr, bfr[ni]);
+          }
+        }
+      }
+#pragma unroll
+      for (int mi = 0; mi < S::RTW; ++mi)
+        if (mt0 + mi < S::MTILES)
+#pragma unroll
+          for (int ni = 0; ni < S::PC; ++ni)
+#pragma unroll
+            for (int hh = 0; hh < 2; ++hh)
+              out((mt0 + mi) * 8 + g, (pass * S::PC + ni) * 8 + 2 * q + hh, acc[mi][ni][hh]);
+    }
+  }
+};
+
+template <int N>
+struct GrpProduct<float, N> {
+  using S = GrpShape<float, N>;
+  template <typename Out>
+  __device__ static void run(const float* Wt, const float* Gs, const int* rowof, int t, Out out) {
+    const int tr = t % S::TR, tc = t / S::TR;
+    float acc[S::RPT][S::CPT];
+#pragma unroll
+    for (int ii = 0; ii < S::RPT; ++ii) {
+      const int row = tr + S::TR * ii;
+#pragma unroll
+      for (int jj = 0; jj < S::CPT; ++jj)
+        acc[ii][jj] = (row >= N && row < 2 * N) ? Wt[rowof[row] * S::LDW + tc + S::TC * jj] : 0.0f;
+    }
+#pragma unroll 4
+    for (int kk = 0; kk < N; ++kk) {
+      const float* wrow = Wt + rowof[kk] * S::LDW + tc;
+      float bv[S::CPT], av[S::RPT];
+#pragma unroll
+      for (int jj = 0; jj < S::CPT; ++jj) bv[jj] = wrow[S::TC * jj];
+#pragma unroll
+      for (int ii = 0; ii < S::RPT; ++ii) av[ii] = Gs[(tr + S::TR * ii) * S::LDG + kk];
+#pragma unroll
+      for (int ii = 0; ii < S::RPT; ++ii)
+#pragma unroll
+        for (int jj = 0; jj < S::CPT; ++jj) acc[ii][jj] = fmaf(av[ii], bv[jj], acc[ii][jj]);
+    }
+#pragma unroll
+    for (int ii = 0; ii < S::RPT; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < S::CPT; ++jj) out(tr + S::TR * ii, tc + S::TC * jj, acc[ii][jj]);
+  }
+};
+
+// CTAs per SM the register budget is sized for (FP64 n=32 is shared-memory
+// bound at 3; FP32 n=32 at 7)
+template <typename T, int N>
+constexpr int grp_min_blocks() { return N == 32 ? (sizeof(T) == 8 ? 3 : 5) : 4; }
+
+template <typename T, int N>
+__global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>()) k_factor_lu_grp(FactorArgs<T> a) {
+  using S = GrpShape<T, N>;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Wt = reinterpret_cast<T*>(smem_raw);          // [2N][LDW] trailing columns, original rows
+  T* Gs = Wt + 2 * N * S::LDW;                     // [MT][LDG] L rows, then G
+  T* slot = Gs + S::MT * S::LDG;                   // [2][NWP][LDS] candidate pivot row + reciprocal
+  int* hdr = reinterpret_cast<int*>(slot + 2 * S::NWP * S::LDS);  // [2][NWP][4] hi, lo, position, thread
+  int* rowof = hdr + 2 * S::NWP * 4;               // position -> original row
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const Dims d = a.d;
+  const int nr = d.nr, nx = d.nx, nb = d.nblock;
+  constexpr int n = N, n2 = 2 * N;
+  constexpr size_t nn = (size_t)N * N;
+  const size_t nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
+  const int k = a.k;
+  const long np = pairs_at_level(nb, k);
+  const bool first = a.first != 0;
+  const bool panel = t < n2;                 // panel row t
+  const bool brow = !panel && t - n2 < nr;   // border row t - 2N
+  const bool top = t < n;
+  const int ri = top ? t : t - n;
+
+  for (long qq = blockIdx.x; qq < np; qq += gridDim.x) {
+    const int j = k + (int)(2L * k * qq), jp = j - k;
+    __syncthreads();  // the previous pair's readers of Wt/Gs are done
+    // ------------------------------------------------------------ load
+    // every global load of the pair is issued before the first shared store
+    constexpr int IT = (int)((nn + S::NTH - 1) / S::NTH), IB = (8 * N + S::NTH - 1) / S::NTH;
+    T row[N], vd[IT], ve[IT], vbt[IB], vbb[IB];
+    if (panel) {
+      const size_t base = top ? (size_t)jp * nn : (size_t)j * nn;
+#pragma unroll
+      for (int c = 0; c < N; ++c) {
+        const size_t o = base + (size_t)c * n + ri;
+        row[c] = top ? ldg_src(first, a.E0, a.E, o) : ldg_src(first, a.D0, a.D, o);
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < N; ++c)
+        row[c] = brow ? ldg_src(first, a.C0, a.C, (size_t)j * nrn + (size_t)c * nr + (t - n2)) : T(0);
+    }
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+      const int idx = t + S::NTH * it;
+      const bool in = idx < (int)nn;
+      vd[it] = in ? ldg_src(first, a.D0, a.D, (size_t)jp * nn + idx) : T(0);
+      ve[it] = in ? ldg_src(first, a.E0, a.E, (size_t)j * nn + idx) : T(0);
+    }
+#pragma unroll
+    for (int it = 0; it < IB; ++it) {
+      const int idx = t + S::NTH * it;
+      const bool in = idx < nx * n;
+      vbt[it] = in ? ldg_src(first, a.B0, a.B, (size_t)jp * nnx + idx) : T(0);
+      vbb[it] = in ? ldg_src(first, a.B0, a.B, (size_t)j * nnx + idx) : T(0);
+    }
+    // trailing columns: TOP rows [D_jp 0 B_jp], BOTTOM rows [0 E_j B_j], zero padding
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+      const int idx = t + S::NTH * it;
+      if (idx < (int)nn) {
+        const int r = idx % n, c = idx / n;
+        Wt[r * S::LDW + c] = vd[it];
+        Wt[r * S::LDW + n + c] = T(0);
+        Wt[(n + r) * S::LDW + c] = T(0);
+        Wt[(n + r) * S::LDW + n + c] = ve[it];
+      }
+    }
+#pragma unroll
+    for (int it = 0; it < IB; ++it) {
+      const int idx = t + S::NTH * it;
+      if (idx < 8 * n) {
+        const int r = idx % n, c = idx / n;
+        Wt[r * S::LDW + n2 + c] = vbt[it];
+        Wt[(n + r) * S::LDW + n2 + c] = vbb[it];
+      }
+    }
+    // --------------------------------------------------- phase 1: panel LU
+    int mypos = t, info = 0;
+    bool done = !panel;  // border and idle lanes never pivot
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      const int par = i & 1;
+      if (w < S::NWP) {
+        // every lane forms the reciprocal of its own candidate while the pivot
+        // is searched; the winner publishes it with its row
+        const T rc = rcp_rn(row[i]);
+        unsigned hi, lo;
+        pivot_key(dev_abs(row[i]), done, hi, lo);
+        const unsigned hmax = __reduce_max_sync(FULL, hi);
+        const unsigned m = __ballot_sync(FULL, hi == hmax && !done);
+        int wl = -1;  // this warp's best candidate lane
+        if (m != 0u) {
+          if (__popc(m) == 1) {
+            wl = __ffs(m) - 1;
+          } else {
+            const bool c1 = hi == hmax && !done;
+            const unsigned lmax = __reduce_max_sync(FULL, c1 ? lo : 0u);
+            const bool cand = c1 && lo == lmax;
+            const unsigned pm = __reduce_min_sync(FULL, cand ? (unsigned)mypos : 0xffffffffu);
+            wl = __ffs(__ballot_sync(FULL, cand && (unsigned)mypos == pm)) - 1;
+          }
+        }
+        int4* h = reinterpret_cast<int4*>(hdr) + par * S::NWP + w;
+        T* sl = slot + (par * S::NWP + w) * S::LDS;
+        if (lane == wl) {
+          *h = make_int4((int)hi, (int)lo, mypos, t);
+#pragma unroll
+          for (int c = (i & ~1); c < N; c += 2) store2(sl + c, row[c], row[c + 1]);
+          sl[N] = rc;
+        } else if (wl < 0 && lane == 0) {
+          *h = make_int4(0, 0, 0x7fffffff, 0);  // no candidate left in this warp
+        }
+      }
+      __syncthreads();
+      int wb = 0;
+      int4 hw = reinterpret_cast<const int4*>(hdr)[par * S::NWP];
+      if (S::NWP == 2) {
+        const int4 h1 = reinterpret_cast<const int4*>(hdr)[par * S::NWP + 1];
+        const unsigned hi0 = (unsigned)hw.x, hi1 = (unsigned)h1.x;
+        const unsigned lo0 = (unsigned)hw.y, lo1 = (unsigned)h1.y;
+        if (hi1 > hi0 || (hi1 == hi0 && (lo1 > lo0 || (lo1 == lo0 && h1.z < hw.z)))) {
+          wb = 1;
+          hw = h1;
+        }
+      }
+      const int pmin = hw.z, p = hw.w;
+      const T* u = slot + (par * S::NWP + wb) * S::LDS;
+      const T piv = u[i];
+      if (piv == T(0) && info == 0) info = i + 1;
+      const T rinv = piv != T(0) ? u[N] : T(0);
+      if (panel) {
+        if (!done && mypos == i && t != p) mypos = pmin;
+        if (t == p) mypos = i;
+      }
+      if ((panel && !done && t != p) || brow) {
+        const T l = row[i] * rinv;
+        row[i] = l;
+#pragma unroll
+        for (int c = (i + 1) & ~1; c < N; c += 2) {
+          T u0, u1;
+          load2(u + c, u0, u1);
+          if (c > i) row[c] = fma(-l, u0, row[c]);
+          row[c + 1] = fma(-l, u1, row[c + 1]);
+        }
+      }
+      if (t == p) done = true;
+    }
+    if (info != 0) {
+      if (t == 0) report(a.st, DEV_ZERO_PIVOT, j, info, k);
+      continue;
+    }
+    // panel factors T_j (L\U and M in getrf row order), row map, C_j U^-1, L rows
+    if (panel) {
+      T* Tj = a.Tm + (size_t)j * szT(d);
+#pragma unroll
+      for (int c = 0; c < N; ++c) Tj[(size_t)mypos + (size_t)c * n2] = row[c];
+      rowof[mypos] = t;
+      a.P[(size_t)j * szP(d) + mypos] = (unsigned char)t;
+      if (mypos < n) {
+#pragma unroll
+        for (int c = 0; c < N; ++c) Gs[mypos * S::LDG + c] = row[c];
+      }
+    } else if (brow) {
+      T* Cj = a.C + (size_t)j * nrn + (t - n2);
+#pragma unroll
+      for (int c = 0; c < N; ++c) Cj[(size_t)c * nr] = row[c];
+    }
+    __syncthreads();
+    // ------------------------------------ phase 2: operator G (X L = R)
+    // R rows: identity for U-row positions, -M for reduced positions, -C' for border rows
+    {
+      T x[N];
+      const bool unit = panel && mypos < n;
+#pragma unroll
+      for (int c = 0; c < N; ++c) x[c] = unit ? (c == mypos ? T(1) : T(0)) : -row[c];
+      // right-looking: once x[mm] is final, update every x[c], c < mm
+#pragma unroll
+      for (int mm = N - 1; mm > 0; --mm) {
+        const T xm = x[mm];
+        const T* Lrow = Gs + mm * S::LDG;
+#pragma unroll
+        for (int c = 0; c < mm; c += 2) {
+          const T l0 = Lrow[c], l1 = Lrow[c + 1];
+          x[c] = fma(-xm, l0, x[c]);
+          if (c + 1 < mm) x[c + 1] = fma(-xm, l1, x[c + 1]);
+        }
+      }
+      __syncthreads();
+      const int grow = panel ? mypos : n2 + (t - n2);
+      if (panel || t - n2 < 8) {
+#pragma unroll
+        for (int c = 0; c < N; ++c) Gs[grow * S::LDG + c] = (panel || brow) ? x[c] : T(0);
+      }
+    }
+    __syncthreads();
+    // ------------------------------------------ phase 3: G * (P W)_top
+    GrpProduct<T, N>::run(Wt, Gs, rowof, t, [&](int prow, int col, T v) {
+      if (prow < n2) {
+        const bool ur = prow < n;
+        const int rr = ur ? prow : prow - n;
+        const size_t blk = ur ? (size_t)j : (size_t)jp;
+        if (col < n) a.D[blk * nn + (size_t)col * n + rr] = v;
+        else if (col < n2) a.E[blk * nn + (size_t)(col - n) * n + rr] = v;
+        else if (col < n2 + nx) a.B[blk * nnx + (size_t)(col - n2) * n + rr] = v;
+      } else {
+        const int rr = prow - n2;
+        if (rr < nr) {
+          if (col < n) {
+            const size_t o = (size_t)jp * nrn + (size_t)col * nr + rr;
+            a.C[o] = ldsrc(first, a.C0, a.C, o) + v;
+          } else if (col < n2) {
+            a.Rbuf[(size_t)j * nrn + (size_t)(col - n) * nr + rr] = v;
+          } else if (col < n2 + nx) {
+            a.Fbuf[(size_t)j * nrnx + (size_t)(col - n2) * nr + rr] = (double)v;
+          }
+        }
+      }
+    });
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Large blocks: one CTA eliminates one pair; the (2n+nr) x (3n+nx) work
 // matrix lives in a global scratch slab of the CTA (column-major, ld = R),
 // which stays in L2 while the CTA works on it.  Same elimination as the warp
@@ -895,6 +1284,7 @@ __global__ void __launch_bounds__(256) k_factor_cta(FactorArgs<T> a, T* slab, si
         block_argmax(best, bi, sv, si);
         if (tid == 0) s_piv[i] = bi;
         const T pv = ci[bi];
+        __syncthreads();  // every thread holds the pivot before column i is swapped
         if (pv == T(0)) { info = i + 1; break; }
         if (bi != i)
           for (int c = tid; c < NC; c += bs) {
@@ -1401,6 +1791,7 @@ __global__ void k_last_factor(Dims d, T* A, int* piv, T* tau, int kind, StatusWo
       block_argmax(best, bi, sv, si);
       if (tid == 0) piv[i] = bi;
       const T pv = A[(size_t)i * N + bi];
+      __syncthreads();  // every thread holds the pivot before column i is swapped
       if (pv == T(0)) { if (tid == 0) report(st, DEV_LAST_SINGULAR, -1, i + 1, -1); return; }
       if (bi != i)
         for (int c = tid; c < N; c += bs) {
@@ -1596,6 +1987,21 @@ static void smem_limit_once(K* kernel, size_t bytes) {
   if (slot < 64) done[slot] = bytes;
 }
 
+// CTAs of `kernel` resident on one SM (cached per kernel)
+template <typename K>
+static int resident_ctas(K* kernel, int threads, size_t smem) {
+  static const void* keys[64];
+  static int value[64];
+  static int used = 0;
+  const void* key = reinterpret_cast<const void*>(kernel);
+  for (int i = 0; i < used; ++i)
+    if (keys[i] == key) return value[i];
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem) != cudaSuccess || nb < 1) nb = 1;
+  if (used < 64) { keys[used] = key; value[used] = nb; ++used; }
+  return nb;
+}
+
 static int grid_for(long work_items, int per_cta, int cap) {
   long g = (work_items + per_cta - 1) / per_cta;
   if (g < 1) g = 1;
@@ -1661,6 +2067,9 @@ struct FactorPlan {
   void (*cta)(FactorArgs<T>, T*, size_t) = nullptr;  // CTA per pair (large n)
   void (*tc)(FactorArgs<T>) = nullptr;               // tensor-core LU (FP64, n = 8, 16)
   size_t tc_smem = 0;
+  void (*grp)(FactorArgs<T>) = nullptr;              // CTA of 2n threads per pair (n = 16, 32)
+  size_t grp_smem = 0;
+  int grp_threads = 0, grp_ctas = 0;
   void (*rows)(FactorArgs<T>) = nullptr;             // register LU (n <= 16)
   void (*smem_k)(FactorArgs<T>) = nullptr;           // shared-memory kernel
   size_t smem = 0;
@@ -1682,18 +2091,37 @@ static FactorPlan<T> plan_factor(const DevState& s) {
            : s.sel == SEL_QR ? k_factor_level<T, SEL_QR> : k_factor_level<T, SEL_QRP>;
   smem_limit_once(p.smem_k, p.smem);
   if constexpr (sizeof(T) == 8) {
-    if (s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 && (n == 16 || n == 8) && s.use_tc) {
+    if (s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 && (n == 16 || n == 8) && s.use_tc &&
+        (s.pair_kernel == PAIR_AUTO || s.pair_kernel == PAIR_TC)) {
       p.tc_smem = tc_smem_per_warp(n) * 4;
       if (n == 16) { p.tc = k_factor_lu_tc<16>; smem_limit_once(k_factor_lu_tc<16>, p.tc_smem); p.tc_cols = TcShape<16>::NTP; }
       else { p.tc = k_factor_lu_tc<8>; smem_limit_once(k_factor_lu_tc<8>, p.tc_smem); p.tc_cols = TcShape<8>::NTP; }
     }
   }
-  if (!p.tc && s.sel == SEL_LU && d.nr <= 4 && d.nx <= 4) {
+  const bool grp_ok = s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 &&
+                      (n == 32 || (n == 16 && (sizeof(T) == 4 || s.pair_kernel == PAIR_GRP)));
+  if (!p.tc && grp_ok && (s.pair_kernel == PAIR_AUTO || s.pair_kernel == PAIR_GRP)) {
+    if (n == 32) {
+      p.grp = k_factor_lu_grp<T, 32>;
+      p.grp_smem = GrpShape<T, 32>::BYTES;
+    } else {
+      p.grp = k_factor_lu_grp<T, 16>;
+      p.grp_smem = GrpShape<T, 16>::BYTES;
+    }
+    p.grp_threads = 2 * n + 32;
+    smem_limit_once(p.grp, p.grp_smem);
+    p.grp_ctas = 148 * resident_ctas(p.grp, p.grp_threads, p.grp_smem);
+  }
+  if (!p.tc && !p.grp && s.sel == SEL_LU && d.nr <= 4 && d.nx <= 4 && s.pair_kernel != PAIR_CTA &&
+      s.pair_kernel != PAIR_SMEM) {
     if (n <= 4) p.rows = k_factor_lu_rows<T, 4, 4, 4>;
     else if (n <= 8) p.rows = k_factor_lu_rows<T, 8, 4, 4>;
     else if (n <= 16) p.rows = k_factor_lu_rows<T, 16, 4, 4>;
   }
-  if (!p.tc && !p.rows && use_cta_kernel(d)) {
+  const bool smem_fits = per_warp <= SMEM_MAX;
+  if (!p.tc && !p.grp && !p.rows &&
+      (use_cta_kernel(d) || s.pair_kernel == PAIR_CTA || !smem_fits) &&
+      (s.pair_kernel != PAIR_SMEM || !smem_fits)) {
     p.cta = s.sel == SEL_LU ? k_factor_cta<T, SEL_LU>
           : s.sel == SEL_QR ? k_factor_cta<T, SEL_QR> : k_factor_cta<T, SEL_QRP>;
   }
@@ -1736,6 +2164,7 @@ static void factor_levels(DevState& s, const FactorPlan<T>& p, const WorkSet<T>&
     a.first = (k == 1);
     const long np = pairs_at_level(nb, k);
     if (p.cta) p.cta<<<grid_for(np, 1, s.slab_ctas), 256, 0, st>>>(a, w.slab, s.slab_elems);
+    else if (p.grp) p.grp<<<grid_for(np, 1, p.grp_ctas), p.grp_threads, p.grp_smem, st>>>(a);
     else if (p.tc) p.tc<<<grid_for(np, 4, 148 * 16), 128, p.tc_smem, st>>>(a);
     else if (p.rows) p.rows<<<grid_for(np, 4, 148 * 16), 128, 0, st>>>(a);
     else p.smem_k<<<grid_for(np, p.wpb, 148 * 16), p.wpb * 32, p.smem, st>>>(a);

@@ -113,6 +113,18 @@ int bcr_factorize_use_thread(bcr_handle h);              /* hxx:396 */
 int bcr_solve_use_thread(bcr_handle h);                  /* hxx:398 */
 int bcr_set_num_parallel_block(bcr_handle h, int npb);   /* hxx:407-423 */
 int bcr_set_precision(bcr_handle h, int precision);      /* extension: FP64 / mixed */
+/* Pair-kernel family of the factorization (extension, no reference
+   counterpart; for tuning and tests).  AUTO picks by block size, selection and
+   precision; a forced family that does not apply to the shape falls back to
+   the next one that does (TC -> GRP -> ROWS -> CTA -> SMEM). */
+#define BCR_PAIR_AUTO 0
+#define BCR_PAIR_TC 1
+#define BCR_PAIR_GRP 2
+#define BCR_PAIR_ROWS 3
+#define BCR_PAIR_CTA 4
+#define BCR_PAIR_SMEM 5
+int bcr_set_pair_kernel(bcr_handle h, int choice);
+
 /* Iterative refinement of the mixed path (extension, no reference counterpart):
    corrections d = A^-1 r from FP64 residuals r = b - A x stop once
    |r|_inf / (|A|_inf |x|_inf + |b|_inf) <= tol (default 1e-12) or after

@@ -61,6 +61,7 @@ SHAPES = [
     (1, 1, 0, 0, 0, 0), (1, 2, 0, 0, 1, 1), (2, 1, 0, 0, 1, 1), (3, 2, 1, 1, 1, 1),
     (5, 3, 0, 2, 2, 0), (8, 4, 2, 2, 3, 3), (33, 5, 1, 0, 0, 2), (100, 8, 0, 0, 2, 2),
     (127, 16, 2, 2, 4, 4), (64, 32, 0, 0, 8, 8), (257, 7, 3, 1, 2, 5), (1000, 2, 0, 0, 0, 0),
+    (40, 20, 1, 1, 2, 2), (33, 24, 0, 0, 4, 4), (70, 32, 2, 1, 3, 4),
 ]
 
 
@@ -210,3 +211,28 @@ def test_gpu_large_blocks(dims, internal):
         assert fwd_err(xg[c, :s.ncols], xo[c, :s.ncols]) < 1e-9, (dims, internal, c)
         if s.nrows == s.ncols:  # rectangular last blocks are least-squares solves
             assert relres(o, s, xg[c], b[c]) < 1e-13
+
+
+FAMILIES = {"tc": B.PAIR_TC, "grp": B.PAIR_GRP, "rows": B.PAIR_ROWS, "cta": B.PAIR_CTA, "smem": B.PAIR_SMEM}
+
+
+@pytest.mark.parametrize("dims", [(129, 16, 2, 2, 4, 4), (97, 32, 0, 0, 8, 8), (64, 32, 2, 1, 3, 4),
+                                  (33, 16, 0, 0, 8, 8), (50, 8, 0, 0, 2, 2)])
+@pytest.mark.parametrize("family", list(FAMILIES))
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gpu_pair_kernel_families(dims, family, precision):
+    """Every pair-kernel family, forced, gives the oracle's solution."""
+    s = synth.collocation(*dims, seed=sum(dims) + 5)
+    b = synth.rhs(s, nrhs=1, seed=3)
+    o = po.Oracle(s, "LU", "LU")
+    assert o.factorize(), o.last_error()
+    xo = o.solve(b)
+    h = gpu_solver(s, "LU", "LU")
+    h.set_pair_kernel(FAMILIES[family])
+    if precision == "mixed":
+        h.set_precision(B.PRECISION_MIXED)
+    assert h.factorize(), h.last_error()
+    x = gpu_solve(h, b)
+    assert fwd_err(x[0, :s.ncols], xo[0, :s.ncols]) < (1e-10 if precision == "fp64" else 1e-8)
+    bar = 1e-13 if precision == "fp64" else 1e-12
+    assert relres(o, s, x[0], b[0]) <= bar
