@@ -167,10 +167,13 @@ class BorderedCR:
 
     def __del__(self):
         h = getattr(self, "h", None)
-        if h is None or _H is None or not h.value:
-            return  # nothing to free, or the interpreter is shutting down
-        self.L.bcr_destroy(h)
-        self.h = _H()
+        if h is None or not h.value:
+            return
+        try:
+            self.L.bcr_destroy(h)
+            h.value = None
+        except TypeError:
+            pass  # interpreter shutdown: the library bindings are already gone
 
     # ------------------------------------------------------------- errors ---
     def last_error(self) -> str:
