@@ -104,6 +104,33 @@ _SIGS = [
     ("bcr_mv_noalloc", [ct.c_int] * 6 + [ct.c_void_p] * 7 + [ct.c_double, ct.c_void_p, ct.c_double,
                                                                ct.c_void_p, ct.c_void_p, ct.c_char_p,
                                                                ct.c_int], ct.c_int),
+    ("bcr_batch_create", [ct.POINTER(ct.c_void_p)], ct.c_int),
+    ("bcr_batch_destroy", [ct.c_void_p], ct.c_int),
+    ("bcr_batch_add", [ct.c_void_p, _H], ct.c_int),
+    ("bcr_batch_size", [ct.c_void_p], ct.c_int),
+    ("bcr_batch_add_device", [ct.c_void_p] + [ct.c_int] * 6 + [ct.c_char_p], ct.c_int),
+    ("bcr_batch_matrix", [ct.c_void_p, ct.c_int] + [ct.POINTER(ct.c_void_p)] * 7, ct.c_int),
+    ("bcr_batch_system_size", [ct.c_void_p, ct.c_int, _ip, _ip], ct.c_int),
+    ("bcr_batch_device_b", [ct.c_void_p, ct.c_int], ct.c_void_p),
+    ("bcr_batch_load_device", [ct.c_void_p, ct.c_int] + [ct.c_void_p] * 7, ct.c_int),
+    ("bcr_batch_prepare", [ct.c_void_p, ct.c_int], ct.c_int),
+    ("bcr_batch_autotune", [ct.c_void_p], ct.c_int),
+    ("bcr_batch_classes", [ct.c_void_p], ct.c_int),
+    ("bcr_batch_class_info", [ct.c_void_p, ct.c_int, _ip, _ip, _ip, _ip], ct.c_int),
+    ("bcr_batch_upload", [ct.c_void_p], ct.c_int),
+    ("bcr_batch_factorize", [ct.c_void_p], ct.c_int),
+    ("bcr_batch_status", [ct.c_void_p, _ip], ct.c_int),
+    ("bcr_batch_solve", [ct.c_void_p, ct.POINTER(_dp)], ct.c_int),
+    ("bcr_batch_factorize_solve", [ct.c_void_p, ct.POINTER(_dp)], ct.c_int),
+    ("bcr_batch_set_rhs", [ct.c_void_p, ct.POINTER(_dp)], ct.c_int),
+    ("bcr_batch_device_x", [ct.c_void_p, ct.c_int], ct.c_void_p),
+    ("bcr_batch_get_x", [ct.c_void_p, ct.POINTER(_dp)], ct.c_int),
+    ("bcr_batch_graph_capture", [ct.c_void_p], ct.c_int),
+    ("bcr_batch_graph_launch", [ct.c_void_p], ct.c_int),
+    ("bcr_batch_check_status", [ct.c_void_p], ct.c_int),
+    ("bcr_batch_stream", [ct.c_void_p], ct.c_void_p),
+    ("bcr_batch_synchronize", [ct.c_void_p], ct.c_int),
+    ("bcr_batch_last_error", [ct.c_void_p], ct.c_char_p),
 ]
 
 GRAPH_FACTORIZE, GRAPH_SOLVE, GRAPH_STEP = 1, 2, 3
@@ -426,3 +453,131 @@ class BorderedCR:
 
     def graph_launch(self, what: int):
         self._check(self.L.bcr_graph_launch(self.h, what))
+
+
+class Batch:
+    """Many independent BorderedCR systems factored and solved together on the
+    device (FP64, internal LU).  The BorderedCR objects must outlive the batch."""
+
+    def __init__(self, systems=()):
+        self.L = lib()
+        self.b = ct.c_void_p()
+        self._check(self.L.bcr_batch_create(ct.byref(self.b)))
+        self.systems = []
+        for h in systems:
+            self.add(h)
+
+    def __del__(self):
+        b = getattr(self, "b", None)
+        if b is None or not b.value:
+            return
+        try:
+            self.L.bcr_batch_destroy(b)
+            b.value = None
+        except TypeError:
+            pass  # interpreter shutdown
+
+    def last_error(self) -> str:
+        return self.L.bcr_batch_last_error(self.b).decode()
+
+    def _check(self, rc: int, numerical_ok: bool = False):
+        if rc == BCR_OK:
+            return True
+        if rc == BCR_NUMERICAL and numerical_ok:
+            return False
+        raise BCRError(f"alglin_b200 batch status {rc}: {self.last_error()}")
+
+    def add(self, h: "BorderedCR"):
+        self._check(self.L.bcr_batch_add(self.b, h.h))
+        self.systems.append(h)
+
+    def add_device(self, nblock, n, qr=0, qx=0, nr=0, nx=0, last="LU"):
+        """A system whose blocks are written on the device (see matrix())."""
+        self._check(self.L.bcr_batch_add_device(self.b, nblock, n, qr, qx, nr, nx, last.encode()))
+        self.systems.append(None)
+
+    def matrix(self, i: int) -> dict:
+        """Device addresses of system i's blocks D, E, B, C, Cq, F, H (reference layout)."""
+        v = [ct.c_void_p() for _ in range(7)]
+        self._check(self.L.bcr_batch_matrix(self.b, i, *[ct.byref(x) for x in v]))
+        return dict(zip("D E B C Cq F H".split(), [x.value or 0 for x in v]))
+
+    def system_size(self, i: int):
+        r, c = ct.c_int(), ct.c_int()
+        self._check(self.L.bcr_batch_system_size(self.b, i, ct.byref(r), ct.byref(c)))
+        return r.value, c.value
+
+    def load_device(self, i: int, D=0, E=0, B=0, C=0, Cq=0, F=0, H=0):
+        """Copy system i's blocks from device addresses (ints; 0 skips a block)."""
+        self._check(self.L.bcr_batch_load_device(self.b, i, D or None, E or None, B or None, C or None,
+                                                 Cq or None, F or None, H or None))
+
+    def device_b(self, i: int) -> int:
+        return self.L.bcr_batch_device_b(self.b, i) or 0
+
+    def __len__(self):
+        return self.L.bcr_batch_size(self.b)
+
+    def prepare(self, autotune: bool = False):
+        self._check(self.L.bcr_batch_prepare(self.b, 1 if autotune else 0))
+
+    def autotune(self):
+        """Time every applicable kernel family and chunk on the loaded systems; keep the fastest."""
+        self._check(self.L.bcr_batch_autotune(self.b))
+
+    def classes(self):
+        """[(n, systems, family, pairs per CTA)] of every kernel group."""
+        out = []
+        for c in range(self.L.bcr_batch_classes(self.b)):
+            v = [ct.c_int() for _ in range(4)]
+            self._check(self.L.bcr_batch_class_info(self.b, c, *[ct.byref(x) for x in v]))
+            out.append(tuple(x.value for x in v))
+        return out
+
+    def upload(self):
+        self._check(self.L.bcr_batch_upload(self.b))
+
+    def factorize(self) -> bool:
+        return self._check(self.L.bcr_batch_factorize(self.b), numerical_ok=True)
+
+    def status(self) -> np.ndarray:
+        codes = np.zeros(len(self), dtype=np.int32)
+        self._check(self.L.bcr_batch_status(self.b, codes.ctypes.data_as(_ip)))
+        return codes
+
+    @staticmethod
+    def _ptrs(xs):
+        for x in xs:
+            assert x.dtype == np.float64 and x.flags.c_contiguous
+        return (_dp * len(xs))(*[x.ctypes.data_as(_dp) for x in xs])
+
+    def solve(self, xs) -> bool:
+        """In place on one float64 vector (length >= max(nrows, ncols)) per system."""
+        return self._check(self.L.bcr_batch_solve(self.b, self._ptrs(xs)), numerical_ok=True)
+
+    def factorize_solve(self, xs) -> bool:
+        return self._check(self.L.bcr_batch_factorize_solve(self.b, self._ptrs(xs)), numerical_ok=True)
+
+    def set_rhs(self, bs):
+        self._check(self.L.bcr_batch_set_rhs(self.b, self._ptrs(bs)))
+
+    def get_x(self, xs):
+        self._check(self.L.bcr_batch_get_x(self.b, self._ptrs(xs)))
+
+    def device_x(self, i: int) -> int:
+        return self.L.bcr_batch_device_x(self.b, i) or 0
+
+    def graph_capture(self):
+        self._check(self.L.bcr_batch_graph_capture(self.b), numerical_ok=False)
+
+    def graph_launch(self):
+        self._check(self.L.bcr_batch_graph_launch(self.b))
+
+    def check_status(self) -> bool:
+        return self._check(self.L.bcr_batch_check_status(self.b), numerical_ok=True)
+
+    def stream(self) -> int:
+        return self.L.bcr_batch_stream(self.b) or 0
+
+    def synchronize(self):
+        self._check(self.L.bcr_batch_synchronize(self.b))

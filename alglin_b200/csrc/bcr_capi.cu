@@ -1241,3 +1241,605 @@ int bcr_synchronize(bcr_handle h) {
 }
 
 }  // extern "C"
+
+// ===================================================================== batch
+// Many independent BorderedCR systems solved together.  The handles are host
+// containers (their loaders fill the host mirrors); the batch packs every
+// system into one device arena for the loaded matrices and one for the
+// working arrays, groups the systems by pair-kernel instance, and runs each
+// level of every system of a group in one launch.
+namespace {
+
+struct BatchTune {
+  int n, nrm, nxm, fam, chunk;
+};
+std::vector<BatchTune> g_batch_tuning;  // in-process autotuner cache
+
+int default_family(const Dims& d) {
+  if ((d.n == 8 || d.n == 16) && bcr::batch_family_ok(bcr::PAIR_TC, d)) return bcr::PAIR_TC;
+  if (d.n == 32 && bcr::batch_family_ok(bcr::PAIR_GRP, d)) return bcr::PAIR_GRP;
+  if (bcr::batch_family_ok(bcr::PAIR_ROWS, d)) return bcr::PAIR_ROWS;
+  return -1;
+}
+
+struct Bump {
+  size_t top = 0;
+  size_t take(size_t bytes) {
+    const size_t o = top;
+    top += (bytes + 255) & ~size_t(255);
+    return o;
+  }
+};
+
+}  // namespace
+
+struct bcr_batch_s {
+  std::vector<bcr_handle> hs;      // null for a system that lives only on the device
+  std::vector<Dims> dims;          // per system
+  std::vector<int> last_sel;       // per system: last-block solver
+  std::vector<size_t> in_len;      // per system: bytes of its loaded matrix in d_in
+  std::vector<bcr::DevState> sys;
+  std::vector<bcr::BatchClass> cls;
+  std::vector<std::vector<int>> members;
+  std::vector<int> cls_of;
+  unsigned char* d_in = nullptr;   // loaded matrices of every system
+  unsigned char* d_work = nullptr; // working arrays, factors, last blocks
+  double* h_in = nullptr;          // pinned staging of d_in
+  size_t in_bytes = 0, work_bytes = 0;
+  std::vector<size_t> in_off;      // per system: byte offset of its D0 in d_in
+  double* d_x = nullptr;           // right-hand sides / solutions, packed
+  double* d_b = nullptr;           // copy of the right-hand sides (graph replay)
+  double* h_x = nullptr;           // pinned staging of d_x
+  std::vector<size_t> x_off;       // per system: element offset in d_x
+  size_t x_elems = 0;
+  bcr::StatusWords* d_st = nullptr;
+  std::vector<bcr::StatusWords> h_st;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  bool prepared = false, factorized = false;
+  std::string err = "no error";
+
+  int fail(int code, const std::string& m) {
+    err = m;
+    return code;
+  }
+  int cuda_fail(cudaError_t e, const char* where) {
+    return fail(BCR_CUDA_ERROR, fmt("alglin_b200 batch: CUDA error in %s: %s\n", where, cudaGetErrorString(e)));
+  }
+
+  void release() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    for (auto& c : cls) bcr::batch_free(c);
+    cls.clear();
+    members.clear();
+    if (d_in) cudaFree(d_in);
+    if (d_work) cudaFree(d_work);
+    if (d_x) cudaFree(d_x);
+    if (d_b) cudaFree(d_b);
+    if (d_st) cudaFree(d_st);
+    if (h_in) cudaFreeHost(h_in);
+    if (h_x) cudaFreeHost(h_x);
+    d_in = d_work = nullptr;
+    d_x = d_b = h_in = h_x = nullptr;
+    d_st = nullptr;
+    prepared = factorized = false;
+  }
+
+  int L(size_t i) const { return std::max(dims[i].n * (dims[i].nblock + 1) + dims[i].qr + dims[i].nr,
+                                          dims[i].n * (dims[i].nblock + 1) + dims[i].qx + dims[i].nx); }
+
+  // pack every handle's host mirrors into the pinned staging buffer
+  void pack_inputs() {
+    for (size_t i = 0; i < hs.size(); ++i) {
+      bcr_handle h = hs[i];
+      if (!h) continue;
+      unsigned char* base = reinterpret_cast<unsigned char*>(h_in);
+      const bcr::DevState& s = sys[i];
+      auto put = [&](const double* dev, const std::vector<double>& v) {
+        if (!v.empty())
+          std::memcpy(base + (reinterpret_cast<const unsigned char*>(dev) - d_in), v.data(), v.size() * 8);
+      };
+      put(s.D0, h->hD); put(s.E0, h->hE); put(s.B0, h->hB); put(s.C0, h->hC);
+      put(s.Cq, h->hCq); put(s.F0, h->hF); put(s.H, h->hH);
+    }
+  }
+
+  // one copy per run of consecutive handle systems (device-only systems keep
+  // what the caller wrote into their part of the arena)
+  int upload_inputs() {
+    if (!h_in) return BCR_OK;
+    pack_inputs();
+    cudaError_t e = cudaSuccess;
+    for (size_t i = 0; i < hs.size() && e == cudaSuccess;) {
+      if (!hs[i]) { ++i; continue; }
+      size_t j = i;
+      while (j + 1 < hs.size() && hs[j + 1]) ++j;
+      const size_t b0 = in_off[i], b1 = in_off[j] + in_len[j];
+      e = cudaMemcpyAsync(d_in + b0, reinterpret_cast<unsigned char*>(h_in) + b0, b1 - b0,
+                          cudaMemcpyHostToDevice, stream);
+      i = j + 1;
+    }
+    return e == cudaSuccess ? BCR_OK : cuda_fail(e, "matrix upload");
+  }
+
+  int prepare(int autotune);
+  int tune_class(size_t c);
+  void enqueue_factorize() {
+    for (auto& c : cls) bcr::batch_factorize(c, stream);
+  }
+  void enqueue_solve() {
+    for (auto& c : cls) bcr::batch_solve(c, stream);
+  }
+  int read_status() {
+    cudaError_t e = cudaMemcpyAsync(h_st.data(), d_st, h_st.size() * sizeof(bcr::StatusWords),
+                                    cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(e, "batch status");
+    for (size_t i = 0; i < h_st.size(); ++i)
+      if (h_st[i].code != 0) {
+        factorized = false;
+        return fail(BCR_NUMERICAL,
+                    fmt("batch system %zu: factorization failed (code %d, block %d, info %d)\n", i,
+                        h_st[i].code, h_st[i].block, h_st[i].info));
+      }
+    factorized = true;
+    return BCR_OK;
+  }
+};
+
+int bcr_batch_s::prepare(int autotune) {
+  release();
+  if (hs.empty()) return fail(BCR_BAD_ARGUMENT, "bcr_batch_prepare: the batch is empty\n");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(BCR_CUDA_ERROR, "alglin_b200: no CUDA device is available (the solver has no CPU path)\n");
+  if (!stream) {
+    cudaError_t e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+  }
+  const size_t ns = hs.size();
+  sys.assign(ns, bcr::DevState{});
+  dims.resize(ns);
+  last_sel.resize(ns);
+  in_off.assign(ns, 0);
+  x_off.assign(ns, 0);
+  cls_of.assign(ns, -1);
+  // ---------------------------------------------------------- validation
+  std::vector<int> fam(ns);
+  bool any_handle = false;
+  for (size_t i = 0; i < ns; ++i) {
+    bcr_handle h = hs[i];
+    if (h) {
+      any_handle = true;
+      if (!h->allocated) return fail(BCR_BAD_ARGUMENT, fmt("batch system %zu: allocate() was not called\n", i));
+      if (h->sel != bcr::SEL_LU)
+        return fail(BCR_BAD_ARGUMENT, fmt("batch system %zu: batches support the internal LU selection only\n", i));
+      if (h->precision != BCR_PRECISION_FP64)
+        return fail(BCR_BAD_ARGUMENT, fmt("batch system %zu: batches run in FP64\n", i));
+      dims[i] = h->d;
+      last_sel[i] = h->sel_last;
+    }
+    if (last_sel[i] != bcr::LAST_LU && last_sel[i] != bcr::LAST_QR)
+      return fail(BCR_BAD_ARGUMENT, fmt("batch system %zu: last block solver '%s' is not available on the device\n",
+                                        i, kLastName[last_sel[i]]));
+    fam[i] = default_family(dims[i]);
+    if (fam[i] < 0)
+      return fail(BCR_BAD_ARGUMENT,
+                  fmt("batch system %zu: block size n=%d with nr=%d, nx=%d has no batched pair kernel\n", i,
+                      dims[i].n, dims[i].nr, dims[i].nx));
+  }
+  // ------------------------------------------------------------ layout
+  Bump in, work;
+  struct Off { size_t D0, E0, B0, C0, Cq, F0, H, D, E, B, C, T, P, Rbuf, Fbuf, XB, Ffin, Hl, tau, piv; };
+  std::vector<Off> off(ns);
+  in_len.assign(ns, 0);
+  for (size_t i = 0; i < ns; ++i) {
+    const Dims& d = dims[i];
+    const size_t nb = d.nblock, n = d.n, nr = d.nr, nx = d.nx, qx = d.qx, qr = d.qr;
+    const size_t Lb = std::max(d.Nr, d.Nc);
+    Off& o = off[i];
+    o.D0 = in.take(nb * n * n * 8); o.E0 = in.take(nb * n * n * 8); o.B0 = in.take(nb * n * nx * 8);
+    o.C0 = in.take((nb + 1) * nr * n * 8); o.Cq = in.take(nr * qx * 8); o.F0 = in.take(nr * nx * 8);
+    o.H = in.take((n + qr) * d.Nc * 8);
+    in_len[i] = in.top - o.D0;
+    o.D = work.take(nb * n * n * 8); o.E = work.take(nb * n * n * 8); o.B = work.take(nb * n * nx * 8);
+    o.C = work.take((nb + 1) * nr * n * 8); o.T = work.take(nb * (2 * n * n + n) * 8);
+    o.P = work.take(nb * 3 * n); o.Rbuf = work.take(nb * nr * n * 8); o.Fbuf = work.take(nb * nr * nx * 8);
+    o.XB = work.take(nb * nr * 8); o.Ffin = work.take(std::max<size_t>(nr * nx, 1) * 8);
+    o.Hl = work.take((size_t)d.Nr * d.Nc * 8); o.tau = work.take(Lb * 8); o.piv = work.take(Lb * 4);
+    x_off[i] = x_elems;
+    x_elems += ((size_t)L(i) + 31) & ~size_t(31);
+  }
+  in_bytes = std::max<size_t>(in.top, 256);
+  work_bytes = std::max<size_t>(work.top, 256);
+  cudaError_t e = cudaMalloc(&d_in, in_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&d_work, work_bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&d_x, std::max<size_t>(x_elems, 1) * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&d_b, std::max<size_t>(x_elems, 1) * 8);
+  if (e == cudaSuccess) e = cudaMalloc(&d_st, ns * sizeof(bcr::StatusWords));
+  if (e == cudaSuccess && any_handle) e = cudaMallocHost(&h_in, in_bytes);
+  if (e == cudaSuccess) e = cudaMallocHost(&h_x, std::max<size_t>(x_elems, 1) * 8);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    release();
+    return cuda_fail(e, "batch allocation");
+  }
+  if (h_in) std::memset(h_in, 0, in_bytes);
+  cudaMemsetAsync(d_in, 0, in_bytes, stream);
+  std::memset(h_x, 0, std::max<size_t>(x_elems, 1) * 8);
+  h_st.assign(ns, bcr::StatusWords{});
+  for (size_t i = 0; i < ns; ++i) {
+    const Off& o = off[i];
+    bcr::DevState& s = sys[i];
+    auto I = [&](size_t b) { return reinterpret_cast<double*>(d_in + b); };
+    auto W = [&](size_t b) { return reinterpret_cast<double*>(d_work + b); };
+    s.d = dims[i];
+    s.sel = bcr::SEL_LU;
+    s.sel_last = last_sel[i];
+    s.D0 = I(o.D0); s.E0 = I(o.E0); s.B0 = I(o.B0); s.C0 = I(o.C0); s.Cq = I(o.Cq); s.F0 = I(o.F0); s.H = I(o.H);
+    s.D = W(o.D); s.E = W(o.E); s.B = W(o.B); s.C = W(o.C); s.T = W(o.T);
+    s.P = d_work + o.P;
+    s.Rbuf = W(o.Rbuf); s.Fbuf = W(o.Fbuf); s.XB = W(o.XB); s.xb_cap = 1;
+    s.Ffin = W(o.Ffin); s.Hl = W(o.Hl); s.tau_l = W(o.tau); s.piv_l = reinterpret_cast<int*>(d_work + o.piv);
+    s.st = d_st + i;
+    s.bx = d_x + x_off[i];
+    s.bldx = L(i);
+    in_off[i] = o.D0;
+  }
+  cudaMemsetAsync(d_work, 0, work_bytes, stream);
+  int rc = upload_inputs();
+  if (rc) return rc;
+  // ----------------------------------------------------------- classes
+  std::vector<std::pair<long, int>> keys;  // (n * 8 + family) -> class
+  for (size_t i = 0; i < ns; ++i) {
+    const long key = (long)dims[i].n * 8 + fam[i];
+    int c = -1;
+    for (auto& kv : keys)
+      if (kv.first == key) c = kv.second;
+    if (c < 0) {
+      c = (int)members.size();
+      keys.push_back({key, c});
+      members.emplace_back();
+    }
+    members[c].push_back((int)i);
+    cls_of[i] = c;
+  }
+  cls.assign(members.size(), bcr::BatchClass{});
+  for (size_t c = 0; c < members.size(); ++c) {
+    cls[c].fam = fam[members[c][0]];
+    std::vector<bcr::DevState> v;
+    for (int i : members[c]) v.push_back(sys[i]);
+    // a tuned choice for this shape, if one is cached
+    const Dims& d0 = dims[members[c][0]];
+    int nrm = 0, nxm = 0;
+    for (int i : members[c]) { nrm = std::max(nrm, dims[i].nr); nxm = std::max(nxm, dims[i].nx); }
+    for (const auto& t : g_batch_tuning)
+      if (t.n == d0.n && t.nrm == nrm && t.nxm == nxm) { cls[c].fam = t.fam; cls[c].chunk = t.chunk; }
+    if (bcr::batch_build(cls[c], v, 1)) {
+      release();
+      return fail(BCR_CUDA_ERROR, "alglin_b200 batch: table upload failed\n");
+    }
+  }
+  e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return cuda_fail(e, "batch prepare");
+  prepared = true;
+  if (autotune)
+    for (size_t c = 0; c < cls.size(); ++c)
+      if ((rc = tune_class(c))) return rc;
+  return BCR_OK;
+}
+
+// time every applicable (family, chunk) on this class's own systems and keep
+// the fastest; the choice is cached for later batches of the same shape
+int bcr_batch_s::tune_class(size_t ci) {
+  bcr::BatchClass& c = cls[ci];
+  std::vector<bcr::DevState> v;
+  int nrm = 0, nxm = 0;
+  for (int i : members[ci]) {
+    v.push_back(sys[i]);
+    nrm = std::max(nrm, sys[i].d.nr);
+    nxm = std::max(nxm, sys[i].d.nx);
+  }
+  Dims dm = sys[members[ci][0]].d;
+  dm.nr = nrm;
+  dm.nx = nxm;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int bf = c.fam, bc = c.chunk;
+  for (int f : {bcr::PAIR_TC, bcr::PAIR_GRP, bcr::PAIR_ROWS}) {
+    if (!bcr::batch_family_ok(f, dm)) continue;
+    for (int ch : {2, 4, 8, 16}) {
+      c.fam = f;
+      c.chunk = ch;
+      if (bcr::batch_build(c, v, 1)) return fail(BCR_CUDA_ERROR, "alglin_b200 batch: table upload failed\n");
+      bcr::batch_factorize(c, stream);  // warm-up (also sets kernel attributes)
+      cudaEventRecord(e0, stream);
+      for (int r = 0; r < 3; ++r) bcr::batch_factorize(c, stream);
+      cudaEventRecord(e1, stream);
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e != cudaSuccess) return cuda_fail(e, "batch autotune");
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) { best = ms; bf = f; bc = ch; }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c.fam = bf;
+  c.chunk = bc;
+  if (bcr::batch_build(c, v, 1)) return fail(BCR_CUDA_ERROR, "alglin_b200 batch: table upload failed\n");
+  bool found = false;
+  for (auto& t : g_batch_tuning)
+    if (t.n == dm.n && t.nrm == nrm && t.nxm == nxm) { t.fam = bf; t.chunk = bc; found = true; }
+  if (!found) g_batch_tuning.push_back({dm.n, nrm, nxm, bf, bc});
+  return BCR_OK;
+}
+
+#define B_CHECK(b)                                 \
+  do {                                             \
+    if (!(b)) return BCR_BAD_ARGUMENT;             \
+  } while (0)
+#define B_READY(b)                                                                            \
+  do {                                                                                        \
+    B_CHECK(b);                                                                               \
+    if (!(b)->prepared) return (b)->fail(BCR_BAD_ARGUMENT, "bcr_batch: prepare() must be called first\n"); \
+  } while (0)
+
+extern "C" {
+
+int bcr_batch_create(bcr_batch* out) {
+  if (!out) return BCR_BAD_ARGUMENT;
+  *out = new bcr_batch_s;
+  return BCR_OK;
+}
+
+int bcr_batch_destroy(bcr_batch b) {
+  if (!b) return BCR_OK;
+  b->release();
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return BCR_OK;
+}
+
+int bcr_batch_add(bcr_batch b, bcr_handle h) {
+  B_CHECK(b);
+  if (!h) return b->fail(BCR_BAD_ARGUMENT, "bcr_batch_add: null handle\n");
+  b->release();
+  b->hs.push_back(h);
+  b->dims.push_back(h->d);
+  b->last_sel.push_back(h->sel_last);
+  return BCR_OK;
+}
+
+int bcr_batch_add_device(bcr_batch b, int nblock, int n, int qr, int qx, int nr, int nx, const char* last) {
+  B_CHECK(b);
+  if (nblock < 1 || n < 1 || qr < 0 || qx < 0 || nr < 0 || nx < 0)
+    return b->fail(BCR_BAD_ARGUMENT, fmt("bcr_batch_add_device( nblock=%d, n=%d, qr=%d, qx=%d, nr=%d, nx=%d ) bad sizes\n",
+                                         nblock, n, qr, qx, nr, nx));
+  const std::string ls = last ? last : "LU";
+  int sl;
+  if (ls == "LU") sl = bcr::LAST_LU;
+  else if (ls == "QR") sl = bcr::LAST_QR;
+  else return b->fail(BCR_BAD_ARGUMENT, fmt("bcr_batch_add_device: last block solver '%s' is not available\n", ls.c_str()));
+  b->release();
+  Dims d{};
+  d.nblock = nblock; d.n = n; d.qr = qr; d.qx = qx; d.nr = nr; d.nx = nx;
+  d.Nr = 2 * n + qr + nr;
+  d.Nc = 2 * n + qx + nx;
+  b->hs.push_back(nullptr);
+  b->dims.push_back(d);
+  b->last_sel.push_back(sl);
+  return BCR_OK;
+}
+
+int bcr_batch_matrix(bcr_batch b, int i, double** D, double** E, double** B, double** C, double** Cq,
+                     double** F, double** H) {
+  B_READY(b);
+  if (i < 0 || i >= (int)b->hs.size()) return b->fail(BCR_BAD_ARGUMENT, "bcr_batch_matrix: bad system index\n");
+  const bcr::DevState& s = b->sys[i];
+  if (D) *D = s.D0;
+  if (E) *E = s.E0;
+  if (B) *B = s.B0;
+  if (C) *C = s.C0;
+  if (Cq) *Cq = s.Cq;
+  if (F) *F = s.F0;
+  if (H) *H = s.H;
+  return BCR_OK;
+}
+
+int bcr_batch_load_device(bcr_batch b, int i, const double* D, const double* E, const double* B, const double* C,
+                          const double* Cq, const double* F, const double* H) {
+  B_READY(b);
+  if (i < 0 || i >= (int)b->hs.size()) return b->fail(BCR_BAD_ARGUMENT, "bcr_batch_load_device: bad system index\n");
+  const Dims& d = b->dims[i];
+  const bcr::DevState& s = b->sys[i];
+  const size_t nb = d.nblock, n = d.n;
+  const struct { double* dst; const double* src; size_t count; } cp[] = {
+      {s.D0, D, nb * n * n}, {s.E0, E, nb * n * n}, {s.B0, B, nb * n * d.nx},
+      {s.C0, C, (nb + 1) * d.nr * n}, {s.Cq, Cq, (size_t)d.nr * d.qx}, {s.F0, F, (size_t)d.nr * d.nx},
+      {s.H, H, (size_t)(n + d.qr) * d.Nc}};
+  for (const auto& c : cp)
+    if (c.src && c.count) {
+      cudaError_t e = cudaMemcpyAsync(c.dst, c.src, c.count * 8, cudaMemcpyDeviceToDevice, b->stream);
+      if (e != cudaSuccess) return b->cuda_fail(e, "bcr_batch_load_device");
+    }
+  return BCR_OK;
+}
+
+double* bcr_batch_device_b(bcr_batch b, int i) {
+  if (!b || !b->prepared || i < 0 || i >= (int)b->hs.size()) return nullptr;
+  return b->d_b + b->x_off[i];
+}
+
+int bcr_batch_system_size(bcr_batch b, int i, int* nrows, int* ncols) {
+  B_CHECK(b);
+  if (i < 0 || i >= (int)b->dims.size()) return b->fail(BCR_BAD_ARGUMENT, "bcr_batch_system_size: bad index\n");
+  const Dims& d = b->dims[i];
+  if (nrows) *nrows = d.n * (d.nblock + 1) + d.qr + d.nr;
+  if (ncols) *ncols = d.n * (d.nblock + 1) + d.qx + d.nx;
+  return BCR_OK;
+}
+
+int bcr_batch_size(bcr_batch b) { return b ? (int)b->hs.size() : 0; }
+
+int bcr_batch_prepare(bcr_batch b, int autotune) {
+  B_CHECK(b);
+  return b->prepare(autotune);
+}
+
+int bcr_batch_autotune(bcr_batch b) {
+  B_READY(b);
+  if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  for (size_t c = 0; c < b->cls.size(); ++c) {
+    int rc = b->tune_class(c);
+    if (rc) return rc;
+  }
+  return BCR_OK;
+}
+
+int bcr_batch_classes(bcr_batch b) { return b && b->prepared ? (int)b->cls.size() : 0; }
+
+int bcr_batch_class_info(bcr_batch b, int c, int* n, int* nsys, int* family, int* chunk) {
+  B_READY(b);
+  if (c < 0 || c >= (int)b->cls.size()) return b->fail(BCR_BAD_ARGUMENT, "bcr_batch_class_info: bad class\n");
+  if (n) *n = b->cls[c].n;
+  if (nsys) *nsys = b->cls[c].nsys;
+  if (family) *family = b->cls[c].fam;
+  if (chunk) *chunk = b->cls[c].chunk;
+  return BCR_OK;
+}
+
+int bcr_batch_upload(bcr_batch b) {
+  B_READY(b);
+  int rc = b->upload_inputs();
+  if (rc) return rc;
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  return e == cudaSuccess ? BCR_OK : b->cuda_fail(e, "batch upload");
+}
+
+int bcr_batch_factorize(bcr_batch b) {
+  B_READY(b);
+  b->enqueue_factorize();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return b->cuda_fail(e, "batch factorize");
+  return b->read_status();
+}
+
+int bcr_batch_status(bcr_batch b, int* codes) {
+  B_READY(b);
+  for (size_t i = 0; i < b->h_st.size(); ++i) codes[i] = b->h_st[i].code;
+  return BCR_OK;
+}
+
+static int batch_rhs_in(bcr_batch b, double* const* x) {
+  for (size_t i = 0; i < b->hs.size(); ++i)
+    std::memcpy(b->h_x + b->x_off[i], x[i], (size_t)b->L(i) * 8);
+  cudaError_t e = cudaMemcpyAsync(b->d_x, b->h_x, b->x_elems * 8, cudaMemcpyHostToDevice, b->stream);
+  return e == cudaSuccess ? BCR_OK : b->cuda_fail(e, "batch rhs upload");
+}
+
+static int batch_rhs_out(bcr_batch b, double* const* x) {
+  cudaError_t e = cudaMemcpyAsync(b->h_x, b->d_x, b->x_elems * 8, cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return b->cuda_fail(e, "batch solution download");
+  for (size_t i = 0; i < b->hs.size(); ++i)
+    std::memcpy(x[i], b->h_x + b->x_off[i], (size_t)b->L(i) * 8);
+  return BCR_OK;
+}
+
+int bcr_batch_solve(bcr_batch b, double* const* x) {
+  B_READY(b);
+  if (!x) return b->fail(BCR_BAD_ARGUMENT, "bcr_batch_solve: null vector list\n");
+  if (!b->factorized) return b->fail(BCR_NUMERICAL, "bcr_batch_solve: the batch is not factorized\n");
+  int rc = batch_rhs_in(b, x);
+  if (rc) return rc;
+  b->enqueue_solve();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return b->cuda_fail(e, "batch solve");
+  return batch_rhs_out(b, x);
+}
+
+int bcr_batch_factorize_solve(bcr_batch b, double* const* x) {
+  B_READY(b);
+  if (!x) return b->fail(BCR_BAD_ARGUMENT, "bcr_batch_factorize_solve: null vector list\n");
+  int rc = b->upload_inputs();
+  if (rc) return rc;
+  if ((rc = batch_rhs_in(b, x))) return rc;
+  b->enqueue_factorize();
+  b->enqueue_solve();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return b->cuda_fail(e, "batch factorize_solve");
+  if ((rc = b->read_status())) return rc;
+  return batch_rhs_out(b, x);
+}
+
+double* bcr_batch_device_x(bcr_batch b, int i) {
+  if (!b || !b->prepared || i < 0 || i >= (int)b->hs.size()) return nullptr;
+  return b->d_x + b->x_off[i];
+}
+
+int bcr_batch_set_rhs(bcr_batch b, const double* const* rhs) {
+  B_READY(b);
+  for (size_t i = 0; i < b->hs.size(); ++i)
+    std::memcpy(b->h_x + b->x_off[i], rhs[i], (size_t)b->L(i) * 8);
+  cudaError_t e = cudaMemcpyAsync(b->d_b, b->h_x, b->x_elems * 8, cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_x, b->d_b, b->x_elems * 8, cudaMemcpyDeviceToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  return e == cudaSuccess ? BCR_OK : b->cuda_fail(e, "batch rhs");
+}
+
+int bcr_batch_get_x(bcr_batch b, double* const* x) {
+  B_READY(b);
+  return batch_rhs_out(b, x);
+}
+
+int bcr_batch_graph_capture(bcr_batch b) {
+  B_READY(b);
+  // eager run first: kernel attributes, status check
+  cudaMemcpyAsync(b->d_x, b->d_b, b->x_elems * 8, cudaMemcpyDeviceToDevice, b->stream);
+  b->enqueue_factorize();
+  b->enqueue_solve();
+  int rc = b->read_status();
+  if (rc) return rc;
+  if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) return b->cuda_fail(e, "cudaStreamBeginCapture");
+  cudaMemcpyAsync(b->d_x, b->d_b, b->x_elems * 8, cudaMemcpyDeviceToDevice, b->stream);
+  b->enqueue_factorize();
+  b->enqueue_solve();
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(b->stream, &g);
+  if (e != cudaSuccess) { cudaGetLastError(); return b->cuda_fail(e, "cudaStreamEndCapture"); }
+  e = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { b->graph = nullptr; return b->cuda_fail(e, "cudaGraphInstantiate"); }
+  return BCR_OK;
+}
+
+int bcr_batch_graph_launch(bcr_batch b) {
+  B_READY(b);
+  if (!b->graph) return b->fail(BCR_BAD_ARGUMENT, "bcr_batch_graph_launch: no graph captured\n");
+  cudaError_t e = cudaGraphLaunch(b->graph, b->stream);
+  return e == cudaSuccess ? BCR_OK : b->cuda_fail(e, "cudaGraphLaunch");
+}
+
+int bcr_batch_check_status(bcr_batch b) {
+  B_READY(b);
+  return b->read_status();
+}
+
+void* bcr_batch_stream(bcr_batch b) { return b ? b->stream : nullptr; }
+
+int bcr_batch_synchronize(bcr_batch b) {
+  B_CHECK(b);
+  if (!b->stream) return BCR_OK;
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  return e == cudaSuccess ? BCR_OK : b->cuda_fail(e, "batch synchronize");
+}
+
+const char* bcr_batch_last_error(bcr_batch b) { return b ? b->err.c_str() : "invalid batch"; }
+
+}  // extern "C"

@@ -46,6 +46,12 @@ __host__ __device__ inline long pairs_at_level(int nblock, int k) {
   return nblock > k ? (long)(nblock - k - 1) / (2L * k) + 1 : 0;
 }
 
+// one CTA of a batched launch: pairs [q0, q1) of system `sys` at the level
+struct BatchCta {
+  int sys, pad;
+  long q0, q1;
+};
+
 // status layout: [0] code, [1] block index, [2] LAPACK-style info, [3] level
 struct StatusWords { int code, block, info, level; };
 

@@ -1,6 +1,7 @@
 // Host-side launchers for the BorderedCR device kernels (internal interface
 // between the C-ABI layer and the CUDA translation units).
 #pragma once
+#include <vector>
 #include <cuda_runtime.h>
 
 #include "bcr_common.cuh"
@@ -14,6 +15,8 @@ struct DevState {
   int sel_last;   // LastKind actually used (after fallback)
   int use_tc;     // allow the FP64 tensor-core pair kernel
   int pair_kernel;  // PairKernel: AUTO, or a forced pair-kernel family
+  double* bx;       // batch: right-hand side / solution of this system
+  int bldx;         // batch: its leading dimension
   // loaded matrix (reference layout), never modified on the device
   double *D0, *E0, *B0, *C0, *Cq, *F0, *H;
   // working blocks / factors
@@ -65,5 +68,34 @@ void launch_axpy(double* y, const double* x, long len, cudaStream_t st);
 
 // smem bytes needed by one warp of the panel kernel; 0 if it does not fit
 size_t panel_smem_per_warp(const Dims& d, int elem_bytes);
+
+// ---------------------------------------------------------------------------
+// batches of independent systems.  Systems that run the same pair-kernel
+// instance form a class; every launch of a class covers all its systems
+// through a CTA -> (system, pair range) map.
+// ---------------------------------------------------------------------------
+struct BatchClass {
+  int nsys = 0;
+  int fam = PAIR_AUTO;   // PAIR_TC, PAIR_GRP or PAIR_ROWS
+  int chunk = 8;         // pairs per CTA of the factorization launches
+  int n = 0, nrm = 0, nxm = 0, levels = 0, nrhs = 1;
+  size_t last_smem = 0;
+  void* fa = nullptr;    // device FactorArgs<double>[nsys]
+  void* sf = nullptr;    // device SweepArgs<double>[nsys], forward layout
+  void* sb = nullptr;    // device SweepArgs<double>[nsys], backward layout
+  void* ld = nullptr;    // device last-block descriptors [nsys]
+  BatchCta* fmap = nullptr;  // device: factorization chunks of every level
+  BatchCta* smap = nullptr;  // device: sweep chunks of every level
+  std::vector<long> foff, fcnt, soff, scnt;
+};
+
+// the pair-kernel families a batch class may use for systems of shape d (LU)
+bool batch_family_ok(int fam, const Dims& d);
+// tables and maps of one class; sys[i] holds the device pointers of system i
+// (x, ldx: its right-hand side; st: its status word)
+int batch_build(BatchClass& c, const std::vector<DevState>& sys, int nrhs);
+void batch_free(BatchClass& c);
+void batch_factorize(BatchClass& c, cudaStream_t st);
+void batch_solve(BatchClass& c, cudaStream_t st);
 
 }  // namespace bcr

@@ -21,6 +21,7 @@
 // C_jp); dC_jpp goes to a per-block scratch slot and is added to C_jpp by
 // k_border_fix after the level, because C_jpp is also C_jp of pair j+2k.
 // The F updates dF go to a per-block slot and are summed in a fixed order.
+#include <cmath>
 #include <cstdio>
 
 #include "bcr_device.h"
@@ -54,6 +55,30 @@ struct FactorArgs {
 template <typename T>
 __device__ __forceinline__ T ldsrc(bool first, const double* orig, const T* work, size_t i) {
   return first ? T(orig[i]) : work[i];
+}
+
+// Pair range of one worker (warp or CTA).  Single system: a grid-stride loop
+// over the level's pairs.  Batch: CTA b works on pairs [q0, q1) of system
+// cmap[b].sys, whose arguments come from the table; the level is the batch's.
+__device__ __forceinline__ void take_level(FactorArgs<float>& a, const FactorArgs<float>& a0) { a.k = a0.k; a.first = a0.first; }
+__device__ __forceinline__ void take_level(FactorArgs<double>& a, const FactorArgs<double>& a0) { a.k = a0.k; a.first = a0.first; }
+
+template <typename A>
+__device__ __forceinline__ void pair_range(const A& a0, const A* tab, const BatchCta* cmap, int workers, int worker,
+                                           A& a, long& q0, long& q1, long& qs) {
+  if (cmap) {
+    const BatchCta c = cmap[blockIdx.x];
+    a = tab[c.sys];
+    take_level(a, a0);
+    q0 = c.q0 + worker;
+    q1 = c.q1;
+    qs = workers;
+  } else {
+    a = a0;
+    q0 = (long)blockIdx.x * workers + worker;
+    q1 = pairs_at_level(a.d.nblock, a.k);
+    qs = (long)gridDim.x * workers;
+  }
 }
 
 // the same through the read-only path; every load of a pair kernel's load
@@ -212,9 +237,13 @@ __device__ int warp_eliminate_qr(T* W, int ldw, int n, int R, int NC, int* ipiv,
 }
 
 template <typename T, int SEL>
-__global__ void __launch_bounds__(WARPS_PANEL * 32) k_factor_level(FactorArgs<T> a) {
+__global__ void __launch_bounds__(WARPS_PANEL * 32) k_factor_level(FactorArgs<T> a0, const FactorArgs<T>* tab,
+                                                               const BatchCta* cmap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  FactorArgs<T> a;
+  long q0, q1, qs;
+  pair_range(a0, tab, cmap, wpb, warp, a, q0, q1, qs);
   const Dims d = a.d;
   const int n = d.n, nr = d.nr, nx = d.nx, nb = d.nblock;
   const int n2 = 2 * n, R = n2 + nr, NC = 3 * n + nx, ldw = a.ldw;
@@ -224,10 +253,9 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_factor_level(FactorArgs<T>
   T* tau = reinterpret_cast<T*>(smem_raw) + wpb * wsz + warp * n;
   int* ipiv = reinterpret_cast<int*>(reinterpret_cast<T*>(smem_raw) + wpb * wsz + wpb * n) + warp * n;
   const int k = a.k;
-  const long np = pairs_at_level(nb, k);
   const bool first = a.first != 0;
 
-  for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
+  for (long q = q0; q < q1; q += qs) {
     const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
     // ---------------------------------------------------------------- load
     {
@@ -348,24 +376,27 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_factor_level(FactorArgs<T>
 // the same pivot rows, which yields C_j U^-1 and the C/F Schur updates.
 // ---------------------------------------------------------------------------
 template <typename T, int N, int NXM, int NRM>
-__global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<T> a) {
+__global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<T> a0, const FactorArgs<T>* tab,
+                                                         const BatchCta* cmap) {
   constexpr int NC = 3 * N + NXM;
   constexpr int NCP = (NC + 1) & ~1;
   constexpr int SLOTS = (NC + 31) / 32;
   constexpr unsigned FULL = 0xffffffffu;
   __shared__ __align__(16) T ubuf[4][NCP];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  FactorArgs<T> a;
+  long q0, q1, qs;
+  pair_range(a0, tab, cmap, wpb, warp, a, q0, q1, qs);
   const Dims d = a.d;
-  const int n = d.n, nr = d.nr, nx = d.nx, nb = d.nblock, n2 = 2 * n;
+  const int n = d.n, nr = d.nr, nx = d.nx, n2 = 2 * n;
   const size_t nn = (size_t)n * n, nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
   T* ub = ubuf[warp];
   const int k = a.k;
-  const long np = pairs_at_level(nb, k);
   const bool first = a.first != 0;
   const bool act = lane < n2, top = lane < n;
   const int ri = top ? lane : lane - n;
 
-  for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
+  for (long q = q0; q < q1; q += qs) {
     const int j = k + (int)(2L * k * q), jp = j - k;
     T row[NC];
     {
@@ -544,24 +575,27 @@ size_t tc_smem_per_warp(int n) {
 }
 
 template <int N>
-__global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a) {
+__global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a0, const FactorArgs<double>* tab,
+                                                       const BatchCta* cmap) {
   using S = TcShape<N>;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  FactorArgs<double> a;
+  long q0, q1, qs;
+  pair_range(a0, tab, cmap, wpb, warp, a, q0, q1, qs);
   double* Wt = reinterpret_cast<double*>(smem_raw + (size_t)warp * S::BYTES);
   double* Gs = Wt + S::WS;
   double* bc = Gs + S::GS;                        // pivot row + its reciprocal
   int* rowof = reinterpret_cast<int*>(bc + N + 2);
   const Dims d = a.d;
-  const int nr = d.nr, nx = d.nx, nb = d.nblock;
+  const int nr = d.nr, nx = d.nx;
   constexpr int n = N, n2 = 2 * N;
   constexpr size_t nn = (size_t)N * N;
   const size_t nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
   const int nrf = a.nrf;             // fused right-hand sides
   const int NT = n2 + nx + nrf;      // live trailing columns
   const int k = a.k;
-  const long np = pairs_at_level(nb, k);
   const bool first = a.first != 0;
   const double* srcD = first ? a.D0 : a.D;
   const double* srcE = first ? a.E0 : a.E;
@@ -571,7 +605,7 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a) {
   const int ri = top ? lane : lane - n;
   const int g = lane >> 2, t = lane & 3;
 
-  for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
+  for (long q = q0; q < q1; q += qs) {
     const int j = k + (int)(2L * k * q), jp = j - k;
     // ------------------------------------------------------------ load
     double rowA[N], rowC[N];
@@ -971,7 +1005,8 @@ template <typename T, int N>
 constexpr int grp_min_blocks() { return N == 32 ? (sizeof(T) == 8 ? 3 : 5) : 4; }
 
 template <typename T, int N>
-__global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>()) k_factor_lu_grp(FactorArgs<T> a) {
+__global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
+    k_factor_lu_grp(FactorArgs<T> a0, const FactorArgs<T>* tab, const BatchCta* cmap) {
   using S = GrpShape<T, N>;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -981,20 +1016,22 @@ __global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>()) k_factor_l
   int* hdr = reinterpret_cast<int*>(slot + 2 * S::NWP * S::LDS);  // [2][NWP][4] hi, lo, position, thread
   int* rowof = hdr + 2 * S::NWP * 4;               // position -> original row
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  FactorArgs<T> a;
+  long q0, q1, qs;
+  pair_range(a0, tab, cmap, 1, 0, a, q0, q1, qs);
   const Dims d = a.d;
-  const int nr = d.nr, nx = d.nx, nb = d.nblock;
+  const int nr = d.nr, nx = d.nx;
   constexpr int n = N, n2 = 2 * N;
   constexpr size_t nn = (size_t)N * N;
   const size_t nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
   const int k = a.k;
-  const long np = pairs_at_level(nb, k);
   const bool first = a.first != 0;
   const bool panel = t < n2;                 // panel row t
   const bool brow = !panel && t - n2 < nr;   // border row t - 2N
   const bool top = t < n;
   const int ri = top ? t : t - n;
 
-  for (long qq = blockIdx.x; qq < np; qq += gridDim.x) {
+  for (long qq = q0; qq < q1; qq += qs) {
     const int j = k + (int)(2L * k * qq), jp = j - k;
     __syncthreads();  // the previous pair's readers of Wt/Gs are done
     // ------------------------------------------------------------ load
@@ -1424,14 +1461,13 @@ __global__ void k_border_fix(Dims d, T* C, const T* Rbuf, int k) {
 // part[g]; otherwise (one CTA) it writes out = base + sum (column height h).
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_reduce_tree(const T* buf, int stride, long first, long count,
-                                                     int m, long chunk, T* part, const T* base, int h,
-                                                     int ldb, T* out, int ldo) {
+__device__ void reduce_tree_body(const T* buf, int stride, long first, long count, int m, long chunk,
+                                 T* part, const T* base, int h, int ldb, T* out, int ldo, int blk) {
   __shared__ T red[256];
   const int tid = threadIdx.x;
   const int S = 256 / m;  // items reduced in parallel per element
   const int e = tid % m, g = tid / m;
-  const long b0 = first + (long)blockIdx.x * chunk;
+  const long b0 = first + (long)blk * chunk;
   const long b1 = min(first + count, b0 + chunk);
   T a0 = T(0), a1 = T(0);
   if (g < S) {
@@ -1454,9 +1490,16 @@ __global__ void __launch_bounds__(256) k_reduce_tree(const T* buf, int stride, l
       const int r = e % h, c = e / h;
       out[(size_t)c * ldo + r] = (base ? base[(size_t)c * ldb + r] : T(0)) + s;
     } else {
-      part[(size_t)blockIdx.x * m + e] = s;
+      part[(size_t)blk * m + e] = s;
     }
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_reduce_tree(const T* buf, int stride, long first, long count,
+                                                     int m, long chunk, T* part, const T* base, int h,
+                                                     int ldb, T* out, int ldo) {
+  reduce_tree_body(buf, stride, first, count, m, chunk, part, base, h, ldb, out, ldo, (int)blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1474,15 +1517,21 @@ struct SweepArgs {
   int k, ldw, sel;
 };
 
+__device__ __forceinline__ void take_level(SweepArgs<float>& a, const SweepArgs<float>& a0) { a.k = a0.k; }
+__device__ __forceinline__ void take_level(SweepArgs<double>& a, const SweepArgs<double>& a0) { a.k = a0.k; }
+
 template <typename T>
-__global__ void __launch_bounds__(WARPS_PANEL * 32) k_forward_level(SweepArgs<T> a) {
+__global__ void __launch_bounds__(WARPS_PANEL * 32) k_forward_level(SweepArgs<T> a0, const SweepArgs<T>* tab,
+                                                                const BatchCta* cmap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  SweepArgs<T> a;
+  long q0, q1, qs;
+  pair_range(a0, tab, cmap, wpb, warp, a, q0, q1, qs);
   const Dims d = a.d;
   const int n = d.n, nr = d.nr, n2 = 2 * n, nrhs = a.nrhs, ldw = a.ldw, k = a.k;
   double* W = reinterpret_cast<double*>(smem_raw) + (size_t)warp * ldw * nrhs;
-  const long np = pairs_at_level(d.nblock, k);
-  for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
+  for (long q = q0; q < q1; q += qs) {
     const int j = k + (int)(2L * k * q), jp = j - k;
     const T* Tj = a.Tm + (size_t)j * szT(d);
     const unsigned char* Pj = a.P + (size_t)j * szP(d);
@@ -1538,15 +1587,18 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_forward_level(SweepArgs<T>
 }
 
 template <typename T>
-__global__ void __launch_bounds__(WARPS_PANEL * 32) k_backward_level(SweepArgs<T> a) {
+__global__ void __launch_bounds__(WARPS_PANEL * 32) k_backward_level(SweepArgs<T> a0, const SweepArgs<T>* tab,
+                                                                 const BatchCta* cmap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  SweepArgs<T> a;
+  long q0, q1, qs;
+  pair_range(a0, tab, cmap, wpb, warp, a, q0, q1, qs);
   const Dims d = a.d;
   const int n = d.n, nx = d.nx, n2 = 2 * n, nrhs = a.nrhs, k = a.k, nb = d.nblock;
   double* Y = reinterpret_cast<double*>(smem_raw) + (size_t)warp * a.ldw;
-  const long np = pairs_at_level(nb, k);
   const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
-  for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
+  for (long q = q0; q < q1; q += qs) {
     const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
     const T* Dj = a.D + (size_t)j * n * n;
     const T* Ej = a.E + (size_t)j * n * n;
@@ -1589,15 +1641,18 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_backward_level(SweepArgs<T
 // All loads of a pair are issued before the first use.
 // ---------------------------------------------------------------------------
 template <typename TF, int N, int NRM, bool LU>
-__global__ void __launch_bounds__(256, 2) k_forward_rows(SweepArgs<TF> a) {
+__global__ void __launch_bounds__(256, 2) k_forward_rows(SweepArgs<TF> a0, const SweepArgs<TF>* tab,
+                                                         const BatchCta* cmap) {
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  SweepArgs<TF> a;
+  long q0, q1, qs;
+  pair_range(a0, tab, cmap, wpb, warp, a, q0, q1, qs);
   const Dims d = a.d;
-  const int n = d.n, nr = d.nr, nb = d.nblock, n2 = 2 * n, nrhs = a.nrhs, k = a.k;
+  const int n = d.n, nr = d.nr, n2 = 2 * n, nrhs = a.nrhs, k = a.k;
   const bool act = lane < n2;
   constexpr bool lu = LU;
-  const long np = pairs_at_level(nb, k);
-  for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
+  for (long q = q0; q < q1; q += qs) {
     const int j = k + (int)(2L * k * q), jp = j - k;
     const TF* Tj = a.Tm + (size_t)j * szT(d);
     double t[N];
@@ -1650,17 +1705,20 @@ __global__ void __launch_bounds__(256, 2) k_forward_rows(SweepArgs<TF> a) {
 }
 
 template <typename TF, int N, int NXM>
-__global__ void __launch_bounds__(256, 2) k_backward_rows(SweepArgs<TF> a) {
+__global__ void __launch_bounds__(256, 2) k_backward_rows(SweepArgs<TF> a0, const SweepArgs<TF>* tab,
+                                                          const BatchCta* cmap) {
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  SweepArgs<TF> a;
+  long q0, q1, qs;
+  pair_range(a0, tab, cmap, wpb, warp, a, q0, q1, qs);
   const Dims d = a.d;
   const int n = d.n, nx = d.nx, nb = d.nblock, n2 = 2 * n, nrhs = a.nrhs, k = a.k;
   const int i = lane & 15;
   const bool hi = lane >= 16, rowok = i < n;
   const bool qrp = a.sel == SEL_QRP;
-  const long np = pairs_at_level(nb, k);
   const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
-  for (long q = (long)blockIdx.x * wpb + warp; q < np; q += (long)gridDim.x * wpb) {
+  for (long q = q0; q < q1; q += qs) {
     const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
     const TF* Mt = (hi ? a.E : a.D) + (size_t)j * n * n;
     const TF* Tj = a.Tm + (size_t)j * szT(d);
@@ -1714,12 +1772,13 @@ __global__ void __launch_bounds__(256, 2) k_backward_rows(SweepArgs<TF> a) {
 // one CTA; the Nr x Nc matrix lives in global memory (L2 resident)
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_last_assemble(Dims d, const T* D, const T* E, const T* B, const T* C,
-                                const double* H, const double* Cq, const double* Ffin, double* Hl) {
+__device__ void last_assemble_range(Dims d, const T* D, const T* E, const T* B, const T* C,
+                                    const double* H, const double* Cq, const double* Ffin, double* Hl,
+                                    int e0, int es) {
   const int n = d.n, Nr = d.Nr, Nc = d.Nc, qx = d.qx, nr = d.nr, m = n + d.qr;
   const int total = Nr * Nc;
   const T* CN = C + (size_t)d.nblock * nr * n;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+  for (int e = e0; e < total; e += es) {
     const int r = e % Nr, c = e / Nr;
     double v = 0.0;
     if (r < n) {
@@ -1737,6 +1796,13 @@ __global__ void k_last_assemble(Dims d, const T* D, const T* E, const T* B, cons
     }
     Hl[e] = v;
   }
+}
+
+template <typename T>
+__global__ void k_last_assemble(Dims d, const T* D, const T* E, const T* B, const T* C,
+                                const double* H, const double* Cq, const double* Ffin, double* Hl) {
+  last_assemble_range(d, D, E, B, C, H, Cq, Ffin, Hl, blockIdx.x * blockDim.x + threadIdx.x,
+                      gridDim.x * blockDim.x);
 }
 
 template <typename T>
@@ -1775,7 +1841,7 @@ __device__ T block_sum(T v, T* sv) {
 
 // kind: LAST_LU or LAST_QR (others are rejected on the host)
 template <typename T>
-__global__ void k_last_factor(Dims d, T* A, int* piv, T* tau, int kind, StatusWords* st) {
+__device__ void last_factor_body(Dims d, T* A, int* piv, T* tau, int kind, StatusWords* st) {
   __shared__ T sv[32];
   __shared__ int si[32];
   const int M = d.Nr, N = d.Nc, tid = threadIdx.x, bs = blockDim.x;
@@ -1843,8 +1909,8 @@ __global__ void k_last_factor(Dims d, T* A, int* piv, T* tau, int kind, StatusWo
 }
 
 template <typename T>
-__global__ void k_last_solve(Dims d, const T* A, const int* piv, const T* tau, int kind, T* x,
-                             int ldx, int nrhs) {
+__device__ void last_solve_body(Dims d, const T* A, const int* piv, const T* tau, int kind, T* x,
+                                int ldx, int nrhs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* b = reinterpret_cast<T*>(smem_raw);
   __shared__ T sv[32];
@@ -1893,6 +1959,17 @@ __global__ void k_last_solve(Dims d, const T* A, const int* piv, const T* tau, i
     }
     __syncthreads();
   }
+}
+
+template <typename T>
+__global__ void k_last_factor(Dims d, T* A, int* piv, T* tau, int kind, StatusWords* st) {
+  last_factor_body(d, A, piv, tau, kind, st);
+}
+
+template <typename T>
+__global__ void k_last_solve(Dims d, const T* A, const int* piv, const T* tau, int kind, T* x,
+                             int ldx, int nrhs) {
+  last_solve_body(d, A, piv, tau, kind, x, ldx, nrhs);
 }
 
 // ---------------------------------------------------------------------------
@@ -2065,13 +2142,13 @@ static WorkSet<float> work_set(DevState& s, float*) {
 template <typename T>
 struct FactorPlan {
   void (*cta)(FactorArgs<T>, T*, size_t) = nullptr;  // CTA per pair (large n)
-  void (*tc)(FactorArgs<T>) = nullptr;               // tensor-core LU (FP64, n = 8, 16)
+  void (*tc)(FactorArgs<T>, const FactorArgs<T>*, const BatchCta*) = nullptr;               // tensor-core LU (FP64, n = 8, 16)
   size_t tc_smem = 0;
-  void (*grp)(FactorArgs<T>) = nullptr;              // CTA of 2n threads per pair (n = 16, 32)
+  void (*grp)(FactorArgs<T>, const FactorArgs<T>*, const BatchCta*) = nullptr;              // CTA of 2n threads per pair (n = 16, 32)
   size_t grp_smem = 0;
   int grp_threads = 0, grp_ctas = 0;
-  void (*rows)(FactorArgs<T>) = nullptr;             // register LU (n <= 16)
-  void (*smem_k)(FactorArgs<T>) = nullptr;           // shared-memory kernel
+  void (*rows)(FactorArgs<T>, const FactorArgs<T>*, const BatchCta*) = nullptr;             // register LU (n <= 16)
+  void (*smem_k)(FactorArgs<T>, const FactorArgs<T>*, const BatchCta*) = nullptr;           // shared-memory kernel
   size_t smem = 0;
   int wpb = 1;
   int tc_cols = 0;                                   // trailing-column capacity of tc
@@ -2164,10 +2241,10 @@ static void factor_levels(DevState& s, const FactorPlan<T>& p, const WorkSet<T>&
     a.first = (k == 1);
     const long np = pairs_at_level(nb, k);
     if (p.cta) p.cta<<<grid_for(np, 1, s.slab_ctas), 256, 0, st>>>(a, w.slab, s.slab_elems);
-    else if (p.grp) p.grp<<<grid_for(np, 1, p.grp_ctas), p.grp_threads, p.grp_smem, st>>>(a);
-    else if (p.tc) p.tc<<<grid_for(np, 4, 148 * 16), 128, p.tc_smem, st>>>(a);
-    else if (p.rows) p.rows<<<grid_for(np, 4, 148 * 16), 128, 0, st>>>(a);
-    else p.smem_k<<<grid_for(np, p.wpb, 148 * 16), p.wpb * 32, p.smem, st>>>(a);
+    else if (p.grp) p.grp<<<grid_for(np, 1, p.grp_ctas), p.grp_threads, p.grp_smem, st>>>(a, nullptr, nullptr);
+    else if (p.tc) p.tc<<<grid_for(np, 4, 148 * 16), 128, p.tc_smem, st>>>(a, nullptr, nullptr);
+    else if (p.rows) p.rows<<<grid_for(np, 4, 148 * 16), 128, 0, st>>>(a, nullptr, nullptr);
+    else p.smem_k<<<grid_for(np, p.wpb, 148 * 16), p.wpb * 32, p.smem, st>>>(a, nullptr, nullptr);
     check_launch("k_factor_level");
     if (nrn) {
       const long tot = np * (long)nrn;
@@ -2208,8 +2285,8 @@ void launch_factorize(DevState& s, cudaStream_t st) {
 // sweep kernels for one chunk of right-hand sides
 template <typename T>
 struct SweepPlan {
-  void (*fwd)(SweepArgs<T>) = nullptr;
-  void (*bwd)(SweepArgs<T>) = nullptr;
+  void (*fwd)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*) = nullptr;
+  void (*bwd)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*) = nullptr;
 };
 
 template <typename T>
@@ -2266,8 +2343,8 @@ static void forward_levels(DevState& s, const SweepPlan<T>& p, const WorkSet<T>&
   for (int K = 1; K < d.nblock; K *= 2) {
     a.k = K;
     const long np = pairs_at_level(d.nblock, K);
-    if (p.fwd) p.fwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a);
-    else k_forward_level<T><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_f, st>>>(a);
+    if (p.fwd) p.fwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a, nullptr, nullptr);
+    else k_forward_level<T><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_f, st>>>(a, nullptr, nullptr);
     check_launch("k_forward_level");
   }
   reduce_xb(s, x, ldx, nrhs, st);
@@ -2286,8 +2363,8 @@ static void last_and_backward(DevState& s, const SweepPlan<T>& p, const WorkSet<
   for (int k = top_level(d.nblock); (k /= 2) > 0;) {
     a.k = k;
     const long np = pairs_at_level(d.nblock, k);
-    if (p.bwd) p.bwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a);
-    else k_backward_level<T><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_b, st>>>(a);
+    if (p.bwd) p.bwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a, nullptr, nullptr);
+    else k_backward_level<T><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_b, st>>>(a, nullptr, nullptr);
     check_launch("k_backward_level");
   }
 }
@@ -2408,6 +2485,294 @@ void launch_residual(DevState& s, const double* b, const double* x, double* r, u
 void launch_axpy(double* y, const double* x, long len, cudaStream_t st) {
   k_axpy<<<grid_for(len, 256, 148 * 4), 256, 0, st>>>(y, x, len);
   check_launch("k_axpy");
+}
+
+// ---------------------------------------------------------------------------
+// batches of independent systems (FP64, internal LU)
+// ---------------------------------------------------------------------------
+struct LastDesc {
+  Dims d;
+  const double *D0, *E0, *B0, *C0, *H, *Cq, *F0, *Fbuf, *XB;
+  double *D, *E, *B, *C, *Ffin, *Hl, *tau, *x;
+  int* piv;
+  int kind, ldx;
+  StatusWords* st;
+};
+
+// status reset and the blocks the first level does not touch (odd tail, C_N)
+__global__ void __launch_bounds__(256) kb_begin(const LastDesc* t) {
+  const LastDesc& L = t[blockIdx.x];
+  const Dims d = L.d;
+  const int nb = d.nblock;
+  const size_t nn = (size_t)d.n * d.n, nnx = (size_t)d.n * d.nx, nrn = (size_t)d.nr * d.n;
+  if (threadIdx.x == 0) *L.st = StatusWords{0, 0, 0, 0};
+  if (nb % 2 == 1) {
+    const size_t b = (size_t)(nb - 1);
+    for (size_t e = threadIdx.x; e < nn; e += blockDim.x) {
+      L.D[b * nn + e] = L.D0[b * nn + e];
+      L.E[b * nn + e] = L.E0[b * nn + e];
+    }
+    for (size_t e = threadIdx.x; e < nnx; e += blockDim.x) L.B[b * nnx + e] = L.B0[b * nnx + e];
+    for (size_t e = threadIdx.x; e < nrn; e += blockDim.x) L.C[b * nrn + e] = L.C0[b * nrn + e];
+  }
+  for (size_t e = threadIdx.x; e < nrn; e += blockDim.x) L.C[(size_t)nb * nrn + e] = L.C0[(size_t)nb * nrn + e];
+}
+
+// C_jpp += dC_jpp for the pairs of each chunk (one writer per target block)
+__global__ void __launch_bounds__(128) kb_border_fix(const FactorArgs<double>* tab, const BatchCta* cmap, int k) {
+  const BatchCta c = cmap[blockIdx.x];
+  const FactorArgs<double>& a = tab[c.sys];
+  const Dims d = a.d;
+  const size_t nrn = (size_t)d.nr * d.n;
+  for (long q = c.q0; q < c.q1; ++q) {
+    const int j = k + (int)(2L * k * q), jpp = min(j + k, d.nblock);
+    for (size_t e = threadIdx.x; e < nrn; e += blockDim.x) a.C[(size_t)jpp * nrn + e] += a.Rbuf[(size_t)j * nrn + e];
+  }
+}
+
+// F = F0 + sum of the Schur updates, one CTA per system (fixed order)
+__global__ void __launch_bounds__(256) kb_reduce_F(const LastDesc* t) {
+  const LastDesc& L = t[blockIdx.x];
+  const Dims d = L.d;
+  const int m = d.nr * d.nx;
+  if (m == 0) return;
+  const long cnt = d.nblock - 1;
+  reduce_tree_body(L.Fbuf, m, 1, cnt, m, cnt > 0 ? cnt : 1, (double*)nullptr, L.F0, d.nr, d.nr, L.Ffin, d.nr, 0);
+}
+
+__global__ void __launch_bounds__(256) kb_last_assemble(const LastDesc* t) {
+  const LastDesc& L = t[blockIdx.x];
+  last_assemble_range(L.d, (const double*)L.D, (const double*)L.E, (const double*)L.B, (const double*)L.C,
+                      L.H, L.Cq, L.Ffin, L.Hl, (int)threadIdx.x, (int)blockDim.x);
+}
+
+__global__ void __launch_bounds__(512) kb_last_factor(const LastDesc* t) {
+  const LastDesc& L = t[blockIdx.x];
+  if (L.st->code != 0) return;  // a pair of this system already failed
+  last_factor_body(L.d, L.Hl, L.piv, L.tau, L.kind, L.st);
+}
+
+// xb += sum of the per-block -C'_j x_j contributions, one CTA per system
+__global__ void __launch_bounds__(256) kb_reduce_xb(const LastDesc* t, int nrhs) {
+  const LastDesc& L = t[blockIdx.x];
+  const Dims d = L.d;
+  if (d.nr == 0) return;
+  const int m = d.nr * nrhs;
+  const long cnt = d.nblock - 1;
+  double* xb = L.x + (size_t)(d.nblock + 1) * d.n + d.qr;
+  reduce_tree_body(L.XB, m, 1, cnt, m, cnt > 0 ? cnt : 1, (double*)nullptr, (const double*)xb, d.nr, L.ldx, xb,
+                   L.ldx, 0);
+}
+
+__global__ void __launch_bounds__(256) kb_last_solve(const LastDesc* t, int nrhs) {
+  const LastDesc& L = t[blockIdx.x];
+  last_solve_body(L.d, (const double*)L.Hl, (const int*)L.piv, (const double*)L.tau, L.kind, L.x, L.ldx, nrhs);
+}
+
+bool batch_family_ok(int fam, const Dims& d) {
+  if (d.nr > 8 || d.nx > 8) return false;
+  switch (fam) {
+    case PAIR_TC: return d.n == 8 || d.n == 16;
+    case PAIR_GRP: return d.n == 16 || d.n == 32;
+    case PAIR_ROWS: return d.n <= 16 && d.nr <= 4 && d.nx <= 4;
+    default: return false;
+  }
+}
+
+static void build_map(const std::vector<DevState>& sys, int levels, int chunk, std::vector<BatchCta>& map,
+                      std::vector<long>& off, std::vector<long>& cnt) {
+  off.assign(levels, 0);
+  cnt.assign(levels, 0);
+  for (int L = 0; L < levels; ++L) {
+    const int k = 1 << L;
+    off[L] = (long)map.size();
+    for (size_t i = 0; i < sys.size(); ++i) {
+      const long np = pairs_at_level(sys[i].d.nblock, k);
+      for (long q0 = 0; q0 < np; q0 += chunk) {
+        BatchCta c;
+        c.sys = (int)i;
+        c.pad = 0;
+        c.q0 = q0;
+        c.q1 = q0 + chunk < np ? q0 + chunk : np;
+        map.push_back(c);
+      }
+    }
+    cnt[L] = (long)map.size() - off[L];
+  }
+}
+
+template <typename X>
+static int upload_table(void*& dst, const std::vector<X>& v) {
+  if (cudaMalloc(&dst, std::max<size_t>(v.size(), 1) * sizeof(X)) != cudaSuccess) return 1;
+  if (!v.empty() && cudaMemcpy(dst, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice) != cudaSuccess) return 1;
+  return 0;
+}
+
+void batch_free(BatchClass& c) {
+  for (void** p : {&c.fa, &c.sf, &c.sb, &c.ld})
+    if (*p) { cudaFree(*p); *p = nullptr; }
+  if (c.fmap) { cudaFree(c.fmap); c.fmap = nullptr; }
+  if (c.smap) { cudaFree(c.smap); c.smap = nullptr; }
+  c.foff.clear(); c.fcnt.clear(); c.soff.clear(); c.scnt.clear();
+}
+
+int batch_build(BatchClass& c, const std::vector<DevState>& sys, int nrhs) {
+  batch_free(c);
+  c.nsys = (int)sys.size();
+  c.nrhs = nrhs;
+  c.levels = 0;
+  c.nrm = c.nxm = 0;
+  size_t lmax = 0;
+  std::vector<FactorArgs<double>> fa(sys.size());
+  std::vector<SweepArgs<double>> sf(sys.size()), sb(sys.size());
+  std::vector<LastDesc> ld(sys.size());
+  for (size_t i = 0; i < sys.size(); ++i) {
+    const DevState& s = sys[i];
+    const Dims d = s.d;
+    c.n = d.n;
+    c.nrm = std::max(c.nrm, d.nr);
+    c.nxm = std::max(c.nxm, d.nx);
+    int K = 1, lev = 0;
+    while (K < d.nblock) { K *= 2; ++lev; }
+    c.levels = std::max(c.levels, lev);
+    lmax = std::max<size_t>(lmax, (size_t)std::max(d.Nr, d.Nc));
+    FactorArgs<double> a{};
+    a.d = d;
+    a.D0 = s.D0; a.E0 = s.E0; a.B0 = s.B0; a.C0 = s.C0;
+    a.D = s.D; a.E = s.E; a.B = s.B; a.C = s.C; a.Tm = s.T; a.P = s.P;
+    a.Rbuf = s.Rbuf; a.Fbuf = s.Fbuf; a.st = s.st;
+    a.ldw = odd_ld(2 * d.n + d.nr);
+    a.x = nullptr; a.ldx = 0; a.nrf = 0; a.XB = s.XB;
+    fa[i] = a;
+    SweepArgs<double> w{};
+    w.d = d;
+    w.D = s.D; w.E = s.E; w.B = s.B; w.C = s.C; w.Tm = s.T; w.P = s.P;
+    w.x = s.bx; w.ldx = s.bldx; w.nrhs = nrhs; w.XB = s.XB; w.sel = SEL_LU;
+    w.ldw = odd_ld(2 * d.n);
+    sf[i] = w;
+    w.ldw = d.n;
+    sb[i] = w;
+    LastDesc l{};
+    l.d = d;
+    l.D0 = s.D0; l.E0 = s.E0; l.B0 = s.B0; l.C0 = s.C0; l.H = s.H; l.Cq = s.Cq; l.F0 = s.F0;
+    l.Fbuf = s.Fbuf; l.XB = s.XB;
+    l.D = s.D; l.E = s.E; l.B = s.B; l.C = s.C; l.Ffin = s.Ffin; l.Hl = s.Hl; l.tau = s.tau_l; l.x = s.bx;
+    l.piv = s.piv_l; l.kind = s.sel_last; l.ldx = s.bldx; l.st = s.st;
+    ld[i] = l;
+  }
+  c.last_smem = lmax * 8;
+  std::vector<BatchCta> fmap, smap;
+  build_map(sys, c.levels, c.chunk, fmap, c.foff, c.fcnt);
+  build_map(sys, c.levels, 8, smap, c.soff, c.scnt);
+  int bad = upload_table(c.fa, fa) | upload_table(c.sf, sf) | upload_table(c.sb, sb) | upload_table(c.ld, ld);
+  void* m1 = nullptr;
+  void* m2 = nullptr;
+  bad |= upload_table(m1, fmap) | upload_table(m2, smap);
+  c.fmap = static_cast<BatchCta*>(m1);
+  c.smap = static_cast<BatchCta*>(m2);
+  return bad;
+}
+
+// one batched launch of the class's pair kernel at level `L`
+static void batch_pairs(BatchClass& c, int L, cudaStream_t st) {
+  const long cnt = c.fcnt[L];
+  if (cnt == 0) return;
+  FactorArgs<double> a0{};
+  a0.k = 1 << L;
+  a0.first = L == 0;
+  const FactorArgs<double>* tab = static_cast<const FactorArgs<double>*>(c.fa);
+  const BatchCta* map = c.fmap + c.foff[L];
+  const unsigned g = (unsigned)cnt;
+  if (c.fam == PAIR_TC) {
+    if (c.n == 16) {
+      const size_t sm = tc_smem_per_warp(16) * 4;
+      smem_limit_once(k_factor_lu_tc<16>, sm);
+      k_factor_lu_tc<16><<<g, 128, sm, st>>>(a0, tab, map);
+    } else {
+      const size_t sm = tc_smem_per_warp(8) * 4;
+      smem_limit_once(k_factor_lu_tc<8>, sm);
+      k_factor_lu_tc<8><<<g, 128, sm, st>>>(a0, tab, map);
+    }
+  } else if (c.fam == PAIR_GRP) {
+    if (c.n == 32) {
+      smem_limit_once(k_factor_lu_grp<double, 32>, GrpShape<double, 32>::BYTES);
+      k_factor_lu_grp<double, 32><<<g, 96, GrpShape<double, 32>::BYTES, st>>>(a0, tab, map);
+    } else {
+      smem_limit_once(k_factor_lu_grp<double, 16>, GrpShape<double, 16>::BYTES);
+      k_factor_lu_grp<double, 16><<<g, 64, GrpShape<double, 16>::BYTES, st>>>(a0, tab, map);
+    }
+  } else {
+    if (c.n <= 4) k_factor_lu_rows<double, 4, 4, 4><<<g, 128, 0, st>>>(a0, tab, map);
+    else if (c.n <= 8) k_factor_lu_rows<double, 8, 4, 4><<<g, 128, 0, st>>>(a0, tab, map);
+    else k_factor_lu_rows<double, 16, 4, 4><<<g, 128, 0, st>>>(a0, tab, map);
+  }
+  check_launch("batched pair kernel");
+  if (c.nrm > 0) {
+    kb_border_fix<<<g, 128, 0, st>>>(tab, map, 1 << L);
+    check_launch("kb_border_fix");
+  }
+}
+
+void batch_factorize(BatchClass& c, cudaStream_t st) {
+  if (c.nsys == 0) return;
+  const LastDesc* ld = static_cast<const LastDesc*>(c.ld);
+  kb_begin<<<c.nsys, 256, 0, st>>>(ld);
+  check_launch("kb_begin");
+  for (int L = 0; L < c.levels; ++L) batch_pairs(c, L, st);
+  kb_reduce_F<<<c.nsys, 256, 0, st>>>(ld);
+  kb_last_assemble<<<c.nsys, 256, 0, st>>>(ld);
+  kb_last_factor<<<c.nsys, 512, 0, st>>>(ld);
+  check_launch("batched last block");
+}
+
+template <int N>
+static void batch_sweeps_rows(BatchClass& c, cudaStream_t st, bool forward, int L) {
+  const bool r4 = c.nrm <= 4, x4 = c.nxm <= 4;
+  const BatchCta* map = c.smap + c.soff[L];
+  const unsigned g = (unsigned)c.scnt[L];
+  SweepArgs<double> a0{};
+  a0.k = 1 << L;
+  if (forward) {
+    const SweepArgs<double>* tab = static_cast<const SweepArgs<double>*>(c.sf);
+    if (r4) k_forward_rows<double, N, 4, true><<<g, 256, 0, st>>>(a0, tab, map);
+    else k_forward_rows<double, N, 8, true><<<g, 256, 0, st>>>(a0, tab, map);
+  } else {
+    const SweepArgs<double>* tab = static_cast<const SweepArgs<double>*>(c.sb);
+    if (x4) k_backward_rows<double, N, 4><<<g, 256, 0, st>>>(a0, tab, map);
+    else k_backward_rows<double, N, 8><<<g, 256, 0, st>>>(a0, tab, map);
+  }
+}
+
+static void batch_sweep_level(BatchClass& c, cudaStream_t st, bool forward, int L) {
+  if (c.scnt[L] == 0) return;
+  if (c.n <= 4) batch_sweeps_rows<4>(c, st, forward, L);
+  else if (c.n <= 8) batch_sweeps_rows<8>(c, st, forward, L);
+  else if (c.n <= 16) batch_sweeps_rows<16>(c, st, forward, L);
+  else {
+    const BatchCta* map = c.smap + c.soff[L];
+    const unsigned g = (unsigned)c.scnt[L];
+    SweepArgs<double> a0{};
+    a0.k = 1 << L;
+    if (forward) {
+      const size_t sm = (size_t)odd_ld(2 * c.n) * c.nrhs * 8 * WARPS_PANEL;
+      smem_limit_once(k_forward_level<double>, sm);
+      k_forward_level<double><<<g, WARPS_PANEL * 32, sm, st>>>(a0, static_cast<const SweepArgs<double>*>(c.sf), map);
+    } else {
+      const size_t sm = (size_t)c.n * 8 * WARPS_PANEL;
+      k_backward_level<double><<<g, WARPS_PANEL * 32, sm, st>>>(a0, static_cast<const SweepArgs<double>*>(c.sb), map);
+    }
+  }
+  check_launch(forward ? "batched forward sweep" : "batched backward sweep");
+}
+
+void batch_solve(BatchClass& c, cudaStream_t st) {
+  if (c.nsys == 0) return;
+  const LastDesc* ld = static_cast<const LastDesc*>(c.ld);
+  for (int L = 0; L < c.levels; ++L) batch_sweep_level(c, st, true, L);
+  kb_reduce_xb<<<c.nsys, 256, 0, st>>>(ld, c.nrhs);
+  kb_last_solve<<<c.nsys, 256, c.last_smem, st>>>(ld, c.nrhs);
+  for (int L = c.levels - 1; L >= 0; --L) batch_sweep_level(c, st, false, L);
+  check_launch("batched solve");
 }
 
 }  // namespace bcr

@@ -231,3 +231,50 @@ def rhs(s: BABD, nrhs: int = 1, seed: int = 1) -> np.ndarray:
     b = np.zeros((nrhs, L))
     b[:, :s.nrows] = rng.standard_normal((nrhs, s.nrows))
     return b
+
+
+def batch_dims(nsys: int, nblock_lo: int = 64, nblock_hi: int = 4096, ns=(4, 8, 16, 32),
+               borders=(0, 2, 4), seed: int = 0):
+    """Sizes of the uneven batch workload: nblock ~ U{lo..hi}, n drawn from ns,
+    nr = nx drawn from borders, qr = qx = 0; system s is then generated by
+    collocation(..., seed=s)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(nsys):
+        nb = int(rng.integers(nblock_lo, nblock_hi + 1))
+        n = int(rng.choice(ns))
+        b = int(rng.choice(borders))
+        out.append((nb, n, 0, 0, b, b))
+    return out
+
+
+def collocation_torch(torch, nblock, n, qr=0, qx=0, nr=0, nx=0, kappa=1.0, seed=0, device="cuda"):
+    """The collocation generator's distributions drawn on the device with torch
+    (its own random stream, so the values differ from collocation()); returns
+    contiguous float64 tensors D, E, B, C, Cq, F, H in the reference layout."""
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    f64 = torch.float64
+    h = 1.0 / nblock
+    J = torch.randn((nblock, n, n), generator=g, device=device, dtype=f64) * (kappa / n) ** 0.5
+    eye = torch.eye(n, device=device, dtype=f64)
+    D = (-eye - 0.5 * h * J).contiguous()
+    E = (eye - 0.5 * h * J).contiguous()
+    B = torch.randn((nblock, nx, n), generator=g, device=device, dtype=f64) * 0.1 ** 0.5
+    C = torch.randn((nblock + 1, n, nr), generator=g, device=device, dtype=f64) * 0.1 ** 0.5
+    F = torch.randn((nx, nr), generator=g, device=device, dtype=f64) * 0.1 ** 0.5
+    for i in range(min(nr, nx)):
+        F[i, i] += 1.0
+    Cq = torch.randn((qx, nr), generator=g, device=device, dtype=f64) * 0.1 ** 0.5
+    m, Nc = n + qr, 2 * n + qx + nx
+    Hm = torch.zeros((m, Nc), device=device, dtype=f64)
+    Hm[:, 0:2 * n] = torch.randn((m, 2 * n), generator=g, device=device, dtype=f64) * 0.1
+    half = n // 2
+    idx = torch.arange(half, device=device)
+    Hm[idx, idx] += 1.0
+    idx2 = torch.arange(half, n, device=device)
+    Hm[idx2, n + idx2] += 1.0
+    Hm[:, 2 * n:2 * n + qx] = torch.randn((m, qx), generator=g, device=device, dtype=f64)
+    Hm[:, 2 * n + qx:] = torch.randn((m, nx), generator=g, device=device, dtype=f64) * 0.1
+    H = Hm.t().contiguous()
+    return D, E, B, C, Cq, F, H

@@ -215,6 +215,57 @@ int bcr_mv_noalloc(int nblock, int n, int qr, int qx, int nr, int nx,
                    double alpha, const double *x, double beta, double *res,
                    void *stream, char *errbuf, int errlen);
 
+/* --- batches of independent systems -----------------------------------------
+ * No counterpart in the reference (each BorderedCR object there is factored
+ * on its own thread pool).  Many systems -- each a bcr_handle filled through
+ * the usual loaders, internal LU, last block LU or QR, FP64 -- are factored
+ * and solved together: prepare() packs every system into one device arena,
+ * groups the systems by pair-kernel instance (by block size n) and runs each
+ * cyclic-reduction level of all systems of a group in one launch.  Systems
+ * may differ in nblock, n (4..16 with nr, nx <= 4; 8, 16, 32 with nr, nx <= 8)
+ * and borders.  The handles must stay alive while the batch uses them: their
+ * host copies are read at prepare() and upload(). */
+typedef struct bcr_batch_s *bcr_batch;
+int bcr_batch_create(bcr_batch *out);
+int bcr_batch_destroy(bcr_batch b);
+int bcr_batch_add(bcr_batch b, bcr_handle h);
+/* a system that lives only on the device (no handle, no host copy): after
+   prepare(), bcr_batch_matrix() gives the device addresses of its blocks in
+   the reference layout (see bcr_block_data) for the caller to fill; last is
+   "LU" or "QR" */
+int bcr_batch_add_device(bcr_batch b, int nblock, int n, int qr, int qx, int nr, int nx, const char *last);
+int bcr_batch_matrix(bcr_batch b, int i, double **D, double **E, double **B, double **C, double **Cq,
+                     double **F, double **H);
+int bcr_batch_system_size(bcr_batch b, int i, int *nrows, int *ncols);
+/* copy system i's blocks from caller device buffers (reference layout,
+   contiguous; NULL skips a block), enqueued on the batch stream */
+int bcr_batch_load_device(bcr_batch b, int i, const double *D, const double *E, const double *B,
+                          const double *C, const double *Cq, const double *F, const double *H);
+int bcr_batch_size(bcr_batch b);
+/* autotune != 0: time every applicable pair-kernel family and pairs-per-CTA
+   chunk on each group's own systems and keep the fastest (cached per shape) */
+int bcr_batch_prepare(bcr_batch b, int autotune);
+int bcr_batch_autotune(bcr_batch b);  /* the same tuning later, e.g. after bcr_batch_load_device */
+int bcr_batch_classes(bcr_batch b);
+int bcr_batch_class_info(bcr_batch b, int cls, int *n, int *nsys, int *family, int *chunk);
+int bcr_batch_upload(bcr_batch b);                       /* re-read the handles' matrices */
+int bcr_batch_factorize(bcr_batch b);                    /* BCR_NUMERICAL if any system failed */
+int bcr_batch_status(bcr_batch b, int *codes);           /* per system: 0 ok, else device code */
+int bcr_batch_solve(bcr_batch b, double *const *x);      /* x[i]: host vector of system i, in place */
+int bcr_batch_factorize_solve(bcr_batch b, double *const *x);  /* upload + factorize + solve */
+/* device-resident use: rhs copies kept on the device, a graph of the whole
+   factorize + solve step, solutions in device vectors */
+int bcr_batch_set_rhs(bcr_batch b, const double *const *rhs);
+double *bcr_batch_device_x(bcr_batch b, int i);
+double *bcr_batch_device_b(bcr_batch b, int i);  /* device copy of the rhs the graph starts from */
+int bcr_batch_get_x(bcr_batch b, double *const *x);
+int bcr_batch_graph_capture(bcr_batch b);
+int bcr_batch_graph_launch(bcr_batch b);
+int bcr_batch_check_status(bcr_batch b);
+void *bcr_batch_stream(bcr_batch b);
+int bcr_batch_synchronize(bcr_batch b);
+const char *bcr_batch_last_error(bcr_batch b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,163 @@
+"""GPU tests of batches of independent systems (uneven nblock, n and borders)
+against the CPU oracle, system by system.
+
+Bars (FP64): forward error against the oracle solution <= 1e-10 and relative
+residual ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= 1e-13.
+"""
+import numpy as np
+import pytest
+
+from alglin_b200 import bcr as B
+from alglin_b200 import synth
+from oracle import pyoracle as po
+from tests._util import block_norm_inf, fwd_err
+
+pytestmark = pytest.mark.gpu
+
+
+def relres(o, s, x, b):
+    r = b[:s.nrows] - o.mv(x[:s.ncols])
+    return np.abs(r).max() / (block_norm_inf(s) * np.abs(x[:s.ncols]).max() + np.abs(b[:s.nrows]).max())
+
+
+def make_systems(nsys, lo, hi, seed, ns=(4, 8, 16, 32), borders=(0, 2, 4)):
+    dims = synth.batch_dims(nsys, lo, hi, ns=ns, borders=borders, seed=seed)
+    systems = [synth.collocation(*d, seed=1000 + i) for i, d in enumerate(dims)]
+    rhs = [synth.rhs(s, 1, seed=2000 + i)[0] for i, s in enumerate(systems)]
+    return systems, rhs
+
+
+def handles_for(systems):
+    hs = []
+    for s in systems:
+        h = B.BorderedCR()
+        h.load_system(s)
+        h.select("LU")
+        h.select_last("LU")
+        hs.append(h)
+    return hs
+
+
+def check_against_oracle(systems, rhs, xs):
+    for i, (s, b, x) in enumerate(zip(systems, rhs, xs)):
+        o = po.Oracle(s, "LU", "LU")
+        assert o.factorize(), o.last_error()
+        xo = o.solve(b[None, :])[0]
+        assert fwd_err(x[:s.ncols], xo[:s.ncols]) < 1e-10, i
+        assert relres(o, s, x, b) <= 1e-13, i
+
+
+@pytest.mark.parametrize("autotune", [False, True])
+def test_batch_matches_oracle(autotune):
+    systems, rhs = make_systems(28, 1, 300, seed=5)
+    hs = handles_for(systems)
+    bt = B.Batch(hs)
+    bt.prepare(autotune=autotune)
+    assert len(bt) == 28
+    cls = bt.classes()
+    assert sum(c[1] for c in cls) == 28
+    assert bt.factorize(), bt.last_error()
+    xs = [b.copy() for b in rhs]
+    assert bt.solve(xs), bt.last_error()
+    check_against_oracle(systems, rhs, xs)
+    # the batch agrees with each system solved on its own
+    for h, b, x in zip(hs[:6], rhs[:6], xs[:6]):
+        assert h.factorize(), h.last_error()
+        y = b.copy()
+        assert h.solve(y)
+        assert np.abs(y - x).max() <= 1e-12 * max(1.0, np.abs(y).max())
+
+
+def test_batch_factorize_solve_and_graph():
+    torch = pytest.importorskip("torch")
+    systems, rhs = make_systems(17, 60, 400, seed=9)
+    bt = B.Batch(handles_for(systems))
+    bt.prepare()
+    xs = [b.copy() for b in rhs]
+    assert bt.factorize_solve(xs), bt.last_error()
+    check_against_oracle(systems, rhs, xs)
+    # device-resident graph of the whole step, replayed
+    bt.set_rhs(rhs)
+    bt.graph_capture()
+    for _ in range(3):
+        bt.graph_launch()
+    bt.synchronize()
+    assert bt.check_status()
+    ys = [np.zeros_like(b) for b in rhs]
+    bt.get_x(ys)
+    for x, y in zip(xs, ys):
+        assert np.array_equal(x, y)  # the replay is bit-identical to the eager run
+
+
+def test_batch_device_only_systems():
+    torch = pytest.importorskip("torch")
+    systems, rhs = make_systems(9, 30, 200, seed=13)
+    bt = B.Batch()
+    for s in systems:
+        bt.add_device(s.nblock, s.n, s.qr, s.qx, s.nr, s.nx)
+    bt.prepare()
+    keep = []
+    for i, s in enumerate(systems):
+        ts = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (s.D, s.E, s.B, s.C, s.Cq, s.F, s.H)]
+        keep.append(ts)
+        bt.load_device(i, *[t.data_ptr() if t.numel() else 0 for t in ts])
+    bt.synchronize()
+    assert bt.factorize(), bt.last_error()
+    xs = [b.copy() for b in rhs]
+    assert bt.solve(xs), bt.last_error()
+    check_against_oracle(systems, rhs, xs)
+
+
+def test_batch_mixed_with_single_blocks_and_qr_last():
+    # nblock = 1, odd and even nblock, a non-square last block solved by QR
+    dims = [(1, 4, 0, 0, 0, 0), (2, 8, 0, 0, 2, 2), (3, 16, 0, 0, 4, 4), (7, 32, 0, 0, 2, 2),
+            (64, 16, 1, 0, 2, 2)]
+    systems = [synth.collocation(*d, seed=40 + i) for i, d in enumerate(dims)]
+    rhs = [synth.rhs(s, 1, seed=i)[0] for i, s in enumerate(systems)]
+    hs = []
+    for s in systems:
+        h = B.BorderedCR()
+        h.load_system(s)
+        h.select("LU")
+        h.select_last("LU" if s.Nr == s.Nc else "QR")
+        hs.append(h)
+    bt = B.Batch(hs)
+    bt.prepare()
+    assert bt.factorize(), bt.last_error()
+    xs = [b.copy() for b in rhs]
+    assert bt.solve(xs)
+    for s, b, x, h in zip(systems, rhs, xs, hs):
+        last = "LU" if s.Nr == s.Nc else "QR"
+        o = po.Oracle(s, "LU", last)
+        assert o.factorize(), o.last_error()
+        xo = o.solve(b[None, :])[0]
+        assert fwd_err(x[:s.ncols], xo[:s.ncols]) < 1e-10
+
+
+def test_batch_reports_the_failing_system():
+    systems, rhs = make_systems(6, 20, 60, seed=3, ns=(8, 16))
+    bad = 4
+    systems[bad].D[:] = 0.0
+    systems[bad].E[:] = 0.0  # every panel is zero: the first pair fails
+    bt = B.Batch(handles_for(systems))
+    bt.prepare()
+    assert not bt.factorize()
+    codes = bt.status()
+    assert codes[bad] != 0
+    assert all(codes[i] == 0 for i in range(len(systems)) if i != bad)
+    assert f"system {bad}" in bt.last_error()
+
+
+def test_batch_rejects_unsupported():
+    s = synth.collocation(10, 5, 0, 0, 6, 6, seed=1)  # n=5 with nr > 4: no batched kernel
+    h = B.BorderedCR()
+    h.load_system(s)
+    bt = B.Batch([h])
+    with pytest.raises(B.BCRError, match="no batched pair kernel"):
+        bt.prepare()
+    h2 = B.BorderedCR()
+    h2.load_system(synth.collocation(10, 8, 0, 0, 2, 2, seed=1))
+    h2.select("QR")
+    bt2 = B.Batch([h2])
+    with pytest.raises(B.BCRError, match="internal LU"):
+        bt2.prepare()
