@@ -63,10 +63,10 @@ __device__ __forceinline__ T ldsrc(bool first, const double* orig, const T* work
 __device__ __forceinline__ void take_level(FactorArgs<float>& a, const FactorArgs<float>& a0) { a.k = a0.k; a.first = a0.first; }
 __device__ __forceinline__ void take_level(FactorArgs<double>& a, const FactorArgs<double>& a0) { a.k = a0.k; a.first = a0.first; }
 
-template <typename A>
+template <bool BATCH, typename A>
 __device__ __forceinline__ void pair_range(const A& a0, const A* tab, const BatchCta* cmap, int workers, int worker,
                                            A& a, long& q0, long& q1, long& qs) {
-  if (cmap) {
+  if constexpr (BATCH) {
     const BatchCta c = cmap[blockIdx.x];
     a = tab[c.sys];
     take_level(a, a0);
@@ -74,9 +74,8 @@ __device__ __forceinline__ void pair_range(const A& a0, const A* tab, const Batc
     q1 = c.q1;
     qs = workers;
   } else {
-    a = a0;
     q0 = (long)blockIdx.x * workers + worker;
-    q1 = pairs_at_level(a.d.nblock, a.k);
+    q1 = pairs_at_level(a0.d.nblock, a0.k);
     qs = (long)gridDim.x * workers;
   }
 }
@@ -236,14 +235,15 @@ __device__ int warp_eliminate_qr(T* W, int ldw, int n, int R, int NC, int* ipiv,
   return 0;
 }
 
-template <typename T, int SEL>
+template <typename T, int SEL, bool BATCH = false>
 __global__ void __launch_bounds__(WARPS_PANEL * 32) k_factor_level(FactorArgs<T> a0, const FactorArgs<T>* tab,
                                                                const BatchCta* cmap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  FactorArgs<T> a;
+  FactorArgs<T> ab;  // this CTA's system (batch only)
   long q0, q1, qs;
-  pair_range(a0, tab, cmap, wpb, warp, a, q0, q1, qs);
+  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
+  const FactorArgs<T>& a = BATCH ? ab : a0;
   const Dims d = a.d;
   const int n = d.n, nr = d.nr, nx = d.nx, nb = d.nblock;
   const int n2 = 2 * n, R = n2 + nr, NC = 3 * n + nx, ldw = a.ldw;
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_factor_level(FactorArgs<T>
 // the lanes by column (lane c holds column c, and c+32) and are eliminated with
 // the same pivot rows, which yields C_j U^-1 and the C/F Schur updates.
 // ---------------------------------------------------------------------------
-template <typename T, int N, int NXM, int NRM>
+template <typename T, int N, int NXM, int NRM, bool BATCH = false>
 __global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<T> a0, const FactorArgs<T>* tab,
                                                          const BatchCta* cmap) {
   constexpr int NC = 3 * N + NXM;
@@ -384,9 +384,10 @@ __global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<T> a0, const 
   constexpr unsigned FULL = 0xffffffffu;
   __shared__ __align__(16) T ubuf[4][NCP];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  FactorArgs<T> a;
+  FactorArgs<T> ab;  // this CTA's system (batch only)
   long q0, q1, qs;
-  pair_range(a0, tab, cmap, wpb, warp, a, q0, q1, qs);
+  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
+  const FactorArgs<T>& a = BATCH ? ab : a0;
   const Dims d = a.d;
   const int n = d.n, nr = d.nr, nx = d.nx, n2 = 2 * n;
   const size_t nn = (size_t)n * n, nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
@@ -574,16 +575,17 @@ size_t tc_smem_per_warp(int n) {
   return n == 16 ? TcShape<16>::BYTES : n == 8 ? TcShape<8>::BYTES : 0;
 }
 
-template <int N>
+template <int N, bool BATCH = false>
 __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a0, const FactorArgs<double>* tab,
                                                        const BatchCta* cmap) {
   using S = TcShape<N>;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  FactorArgs<double> a;
+  FactorArgs<double> ab;  // this CTA's system (batch only)
   long q0, q1, qs;
-  pair_range(a0, tab, cmap, wpb, warp, a, q0, q1, qs);
+  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
+  const FactorArgs<double>& a = BATCH ? ab : a0;
   double* Wt = reinterpret_cast<double*>(smem_raw + (size_t)warp * S::BYTES);
   double* Gs = Wt + S::WS;
   double* bc = Gs + S::GS;                        // pivot row + its reciprocal
@@ -894,7 +896,9 @@ struct GrpShape {
   static constexpr int NWA = NTH / 32;
   static constexpr int MT = 2 * N + 8;     // product rows: U-row, reduced row, border (nr <= 8)
   static constexpr int NTC = 2 * N + 8;    // trailing columns: x_jp, x_jpp, xb (nx <= 8)
-  static constexpr int LDW = NTC + 1;      // trailing rows (odd: conflict-light transposed stores)
+  // trailing rows, compact: a TOP row keeps [D_jp | B_jp], a BOTTOM row
+  // [E_j | B_j]; the structurally zero half of each row is not stored
+  static constexpr int LDW = N + 8 + 1;
   static constexpr int LDG = N + 4;        // G rows (16-byte aligned rows, conflict-free fragments)
   static constexpr int LDS = N + 2;
   // FP64 product: DMMA tiles, warp w owns row tiles [w*RTW, (w+1)*RTW)
@@ -908,6 +912,18 @@ struct GrpShape {
       (size_t)(2 * N * LDW + MT * LDG + 2 * NWP * LDS) * sizeof(T) + (size_t)(2 * NWP * 4 + 2 * N) * sizeof(int);
   static_assert(MT % TR == 0 && NTC % TC == 0 && NTILES % PC == 0, "product tiling");
 };
+
+// element (row, col) of the trailing part of the work matrix from the compact
+// rows: columns [0,N) x_jp (TOP rows only), [N,2N) x_jpp (BOTTOM rows only),
+// [2N, 2N+8) xb
+template <typename T, int N>
+__device__ __forceinline__ T w_at(const T* Wt, int row, int col) {
+  constexpr int LDW = GrpShape<T, N>::LDW;
+  const bool top = row < N;
+  if (col < N) return top ? Wt[row * LDW + col] : T(0);
+  if (col < 2 * N) return top ? T(0) : Wt[row * LDW + col - N];
+  return Wt[row * LDW + col - N];
+}
 
 // G * (P W)_top + [0; (P W)_bot; 0] -> the U-row of block j, the reduced row of
 // block jp and the border updates (C_jp, the C_jpp buffer, the F buffer)
@@ -931,9 +947,9 @@ struct GrpProduct<double, N> {
           const int row = (mt0 + mi) * 8 + g, col = (pass * S::PC + ni) * 8 + 2 * q;
           double c0 = 0.0, c1 = 0.0;
           if (mt0 + mi < S::MTILES && row >= N && row < 2 * N) {
-            const double* wr = Wt + rowof[row] * S::LDW + col;
-            c0 = wr[0];
-            c1 = wr[1];
+            const int orow = rowof[row];
+            c0 = w_at<double, N>(Wt, orow, col);
+            c1 = w_at<double, N>(Wt, orow, col + 1);
           }
           acc[mi][ni][0] = c0;
           acc[mi][ni][1] = c1;
@@ -941,9 +957,9 @@ struct GrpProduct<double, N> {
 #pragma unroll
       for (int ks = 0; ks < N / 4; ++ks) {
         double bfr[S::PC];
-        const double* wrow = Wt + rowof[ks * 4 + q] * S::LDW + pass * S::PC * 8 + g;
+        const int orow = rowof[ks * 4 + q];
 #pragma unroll
-        for (int ni = 0; ni < S::PC; ++ni) bfr[ni] = wrow[ni * 8];
+        for (int ni = 0; ni < S::PC; ++ni) bfr[ni] = w_at<double, N>(Wt, orow, (pass * S::PC + ni) * 8 + g);
 #pragma unroll
         for (int mi = 0; mi < S::RTW; ++mi) {
           if (mt0 + mi < S::MTILES) {
@@ -977,14 +993,14 @@ struct GrpProduct<float, N> {
       const int row = tr + S::TR * ii;
 #pragma unroll
       for (int jj = 0; jj < S::CPT; ++jj)
-        acc[ii][jj] = (row >= N && row < 2 * N) ? Wt[rowof[row] * S::LDW + tc + S::TC * jj] : 0.0f;
+        acc[ii][jj] = (row >= N && row < 2 * N) ? w_at<float, N>(Wt, rowof[row], tc + S::TC * jj) : 0.0f;
     }
 #pragma unroll 4
     for (int kk = 0; kk < N; ++kk) {
-      const float* wrow = Wt + rowof[kk] * S::LDW + tc;
+      const int orow = rowof[kk];
       float bv[S::CPT], av[S::RPT];
 #pragma unroll
-      for (int jj = 0; jj < S::CPT; ++jj) bv[jj] = wrow[S::TC * jj];
+      for (int jj = 0; jj < S::CPT; ++jj) bv[jj] = w_at<float, N>(Wt, orow, tc + S::TC * jj);
 #pragma unroll
       for (int ii = 0; ii < S::RPT; ++ii) av[ii] = Gs[(tr + S::TR * ii) * S::LDG + kk];
 #pragma unroll
@@ -1000,11 +1016,11 @@ struct GrpProduct<float, N> {
 };
 
 // CTAs per SM the register budget is sized for (FP64 n=32 is shared-memory
-// bound at 3; FP32 n=32 at 7)
+// bound at 5, FP32 n=32 register bound at 6)
 template <typename T, int N>
-constexpr int grp_min_blocks() { return N == 32 ? (sizeof(T) == 8 ? 3 : 5) : 4; }
+constexpr int grp_min_blocks() { return N == 32 ? (sizeof(T) == 8 ? 5 : 6) : 4; }
 
-template <typename T, int N>
+template <typename T, int N, bool BATCH = false>
 __global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
     k_factor_lu_grp(FactorArgs<T> a0, const FactorArgs<T>* tab, const BatchCta* cmap) {
   using S = GrpShape<T, N>;
@@ -1016,9 +1032,10 @@ __global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
   int* hdr = reinterpret_cast<int*>(slot + 2 * S::NWP * S::LDS);  // [2][NWP][4] hi, lo, position, thread
   int* rowof = hdr + 2 * S::NWP * 4;               // position -> original row
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  FactorArgs<T> a;
+  FactorArgs<T> ab;  // this CTA's system (batch only)
   long q0, q1, qs;
-  pair_range(a0, tab, cmap, 1, 0, a, q0, q1, qs);
+  pair_range<BATCH>(a0, tab, cmap, 1, 0, ab, q0, q1, qs);
+  const FactorArgs<T>& a = BATCH ? ab : a0;
   const Dims d = a.d;
   const int nr = d.nr, nx = d.nx;
   constexpr int n = N, n2 = 2 * N;
@@ -1038,42 +1055,44 @@ __global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
     // every global load of the pair is issued before the first shared store
     constexpr int IT = (int)((nn + S::NTH - 1) / S::NTH), IB = (8 * N + S::NTH - 1) / S::NTH;
     T row[N], vd[IT], ve[IT], vbt[IB], vbb[IB];
-    if (panel) {
-      const size_t base = top ? (size_t)jp * nn : (size_t)j * nn;
+    // the source (loaded FP64 matrix at the first level, working copy after)
+    // is chosen once per pair, so every load below is a plain batched load
+    auto load = [&](const auto* D, const auto* E, const auto* Bm, const auto* C) {
+      if (panel) {
+        const size_t base = top ? (size_t)jp * nn : (size_t)j * nn;
+        const auto* P = top ? E : D;
 #pragma unroll
-      for (int c = 0; c < N; ++c) {
-        const size_t o = base + (size_t)c * n + ri;
-        row[c] = top ? ldg_src(first, a.E0, a.E, o) : ldg_src(first, a.D0, a.D, o);
+        for (int c = 0; c < N; ++c) row[c] = T(__ldg(P + base + (size_t)c * n + ri));
+      } else {
+#pragma unroll
+        for (int c = 0; c < N; ++c)
+          row[c] = brow ? T(__ldg(C + (size_t)j * nrn + (size_t)c * nr + (t - n2))) : T(0);
       }
-    } else {
 #pragma unroll
-      for (int c = 0; c < N; ++c)
-        row[c] = brow ? ldg_src(first, a.C0, a.C, (size_t)j * nrn + (size_t)c * nr + (t - n2)) : T(0);
-    }
+      for (int it = 0; it < IT; ++it) {
+        const int idx = t + S::NTH * it;
+        const bool in = idx < (int)nn;
+        vd[it] = in ? T(__ldg(D + (size_t)jp * nn + idx)) : T(0);
+        ve[it] = in ? T(__ldg(E + (size_t)j * nn + idx)) : T(0);
+      }
 #pragma unroll
-    for (int it = 0; it < IT; ++it) {
-      const int idx = t + S::NTH * it;
-      const bool in = idx < (int)nn;
-      vd[it] = in ? ldg_src(first, a.D0, a.D, (size_t)jp * nn + idx) : T(0);
-      ve[it] = in ? ldg_src(first, a.E0, a.E, (size_t)j * nn + idx) : T(0);
-    }
-#pragma unroll
-    for (int it = 0; it < IB; ++it) {
-      const int idx = t + S::NTH * it;
-      const bool in = idx < nx * n;
-      vbt[it] = in ? ldg_src(first, a.B0, a.B, (size_t)jp * nnx + idx) : T(0);
-      vbb[it] = in ? ldg_src(first, a.B0, a.B, (size_t)j * nnx + idx) : T(0);
-    }
-    // trailing columns: TOP rows [D_jp 0 B_jp], BOTTOM rows [0 E_j B_j], zero padding
+      for (int it = 0; it < IB; ++it) {
+        const int idx = t + S::NTH * it;
+        const bool in = idx < nx * n;
+        vbt[it] = in ? T(__ldg(Bm + (size_t)jp * nnx + idx)) : T(0);
+        vbb[it] = in ? T(__ldg(Bm + (size_t)j * nnx + idx)) : T(0);
+      }
+    };
+    if (first) load(a.D0, a.E0, a.B0, a.C0);
+    else load(a.D, a.E, a.B, a.C);
+    // trailing columns, compact: TOP rows [D_jp B_jp], BOTTOM rows [E_j B_j]
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
       const int idx = t + S::NTH * it;
       if (idx < (int)nn) {
         const int r = idx % n, c = idx / n;
         Wt[r * S::LDW + c] = vd[it];
-        Wt[r * S::LDW + n + c] = T(0);
-        Wt[(n + r) * S::LDW + c] = T(0);
-        Wt[(n + r) * S::LDW + n + c] = ve[it];
+        Wt[(n + r) * S::LDW + c] = ve[it];
       }
     }
 #pragma unroll
@@ -1081,8 +1100,8 @@ __global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
       const int idx = t + S::NTH * it;
       if (idx < 8 * n) {
         const int r = idx % n, c = idx / n;
-        Wt[r * S::LDW + n2 + c] = vbt[it];
-        Wt[(n + r) * S::LDW + n2 + c] = vbb[it];
+        Wt[r * S::LDW + n + c] = vbt[it];
+        Wt[(n + r) * S::LDW + n + c] = vbb[it];
       }
     }
     // --------------------------------------------------- phase 1: panel LU
@@ -1520,14 +1539,15 @@ struct SweepArgs {
 __device__ __forceinline__ void take_level(SweepArgs<float>& a, const SweepArgs<float>& a0) { a.k = a0.k; }
 __device__ __forceinline__ void take_level(SweepArgs<double>& a, const SweepArgs<double>& a0) { a.k = a0.k; }
 
-template <typename T>
+template <typename T, bool BATCH = false>
 __global__ void __launch_bounds__(WARPS_PANEL * 32) k_forward_level(SweepArgs<T> a0, const SweepArgs<T>* tab,
                                                                 const BatchCta* cmap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  SweepArgs<T> a;
+  SweepArgs<T> ab;  // this CTA's system (batch only)
   long q0, q1, qs;
-  pair_range(a0, tab, cmap, wpb, warp, a, q0, q1, qs);
+  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
+  const SweepArgs<T>& a = BATCH ? ab : a0;
   const Dims d = a.d;
   const int n = d.n, nr = d.nr, n2 = 2 * n, nrhs = a.nrhs, ldw = a.ldw, k = a.k;
   double* W = reinterpret_cast<double*>(smem_raw) + (size_t)warp * ldw * nrhs;
@@ -1586,14 +1606,15 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_forward_level(SweepArgs<T>
   }
 }
 
-template <typename T>
+template <typename T, bool BATCH = false>
 __global__ void __launch_bounds__(WARPS_PANEL * 32) k_backward_level(SweepArgs<T> a0, const SweepArgs<T>* tab,
                                                                  const BatchCta* cmap) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  SweepArgs<T> a;
+  SweepArgs<T> ab;  // this CTA's system (batch only)
   long q0, q1, qs;
-  pair_range(a0, tab, cmap, wpb, warp, a, q0, q1, qs);
+  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
+  const SweepArgs<T>& a = BATCH ? ab : a0;
   const Dims d = a.d;
   const int n = d.n, nx = d.nx, n2 = 2 * n, nrhs = a.nrhs, k = a.k, nb = d.nblock;
   double* Y = reinterpret_cast<double*>(smem_raw) + (size_t)warp * a.ldw;
@@ -1640,14 +1661,15 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_backward_level(SweepArgs<T
 //   xb term added and U solved by n broadcast steps (QRP: column-map scatter).
 // All loads of a pair are issued before the first use.
 // ---------------------------------------------------------------------------
-template <typename TF, int N, int NRM, bool LU>
+template <typename TF, int N, int NRM, bool LU, bool BATCH = false>
 __global__ void __launch_bounds__(256, 2) k_forward_rows(SweepArgs<TF> a0, const SweepArgs<TF>* tab,
                                                          const BatchCta* cmap) {
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  SweepArgs<TF> a;
+  SweepArgs<TF> ab;  // this CTA's system (batch only)
   long q0, q1, qs;
-  pair_range(a0, tab, cmap, wpb, warp, a, q0, q1, qs);
+  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
+  const SweepArgs<TF>& a = BATCH ? ab : a0;
   const Dims d = a.d;
   const int n = d.n, nr = d.nr, n2 = 2 * n, nrhs = a.nrhs, k = a.k;
   const bool act = lane < n2;
@@ -1704,14 +1726,15 @@ __global__ void __launch_bounds__(256, 2) k_forward_rows(SweepArgs<TF> a0, const
   }
 }
 
-template <typename TF, int N, int NXM>
+template <typename TF, int N, int NXM, bool BATCH = false>
 __global__ void __launch_bounds__(256, 2) k_backward_rows(SweepArgs<TF> a0, const SweepArgs<TF>* tab,
                                                           const BatchCta* cmap) {
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  SweepArgs<TF> a;
+  SweepArgs<TF> ab;  // this CTA's system (batch only)
   long q0, q1, qs;
-  pair_range(a0, tab, cmap, wpb, warp, a, q0, q1, qs);
+  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
+  const SweepArgs<TF>& a = BATCH ? ab : a0;
   const Dims d = a.d;
   const int n = d.n, nx = d.nx, nb = d.nblock, n2 = 2 * n, nrhs = a.nrhs, k = a.k;
   const int i = lane & 15;
@@ -1763,6 +1786,106 @@ __global__ void __launch_bounds__(256, 2) k_backward_rows(SweepArgs<TF> a0, cons
         }
       }
       if (!hi && rowok) xc[(size_t)j * n + dst] = y;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// sweeps for n = 32: one warp per pair, lane i holds panel positions i and
+// 32 + i (forward) or U-row i (backward); x values are exchanged by shuffles
+// and every factor element is read once, coalesced
+// ---------------------------------------------------------------------------
+template <typename TF, int NRM, bool BATCH = false>
+__global__ void __launch_bounds__(256, 2) k_forward_rows32(SweepArgs<TF> a0, const SweepArgs<TF>* tab,
+                                                           const BatchCta* cmap) {
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr int n = 32, n2 = 64;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  SweepArgs<TF> ab;  // this CTA's system (batch only)
+  long q0, q1, qs;
+  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
+  const SweepArgs<TF>& a = BATCH ? ab : a0;
+  const Dims d = a.d;
+  const int nr = d.nr, nrhs = a.nrhs, k = a.k;
+  for (long q = q0; q < q1; q += qs) {
+    const int j = k + (int)(2L * k * q), jp = j - k;
+    const TF* Tj = a.Tm + (size_t)j * szT(d);
+    const unsigned char* Pj = a.P + (size_t)j * szP(d);
+    const int s0 = Pj[lane], s1 = Pj[n + lane];  // original rows at positions lane, 32 + lane
+    double cp[NRM];
+    const TF* Cj = a.C + (size_t)j * nr * n;
+#pragma unroll
+    for (int r = 0; r < NRM; ++r) cp[r] = r < nr ? double(Cj[(size_t)lane * nr + r]) : 0.0;
+    for (int col = 0; col < nrhs; ++col) {
+      double* xc = a.x + (size_t)col * a.ldx;
+      const double ot = xc[(size_t)jp * n + lane], ob = xc[(size_t)j * n + lane];
+      const double a0t = __shfl_sync(FULL, ot, s0 & 31), a0b = __shfl_sync(FULL, ob, s0 & 31);
+      const double a1t = __shfl_sync(FULL, ot, s1 & 31), a1b = __shfl_sync(FULL, ob, s1 & 31);
+      double w0 = s0 < n ? a0t : a0b, w1 = s1 < n ? a1t : a1b;
+#pragma unroll
+      for (int i = 0; i < n; ++i) {
+        const double wi = __shfl_sync(FULL, w0, i);
+        const double t0 = double(Tj[(size_t)i * n2 + lane]), t1 = double(Tj[(size_t)i * n2 + n + lane]);
+        if (lane > i) w0 = fma(-t0, wi, w0);
+        w1 = fma(-t1, wi, w1);
+      }
+      xc[(size_t)j * n + lane] = w0;
+      xc[(size_t)jp * n + lane] = w1;
+#pragma unroll
+      for (int r = 0; r < NRM; ++r) {
+        if (r < nr) {
+          const double sr = warp_sum(cp[r] * w0);
+          if (lane == 0) a.XB[(size_t)j * nr * nrhs + (size_t)col * nr + r] = -sr;
+        }
+      }
+    }
+  }
+}
+
+template <typename TF, int NXM, bool BATCH = false>
+__global__ void __launch_bounds__(256, 2) k_backward_rows32(SweepArgs<TF> a0, const SweepArgs<TF>* tab,
+                                                            const BatchCta* cmap) {
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr int n = 32, n2 = 64;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  SweepArgs<TF> ab;  // this CTA's system (batch only)
+  long q0, q1, qs;
+  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
+  const SweepArgs<TF>& a = BATCH ? ab : a0;
+  const Dims d = a.d;
+  const int nx = d.nx, nb = d.nblock, nrhs = a.nrhs, k = a.k;
+  const bool qrp = a.sel == SEL_QRP;
+  const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
+  constexpr size_t nn = (size_t)n * n;
+  for (long q = q0; q < q1; q += qs) {
+    const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
+    const TF* Dj = a.D + (size_t)j * nn;
+    const TF* Ej = a.E + (size_t)j * nn;
+    const TF* Bj = a.B + (size_t)j * n * nx;
+    const TF* Tj = a.Tm + (size_t)j * szT(d);
+    const double rdi = 1.0 / double(Tj[(size_t)lane * n2 + lane]);
+    const int dst = qrp ? (int)a.P[(size_t)j * szP(d) + n2 + lane] : lane;
+    for (int col = 0; col < nrhs; ++col) {
+      double* xc = a.x + (size_t)col * a.ldx;
+      const double xjp = xc[(size_t)jp * n + lane], xjpp = xc[(size_t)jpp * n + lane];
+      const double xj = xc[(size_t)j * n + lane];
+      double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+      for (int c = 0; c < n; ++c) {
+        s0 = fma(double(Dj[(size_t)c * n + lane]), __shfl_sync(FULL, xjp, c), s0);
+        s1 = fma(double(Ej[(size_t)c * n + lane]), __shfl_sync(FULL, xjpp, c), s1);
+      }
+#pragma unroll
+      for (int c = 0; c < NXM; ++c)
+        if (c < nx) s0 = fma(double(Bj[(size_t)c * n + lane]), xc[xb_off + c], s0);
+      double y = xj - (s0 + s1);
+#pragma unroll
+      for (int ii = n - 1; ii >= 0; --ii) {
+        const double xi = __shfl_sync(FULL, y * rdi, ii);
+        if (lane == ii) y = xi;
+        else if (lane < ii) y = fma(-double(Tj[(size_t)ii * n2 + lane]), xi, y);
+      }
+      xc[(size_t)j * n + dst] = y;
     }
   }
 }
@@ -2305,6 +2428,10 @@ static SweepPlan<T> plan_sweeps(const DevState& s) {
 #undef BCR_FWD
 #undef BCR_BWD
   }
+  if (n == 32) {
+    if (s.sel == SEL_LU && d.nr <= 8) p.fwd = d.nr <= 4 ? k_forward_rows32<T, 4> : k_forward_rows32<T, 8>;
+    if (d.nx <= 8) p.bwd = d.nx <= 4 ? k_backward_rows32<T, 4> : k_backward_rows32<T, 8>;
+  }
   return p;
 }
 
@@ -2686,25 +2813,25 @@ static void batch_pairs(BatchClass& c, int L, cudaStream_t st) {
   if (c.fam == PAIR_TC) {
     if (c.n == 16) {
       const size_t sm = tc_smem_per_warp(16) * 4;
-      smem_limit_once(k_factor_lu_tc<16>, sm);
-      k_factor_lu_tc<16><<<g, 128, sm, st>>>(a0, tab, map);
+      smem_limit_once(k_factor_lu_tc<16, true>, sm);
+      k_factor_lu_tc<16, true><<<g, 128, sm, st>>>(a0, tab, map);
     } else {
       const size_t sm = tc_smem_per_warp(8) * 4;
-      smem_limit_once(k_factor_lu_tc<8>, sm);
-      k_factor_lu_tc<8><<<g, 128, sm, st>>>(a0, tab, map);
+      smem_limit_once(k_factor_lu_tc<8, true>, sm);
+      k_factor_lu_tc<8, true><<<g, 128, sm, st>>>(a0, tab, map);
     }
   } else if (c.fam == PAIR_GRP) {
     if (c.n == 32) {
-      smem_limit_once(k_factor_lu_grp<double, 32>, GrpShape<double, 32>::BYTES);
-      k_factor_lu_grp<double, 32><<<g, 96, GrpShape<double, 32>::BYTES, st>>>(a0, tab, map);
+      smem_limit_once(k_factor_lu_grp<double, 32, true>, GrpShape<double, 32>::BYTES);
+      k_factor_lu_grp<double, 32, true><<<g, 96, GrpShape<double, 32>::BYTES, st>>>(a0, tab, map);
     } else {
-      smem_limit_once(k_factor_lu_grp<double, 16>, GrpShape<double, 16>::BYTES);
-      k_factor_lu_grp<double, 16><<<g, 64, GrpShape<double, 16>::BYTES, st>>>(a0, tab, map);
+      smem_limit_once(k_factor_lu_grp<double, 16, true>, GrpShape<double, 16>::BYTES);
+      k_factor_lu_grp<double, 16, true><<<g, 64, GrpShape<double, 16>::BYTES, st>>>(a0, tab, map);
     }
   } else {
-    if (c.n <= 4) k_factor_lu_rows<double, 4, 4, 4><<<g, 128, 0, st>>>(a0, tab, map);
-    else if (c.n <= 8) k_factor_lu_rows<double, 8, 4, 4><<<g, 128, 0, st>>>(a0, tab, map);
-    else k_factor_lu_rows<double, 16, 4, 4><<<g, 128, 0, st>>>(a0, tab, map);
+    if (c.n <= 4) k_factor_lu_rows<double, 4, 4, 4, true><<<g, 128, 0, st>>>(a0, tab, map);
+    else if (c.n <= 8) k_factor_lu_rows<double, 8, 4, 4, true><<<g, 128, 0, st>>>(a0, tab, map);
+    else k_factor_lu_rows<double, 16, 4, 4, true><<<g, 128, 0, st>>>(a0, tab, map);
   }
   check_launch("batched pair kernel");
   if (c.nrm > 0) {
@@ -2734,12 +2861,12 @@ static void batch_sweeps_rows(BatchClass& c, cudaStream_t st, bool forward, int 
   a0.k = 1 << L;
   if (forward) {
     const SweepArgs<double>* tab = static_cast<const SweepArgs<double>*>(c.sf);
-    if (r4) k_forward_rows<double, N, 4, true><<<g, 256, 0, st>>>(a0, tab, map);
-    else k_forward_rows<double, N, 8, true><<<g, 256, 0, st>>>(a0, tab, map);
+    if (r4) k_forward_rows<double, N, 4, true, true><<<g, 256, 0, st>>>(a0, tab, map);
+    else k_forward_rows<double, N, 8, true, true><<<g, 256, 0, st>>>(a0, tab, map);
   } else {
     const SweepArgs<double>* tab = static_cast<const SweepArgs<double>*>(c.sb);
-    if (x4) k_backward_rows<double, N, 4><<<g, 256, 0, st>>>(a0, tab, map);
-    else k_backward_rows<double, N, 8><<<g, 256, 0, st>>>(a0, tab, map);
+    if (x4) k_backward_rows<double, N, 4, true><<<g, 256, 0, st>>>(a0, tab, map);
+    else k_backward_rows<double, N, 8, true><<<g, 256, 0, st>>>(a0, tab, map);
   }
 }
 
@@ -2748,18 +2875,32 @@ static void batch_sweep_level(BatchClass& c, cudaStream_t st, bool forward, int 
   if (c.n <= 4) batch_sweeps_rows<4>(c, st, forward, L);
   else if (c.n <= 8) batch_sweeps_rows<8>(c, st, forward, L);
   else if (c.n <= 16) batch_sweeps_rows<16>(c, st, forward, L);
-  else {
+  else if (c.n == 32) {
+    const BatchCta* map = c.smap + c.soff[L];
+    const unsigned g = (unsigned)c.scnt[L];
+    SweepArgs<double> a0{};
+    a0.k = 1 << L;
+    if (forward) {
+      const SweepArgs<double>* tab = static_cast<const SweepArgs<double>*>(c.sf);
+      if (c.nrm <= 4) k_forward_rows32<double, 4, true><<<g, 256, 0, st>>>(a0, tab, map);
+      else k_forward_rows32<double, 8, true><<<g, 256, 0, st>>>(a0, tab, map);
+    } else {
+      const SweepArgs<double>* tab = static_cast<const SweepArgs<double>*>(c.sb);
+      if (c.nxm <= 4) k_backward_rows32<double, 4, true><<<g, 256, 0, st>>>(a0, tab, map);
+      else k_backward_rows32<double, 8, true><<<g, 256, 0, st>>>(a0, tab, map);
+    }
+  } else {
     const BatchCta* map = c.smap + c.soff[L];
     const unsigned g = (unsigned)c.scnt[L];
     SweepArgs<double> a0{};
     a0.k = 1 << L;
     if (forward) {
       const size_t sm = (size_t)odd_ld(2 * c.n) * c.nrhs * 8 * WARPS_PANEL;
-      smem_limit_once(k_forward_level<double>, sm);
-      k_forward_level<double><<<g, WARPS_PANEL * 32, sm, st>>>(a0, static_cast<const SweepArgs<double>*>(c.sf), map);
+      smem_limit_once(k_forward_level<double, true>, sm);
+      k_forward_level<double, true><<<g, WARPS_PANEL * 32, sm, st>>>(a0, static_cast<const SweepArgs<double>*>(c.sf), map);
     } else {
       const size_t sm = (size_t)c.n * 8 * WARPS_PANEL;
-      k_backward_level<double><<<g, WARPS_PANEL * 32, sm, st>>>(a0, static_cast<const SweepArgs<double>*>(c.sb), map);
+      k_backward_level<double, true><<<g, WARPS_PANEL * 32, sm, st>>>(a0, static_cast<const SweepArgs<double>*>(c.sb), map);
     }
   }
   check_launch(forward ? "batched forward sweep" : "batched backward sweep");
