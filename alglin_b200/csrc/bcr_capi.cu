@@ -1666,7 +1666,9 @@ int bcr_batch_load_device(bcr_batch b, int i, const double* D, const double* E, 
       cudaError_t e = cudaMemcpyAsync(c.dst, c.src, c.count * 8, cudaMemcpyDeviceToDevice, b->stream);
       if (e != cudaSuccess) return b->cuda_fail(e, "bcr_batch_load_device");
     }
-  return BCR_OK;
+  // the sources may be released or reused as soon as this returns
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  return e == cudaSuccess ? BCR_OK : b->cuda_fail(e, "bcr_batch_load_device");
 }
 
 double* bcr_batch_device_b(bcr_batch b, int i) {

@@ -10,6 +10,11 @@ Workload (one "step" = factorize + solve of one system):
           (bcr_factorize uploads the matrix from pinned host memory,
            bcr_solve copies the right-hand side in and the solution out)
 
+  variants: the mixed path (FP32 factors + FP64 refinement to rel. residual
+          <= 1e-12) on the same workload; FP64 and mixed on n=32, nblock=65536,
+          nr=nx=8; and a batch of 4096 uneven systems (systems/s, p50/p99 of the
+          batch latency), each through its own CUDA graph, device-timed.
+
 The matrix (0.65 GB) is larger than L2 (126 MB), so no L2 flush is needed
 between steps.  Multi-GPU: one process per GPU, each solving its own system
 (independent replicas, weak scaling, no collective on the data path).
@@ -307,11 +312,117 @@ def run_ours(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if not args.no_variants and world == 1:
+            line["variants"] = variants(torch, bcr, synth, min(args.steps, 10), 3, rank)
         print(json.dumps(line))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def graph_step_time(torch, bcr, h, s, b, steps, warmup, prec):
+    """Device time of one factorize + solve graph step of system s on handle h."""
+    L = max(s.nrows, s.ncols)
+    h.set_precision(prec)
+    h.upload()
+    b_dev = torch.from_numpy(b).cuda()
+    x_dev = torch.empty_like(b_dev)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(h.stream())
+    h.graph_capture(bcr.GRAPH_STEP, 1, x_dev.data_ptr(), L, b_dev.data_ptr())
+    for _ in range(warmup):
+        h.graph_launch(bcr.GRAPH_STEP)
+    h.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        h.graph_launch(bcr.GRAPH_STEP)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    assert h.factorize_status(), h.last_error()
+    it, rr = h.refinement_info()
+    x = x_dev.cpu().numpy()
+    relres = rel_residual_host(h, s, x, b)
+    return {"value": s.ncols / (ms * 1e-3), "unit": "unknowns/s", "ms_per_step": ms,
+            "rel_residual": relres, "refinement_steps": it if prec else 0}
+
+
+def variants(torch, bcr, synth, steps, warmup, rank):
+    """The other measured paths: the mixed path on this workload, both paths on
+    the n=32 workload, and the batch of 4096 uneven systems."""
+    out = {}
+    sB = synth.collocation(**CFG, seed=rank)
+    bB = synth.rhs(sB, 1, seed=1 + rank)[0]
+    h = bcr.BorderedCR()
+    h.load_system(sB)
+    out["B_mixed"] = graph_step_time(torch, bcr, h, sB, bB, steps, warmup, bcr.PRECISION_MIXED)
+    del h
+    cC = dict(synth.CONFIGS["C"])
+    sC = synth.collocation(**cC, kappa=1.0, seed=rank)
+    bC = synth.rhs(sC, 1, seed=1 + rank)[0]
+    hC = bcr.BorderedCR()
+    hC.load_system(sC)
+    f64 = graph_step_time(torch, bcr, hC, sC, bC, steps, warmup, bcr.PRECISION_FP64)
+    mix = graph_step_time(torch, bcr, hC, sC, bC, steps, warmup, bcr.PRECISION_MIXED)
+    del hC
+    wl = "trapezoid-collocation BABD n=32 nblock=65536 nr=nx=8 kappa=1, 1 rhs"
+    out["C_fp64"] = dict(f64, workload=wl)
+    out["C_mixed"] = dict(mix, workload=wl)
+    out["C_mixed_over_fp64"] = mix["value"] / f64["value"]
+    try:
+        out["D_batched_fp64"] = batched(torch, bcr, synth, rank)
+    except Exception as e:  # e.g. not enough device memory on a shared GPU
+        out["D_batched_fp64"] = {"unavailable": str(e)[:200]}
+    return out
+
+
+def batched(torch, bcr, synth, rank, nsys=4096):
+    """4096 independent systems, nblock ~ U{64..4096}, n in {4,8,16,32},
+    nr = nx in {0,2,4}: one CUDA graph per factorize + solve of the whole batch."""
+    from cuda.bindings import runtime as rt
+    dims = synth.batch_dims(nsys, 64, 4096, seed=rank)
+    bt = bcr.Batch()
+    for d in dims:
+        bt.add_device(*d)
+    bt.prepare()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(7 + rank)
+    for i, d in enumerate(dims):
+        ts = synth.collocation_torch(torch, *d, seed=i + nsys * rank)
+        r, c = bt.system_size(i)
+        rhs = torch.zeros(max(r, c), dtype=torch.float64, device="cuda")
+        rhs[:r] = torch.randn(r, generator=g, device="cuda", dtype=torch.float64)
+        torch.cuda.synchronize()  # the blocks and rhs are complete before they are copied
+        bt.load_device(i, *[t.data_ptr() if t.numel() else 0 for t in ts])
+        rt.cudaMemcpy(bt.device_b(i), rhs.data_ptr(), max(r, c) * 8, rt.cudaMemcpyKind.cudaMemcpyDeviceToDevice)
+    bt.autotune()
+    bt.graph_capture()
+    stream = torch.cuda.ExternalStream(bt.stream())
+    for _ in range(3):
+        bt.graph_launch()
+    bt.synchronize()
+    lat = []
+    for _ in range(10):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        bt.graph_launch()
+        e1.record(stream)
+        e1.synchronize()
+        lat.append(e0.elapsed_time(e1))
+    ok = bt.check_status()
+    lat.sort()
+    p50, p99 = lat[len(lat) // 2], lat[-1]
+    unk = sum(n * (nb + 1) + nx for nb, n, _, _, _, nx in dims)
+    return {"systems_per_s": nsys / (p50 * 1e-3), "unknowns_per_s": unk / (p50 * 1e-3),
+            "p50_ms": p50, "p99_ms": p99, "nsys": nsys, "all_factorized": bool(ok),
+            "classes": [{"n": c[0], "systems": c[1], "family": ["auto", "tc", "grp", "rows"][c[2]],
+                         "pairs_per_cta": c[3]} for c in bt.classes()],
+            "workload": "4096 systems, nblock U{64..4096}, n in {4,8,16,32}, nr=nx in {0,2,4}, "
+                        "collocation blocks drawn on the device"}
 
 
 def cpu_baseline(s, b):
@@ -340,6 +451,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--no-variants", action="store_true",
+                    help="skip the mixed-path, n=32 and batched measurements")
     ap.add_argument("--nblock", type=int, default=CFG["nblock"],
                     help="smaller systems for profiling runs (the reported workload is 100000)")
     args = ap.parse_args()

@@ -238,7 +238,9 @@ int bcr_batch_matrix(bcr_batch b, int i, double **D, double **E, double **B, dou
                      double **F, double **H);
 int bcr_batch_system_size(bcr_batch b, int i, int *nrows, int *ncols);
 /* copy system i's blocks from caller device buffers (reference layout,
-   contiguous; NULL skips a block), enqueued on the batch stream */
+   contiguous; NULL skips a block).  The sources must be complete when the
+   call is made (synchronize the stream that wrote them); the call returns
+   when the copies are done, so the sources may then be reused. */
 int bcr_batch_load_device(bcr_batch b, int i, const double *D, const double *E, const double *B,
                           const double *C, const double *Cq, const double *F, const double *H);
 int bcr_batch_size(bcr_batch b);

@@ -99,6 +99,7 @@ def test_batch_device_only_systems():
     keep = []
     for i, s in enumerate(systems):
         ts = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (s.D, s.E, s.B, s.C, s.Cq, s.F, s.H)]
+        torch.cuda.synchronize()
         keep.append(ts)
         bt.load_device(i, *[t.data_ptr() if t.numel() else 0 for t in ts])
     bt.synchronize()
