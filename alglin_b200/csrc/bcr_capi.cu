@@ -135,6 +135,7 @@ struct bcr_handle_s {
     dfree(z.D); dfree(z.E); dfree(z.B); dfree(z.C); dfree(z.T); dfree(z.P);
     dfree(z.Rbuf); dfree(z.Fbuf); dfree(z.XB); dfree(z.part); dfree(z.Ffin); dfree(z.Hl);
     dfree(z.tau_l); dfree(z.piv_l); dfree(z.st); dfree(z.mv_part); dfree(z.slab);
+    dfree(z.Ul); dfree(z.Vl); dfree(z.Sl); dfree(z.Al);
     dfree(z.Df); dfree(z.Ef); dfree(z.Bf); dfree(z.Cf); dfree(z.Tf); dfree(z.Rbuff);
     dfree(dX); dfree(dY); dfree(dB); dfree(dR); dfree(dNorm); dfree(dRow);
     dX_cap = dY_cap = dB_cap = dR_cap = dNorm_cap = dRow_cap = 0;
@@ -185,7 +186,9 @@ struct bcr_handle_s {
     z.part_cap = (int)(parts * 256);
     A(dalloc(z.part, (size_t)z.part_cap));
     A(dalloc(z.Ffin, std::max<size_t>(nr * nx, 1)));
-    A(dalloc(z.Hl, (size_t)d.Nr * d.Nc)); A(dalloc(z.tau_l, Lmax)); A(dalloc(z.piv_l, Lmax));
+    A(dalloc(z.Hl, (size_t)d.Nr * d.Nc)); A(dalloc(z.tau_l, Lmax)); A(dalloc(z.piv_l, 2 * Lmax));
+    A(dalloc(z.Ul, Lmax * Lmax)); A(dalloc(z.Vl, Lmax * Lmax)); A(dalloc(z.Sl, Lmax));
+    A(dalloc(z.Al, (size_t)d.Nr * d.Nc));
     A(dalloc(z.st, 1)); A(dalloc(z.mv_part, (nb + 2) * nr));
     z.slab_elems = bcr::cta_slab_elems(d);
     z.slab_ctas = 148 * 2;  // the CTA-per-pair kernel may be chosen for any n
@@ -267,12 +270,9 @@ struct bcr_handle_s {
 
   // selection state copied into the device state before any launch
   int prepare_launch() {
-    if (sel_last != bcr::LAST_LU && sel_last != bcr::LAST_QR)
-      return fail(BCR_NUMERICAL,
-                  fmt("BorderedCR<t_Value>::load_and_factorize_last failed\n"
-                      "(last block solver '%s' is not available on the device)\n", kLastName[sel_last]));
     s.sel = sel;
     s.sel_last = sel_last;
+    s.sel_last2 = sel_last2;
     s.use_tc = use_tc;
     s.mixed = precision == BCR_PRECISION_MIXED ? 1 : 0;
     if (s.mixed) {
@@ -344,13 +344,8 @@ struct bcr_handle_s {
       return fail(BCR_NUMERICAL, fmt("BorderedCR::buildT [%s] singular R factor at block %d (column %d)\n",
                                      sel == bcr::SEL_QR ? "QR" : "QRP", st.block, st.info));
     }
-    if (st.code == bcr::DEV_LAST_SINGULAR || st.code == bcr::DEV_BAD_SHAPE) {
-      if (sel_last2 != 0)
-        return fail(BCR_NUMERICAL,
-                    fmt("BorderedCR<t_Value>::load_and_factorize_last failed\n"
-                        "(fallback solver '%s' is not available on the device)\n", kLast2Name[sel_last2]));
+    if (st.code == bcr::DEV_LAST_SINGULAR || st.code == bcr::DEV_BAD_SHAPE)
       return fail(BCR_NUMERICAL, "BorderedCR<t_Value>::load_and_factorize_last failed\n");
-    }
     factorized = true;
     return BCR_OK;
   }
@@ -1420,9 +1415,6 @@ int bcr_batch_s::prepare(int autotune) {
       dims[i] = h->d;
       last_sel[i] = h->sel_last;
     }
-    if (last_sel[i] != bcr::LAST_LU && last_sel[i] != bcr::LAST_QR)
-      return fail(BCR_BAD_ARGUMENT, fmt("batch system %zu: last block solver '%s' is not available on the device\n",
-                                        i, kLastName[last_sel[i]]));
     fam[i] = default_family(dims[i]);
     if (fam[i] < 0)
       return fail(BCR_BAD_ARGUMENT,
@@ -1431,7 +1423,7 @@ int bcr_batch_s::prepare(int autotune) {
   }
   // ------------------------------------------------------------ layout
   Bump in, work;
-  struct Off { size_t D0, E0, B0, C0, Cq, F0, H, D, E, B, C, T, P, Rbuf, Fbuf, XB, Ffin, Hl, tau, piv; };
+  struct Off { size_t D0, E0, B0, C0, Cq, F0, H, D, E, B, C, T, P, Rbuf, Fbuf, XB, Ffin, Hl, tau, piv, U, V, S; };
   std::vector<Off> off(ns);
   in_len.assign(ns, 0);
   for (size_t i = 0; i < ns; ++i) {
@@ -1447,7 +1439,11 @@ int bcr_batch_s::prepare(int autotune) {
     o.C = work.take((nb + 1) * nr * n * 8); o.T = work.take(nb * (2 * n * n + n) * 8);
     o.P = work.take(nb * 3 * n); o.Rbuf = work.take(nb * nr * n * 8); o.Fbuf = work.take(nb * nr * nx * 8);
     o.XB = work.take(nb * nr * 8); o.Ffin = work.take(std::max<size_t>(nr * nx, 1) * 8);
-    o.Hl = work.take((size_t)d.Nr * d.Nc * 8); o.tau = work.take(Lb * 8); o.piv = work.take(Lb * 4);
+    o.Hl = work.take((size_t)d.Nr * d.Nc * 8); o.tau = work.take(Lb * 8); o.piv = work.take(2 * Lb * 4);
+    const bool svd = last_sel[i] >= bcr::LAST_SVD;  // the SVD family needs U, V, S
+    o.U = svd ? work.take(Lb * Lb * 8) : 0;
+    o.V = svd ? work.take(Lb * Lb * 8) : 0;
+    o.S = svd ? work.take(Lb * 8) : 0;
     x_off[i] = x_elems;
     x_elems += ((size_t)L(i) + 31) & ~size_t(31);
   }
@@ -1482,6 +1478,9 @@ int bcr_batch_s::prepare(int autotune) {
     s.P = d_work + o.P;
     s.Rbuf = W(o.Rbuf); s.Fbuf = W(o.Fbuf); s.XB = W(o.XB); s.xb_cap = 1;
     s.Ffin = W(o.Ffin); s.Hl = W(o.Hl); s.tau_l = W(o.tau); s.piv_l = reinterpret_cast<int*>(d_work + o.piv);
+    const bool svd = last_sel[i] >= bcr::LAST_SVD;
+    s.Ul = svd ? W(o.U) : nullptr; s.Vl = svd ? W(o.V) : nullptr; s.Sl = svd ? W(o.S) : nullptr;
+    s.Al = nullptr; s.sel_last2 = 0;
     s.st = d_st + i;
     s.bx = d_x + x_off[i];
     s.bldx = L(i);
@@ -1620,10 +1619,12 @@ int bcr_batch_add_device(bcr_batch b, int nblock, int n, int qr, int qx, int nr,
     return b->fail(BCR_BAD_ARGUMENT, fmt("bcr_batch_add_device( nblock=%d, n=%d, qr=%d, qx=%d, nr=%d, nx=%d ) bad sizes\n",
                                          nblock, n, qr, qx, nr, nx));
   const std::string ls = last ? last : "LU";
-  int sl;
-  if (ls == "LU") sl = bcr::LAST_LU;
-  else if (ls == "QR") sl = bcr::LAST_QR;
-  else return b->fail(BCR_BAD_ARGUMENT, fmt("bcr_batch_add_device: last block solver '%s' is not available\n", ls.c_str()));
+  static const char* names[] = {"LU", "LUPQ", "QR", "QRP", "SVD", "LSS", "LSY", "PINV"};
+  int sl = -1;
+  for (int k = 0; k < 8; ++k)
+    if (ls == names[k]) sl = k;
+  if (sl < 0)
+    return b->fail(BCR_BAD_ARGUMENT, fmt("bcr_batch_add_device: unknown last block solver '%s'\n", ls.c_str()));
   b->release();
   Dims d{};
   d.nblock = nblock; d.n = n; d.qr = qr; d.qx = qx; d.nr = nr; d.nx = nx;

@@ -52,8 +52,12 @@ struct BatchCta {
   long q0, q1;
 };
 
-// status layout: [0] code, [1] block index, [2] LAPACK-style info, [3] level
-struct StatusWords { int code, block, info, level; };
+// factorization of the last block actually in use (written by the device)
+enum LastFact : int { FACT_LU = 0, FACT_LUPQ = 1, FACT_QR = 2, FACT_QRP = 3, FACT_SVD = 4, FACT_SVD_T = 5 };
+
+// status layout: [0] code, [1] block index, [2] LAPACK-style info, [3] level,
+// [4] LastFact of the last block
+struct StatusWords { int code, block, info, level, kind; };
 
 __device__ inline void report(StatusWords* st, int code, int block, int info, int level) {
   if (atomicCAS(&st->code, 0, code) == 0) {

@@ -30,7 +30,10 @@ struct DevState {
   double *Ffin;         // F + sum of Schur updates (nr x nx)
   double *Hl;           // last block Nr x Nc
   double *tau_l;        // last block Householder scalars
-  int* piv_l;           // last block pivots
+  int* piv_l;           // last block pivots: rows, then columns (2 * max(Nr, Nc))
+  double *Ul, *Vl, *Sl; // last block SVD: W = U*S (max(Nr,Nc) x min), V, S
+  double* Al;           // copy of the assembled last block for the fallback solver
+  int sel_last2;        // fallback solver (0: none, else the SVD family)
   StatusWords* st;      // device status
   double* mv_part;      // Mv border partials ((nblock+1) x nr)
   // mixed precision: FP32 working blocks and factors (the loaded matrix, F,

@@ -1962,13 +1962,126 @@ __device__ T block_sum(T v, T* sv) {
   return sv[0];
 }
 
-// kind: LAST_LU or LAST_QR (others are rejected on the host)
+// buffers of the last block (one CTA works on them)
+struct LastBufs {
+  double* A;    // Nr x Nc (ld Nr): the assembled block, then its factors
+  double* A2;   // copy for the fallback solver (null when there is none)
+  int* piv;     // row pivots [0, L), column pivots [L, 2L), L = max(Nr, Nc)
+  double* tau;  // Householder scalars
+  double* U;    // SVD: W = U*S, max(Nr,Nc) x min(Nr,Nc)
+  double* V;    // SVD: min x min
+  double* S;    // SVD: singular values
+};
+
+__device__ inline int last_kind_of(int sel_last, int M, int N) {
+  switch (sel_last) {
+    case LAST_LU: return FACT_LU;
+    case LAST_LUPQ: return FACT_LUPQ;
+    case LAST_QR: return FACT_QR;
+    case LAST_QRP: return FACT_QRP;
+    default: return M >= N ? FACT_SVD : FACT_SVD_T;  // SVD, LSS, LSY, PINV
+  }
+}
+
+// Minimum-norm least-squares factorization of the SVD family (the solvers
+// SVD, LSS, LSY and PINV of the reference's LapackWrapper): one-sided Jacobi
+// on W = A (or A^T when Nr < Nc), rotations of a pair of columns p < q by the
+// angle that makes them orthogonal, skipped when |g| <= 1e-15 sqrt(a b); the
+// pairs of a sweep follow the round-robin (circle) schedule, so the Np/2 pairs
+// of a round are independent and run one per warp; at most 80 sweeps, ending
+// at the first sweep without a rotation.  On return W = U*S is split into
+// unit columns U and S.
+__device__ void last_svd(Dims d, const double* A, LastBufs b, StatusWords* st) {
+  __shared__ int rotated;
+  const int M = d.Nr, N = d.Nc, tid = threadIdx.x, bs = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
+  const bool tr = M < N;
+  const int Mp = tr ? N : M, Np = tr ? M : N;
+  double* W = b.U;
+  double* V = b.V;
+  for (int e = tid; e < Mp * Np; e += bs) {
+    const int i = e % Mp, j = e / Mp;
+    W[(size_t)j * Mp + i] = tr ? A[(size_t)i * M + j] : A[(size_t)j * M + i];
+  }
+  for (int e = tid; e < Np * Np; e += bs) V[e] = (e % Np == e / Np) ? 1.0 : 0.0;
+  __syncthreads();
+  const int P = Np + (Np & 1);
+  for (int sweep = 0; sweep < 80; ++sweep) {
+    if (tid == 0) rotated = 0;
+    __syncthreads();
+    for (int r = 0; r < P - 1; ++r) {
+      for (int k = warp; k < P / 2; k += nw) {
+        int p0, q0;
+        if (k == 0) { p0 = P - 1; q0 = r; }
+        else { p0 = (r + k) % (P - 1); q0 = (r - k + P - 1) % (P - 1); }
+        const int p = min(p0, q0), q = max(p0, q0);
+        if (q >= Np) continue;
+        double* wp = W + (size_t)p * Mp;
+        double* wq = W + (size_t)q * Mp;
+        double a = 0.0, bb = 0.0, g = 0.0;
+        for (int i = lane; i < Mp; i += 32) {
+          const double x = wp[i], y = wq[i];
+          a = fma(x, x, a);
+          bb = fma(y, y, bb);
+          g = fma(x, y, g);
+        }
+        a = warp_sum(a);
+        bb = warp_sum(bb);
+        g = warp_sum(g);
+        if (fabs(g) <= 1e-15 * sqrt(a * bb) || g == 0.0) continue;
+        const double zeta = (bb - a) / (2.0 * g);
+        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+        for (int i = lane; i < Mp; i += 32) {
+          const double x = wp[i], y = wq[i];
+          wp[i] = c * x - s * y;
+          wq[i] = s * x + c * y;
+        }
+        double* vp = V + (size_t)p * Np;
+        double* vq = V + (size_t)q * Np;
+        for (int i = lane; i < Np; i += 32) {
+          const double x = vp[i], y = vq[i];
+          vp[i] = c * x - s * y;
+          vq[i] = s * x + c * y;
+        }
+        if (lane == 0) rotated = 1;
+      }
+      __syncthreads();
+    }
+    const int any = rotated;
+    __syncthreads();
+    if (!any) break;
+  }
+  for (int j = warp; j < Np; j += nw) {
+    double* wj = W + (size_t)j * Mp;
+    double s2 = 0.0;
+    for (int i = lane; i < Mp; i += 32) s2 = fma(wj[i], wj[i], s2);
+    const double sj = sqrt(warp_sum(s2));
+    if (lane == 0) b.S[j] = sj;
+    if (sj > 0.0)
+      for (int i = lane; i < Mp; i += 32) wj[i] /= sj;
+  }
+  if (tid == 0) st->kind = tr ? FACT_SVD_T : FACT_SVD;
+  __syncthreads();
+}
+
+// load_and_factorize_last (cc:1281-1374) with the reference's last-block
+// solvers: LU (getrf), LUPQ (complete pivoting), QR (geqrf), QRP (geqp3: the
+// column of largest remaining 2-norm first), and the SVD family
 template <typename T>
-__device__ void last_factor_body(Dims d, T* A, int* piv, T* tau, int kind, StatusWords* st) {
+__device__ void last_factor_body(Dims d, LastBufs b, int sel_last, StatusWords* st) {
   __shared__ T sv[32];
   __shared__ int si[32];
   const int M = d.Nr, N = d.Nc, tid = threadIdx.x, bs = blockDim.x;
-  if (kind == LAST_LU) {
+  const int kind = last_kind_of(sel_last, M, N);
+  T* A = b.A;
+  int* piv = b.piv;
+  T* tau = b.tau;
+  if (kind == FACT_SVD || kind == FACT_SVD_T) {
+    last_svd(d, A, b, st);
+    return;
+  }
+  if (kind == FACT_LU) {
     if (M != N) { if (tid == 0) report(st, DEV_BAD_SHAPE, -1, 0, -1); return; }
     for (int i = 0; i < N; ++i) {
       T best = T(-1);
@@ -1997,9 +2110,71 @@ __device__ void last_factor_body(Dims d, T* A, int* piv, T* tau, int kind, Statu
       }
       __syncthreads();
     }
-  } else {  // Householder QR, M >= N
-    if (M < N) { if (tid == 0) report(st, DEV_BAD_SHAPE, -1, 0, -1); return; }
+  } else if (kind == FACT_LUPQ) {
+    if (M != N) { if (tid == 0) report(st, DEV_BAD_SHAPE, -1, 0, -1); return; }
+    const int L = M > N ? M : N;
     for (int i = 0; i < N; ++i) {
+      // largest |a| of the trailing block, first in column-major order on ties
+      const int w = N - i;
+      T best = T(-1);
+      int bidx = i * N + i;
+      for (int e = tid; e < w * w; e += bs) {
+        const int r = i + e % w, c = i + e / w;
+        const T v = dev_abs(A[(size_t)c * N + r]);
+        const int idx = c * N + r;
+        if (v > best || (v == best && idx < bidx)) { best = v; bidx = idx; }
+      }
+      block_argmax(best, bidx, sv, si);
+      const int pr = bidx % N, pc = bidx / N;
+      if (tid == 0) { piv[i] = pr; piv[L + i] = pc; }
+      __syncthreads();
+      if (best == T(0)) { if (tid == 0) report(st, DEV_LAST_SINGULAR, -1, i + 1, -1); return; }
+      if (pr != i)
+        for (int c = tid; c < N; c += bs) {
+          T t = A[(size_t)c * N + i]; A[(size_t)c * N + i] = A[(size_t)c * N + pr]; A[(size_t)c * N + pr] = t;
+        }
+      __syncthreads();
+      if (pc != i)
+        for (int r = tid; r < N; r += bs) {
+          T t = A[(size_t)i * N + r]; A[(size_t)i * N + r] = A[(size_t)pc * N + r]; A[(size_t)pc * N + r] = t;
+        }
+      __syncthreads();
+      const T pv = A[(size_t)i * N + i];
+      __syncthreads();
+      for (int r = i + 1 + tid; r < N; r += bs) A[(size_t)i * N + r] /= pv;
+      __syncthreads();
+      const int Lr = N - i - 1;
+      for (int e = tid; e < Lr * Lr; e += bs) {
+        const int r = i + 1 + e % Lr, c = i + 1 + e / Lr;
+        A[(size_t)c * N + r] -= A[(size_t)i * N + r] * A[(size_t)c * N + i];
+      }
+      __syncthreads();
+    }
+  } else {  // Householder QR (QRP: largest remaining column first), M >= N
+    if (M < N) { if (tid == 0) report(st, DEV_BAD_SHAPE, -1, 0, -1); return; }
+    const int L = M > N ? M : N;
+    if (kind == FACT_QRP)
+      for (int c = tid; c < N; c += bs) piv[L + c] = c;
+    __syncthreads();
+    for (int i = 0; i < N; ++i) {
+      if (kind == FACT_QRP) {
+        T best = T(-1);
+        int bc = i;
+        for (int c = i + tid; c < N; c += bs) {
+          const T* col = A + (size_t)c * M;
+          T s2 = T(0);
+          for (int r = i; r < M; ++r) s2 += col[r] * col[r];
+          if (s2 > best) { best = s2; bc = c; }
+        }
+        block_argmax(best, bc, sv, si);
+        if (bc != i) {
+          for (int r = tid; r < M; r += bs) {
+            T t = A[(size_t)i * M + r]; A[(size_t)i * M + r] = A[(size_t)bc * M + r]; A[(size_t)bc * M + r] = t;
+          }
+          if (tid == 0) { const int t = piv[L + i]; piv[L + i] = piv[L + bc]; piv[L + bc] = t; }
+        }
+        __syncthreads();
+      }
       T* v = A + (size_t)i * M;
       const T alpha = v[i];
       T s = T(0);
@@ -2029,52 +2204,126 @@ __device__ void last_factor_body(Dims d, T* A, int* piv, T* tau, int kind, Statu
       __syncthreads();
     }
   }
+  if (tid == 0) st->kind = kind;
+}
+
+// the select_last2 fallback (cc:1347-1369): when the chosen solver failed on
+// the last block, factor the saved copy with the SVD family instead
+__device__ void last_fallback_body(Dims d, LastBufs b, StatusWords* st) {
+  const int code = st->code;
+  __syncthreads();
+  if (code != DEV_LAST_SINGULAR && code != DEV_BAD_SHAPE) return;
+  if (threadIdx.x == 0) *st = StatusWords{0, 0, 0, 0, 0};
+  __syncthreads();
+  last_svd(d, b.A2, b, st);
 }
 
 template <typename T>
-__device__ void last_solve_body(Dims d, const T* A, const int* piv, const T* tau, int kind, T* x,
-                                int ldx, int nrhs) {
+__device__ void last_solve_body(Dims d, LastBufs lb, const StatusWords* st, T* x, int ldx, int nrhs) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* b = reinterpret_cast<T*>(smem_raw);
-  __shared__ T sv[32];
   const int n = d.n, M = d.Nr, N = d.Nc, tid = threadIdx.x, bs = blockDim.x;
+  const int L = M > N ? M : N;
+  T* b = reinterpret_cast<T*>(smem_raw);
+  T* tmp = b + L;
+  __shared__ T sv[32];
+  const int kind = st->kind;
+  const T* A = lb.A;
+  const int* piv = lb.piv;
+  const T* tau = lb.tau;
   const size_t off = (size_t)d.nblock * n;
+  T tol = T(0);
+  if (kind == FACT_SVD || kind == FACT_SVD_T) {
+    const int Np = kind == FACT_SVD ? N : M;
+    T smax = T(0);
+    for (int j = tid; j < Np; j += bs) smax = fmax(smax, lb.S[j]);
+    for (int o = 16; o > 0; o >>= 1) smax = fmax(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+    if ((tid & 31) == 0) sv[tid >> 5] = smax;
+    __syncthreads();
+    if (tid == 0) {
+      T m = T(0);
+      for (int w = 0; w < (bs >> 5); ++w) m = fmax(m, sv[w]);
+      sv[0] = m;
+    }
+    __syncthreads();
+    tol = sv[0] * T(1e-12);
+    __syncthreads();
+  }
   for (int c = 0; c < nrhs; ++c) {
     T* xc = x + (size_t)c * ldx;
     for (int r = tid; r < M; r += bs) b[r] = r < n ? xc[r] : xc[off + (r - n)];
     __syncthreads();
-    if (kind == LAST_LU) {
-      if (tid == 0)
-        for (int i = 0; i < N; ++i) {
-          const int p = piv[i];
-          if (p != i) { T t = b[i]; b[i] = b[p]; b[p] = t; }
-        }
-      __syncthreads();
-      for (int i = 0; i < N; ++i) {
-        const T bi = b[i];
-        for (int r = i + 1 + tid; r < N; r += bs) b[r] -= A[(size_t)i * N + r] * bi;
-        __syncthreads();
-      }
-    } else {
-      for (int i = 0; i < N; ++i) {
-        const T* v = A + (size_t)i * M;
+    if (kind == FACT_SVD || kind == FACT_SVD_T) {
+      // x = V S^+ U^T b (Nr >= Nc) or x = U S^+ V^T b (Nr < Nc)
+      const bool trn = kind == FACT_SVD_T;
+      const int Mp = trn ? N : M, Np = trn ? M : N;
+      const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
+      for (int j = warp; j < Np; j += nw) {
+        const T sj = lb.S[j];
         T s = T(0);
-        for (int r = i + 1 + tid; r < M; r += bs) s += v[r] * b[r];
-        s = block_sum(s, sv);
-        s = (s + b[i]) * tau[i];
+        if (sj > tol) {
+          const T* col = trn ? lb.V + (size_t)j * Np : lb.U + (size_t)j * Mp;
+          const int len = trn ? Np : Mp;
+          for (int i = lane; i < len; i += 32) s = fma(col[i], b[i], s);
+          s = warp_sum(s) / sj;
+        }
+        if (lane == 0) tmp[j] = s;
+      }
+      __syncthreads();
+      const int nout = trn ? Mp : Np;
+      for (int i = tid; i < nout; i += bs) {
+        T s = T(0);
+        for (int j = 0; j < Np; ++j)
+          s = fma(trn ? lb.U[(size_t)j * Mp + i] : lb.V[(size_t)j * Np + i], tmp[j], s);
+        b[i] = s;
+      }
+      __syncthreads();
+    } else {
+      if (kind == FACT_LU || kind == FACT_LUPQ) {
+        if (tid == 0)
+          for (int i = 0; i < N; ++i) {
+            const int p = piv[i];
+            if (p != i) { T t = b[i]; b[i] = b[p]; b[p] = t; }
+          }
         __syncthreads();
-        if (tid == 0) b[i] -= s;
-        for (int r = i + 1 + tid; r < M; r += bs) b[r] -= s * v[r];
+        for (int i = 0; i < N; ++i) {
+          const T bi = b[i];
+          for (int r = i + 1 + tid; r < N; r += bs) b[r] -= A[(size_t)i * N + r] * bi;
+          __syncthreads();
+        }
+      } else {
+        for (int i = 0; i < N; ++i) {
+          const T* v = A + (size_t)i * M;
+          T s = T(0);
+          for (int r = i + 1 + tid; r < M; r += bs) s += v[r] * b[r];
+          s = block_sum(s, sv);
+          s = (s + b[i]) * tau[i];
+          __syncthreads();
+          if (tid == 0) b[i] -= s;
+          for (int r = i + 1 + tid; r < M; r += bs) b[r] -= s * v[r];
+          __syncthreads();
+        }
+      }
+      const int lda = (kind == FACT_LU || kind == FACT_LUPQ) ? N : M;
+      for (int i = N - 1; i >= 0; --i) {
+        const T xi = b[i] / A[(size_t)i * lda + i];
+        __syncthreads();
+        if (tid == 0) b[i] = xi;
+        for (int r = tid; r < i; r += bs) b[r] -= A[(size_t)i * lda + r] * xi;
         __syncthreads();
       }
-    }
-    const int lda = kind == LAST_LU ? N : M;
-    for (int i = N - 1; i >= 0; --i) {
-      const T xi = b[i] / A[(size_t)i * lda + i];
-      __syncthreads();
-      if (tid == 0) b[i] = xi;
-      for (int r = tid; r < i; r += bs) b[r] -= A[(size_t)i * lda + r] * xi;
-      __syncthreads();
+      if (kind == FACT_LUPQ) {
+        if (tid == 0)
+          for (int i = N - 1; i >= 0; --i) {
+            const int q = piv[L + i];
+            if (q != i) { T t = b[i]; b[i] = b[q]; b[q] = t; }
+          }
+        __syncthreads();
+      } else if (kind == FACT_QRP) {
+        for (int i = tid; i < N; i += bs) tmp[piv[L + i]] = b[i];
+        __syncthreads();
+        for (int i = tid; i < N; i += bs) b[i] = tmp[i];
+        __syncthreads();
+      }
     }
     for (int r = tid; r < N; r += bs) {
       if (r < n) xc[r] = b[r];
@@ -2085,14 +2334,21 @@ __device__ void last_solve_body(Dims d, const T* A, const int* piv, const T* tau
 }
 
 template <typename T>
-__global__ void k_last_factor(Dims d, T* A, int* piv, T* tau, int kind, StatusWords* st) {
-  last_factor_body(d, A, piv, tau, kind, st);
+__global__ void k_last_factor(Dims d, LastBufs b, int sel_last, StatusWords* st) {
+  last_factor_body<T>(d, b, sel_last, st);
 }
 
+__global__ void k_last_fallback(Dims d, LastBufs b, StatusWords* st) { last_fallback_body(d, b, st); }
+
 template <typename T>
-__global__ void k_last_solve(Dims d, const T* A, const int* piv, const T* tau, int kind, T* x,
-                             int ldx, int nrhs) {
-  last_solve_body(d, A, piv, tau, kind, x, ldx, nrhs);
+__global__ void k_last_solve(Dims d, LastBufs b, const StatusWords* st, T* x, int ldx, int nrhs) {
+  last_solve_body<T>(d, b, st, x, ldx, nrhs);
+}
+
+static LastBufs last_bufs(const DevState& s) {
+  LastBufs b;
+  b.A = s.Hl; b.A2 = s.Al; b.piv = s.piv_l; b.tau = s.tau_l; b.U = s.Ul; b.V = s.Vl; b.S = s.Sl;
+  return b;
 }
 
 // ---------------------------------------------------------------------------
@@ -2387,8 +2643,16 @@ static void factor_last(DevState& s, const WorkSet<T>& w, cudaStream_t st) {
   k_last_assemble<T><<<grid_for((long)d.Nr * d.Nc, 256, 64), 256, 0, st>>>(
       d, w.D, w.E, w.B, w.C, s.H, s.Cq, s.Ffin, s.Hl);
   check_launch("k_last_assemble");
-  k_last_factor<double><<<1, 512, 0, st>>>(d, s.Hl, s.piv_l, s.tau_l, s.sel_last, s.st);
+  if (s.sel_last2) {  // a copy of the assembled block for the fallback solver
+    cudaMemcpyAsync(s.Al, s.Hl, (size_t)d.Nr * d.Nc * 8, cudaMemcpyDeviceToDevice, st);
+  }
+  const LastBufs lb = last_bufs(s);
+  k_last_factor<double><<<1, 512, 0, st>>>(d, lb, s.sel_last, s.st);
   check_launch("k_last_factor");
+  if (s.sel_last2) {
+    k_last_fallback<<<1, 512, 0, st>>>(d, lb, s.st);
+    check_launch("k_last_fallback");
+  }
 }
 
 template <typename T>
@@ -2481,8 +2745,8 @@ template <typename T>
 static void last_and_backward(DevState& s, const SweepPlan<T>& p, const WorkSet<T>& w, double* x, int ldx,
                               int nrhs, cudaStream_t st) {
   const Dims d = s.d;
-  const size_t smem_l = (size_t)(d.Nr > d.Nc ? d.Nr : d.Nc) * 8;
-  k_last_solve<double><<<1, 256, smem_l, st>>>(d, s.Hl, s.piv_l, s.tau_l, s.sel_last, x, ldx, nrhs);
+  const size_t smem_l = 2 * (size_t)(d.Nr > d.Nc ? d.Nr : d.Nc) * 8;
+  k_last_solve<double><<<1, 256, smem_l, st>>>(d, last_bufs(s), s.st, x, ldx, nrhs);
   check_launch("k_last_solve");
   SweepArgs<T> a = sweep_args(s, w, x, ldx, nrhs);
   a.ldw = d.n;
@@ -2624,6 +2888,7 @@ struct LastDesc {
   int* piv;
   int kind, ldx;
   StatusWords* st;
+  LastBufs lb;
 };
 
 // status reset and the blocks the first level does not touch (odd tail, C_N)
@@ -2632,7 +2897,7 @@ __global__ void __launch_bounds__(256) kb_begin(const LastDesc* t) {
   const Dims d = L.d;
   const int nb = d.nblock;
   const size_t nn = (size_t)d.n * d.n, nnx = (size_t)d.n * d.nx, nrn = (size_t)d.nr * d.n;
-  if (threadIdx.x == 0) *L.st = StatusWords{0, 0, 0, 0};
+  if (threadIdx.x == 0) *L.st = StatusWords{0, 0, 0, 0, 0};
   if (nb % 2 == 1) {
     const size_t b = (size_t)(nb - 1);
     for (size_t e = threadIdx.x; e < nn; e += blockDim.x) {
@@ -2676,7 +2941,8 @@ __global__ void __launch_bounds__(256) kb_last_assemble(const LastDesc* t) {
 __global__ void __launch_bounds__(512) kb_last_factor(const LastDesc* t) {
   const LastDesc& L = t[blockIdx.x];
   if (L.st->code != 0) return;  // a pair of this system already failed
-  last_factor_body(L.d, L.Hl, L.piv, L.tau, L.kind, L.st);
+  __syncthreads();
+  last_factor_body<double>(L.d, L.lb, L.kind, L.st);
 }
 
 // xb += sum of the per-block -C'_j x_j contributions, one CTA per system
@@ -2693,7 +2959,7 @@ __global__ void __launch_bounds__(256) kb_reduce_xb(const LastDesc* t, int nrhs)
 
 __global__ void __launch_bounds__(256) kb_last_solve(const LastDesc* t, int nrhs) {
   const LastDesc& L = t[blockIdx.x];
-  last_solve_body(L.d, (const double*)L.Hl, (const int*)L.piv, (const double*)L.tau, L.kind, L.x, L.ldx, nrhs);
+  last_solve_body<double>(L.d, L.lb, L.st, L.x, L.ldx, nrhs);
 }
 
 bool batch_family_ok(int fam, const Dims& d) {
@@ -2785,9 +3051,10 @@ int batch_build(BatchClass& c, const std::vector<DevState>& sys, int nrhs) {
     l.Fbuf = s.Fbuf; l.XB = s.XB;
     l.D = s.D; l.E = s.E; l.B = s.B; l.C = s.C; l.Ffin = s.Ffin; l.Hl = s.Hl; l.tau = s.tau_l; l.x = s.bx;
     l.piv = s.piv_l; l.kind = s.sel_last; l.ldx = s.bldx; l.st = s.st;
+    l.lb = last_bufs(s);
     ld[i] = l;
   }
-  c.last_smem = lmax * 8;
+  c.last_smem = 2 * lmax * 8;
   std::vector<BatchCta> fmap, smap;
   build_map(sys, c.levels, c.chunk, fmap, c.foff, c.fcnt);
   build_map(sys, c.levels, 8, smap, c.soff, c.scnt);

@@ -218,12 +218,13 @@ int bcr_mv_noalloc(int nblock, int n, int qr, int qx, int nr, int nx,
 /* --- batches of independent systems -----------------------------------------
  * No counterpart in the reference (each BorderedCR object there is factored
  * on its own thread pool).  Many systems -- each a bcr_handle filled through
- * the usual loaders, internal LU, last block LU or QR, FP64 -- are factored
+ * the usual loaders, internal LU, FP64 -- are factored
  * and solved together: prepare() packs every system into one device arena,
  * groups the systems by pair-kernel instance (by block size n) and runs each
  * cyclic-reduction level of all systems of a group in one launch.  Systems
- * may differ in nblock, n (4..16 with nr, nx <= 4; 8, 16, 32 with nr, nx <= 8)
- * and borders.  The handles must stay alive while the batch uses them: their
+ * may differ in nblock, n (4..16 with nr, nx <= 4; 8, 16, 32 with nr, nx <= 8),
+ * borders and last-block solver (select_last2 fallbacks are not applied).
+ * The handles must stay alive while the batch uses them: their
  * host copies are read at prepare() and upload(). */
 typedef struct bcr_batch_s *bcr_batch;
 int bcr_batch_create(bcr_batch *out);
@@ -232,7 +233,8 @@ int bcr_batch_add(bcr_batch b, bcr_handle h);
 /* a system that lives only on the device (no handle, no host copy): after
    prepare(), bcr_batch_matrix() gives the device addresses of its blocks in
    the reference layout (see bcr_block_data) for the caller to fill; last is
-   "LU" or "QR" */
+   the last-block solver ("LU", "LUPQ", "QR", "QRP", "SVD", "LSS", "LSY",
+   "PINV") */
 int bcr_batch_add_device(bcr_batch b, int nblock, int n, int qr, int qx, int nr, int nx, const char *last);
 int bcr_batch_matrix(bcr_batch b, int i, double **D, double **E, double **B, double **C, double **Cq,
                      double **F, double **H);

@@ -15,7 +15,7 @@ from tests._util import GOLDEN_CASES, block_norm_inf, fwd_err, load_golden
 
 pytestmark = pytest.mark.gpu
 
-DEVICE_LAST = ("LU", "QR")   # last-block solvers implemented on the device
+DEVICE_LAST = ("LU", "LUPQ", "QR", "QRP", "SVD", "LSS", "LSY", "PINV")  # all on the device
 
 
 def gpu_solver(s, internal="LU", last="LU", last2="NONE"):
@@ -70,9 +70,7 @@ SHAPES = [
 def test_gpu_matches_oracle_random(dims, internal):
     s = synth.collocation(*dims, seed=sum(dims)) if dims[1] > 1 else synth.dominant(*dims, seed=1)
     b = synth.rhs(s, nrhs=2, seed=7)
-    last = "LU" if s.Nr == s.Nc else "QR"
-    if s.Nr < s.Nc:
-        pytest.skip("under-determined last block needs the SVD family")
+    last = "LU" if s.Nr == s.Nc else ("QR" if s.Nr > s.Nc else "PINV")
     o = po.Oracle(s, internal, last)
     assert o.factorize(), o.last_error()
     xo = o.solve(b)
@@ -236,3 +234,52 @@ def test_gpu_pair_kernel_families(dims, family, precision):
     assert fwd_err(x[0, :s.ncols], xo[0, :s.ncols]) < (1e-10 if precision == "fp64" else 1e-8)
     bar = 1e-13 if precision == "fp64" else 1e-12
     assert relres(o, s, x[0], b[0]) <= bar
+
+
+@pytest.mark.parametrize("last", ["LU", "LUPQ", "QR", "QRP", "SVD", "LSS", "LSY", "PINV"])
+@pytest.mark.parametrize("dims", [(40, 6, 1, 1, 2, 2), (17, 16, 2, 2, 4, 4), (9, 3, 0, 2, 1, 0)])
+def test_gpu_last_block_solvers(dims, last):
+    """Every last-block solver against the oracle (square, and the
+    under-determined shape for the SVD family: minimum-norm solution)."""
+    s = synth.collocation(*dims, seed=sum(dims) + 3)
+    if s.Nr != s.Nc and last in ("LU", "LUPQ"):
+        pytest.skip("LU and LUPQ need a square last block")
+    if s.Nr < s.Nc and last in ("QR", "QRP"):
+        pytest.skip("QR and QRP need Nr >= Nc")
+    b = synth.rhs(s, nrhs=2, seed=4)
+    o = po.Oracle(s, "LU", last)
+    assert o.factorize(), o.last_error()
+    xo = o.solve(b)
+    h = gpu_solver(s, "LU", last)
+    assert h.factorize(), h.last_error()
+    xg = gpu_solve(h, b)
+    for c in range(2):
+        assert fwd_err(xg[c, :s.ncols], xo[c, :s.ncols]) < 1e-9, (last, c)
+
+
+@pytest.mark.parametrize("last2", ["SVD", "LSS", "LSY", "PINV"])
+def test_gpu_last_block_fallback(last2):
+    """test18-BorderedCR-coverage.cc:1061-1098: a singular last block is
+    solved by the select_last2 solver (minimum-norm solution)."""
+    s = synth._zeros(1, 1, 0, 0, 1, 1)
+    s.D[0, 0, 0] = 1; s.H[1, 0] = 1; s.C[0, 0, 0] = 1; s.C[1, 0, 0] = 1
+    h = gpu_solver(s, "LU", "LU", last2)
+    assert h.factorize(), h.last_error()
+    o = po.Oracle(s, "LU", "LU", last2)
+    assert o.factorize()
+    xref = np.array([2.0, -1.0, 0.0])
+    b = np.zeros((1, 3))
+    b[0] = o.mv(xref)
+    xg = gpu_solve(h, b)[0]
+    xo = o.solve(b)[0]
+    assert np.abs(xg - xo).max() < 1e-12
+    assert np.abs(xg - xref).max() < 5e-9
+
+
+def test_gpu_fallback_not_used_when_primary_succeeds():
+    s = synth.collocation(33, 8, 0, 0, 2, 2, seed=8)
+    b = synth.rhs(s, nrhs=1, seed=2)
+    h1 = gpu_solver(s, "LU", "LU", "NONE")
+    h2 = gpu_solver(s, "LU", "LU", "PINV")
+    assert h1.factorize() and h2.factorize()
+    assert np.array_equal(gpu_solve(h1, b), gpu_solve(h2, b))
