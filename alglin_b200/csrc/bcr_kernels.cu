@@ -1250,6 +1250,256 @@ __global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
 }
 
 // ---------------------------------------------------------------------------
+// Large blocks, LU: blocked right-looking elimination of the pair's work
+// matrix (one CTA per pair, the matrix in the CTA's global slab, L2
+// resident).  The panel columns go in blocks of BLK_W: a block is factored in
+// shared memory with the getrf pivot rule (border rows eliminated, never
+// pivots), its row interchanges are applied to every other column, the
+// BLK_W rows of the trailing columns are solved with the block's unit lower
+// triangle, and the rows below are updated with one product of depth BLK_W
+// -- FP64 tensor cores (DMMA 8x8x4) for double, FMA tiles for float.  The
+// result equals the unblocked elimination (getrf on the panel followed by
+// the trailing updates) up to rounding order.
+// ---------------------------------------------------------------------------
+constexpr int BLK_W = 32;
+
+// W[c*R + r] -= sum_m L[m*LD + r] * W[c*R + k0 + m] for r in [r0, R), c in [c0, NC), m < w
+// L: the factored block in shared memory (column m, row r), U: rows [k0, k0+w) of W
+template <typename T>
+__device__ void blk_update(T* W, int R, int NC, const T* Lsm, int LD, int k0, int w, int r0, int c0) {
+  const int tid = threadIdx.x, bs = blockDim.x;
+  const int rows = R - r0, cols = NC - c0;
+  if (rows <= 0 || cols <= 0) return;
+  if constexpr (sizeof(T) == 8) {
+    // 16 x 16 output per warp iteration (2 x 2 DMMA tiles)
+    const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
+    const int g = lane >> 2, q = lane & 3;
+    const int tr = (rows + 15) / 16, tc = (cols + 15) / 16;
+    for (int t = warp; t < tr * tc; t += nw) {
+      const int rb = r0 + (t % tr) * 16, cb = c0 + (t / tr) * 16;
+      double acc[2][2][2] = {};
+      for (int ks = 0; ks < (w + 3) / 4; ++ks) {
+        const int m = ks * 4 + q;
+        const bool mk = m < w;
+        double af[2], bf[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int r = rb + u * 8 + g;
+          af[u] = (mk && r < R) ? Lsm[(size_t)m * LD + r] : 0.0;
+          const int c = cb + u * 8 + g;
+          bf[u] = (mk && c < NC) ? W[(size_t)c * R + k0 + m] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+#pragma unroll
+          for (int v = 0; v < 2; ++v) dmma_8x8x4(acc[u][v][0], acc[u][v][1], af[u], bf[v]);
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int v = 0; v < 2; ++v)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int r = rb + u * 8 + g, c = cb + v * 8 + 2 * q + h;
+            if (r < R && c < NC) W[(size_t)c * R + r] -= acc[u][v][h];
+          }
+    }
+  } else {
+    // 4 x 4 output per thread
+    const int tr = (rows + 3) / 4, tc = (cols + 3) / 4;
+    for (int t = tid; t < tr * tc; t += bs) {
+      const int rb = r0 + (t % tr) * 4, cb = c0 + (t / tr) * 4;
+      T acc[4][4] = {};
+      for (int m = 0; m < w; ++m) {
+        T av[4], bv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          av[u] = rb + u < R ? Lsm[(size_t)m * LD + rb + u] : T(0);
+          bv[u] = cb + u < NC ? W[(size_t)(cb + u) * R + k0 + m] : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) acc[u][v] = fma(av[u], bv[v], acc[u][v]);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          if (rb + u < R && cb + v < NC) W[(size_t)(cb + v) * R + rb + u] -= acc[u][v];
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T* slab, size_t slab_elems) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ T sv[32];
+  __shared__ int si[32];
+  __shared__ int s_piv[256];
+  const int tid = threadIdx.x, bs = blockDim.x;
+  const Dims d = a.d;
+  const int n = d.n, nr = d.nr, nx = d.nx, nb = d.nblock;
+  const int n2 = 2 * n, R = n2 + nr, NC = 3 * n + nx;
+  const size_t nn = (size_t)n * n, nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
+  T* Pb = reinterpret_cast<T*>(smem_raw);  // [BLK_W][R] the current panel block, column-major
+  T* W = slab + (size_t)blockIdx.x * slab_elems;
+  const int k = a.k;
+  const long np = pairs_at_level(nb, k);
+  const bool first = a.first != 0;
+  for (long q = blockIdx.x; q < np; q += gridDim.x) {
+    const int j = k + (int)(2L * k * q), jp = j - k;
+    const size_t oj = (size_t)j * nn, ojp = (size_t)jp * nn;
+    // ------------------------------------------------------------ load
+    for (int idx = tid; idx < (int)nn; idx += bs) {
+      const int i = idx % n, c = idx / n;
+      W[(size_t)c * R + i] = ldsrc(first, a.E0, a.E, ojp + idx);
+      W[(size_t)(n + c) * R + i] = ldsrc(first, a.D0, a.D, ojp + idx);
+      W[(size_t)(n2 + c) * R + i] = T(0);
+      W[(size_t)c * R + n + i] = ldsrc(first, a.D0, a.D, oj + idx);
+      W[(size_t)(n + c) * R + n + i] = T(0);
+      W[(size_t)(n2 + c) * R + n + i] = ldsrc(first, a.E0, a.E, oj + idx);
+    }
+    for (int idx = tid; idx < (int)nnx; idx += bs) {
+      const int i = idx % n, c = idx / n;
+      W[(size_t)(3 * n + c) * R + i] = ldsrc(first, a.B0, a.B, (size_t)jp * nnx + idx);
+      W[(size_t)(3 * n + c) * R + n + i] = ldsrc(first, a.B0, a.B, (size_t)j * nnx + idx);
+    }
+    for (int idx = tid; idx < (int)nrn; idx += bs) {
+      const int r = idx % nr, c = idx / nr;
+      W[(size_t)c * R + n2 + r] = ldsrc(first, a.C0, a.C, (size_t)j * nrn + idx);
+      W[(size_t)(n + c) * R + n2 + r] = T(0);
+      W[(size_t)(n2 + c) * R + n2 + r] = T(0);
+    }
+    for (int idx = tid; idx < (int)nrnx; idx += bs) {
+      const int r = idx % nr, c = idx / nr;
+      W[(size_t)(3 * n + c) * R + n2 + r] = T(0);
+    }
+    __syncthreads();
+    // ------------------------------------------------- blocked elimination
+    int info = 0;
+    for (int kb = 0; kb < n && info == 0; kb += BLK_W) {
+      const int w = n - kb < BLK_W ? n - kb : BLK_W;
+      // stage the block's columns (all rows) in shared memory
+      for (int e = tid; e < w * R; e += bs) {
+        const int r = e % R, c = e / R;
+        Pb[(size_t)c * R + r] = W[(size_t)(kb + c) * R + r];
+      }
+      __syncthreads();
+      for (int i = 0; i < w; ++i) {
+        const int gi = kb + i;
+        T* ci = Pb + (size_t)i * R;
+        T best = T(-1);
+        int bi = gi;  // stays in range even when every candidate is NaN
+        for (int r = gi + tid; r < n2; r += bs) {
+          const T v = dev_abs(ci[r]);
+          if (v > best) { best = v; bi = r; }
+        }
+        block_argmax(best, bi, sv, si);
+        if (tid == 0) s_piv[gi] = bi;
+        const T pv = ci[bi];
+        __syncthreads();  // every thread holds the pivot before the rows are swapped
+        if (pv == T(0)) { info = gi + 1; break; }
+        if (bi != gi && tid < w) {
+          T* col = Pb + (size_t)tid * R;
+          const T t = col[gi]; col[gi] = col[bi]; col[bi] = t;
+        }
+        __syncthreads();
+        const T rinv = T(1) / pv;
+        for (int r = gi + 1 + tid; r < R; r += bs) ci[r] *= rinv;
+        __syncthreads();
+        const int rows = R - gi - 1, cols = w - i - 1;
+        for (int e = tid; e < rows * cols; e += bs) {
+          const int r = gi + 1 + e % rows, c = i + 1 + e / rows;
+          Pb[(size_t)c * R + r] -= ci[r] * Pb[(size_t)c * R + gi];
+        }
+        __syncthreads();
+      }
+      if (info != 0) break;
+      // the factored block back to the slab, its interchanges on every other column
+      for (int e = tid; e < w * R; e += bs) {
+        const int r = e % R, c = e / R;
+        W[(size_t)(kb + c) * R + r] = Pb[(size_t)c * R + r];
+      }
+      for (int c = tid; c < NC; c += bs) {
+        if (c >= kb && c < kb + w) continue;
+        T* col = W + (size_t)c * R;
+        for (int i = 0; i < w; ++i) {
+          const int p = s_piv[kb + i];
+          if (p != kb + i) { const T t = col[kb + i]; col[kb + i] = col[p]; col[p] = t; }
+        }
+      }
+      __syncthreads();
+      // rows [kb, kb+w) of the columns right of the block: unit lower solve
+      for (int c = kb + w + tid; c < NC; c += bs) {
+        T* col = W + (size_t)c * R + kb;
+        T y[BLK_W];
+#pragma unroll
+        for (int r = 0; r < BLK_W; ++r) y[r] = r < w ? col[r] : T(0);
+#pragma unroll
+        for (int m = 0; m < BLK_W; ++m) {
+#pragma unroll
+          for (int r = m + 1; r < BLK_W; ++r)
+            if (r < w) y[r] = fma(-Pb[(size_t)m * R + kb + r], y[m], y[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < BLK_W; ++r)
+          if (r < w) col[r] = y[r];
+      }
+      __syncthreads();
+      // rows below the block: one product of depth w
+      blk_update<T>(W, R, NC, Pb, R, kb, w, kb + w, kb + w);
+      __syncthreads();
+    }
+    if (info != 0) {
+      if (tid == 0) report(a.st, DEV_ZERO_PIVOT, j, info, k);
+      __syncthreads();
+      continue;
+    }
+    // ---------------------------------------------------------------- store
+    T* Tj = a.Tm + (size_t)j * szT(d);
+    for (int idx = tid; idx < (int)(2 * nn); idx += bs) {
+      const int r = idx % n2, c = idx / n2;
+      Tj[idx] = W[(size_t)c * R + r];
+    }
+    unsigned char* Pj = a.P + (size_t)j * szP(d);
+    if (tid == 0) {
+      // row map (getrf order) from the interchange sequence
+      unsigned char mp[512];
+      for (int r = 0; r < n2; ++r) mp[r] = (unsigned char)r;
+      for (int i = 0; i < n; ++i) { const unsigned char t = mp[i]; mp[i] = mp[s_piv[i]]; mp[s_piv[i]] = t; }
+      for (int r = 0; r < n2; ++r) Pj[r] = mp[r];
+      for (int i = 0; i < n; ++i) Pj[n2 + i] = (unsigned char)i;
+    }
+    for (int idx = tid; idx < (int)nn; idx += bs) {
+      const int i = idx % n, c = idx / n;
+      a.D[oj + idx] = W[(size_t)(n + c) * R + i];
+      a.E[oj + idx] = W[(size_t)(n2 + c) * R + i];
+      a.D[ojp + idx] = W[(size_t)(n + c) * R + n + i];
+      a.E[ojp + idx] = W[(size_t)(n2 + c) * R + n + i];
+    }
+    for (int idx = tid; idx < (int)nnx; idx += bs) {
+      const int i = idx % n, c = idx / n;
+      a.B[(size_t)j * nnx + idx] = W[(size_t)(3 * n + c) * R + i];
+      a.B[(size_t)jp * nnx + idx] = W[(size_t)(3 * n + c) * R + n + i];
+    }
+    for (int idx = tid; idx < (int)nrn; idx += bs) {
+      const int r = idx % nr, c = idx / nr;
+      const size_t oc = (size_t)jp * nrn + idx;
+      a.C[(size_t)j * nrn + idx] = W[(size_t)c * R + n2 + r];
+      const T cjp = first ? T(a.C0[oc]) : a.C[oc];
+      a.C[oc] = cjp + W[(size_t)(n + c) * R + n2 + r];
+      a.Rbuf[(size_t)j * nrn + idx] = W[(size_t)(n2 + c) * R + n2 + r];
+    }
+    for (int idx = tid; idx < (int)nrnx; idx += bs) {
+      const int r = idx % nr, c = idx / nr;
+      a.Fbuf[(size_t)j * nrnx + idx] = W[(size_t)(3 * n + c) * R + n2 + r];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Large blocks: one CTA eliminates one pair; the (2n+nr) x (3n+nx) work
 // matrix lives in a global scratch slab of the CTA (column-major, ld = R),
 // which stays in L2 while the CTA works on it.  Same elimination as the warp
@@ -2521,6 +2771,8 @@ static WorkSet<float> work_set(DevState& s, float*) {
 template <typename T>
 struct FactorPlan {
   void (*cta)(FactorArgs<T>, T*, size_t) = nullptr;  // CTA per pair (large n)
+  void (*blk)(FactorArgs<T>, T*, size_t) = nullptr;  // CTA per pair, blocked LU (large n)
+  size_t blk_smem = 0;
   void (*tc)(FactorArgs<T>, const FactorArgs<T>*, const BatchCta*) = nullptr;               // tensor-core LU (FP64, n = 8, 16)
   size_t tc_smem = 0;
   void (*grp)(FactorArgs<T>, const FactorArgs<T>*, const BatchCta*) = nullptr;              // CTA of 2n threads per pair (n = 16, 32)
@@ -2545,7 +2797,7 @@ static FactorPlan<T> plan_factor(const DevState& s) {
   p.smem = per_warp * p.wpb;
   p.smem_k = s.sel == SEL_LU ? k_factor_level<T, SEL_LU>
            : s.sel == SEL_QR ? k_factor_level<T, SEL_QR> : k_factor_level<T, SEL_QRP>;
-  smem_limit_once(p.smem_k, p.smem);
+  if (p.smem <= SMEM_MAX) smem_limit_once(p.smem_k, p.smem);
   if constexpr (sizeof(T) == 8) {
     if (s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 && (n == 16 || n == 8) && s.use_tc &&
         (s.pair_kernel == PAIR_AUTO || s.pair_kernel == PAIR_TC)) {
@@ -2580,6 +2832,12 @@ static FactorPlan<T> plan_factor(const DevState& s) {
       (s.pair_kernel != PAIR_SMEM || !smem_fits)) {
     p.cta = s.sel == SEL_LU ? k_factor_cta<T, SEL_LU>
           : s.sel == SEL_QR ? k_factor_cta<T, SEL_QR> : k_factor_cta<T, SEL_QRP>;
+    const size_t bsm = (size_t)BLK_W * (2 * n + d.nr) * sizeof(T);
+    if (s.sel == SEL_LU && n <= 128 && bsm <= SMEM_MAX) {
+      p.blk = k_factor_lu_blocked<T>;
+      p.blk_smem = bsm;
+      smem_limit_once(p.blk, bsm);
+    }
   }
   return p;
 }
@@ -2619,7 +2877,8 @@ static void factor_levels(DevState& s, const FactorPlan<T>& p, const WorkSet<T>&
     a.k = k;
     a.first = (k == 1);
     const long np = pairs_at_level(nb, k);
-    if (p.cta) p.cta<<<grid_for(np, 1, s.slab_ctas), 256, 0, st>>>(a, w.slab, s.slab_elems);
+    if (p.blk) p.blk<<<grid_for(np, 1, s.slab_ctas), 256, p.blk_smem, st>>>(a, w.slab, s.slab_elems);
+    else if (p.cta) p.cta<<<grid_for(np, 1, s.slab_ctas), 256, 0, st>>>(a, w.slab, s.slab_elems);
     else if (p.grp) p.grp<<<grid_for(np, 1, p.grp_ctas), p.grp_threads, p.grp_smem, st>>>(a, nullptr, nullptr);
     else if (p.tc) p.tc<<<grid_for(np, 4, 148 * 16), 128, p.tc_smem, st>>>(a, nullptr, nullptr);
     else if (p.rows) p.rows<<<grid_for(np, 4, 148 * 16), 128, 0, st>>>(a, nullptr, nullptr);

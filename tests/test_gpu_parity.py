@@ -191,11 +191,13 @@ def test_gpu_factorize_solve_fused(dims, internal, nrhs):
 
 
 @pytest.mark.parametrize("dims", [(65, 32, 0, 0, 8, 8), (17, 48, 2, 3, 4, 1), (9, 64, 1, 1, 2, 2),
-                                  (5, 128, 4, 4, 16, 16)])
+                                  (5, 128, 4, 4, 16, 16), (12, 40, 0, 0, 3, 3), (6, 100, 2, 2, 5, 5),
+                                  (7, 27, 1, 1, 2, 2)])
 @pytest.mark.parametrize("internal", ["LU", "QR", "QRP"])
 def test_gpu_large_blocks(dims, internal):
     """n > 24 runs one CTA per pair with the work matrix in a global slab
-    (config C has n=32, config E n=128)."""
+    (blocked LU in panels of 32 columns; config C has n=32, config E n=128);
+    n = 27, 40 and 100 leave a partial last panel block."""
     s = synth.collocation(*dims, seed=sum(dims))
     b = synth.rhs(s, nrhs=2, seed=3)
     last = "LU" if s.Nr == s.Nc else "QR"
