@@ -1262,6 +1262,7 @@ __global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
 // the trailing updates) up to rounding order.
 // ---------------------------------------------------------------------------
 constexpr int BLK_W = 32;
+constexpr int BLK_ROWS_MAX = 512;  // 2n + nr of the blocked kernel
 
 // W[c*R + r] -= sum_m L[m*LD + r] * W[c*R + k0 + m] for r in [r0, R), c in [c0, NC), m < w
 // L: the factored block in shared memory (column m, row r), U: rows [k0, k0+w) of W
@@ -1275,24 +1276,19 @@ __device__ void blk_update(T* W, int R, int NC, const T* Lsm, int LD, int k0, in
     const int lane = tid & 31, warp = tid >> 5, nw = bs >> 5;
     const int g = lane >> 2, q = lane & 3;
     const int tr = (rows + 15) / 16, tc = (cols + 15) / 16;
+    constexpr int KS = BLK_W / 4;
     for (int t = warp; t < tr * tc; t += nw) {
       const int rb = r0 + (t % tr) * 16, cb = c0 + (t / tr) * 16;
-      double acc[2][2][2] = {};
-      for (int ks = 0; ks < (w + 3) / 4; ++ks) {
+      // every global load of the tile (B fragments, C) is in flight at once
+      double bf[KS][2], cv[2][2][2];
+#pragma unroll
+      for (int ks = 0; ks < KS; ++ks) {
         const int m = ks * 4 + q;
-        const bool mk = m < w;
-        double af[2], bf[2];
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const int r = rb + u * 8 + g;
-          af[u] = (mk && r < R) ? Lsm[(size_t)m * LD + r] : 0.0;
-          const int c = cb + u * 8 + g;
-          bf[u] = (mk && c < NC) ? W[(size_t)c * R + k0 + m] : 0.0;
+        for (int v = 0; v < 2; ++v) {
+          const int c = cb + v * 8 + g;
+          bf[ks][v] = (m < w && c < NC) ? W[(size_t)c * R + k0 + m] : 0.0;
         }
-#pragma unroll
-        for (int u = 0; u < 2; ++u)
-#pragma unroll
-          for (int v = 0; v < 2; ++v) dmma_8x8x4(acc[u][v][0], acc[u][v][1], af[u], bf[v]);
       }
 #pragma unroll
       for (int u = 0; u < 2; ++u)
@@ -1301,7 +1297,31 @@ __device__ void blk_update(T* W, int R, int NC, const T* Lsm, int LD, int k0, in
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const int r = rb + u * 8 + g, c = cb + v * 8 + 2 * q + h;
-            if (r < R && c < NC) W[(size_t)c * R + r] -= acc[u][v][h];
+            cv[u][v][h] = (r < R && c < NC) ? W[(size_t)c * R + r] : 0.0;
+          }
+      double acc[2][2][2] = {};
+#pragma unroll
+      for (int ks = 0; ks < KS; ++ks) {
+        const int m = ks * 4 + q;
+        double af[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int r = rb + u * 8 + g;
+          af[u] = (m < w && r < R) ? Lsm[(size_t)m * LD + r] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+#pragma unroll
+          for (int v = 0; v < 2; ++v) dmma_8x8x4(acc[u][v][0], acc[u][v][1], af[u], bf[ks][v]);
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int v = 0; v < 2; ++v)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int r = rb + u * 8 + g, c = cb + v * 8 + 2 * q + h;
+            if (r < R && c < NC) W[(size_t)c * R + r] = cv[u][v][h] - acc[u][v][h];
           }
     }
   } else {
@@ -1310,6 +1330,7 @@ __device__ void blk_update(T* W, int R, int NC, const T* Lsm, int LD, int k0, in
     for (int t = tid; t < tr * tc; t += bs) {
       const int rb = r0 + (t % tr) * 4, cb = c0 + (t / tr) * 4;
       T acc[4][4] = {};
+#pragma unroll 4
       for (int m = 0; m < w; ++m) {
         T av[4], bv[4];
 #pragma unroll
@@ -1337,12 +1358,15 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
   __shared__ T sv[32];
   __shared__ int si[32];
   __shared__ int s_piv[256];
+  __shared__ int s_src[2 * BLK_W], s_dst[2 * BLK_W], s_cnt;
+  __shared__ int s_perm[BLK_ROWS_MAX];
   const int tid = threadIdx.x, bs = blockDim.x;
   const Dims d = a.d;
   const int n = d.n, nr = d.nr, nx = d.nx, nb = d.nblock;
   const int n2 = 2 * n, R = n2 + nr, NC = 3 * n + nx;
   const size_t nn = (size_t)n * n, nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
   T* Pb = reinterpret_cast<T*>(smem_raw);  // [BLK_W][R] the current panel block, column-major
+  T* Sg = Pb + (size_t)BLK_W * R;           // [2*BLK_W][BLK_W] staging of interchanged rows
   T* W = slab + (size_t)blockIdx.x * slab_elems;
   const int k = a.k;
   const long np = pairs_at_level(nb, k);
@@ -1351,14 +1375,32 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
     const int j = k + (int)(2L * k * q), jp = j - k;
     const size_t oj = (size_t)j * nn, ojp = (size_t)jp * nn;
     // ------------------------------------------------------------ load
-    for (int idx = tid; idx < (int)nn; idx += bs) {
-      const int i = idx % n, c = idx / n;
-      W[(size_t)c * R + i] = ldsrc(first, a.E0, a.E, ojp + idx);
-      W[(size_t)(n + c) * R + i] = ldsrc(first, a.D0, a.D, ojp + idx);
-      W[(size_t)(n2 + c) * R + i] = T(0);
-      W[(size_t)c * R + n + i] = ldsrc(first, a.D0, a.D, oj + idx);
-      W[(size_t)(n + c) * R + n + i] = T(0);
-      W[(size_t)(n2 + c) * R + n + i] = ldsrc(first, a.E0, a.E, oj + idx);
+    // groups of UL elements per thread: the group's loads are issued before its stores
+    constexpr int UL = 4;
+    for (int base = 0; base < (int)nn; base += bs * UL) {
+      T ejp[UL], djp[UL], dj[UL], ej[UL];
+#pragma unroll
+      for (int u = 0; u < UL; ++u) {
+        const int idx = base + tid + u * bs;
+        const bool in = idx < (int)nn;
+        ejp[u] = in ? ldg_src(first, a.E0, a.E, ojp + idx) : T(0);
+        djp[u] = in ? ldg_src(first, a.D0, a.D, ojp + idx) : T(0);
+        dj[u] = in ? ldg_src(first, a.D0, a.D, oj + idx) : T(0);
+        ej[u] = in ? ldg_src(first, a.E0, a.E, oj + idx) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < UL; ++u) {
+        const int idx = base + tid + u * bs;
+        if (idx < (int)nn) {
+          const int i = idx % n, c = idx / n;
+          W[(size_t)c * R + i] = ejp[u];
+          W[(size_t)(n + c) * R + i] = djp[u];
+          W[(size_t)(n2 + c) * R + i] = T(0);
+          W[(size_t)c * R + n + i] = dj[u];
+          W[(size_t)(n + c) * R + n + i] = T(0);
+          W[(size_t)(n2 + c) * R + n + i] = ej[u];
+        }
+      }
     }
     for (int idx = tid; idx < (int)nnx; idx += bs) {
       const int i = idx % n, c = idx / n;
@@ -1405,13 +1447,12 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
           const T t = col[gi]; col[gi] = col[bi]; col[bi] = t;
         }
         __syncthreads();
+        // one thread per row below the pivot: its multiplier, then its update
         const T rinv = T(1) / pv;
-        for (int r = gi + 1 + tid; r < R; r += bs) ci[r] *= rinv;
-        __syncthreads();
-        const int rows = R - gi - 1, cols = w - i - 1;
-        for (int e = tid; e < rows * cols; e += bs) {
-          const int r = gi + 1 + e % rows, c = i + 1 + e / rows;
-          Pb[(size_t)c * R + r] -= ci[r] * Pb[(size_t)c * R + gi];
+        for (int r = gi + 1 + tid; r < R; r += bs) {
+          const T l = ci[r] * rinv;
+          ci[r] = l;
+          for (int c = i + 1; c < w; ++c) Pb[(size_t)c * R + r] -= l * Pb[(size_t)c * R + gi];
         }
         __syncthreads();
       }
@@ -1421,15 +1462,43 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
         const int r = e % R, c = e / R;
         W[(size_t)(kb + c) * R + r] = Pb[(size_t)c * R + r];
       }
-      for (int c = tid; c < NC; c += bs) {
-        if (c >= kb && c < kb + w) continue;
-        T* col = W + (size_t)c * R;
+      // the block's interchanges as one row permutation of the touched rows,
+      // applied to every other column through a staging buffer
+      for (int r = kb + tid; r < n2; r += bs) s_perm[r] = r;
+      __syncthreads();
+      if (tid == 0) {
         for (int i = 0; i < w; ++i) {
           const int p = s_piv[kb + i];
-          if (p != kb + i) { const T t = col[kb + i]; col[kb + i] = col[p]; col[p] = t; }
+          const int t = s_perm[kb + i]; s_perm[kb + i] = s_perm[p]; s_perm[p] = t;
         }
+        int cnt = 0;
+        for (int r = kb; r < n2; ++r)
+          if (s_perm[r] != r) { s_dst[cnt] = r; s_src[cnt] = s_perm[r]; ++cnt; }
+        s_cnt = cnt;
       }
       __syncthreads();
+      const int cnt = s_cnt;
+      if (cnt > 0) {
+        constexpr int CW = BLK_W;  // columns per stage
+        const int other = NC - w;
+        for (int c0 = 0; c0 < other; c0 += CW) {
+          const int cw = other - c0 < CW ? other - c0 : CW;
+          // consecutive threads take consecutive rows of one column (the rows
+          // [kb, kb+w) come first in the list, so most accesses coalesce)
+          for (int e = tid; e < cnt * cw; e += bs) {
+            const int t = e % cnt, cc = e / cnt;
+            const int col = c0 + cc < kb ? c0 + cc : c0 + cc + w;
+            Sg[cc * (2 * BLK_W) + t] = W[(size_t)col * R + s_src[t]];
+          }
+          __syncthreads();
+          for (int e = tid; e < cnt * cw; e += bs) {
+            const int t = e % cnt, cc = e / cnt;
+            const int col = c0 + cc < kb ? c0 + cc : c0 + cc + w;
+            W[(size_t)col * R + s_dst[t]] = Sg[cc * (2 * BLK_W) + t];
+          }
+          __syncthreads();
+        }
+      }
       // rows [kb, kb+w) of the columns right of the block: unit lower solve
       for (int c = kb + w + tid; c < NC; c += bs) {
         T* col = W + (size_t)c * R + kb;
@@ -1458,9 +1527,18 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
     }
     // ---------------------------------------------------------------- store
     T* Tj = a.Tm + (size_t)j * szT(d);
-    for (int idx = tid; idx < (int)(2 * nn); idx += bs) {
-      const int r = idx % n2, c = idx / n2;
-      Tj[idx] = W[(size_t)c * R + r];
+    for (int base = 0; base < (int)(2 * nn); base += bs * UL) {
+      T v[UL];
+#pragma unroll
+      for (int u = 0; u < UL; ++u) {
+        const int idx = base + tid + u * bs;
+        v[u] = idx < (int)(2 * nn) ? W[(size_t)(idx / n2) * R + idx % n2] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < UL; ++u) {
+        const int idx = base + tid + u * bs;
+        if (idx < (int)(2 * nn)) Tj[idx] = v[u];
+      }
     }
     unsigned char* Pj = a.P + (size_t)j * szP(d);
     if (tid == 0) {
@@ -1471,12 +1549,28 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
       for (int r = 0; r < n2; ++r) Pj[r] = mp[r];
       for (int i = 0; i < n; ++i) Pj[n2 + i] = (unsigned char)i;
     }
-    for (int idx = tid; idx < (int)nn; idx += bs) {
-      const int i = idx % n, c = idx / n;
-      a.D[oj + idx] = W[(size_t)(n + c) * R + i];
-      a.E[oj + idx] = W[(size_t)(n2 + c) * R + i];
-      a.D[ojp + idx] = W[(size_t)(n + c) * R + n + i];
-      a.E[ojp + idx] = W[(size_t)(n2 + c) * R + n + i];
+    for (int base = 0; base < (int)nn; base += bs * UL) {
+      T v0[UL], v1[UL], v2[UL], v3[UL];
+#pragma unroll
+      for (int u = 0; u < UL; ++u) {
+        const int idx = base + tid + u * bs;
+        const int i = idx % n, c = idx / n;
+        const bool in = idx < (int)nn;
+        v0[u] = in ? W[(size_t)(n + c) * R + i] : T(0);
+        v1[u] = in ? W[(size_t)(n2 + c) * R + i] : T(0);
+        v2[u] = in ? W[(size_t)(n + c) * R + n + i] : T(0);
+        v3[u] = in ? W[(size_t)(n2 + c) * R + n + i] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < UL; ++u) {
+        const int idx = base + tid + u * bs;
+        if (idx < (int)nn) {
+          a.D[oj + idx] = v0[u];
+          a.E[oj + idx] = v1[u];
+          a.D[ojp + idx] = v2[u];
+          a.E[ojp + idx] = v3[u];
+        }
+      }
     }
     for (int idx = tid; idx < (int)nnx; idx += bs) {
       const int i = idx % n, c = idx / n;
@@ -2832,8 +2926,8 @@ static FactorPlan<T> plan_factor(const DevState& s) {
       (s.pair_kernel != PAIR_SMEM || !smem_fits)) {
     p.cta = s.sel == SEL_LU ? k_factor_cta<T, SEL_LU>
           : s.sel == SEL_QR ? k_factor_cta<T, SEL_QR> : k_factor_cta<T, SEL_QRP>;
-    const size_t bsm = (size_t)BLK_W * (2 * n + d.nr) * sizeof(T);
-    if (s.sel == SEL_LU && n <= 128 && bsm <= SMEM_MAX) {
+    const size_t bsm = ((size_t)BLK_W * (2 * n + d.nr) + 2 * BLK_W * BLK_W) * sizeof(T);
+    if (s.sel == SEL_LU && n <= 128 && 2 * n + d.nr <= BLK_ROWS_MAX && bsm <= SMEM_MAX) {
       p.blk = k_factor_lu_blocked<T>;
       p.blk_smem = bsm;
       smem_limit_once(p.blk, bsm);
