@@ -38,6 +38,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "BABD factor+solve unknowns/s at rel. residual ≤1e-12: mixed vs plain FP64 GPU"
+# DRAM bytes per block moved by the factorization kernels of this workload,
+# from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum)
+FACT_DRAM_BYTES_PER_BLOCK = 20985
 CFG = dict(nblock=100000, n=16, qr=2, qx=2, nr=4, nx=4)
 
 
@@ -303,7 +306,11 @@ def run_ours(args):
             "rel_residual": relres,
             "roofline": {"bound": "hbm", "kernel": "factorize (all CR level launches)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": FACT_DRAM_BYTES_PER_BLOCK * CFG["nblock"],
+                         "traffic_source": "ncu dram__bytes_read+write of one factorization at "
+                                           "nblock=40000, scaled by nblock "
+                                           "(profiles/dram_factor_solve_n16_nblock40000.md)",
                          "algorithmic_bytes": fact_b},
             "e2e": {"value": world * s.ncols / e2e_t, "unit": "unknowns/s",
                     "h2d_bytes_per_step": nbytes_mat + 8 * L, "d2h_bytes_per_step": 8 * L},
@@ -443,6 +450,30 @@ def cpu_baseline(s, b):
             "sample": "full workload, one factorize+solve of the C oracle"}
 
 
+def run_once(args):
+    """One factorize + solve of a named workload through the C ABI, for profilers."""
+    import torch
+    from alglin_b200 import bcr, synth
+    cfg = dict(synth.CONFIGS[args.once])
+    if args.nblock_once:
+        cfg["nblock"] = args.nblock_once
+    s = synth.collocation(**cfg, seed=0)
+    b = synth.rhs(s, 1, seed=1)[0]
+    L = max(s.nrows, s.ncols)
+    h = bcr.BorderedCR()
+    h.load_system(s)
+    h.set_precision(bcr.PRECISION_MIXED if args.precision == "mixed" else bcr.PRECISION_FP64)
+    h.upload()
+    x = torch.from_numpy(b).cuda()
+    torch.cuda.synchronize()
+    h.factorize_solve_device(1, x.data_ptr(), L)
+    h.synchronize()
+    assert h.factorize_status(), h.last_error()
+    print(json.dumps({"once": args.once, "nblock": cfg["nblock"], "precision": args.precision,
+                      "refinement": h.refinement_info()}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -455,7 +486,13 @@ def main():
                     help="skip the mixed-path, n=32 and batched measurements")
     ap.add_argument("--nblock", type=int, default=CFG["nblock"],
                     help="smaller systems for profiling runs (the reported workload is 100000)")
+    ap.add_argument("--once", choices=["A", "B", "C", "E"],
+                    help="run one factorize+solve of that workload and exit (for profilers)")
+    ap.add_argument("--nblock-once", type=int, default=0, help="nblock of the --once workload")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="path of --once")
     args = ap.parse_args()
+    if args.once:
+        return run_once(args)
     CFG["nblock"] = args.nblock
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     if args.impl == "reference":
