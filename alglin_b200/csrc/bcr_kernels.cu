@@ -562,7 +562,10 @@ struct TcShape {
   static constexpr int MT = 2 * N + 8;             // GEMM rows: U-row, reduced row, border (padded)
   static constexpr int NTILES = (2 * N + 8 + 7) / 8;  // trailing columns 2N + nx, nx <= 8
   static constexpr int NTP = NTILES * 8;
-  static constexpr int LDW = NTP + 1;               // trailing rows (odd: conflict-light)
+  // trailing rows, compact: a TOP row keeps [D_jp | B_jp | x_jp], a BOTTOM row
+  // [E_j | B_j | x_j]; the structurally zero half of each row is not stored
+  static constexpr int LDW = NTP - N + 1;
+  static constexpr int PC = (NTILES + 1) / 2;      // column tiles per product pass
   static constexpr int LDG = N + 4;                 // operator rows (16B aligned, conflict-free A loads)
   static constexpr int KSTEPS = N / 4;
   static constexpr int MTILES = MT / 8;
@@ -571,12 +574,22 @@ struct TcShape {
   static constexpr size_t BYTES = (size_t)(WS + GS + N + 2) * 8 + 2 * N * sizeof(int);
 };
 
+// element (row, col) of the trailing part from the compact rows
+template <int N>
+__device__ __forceinline__ double tc_w(const double* Wt, int row, int col) {
+  constexpr int LDW = TcShape<N>::LDW;
+  const bool top = row < N;
+  if (col < N) return top ? Wt[row * LDW + col] : 0.0;
+  if (col < 2 * N) return top ? 0.0 : Wt[row * LDW + col - N];
+  return Wt[row * LDW + col - N];
+}
+
 size_t tc_smem_per_warp(int n) {
   return n == 16 ? TcShape<16>::BYTES : n == 8 ? TcShape<8>::BYTES : 0;
 }
 
 template <int N, bool BATCH = false>
-__global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a0, const FactorArgs<double>* tab,
+__global__ void __launch_bounds__(128, 4) k_factor_lu_tc(FactorArgs<double> a0, const FactorArgs<double>* tab,
                                                        const BatchCta* cmap) {
   using S = TcShape<N>;
   constexpr unsigned FULL = 0xffffffffu;
@@ -632,9 +645,7 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a0, con
         const int idx = lane + 32 * it;
         const int r = idx % n, c = idx / n;
         Wt[r * S::LDW + c] = Djp[idx];
-        Wt[r * S::LDW + n + c] = 0.0;
-        Wt[(n + r) * S::LDW + c] = 0.0;
-        Wt[(n + r) * S::LDW + n + c] = Ej[idx];
+        Wt[(n + r) * S::LDW + c] = Ej[idx];
       }
       const double* Bjp = srcB + (size_t)jp * nnx;
       const double* Bj = srcB + (size_t)j * nnx;
@@ -643,21 +654,21 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a0, con
         const int idx = lane + 32 * it;
         if (idx < (int)nnx) {
           const int r = idx % n, c = idx / n;
-          Wt[r * S::LDW + n2 + c] = Bjp[idx];
-          Wt[(n + r) * S::LDW + n2 + c] = Bj[idx];
+          Wt[r * S::LDW + n + c] = Bjp[idx];
+          Wt[(n + r) * S::LDW + n + c] = Bj[idx];
         }
       }
       // fused right-hand sides: TOP rows hold x_jp, BOTTOM rows x_j
       for (int idx = lane; idx < n2 * nrf; idx += 32) {
         const int r = idx % n2, c = idx / n2;
         const double* xc = a.x + (size_t)c * a.ldx;
-        Wt[r * S::LDW + n2 + nx + c] = r < n ? xc[(size_t)jp * n + r] : xc[(size_t)j * n + r - n];
+        Wt[r * S::LDW + n + nx + c] = r < n ? xc[(size_t)jp * n + r] : xc[(size_t)j * n + r - n];
       }
       // zero the padding columns of the live rows (they feed padding outputs only,
       // but keep them finite)
       for (int idx = lane; idx < n2 * (S::NTP - NT); idx += 32) {
         const int r = idx % n2, c = NT + idx / n2;
-        Wt[r * S::LDW + c] = 0.0;
+        Wt[r * S::LDW + c - n] = 0.0;
       }
     }
     // --------------------------------------------------- phase 1: panel LU
@@ -790,32 +801,41 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a0, con
     }
     __syncwarp();
     // ----------------------------------------- phase 3: tensor-core GEMM
-    double acc[S::MTILES][S::NTILES][2];
+    // two passes over the column tiles keep the accumulators within budget
+#pragma unroll
+    for (int pass = 0; pass < 2; ++pass) {
+    constexpr int PC = S::PC;
+    double acc[S::MTILES][PC][2];
 #pragma unroll
     for (int mt = 0; mt < S::MTILES; ++mt)
 #pragma unroll
-      for (int nt = 0; nt < S::NTILES; ++nt) {
+      for (int ni = 0; ni < PC; ++ni) {
+        const int nt = pass * PC + ni;
         const int row = mt * 8 + g;
         double c0 = 0.0, c1 = 0.0;
-        if (row >= n && row < n2) {  // (PW)_bot
-          const double* w = Wt + rowof[row] * S::LDW + nt * 8 + 2 * t;
-          c0 = w[0];
-          c1 = w[1];
+        if (nt < S::NTILES && row >= n && row < n2) {  // (PW)_bot
+          const int orow = rowof[row];
+          c0 = tc_w<N>(Wt, orow, nt * 8 + 2 * t);
+          c1 = tc_w<N>(Wt, orow, nt * 8 + 2 * t + 1);
         }
-        acc[mt][nt][0] = c0;
-        acc[mt][nt][1] = c1;
+        acc[mt][ni][0] = c0;
+        acc[mt][ni][1] = c1;
       }
 #pragma unroll
     for (int ks = 0; ks < S::KSTEPS; ++ks) {
-      double bfr[S::NTILES];
-      const double* wrow = Wt + rowof[ks * 4 + t] * S::LDW + g;
+      double bfr[PC];
+      const int orow = rowof[ks * 4 + t];
 #pragma unroll
-      for (int nt = 0; nt < S::NTILES; ++nt) bfr[nt] = wrow[nt * 8];
+      for (int ni = 0; ni < PC; ++ni) {
+        const int nt = pass * PC + ni;
+        bfr[ni] = nt < S::NTILES ? tc_w<N>(Wt, orow, nt * 8 + g) : 0.0;
+      }
 #pragma unroll
       for (int mt = 0; mt < S::MTILES; ++mt) {
         const double afr = Gs[(mt * 8 + g) * S::LDG + ks * 4 + t];
 #pragma unroll
-        for (int nt = 0; nt < S::NTILES; ++nt) dmma_8x8x4(acc[mt][nt][0], acc[mt][nt][1], afr, bfr[nt]);
+        for (int ni = 0; ni < PC; ++ni)
+          if (pass * PC + ni < S::NTILES) dmma_8x8x4(acc[mt][ni][0], acc[mt][ni][1], afr, bfr[ni]);
       }
     }
     // ------------------------------------------------------------ store
@@ -827,11 +847,13 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a0, con
       for (int mt = 0; mt < S::MTILES; ++mt) {
         const int row = mt * 8 + g;
 #pragma unroll
-        for (int nt = 0; nt < S::NTILES; ++nt)
+        for (int ni = 0; ni < PC; ++ni)
 #pragma unroll
           for (int hh = 0; hh < 2; ++hh) {
+            const int nt = pass * PC + ni;
+            if (nt >= S::NTILES) continue;
             const int col = nt * 8 + 2 * t + hh;
-            const double v = acc[mt][nt][hh];
+            const double v = acc[mt][ni][hh];
             if (mt * 8 < n2) {  // panel rows (compile-time per mt)
               const bool ur = row < n;
               const int rr = ur ? row : row - n;
@@ -858,6 +880,7 @@ __global__ void __launch_bounds__(128) k_factor_lu_tc(FactorArgs<double> a0, con
           }
       }
     }
+    }  // pass
     __syncwarp();
   }
 }
