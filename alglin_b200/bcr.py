@@ -131,6 +131,9 @@ _SIGS = [
     ("bcr_batch_stream", [ct.c_void_p], ct.c_void_p),
     ("bcr_batch_synchronize", [ct.c_void_p], ct.c_int),
     ("bcr_batch_last_error", [ct.c_void_p], ct.c_char_p),
+    ("bcr_batch_set_precision", [ct.c_void_p, ct.c_int], ct.c_int),
+    ("bcr_batch_set_refinement", [ct.c_void_p, ct.c_double, ct.c_int], ct.c_int),
+    ("bcr_batch_refinement_info", [ct.c_void_p, ct.POINTER(ct.c_int), _dp], ct.c_int),
 ]
 
 GRAPH_FACTORIZE, GRAPH_SOLVE, GRAPH_STEP = 1, 2, 3
@@ -517,6 +520,20 @@ class Batch:
 
     def __len__(self):
         return self.L.bcr_batch_size(self.b)
+
+    def set_precision(self, p: int):
+        """PRECISION_FP64 or PRECISION_MIXED (FP32 factors + FP64 refinement); before prepare()."""
+        self._check(self.L.bcr_batch_set_precision(self.b, int(p)))
+
+    def set_refinement(self, tol: float = 1e-12, max_iter: int = 10):
+        self._check(self.L.bcr_batch_set_refinement(self.b, float(tol), int(max_iter)))
+
+    def refinement_info(self):
+        """(corrections applied, worst |b-Ax|/(|A||x|+|b|) over the batch) of the last mixed solve."""
+        it = ct.c_int(0)
+        rr = ct.c_double(0.0)
+        self._check(self.L.bcr_batch_refinement_info(self.b, ct.byref(it), ct.byref(rr)))
+        return it.value, rr.value
 
     def prepare(self, autotune: bool = False):
         self._check(self.L.bcr_batch_prepare(self.b, 1 if autotune else 0))

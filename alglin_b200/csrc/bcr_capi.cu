@@ -1246,14 +1246,14 @@ int bcr_synchronize(bcr_handle h) {
 namespace {
 
 struct BatchTune {
-  int n, nrm, nxm, fam, chunk;
+  int n, nrm, nxm, mixed, fam, chunk;
 };
 std::vector<BatchTune> g_batch_tuning;  // in-process autotuner cache
 
-int default_family(const Dims& d) {
-  if ((d.n == 8 || d.n == 16) && bcr::batch_family_ok(bcr::PAIR_TC, d)) return bcr::PAIR_TC;
-  if (d.n == 32 && bcr::batch_family_ok(bcr::PAIR_GRP, d)) return bcr::PAIR_GRP;
-  if (bcr::batch_family_ok(bcr::PAIR_ROWS, d)) return bcr::PAIR_ROWS;
+int default_family(const Dims& d, bool mixed) {
+  if ((d.n == 8 || d.n == 16) && bcr::batch_family_ok(bcr::PAIR_TC, d, mixed)) return bcr::PAIR_TC;
+  if ((d.n == 32 || (mixed && d.n == 16)) && bcr::batch_family_ok(bcr::PAIR_GRP, d, mixed)) return bcr::PAIR_GRP;
+  if (bcr::batch_family_ok(bcr::PAIR_ROWS, d, mixed)) return bcr::PAIR_ROWS;
   return -1;
 }
 
@@ -1289,6 +1289,16 @@ struct bcr_batch_s {
   size_t x_elems = 0;
   bcr::StatusWords* d_st = nullptr;
   std::vector<bcr::StatusWords> h_st;
+  // mixed path: FP32 working arrays, refined solutions, per-system norms
+  int precision = BCR_PRECISION_FP64;
+  double ir_tol = 1e-12;
+  int ir_max = 10;
+  int ir_iters = 0;
+  double ir_worst = 0.0;
+  bool ir_pending = false;
+  double* d_sol = nullptr;             // refined solutions, same packing as d_x
+  double* d_nrm = nullptr;             // 4 per system: |A|, |r|, |x|, |b|
+  unsigned long long* d_worst = nullptr;
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph = nullptr;
   bool prepared = false, factorized = false;
@@ -1313,6 +1323,12 @@ struct bcr_batch_s {
     if (d_x) cudaFree(d_x);
     if (d_b) cudaFree(d_b);
     if (d_st) cudaFree(d_st);
+    if (d_sol) cudaFree(d_sol);
+    if (d_nrm) cudaFree(d_nrm);
+    if (d_worst) cudaFree(d_worst);
+    d_sol = d_nrm = nullptr;
+    d_worst = nullptr;
+    ir_pending = false;
     if (h_in) cudaFreeHost(h_in);
     if (h_x) cudaFreeHost(h_x);
     d_in = d_work = nullptr;
@@ -1366,6 +1382,56 @@ struct bcr_batch_s {
   void enqueue_solve() {
     for (auto& c : cls) bcr::batch_solve(c, stream);
   }
+  bool mixed() const { return precision == BCR_PRECISION_MIXED; }
+  // the worst relative residual of the last mixed solve
+  int read_worst() {
+    if (!ir_pending) return BCR_OK;
+    ir_pending = false;
+    unsigned long long w = 0;
+    cudaError_t e = cudaMemcpyAsync(&w, d_worst, 8, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cuda_fail(e, "batch refinement norms");
+    std::memcpy(&ir_worst, &w, 8);
+    return BCR_OK;
+  }
+  // mixed path: x = A^-1 b with the FP32 factors into the solution region,
+  // then corrections from FP64 residuals (each solved in place in the rhs
+  // region) until the worst system is under ir_tol (adaptive: the host reads
+  // the batch-worst norm after each residual) or for exactly `fixed` steps;
+  // the refined solutions end in the rhs region
+  int solve_mixed(int fixed, bool with_A) {
+    enqueue_solve();
+    cudaMemcpyAsync(d_sol, d_x, x_elems * 8, cudaMemcpyDeviceToDevice, stream);
+    int it = 0;
+    for (;;) {
+      cudaMemsetAsync(d_worst, 0, 8, stream);
+      for (auto& c : cls) bcr::batch_residual(c, with_A && it == 0 ? 1 : 0, d_worst, stream);
+      ir_pending = true;
+      if (fixed < 0) {
+        int rc = read_worst();
+        if (rc) return rc;
+        if (ir_worst <= ir_tol || it >= ir_max) break;
+      } else if (it >= fixed) {
+        break;
+      }
+      enqueue_solve();
+      bcr::batch_axpy(d_sol, d_x, x_elems, stream);
+      ++it;
+    }
+    cudaMemcpyAsync(d_x, d_sol, x_elems * 8, cudaMemcpyDeviceToDevice, stream);
+    ir_iters = it;
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? BCR_OK : cuda_fail(e, "batch refinement");
+  }
+  // the solve step after a factorization, on the rhs region (b kept in d_b)
+  int solve_step(int fixed) {
+    if (!mixed()) {
+      enqueue_solve();
+      cudaError_t e = cudaGetLastError();
+      return e == cudaSuccess ? BCR_OK : cuda_fail(e, "batch solve");
+    }
+    return solve_mixed(fixed, true);
+  }
   int read_status() {
     cudaError_t e = cudaMemcpyAsync(h_st.data(), d_st, h_st.size() * sizeof(bcr::StatusWords),
                                     cudaMemcpyDeviceToHost, stream);
@@ -1415,7 +1481,9 @@ int bcr_batch_s::prepare(int autotune) {
       dims[i] = h->d;
       last_sel[i] = h->sel_last;
     }
-    fam[i] = default_family(dims[i]);
+    if (mixed() && dims[i].Nr != dims[i].Nc)
+      return fail(BCR_BAD_ARGUMENT, fmt("batch system %zu: the mixed-precision path needs a square system\n", i));
+    fam[i] = default_family(dims[i], mixed());
     if (fam[i] < 0)
       return fail(BCR_BAD_ARGUMENT,
                   fmt("batch system %zu: block size n=%d with nr=%d, nx=%d has no batched pair kernel\n", i,
@@ -1435,9 +1503,10 @@ int bcr_batch_s::prepare(int autotune) {
     o.C0 = in.take((nb + 1) * nr * n * 8); o.Cq = in.take(nr * qx * 8); o.F0 = in.take(nr * nx * 8);
     o.H = in.take((n + qr) * d.Nc * 8);
     in_len[i] = in.top - o.D0;
-    o.D = work.take(nb * n * n * 8); o.E = work.take(nb * n * n * 8); o.B = work.take(nb * n * nx * 8);
-    o.C = work.take((nb + 1) * nr * n * 8); o.T = work.take(nb * (2 * n * n + n) * 8);
-    o.P = work.take(nb * 3 * n); o.Rbuf = work.take(nb * nr * n * 8); o.Fbuf = work.take(nb * nr * nx * 8);
+    const size_t ws = mixed() ? 4 : 8;  // bytes of a working element
+    o.D = work.take(nb * n * n * ws); o.E = work.take(nb * n * n * ws); o.B = work.take(nb * n * nx * ws);
+    o.C = work.take((nb + 1) * nr * n * ws); o.T = work.take(nb * (2 * n * n + n) * ws);
+    o.P = work.take(nb * 3 * n); o.Rbuf = work.take(nb * nr * n * ws); o.Fbuf = work.take(nb * nr * nx * 8);
     o.XB = work.take(nb * nr * 8); o.Ffin = work.take(std::max<size_t>(nr * nx, 1) * 8);
     o.Hl = work.take((size_t)d.Nr * d.Nc * 8); o.tau = work.take(Lb * 8); o.piv = work.take(2 * Lb * 4);
     const bool svd = last_sel[i] >= bcr::LAST_SVD;  // the SVD family needs U, V, S
@@ -1454,6 +1523,9 @@ int bcr_batch_s::prepare(int autotune) {
   if (e == cudaSuccess) e = cudaMalloc(&d_x, std::max<size_t>(x_elems, 1) * 8);
   if (e == cudaSuccess) e = cudaMalloc(&d_b, std::max<size_t>(x_elems, 1) * 8);
   if (e == cudaSuccess) e = cudaMalloc(&d_st, ns * sizeof(bcr::StatusWords));
+  if (e == cudaSuccess && mixed()) e = cudaMalloc(&d_sol, std::max<size_t>(x_elems, 1) * 8);
+  if (e == cudaSuccess && mixed()) e = cudaMalloc(&d_nrm, ns * 4 * sizeof(double));
+  if (e == cudaSuccess && mixed()) e = cudaMalloc(&d_worst, 8);
   if (e == cudaSuccess && any_handle) e = cudaMallocHost(&h_in, in_bytes);
   if (e == cudaSuccess) e = cudaMallocHost(&h_x, std::max<size_t>(x_elems, 1) * 8);
   if (e != cudaSuccess) {
@@ -1463,6 +1535,8 @@ int bcr_batch_s::prepare(int autotune) {
   }
   if (h_in) std::memset(h_in, 0, in_bytes);
   cudaMemsetAsync(d_in, 0, in_bytes, stream);
+  cudaMemsetAsync(d_x, 0, std::max<size_t>(x_elems, 1) * 8, stream);  // the padding between systems stays zero
+  cudaMemsetAsync(d_b, 0, std::max<size_t>(x_elems, 1) * 8, stream);
   std::memset(h_x, 0, std::max<size_t>(x_elems, 1) * 8);
   h_st.assign(ns, bcr::StatusWords{});
   for (size_t i = 0; i < ns; ++i) {
@@ -1474,9 +1548,19 @@ int bcr_batch_s::prepare(int autotune) {
     s.sel = bcr::SEL_LU;
     s.sel_last = last_sel[i];
     s.D0 = I(o.D0); s.E0 = I(o.E0); s.B0 = I(o.B0); s.C0 = I(o.C0); s.Cq = I(o.Cq); s.F0 = I(o.F0); s.H = I(o.H);
-    s.D = W(o.D); s.E = W(o.E); s.B = W(o.B); s.C = W(o.C); s.T = W(o.T);
+    s.mixed = mixed() ? 1 : 0;
+    if (mixed()) {
+      auto F = [&](size_t b) { return reinterpret_cast<float*>(d_work + b); };
+      s.Df = F(o.D); s.Ef = F(o.E); s.Bf = F(o.B); s.Cf = F(o.C); s.Tf = F(o.T); s.Rbuff = F(o.Rbuf);
+      s.bsol = d_sol + x_off[i];
+      s.bb = d_b + x_off[i];
+      s.bnrm = d_nrm + 4 * i;
+    } else {
+      s.D = W(o.D); s.E = W(o.E); s.B = W(o.B); s.C = W(o.C); s.T = W(o.T);
+      s.Rbuf = W(o.Rbuf);
+    }
     s.P = d_work + o.P;
-    s.Rbuf = W(o.Rbuf); s.Fbuf = W(o.Fbuf); s.XB = W(o.XB); s.xb_cap = 1;
+    s.Rbuf = mixed() ? nullptr : W(o.Rbuf); s.Fbuf = W(o.Fbuf); s.XB = W(o.XB); s.xb_cap = 1;
     s.Ffin = W(o.Ffin); s.Hl = W(o.Hl); s.tau_l = W(o.tau); s.piv_l = reinterpret_cast<int*>(d_work + o.piv);
     const bool svd = last_sel[i] >= bcr::LAST_SVD;
     s.Ul = svd ? W(o.U) : nullptr; s.Vl = svd ? W(o.V) : nullptr; s.Sl = svd ? W(o.S) : nullptr;
@@ -1513,8 +1597,9 @@ int bcr_batch_s::prepare(int autotune) {
     const Dims& d0 = dims[members[c][0]];
     int nrm = 0, nxm = 0;
     for (int i : members[c]) { nrm = std::max(nrm, dims[i].nr); nxm = std::max(nxm, dims[i].nx); }
+    cls[c].mixed = mixed() ? 1 : 0;
     for (const auto& t : g_batch_tuning)
-      if (t.n == d0.n && t.nrm == nrm && t.nxm == nxm) { cls[c].fam = t.fam; cls[c].chunk = t.chunk; }
+      if (t.n == d0.n && t.nrm == nrm && t.nxm == nxm && t.mixed == cls[c].mixed) { cls[c].fam = t.fam; cls[c].chunk = t.chunk; }
     if (bcr::batch_build(cls[c], v, 1)) {
       release();
       return fail(BCR_CUDA_ERROR, "alglin_b200 batch: table upload failed\n");
@@ -1549,7 +1634,7 @@ int bcr_batch_s::tune_class(size_t ci) {
   float best = 1e30f;
   int bf = c.fam, bc = c.chunk;
   for (int f : {bcr::PAIR_TC, bcr::PAIR_GRP, bcr::PAIR_ROWS}) {
-    if (!bcr::batch_family_ok(f, dm)) continue;
+    if (!bcr::batch_family_ok(f, dm, c.mixed != 0)) continue;
     for (int ch : {2, 4, 8, 16}) {
       c.fam = f;
       c.chunk = ch;
@@ -1572,8 +1657,8 @@ int bcr_batch_s::tune_class(size_t ci) {
   if (bcr::batch_build(c, v, 1)) return fail(BCR_CUDA_ERROR, "alglin_b200 batch: table upload failed\n");
   bool found = false;
   for (auto& t : g_batch_tuning)
-    if (t.n == dm.n && t.nrm == nrm && t.nxm == nxm) { t.fam = bf; t.chunk = bc; found = true; }
-  if (!found) g_batch_tuning.push_back({dm.n, nrm, nxm, bf, bc});
+    if (t.n == dm.n && t.nrm == nrm && t.nxm == nxm && t.mixed == c.mixed) { t.fam = bf; t.chunk = bc; found = true; }
+  if (!found) g_batch_tuning.push_back({dm.n, nrm, nxm, c.mixed, bf, bc});
   return BCR_OK;
 }
 
@@ -1759,9 +1844,8 @@ int bcr_batch_solve(bcr_batch b, double* const* x) {
   if (!b->factorized) return b->fail(BCR_NUMERICAL, "bcr_batch_solve: the batch is not factorized\n");
   int rc = batch_rhs_in(b, x);
   if (rc) return rc;
-  b->enqueue_solve();
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return b->cuda_fail(e, "batch solve");
+  if (b->mixed()) cudaMemcpyAsync(b->d_b, b->d_x, b->x_elems * 8, cudaMemcpyDeviceToDevice, b->stream);
+  if ((rc = b->solve_step(-1))) return rc;
   return batch_rhs_out(b, x);
 }
 
@@ -1771,11 +1855,17 @@ int bcr_batch_factorize_solve(bcr_batch b, double* const* x) {
   int rc = b->upload_inputs();
   if (rc) return rc;
   if ((rc = batch_rhs_in(b, x))) return rc;
+  if (b->mixed()) cudaMemcpyAsync(b->d_b, b->d_x, b->x_elems * 8, cudaMemcpyDeviceToDevice, b->stream);
   b->enqueue_factorize();
-  b->enqueue_solve();
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return b->cuda_fail(e, "batch factorize_solve");
-  if ((rc = b->read_status())) return rc;
+  if (b->mixed()) {  // the refinement needs the factorization's status first
+    if ((rc = b->read_status())) return rc;
+    if ((rc = b->solve_step(-1))) return rc;
+  } else {
+    b->enqueue_solve();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return b->cuda_fail(e, "batch factorize_solve");
+    if ((rc = b->read_status())) return rc;
+  }
   return batch_rhs_out(b, x);
 }
 
@@ -1804,18 +1894,24 @@ int bcr_batch_graph_capture(bcr_batch b) {
   // eager run first: kernel attributes, status check
   cudaMemcpyAsync(b->d_x, b->d_b, b->x_elems * 8, cudaMemcpyDeviceToDevice, b->stream);
   b->enqueue_factorize();
-  b->enqueue_solve();
   int rc = b->read_status();
   if (rc) return rc;
+  if ((rc = b->solve_step(-1))) return rc;
+  rc = b->read_status();
+  if (rc) return rc;
+  // the mixed graph replays the refinement steps the eager run needed
+  const int steps = b->ir_iters;
   if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
   cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed);
   if (e != cudaSuccess) return b->cuda_fail(e, "cudaStreamBeginCapture");
   cudaMemcpyAsync(b->d_x, b->d_b, b->x_elems * 8, cudaMemcpyDeviceToDevice, b->stream);
   b->enqueue_factorize();
-  b->enqueue_solve();
+  rc = b->solve_step(steps);
+  b->ir_pending = false;
   cudaGraph_t g = nullptr;
   e = cudaStreamEndCapture(b->stream, &g);
   if (e != cudaSuccess) { cudaGetLastError(); return b->cuda_fail(e, "cudaStreamEndCapture"); }
+  if (rc) { cudaGraphDestroy(g); return rc; }
   e = cudaGraphInstantiate(&b->graph, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) { b->graph = nullptr; return b->cuda_fail(e, "cudaGraphInstantiate"); }
@@ -1826,7 +1922,36 @@ int bcr_batch_graph_launch(bcr_batch b) {
   B_READY(b);
   if (!b->graph) return b->fail(BCR_BAD_ARGUMENT, "bcr_batch_graph_launch: no graph captured\n");
   cudaError_t e = cudaGraphLaunch(b->graph, b->stream);
-  return e == cudaSuccess ? BCR_OK : b->cuda_fail(e, "cudaGraphLaunch");
+  if (e != cudaSuccess) return b->cuda_fail(e, "cudaGraphLaunch");
+  if (b->mixed()) b->ir_pending = true;
+  return BCR_OK;
+}
+
+int bcr_batch_set_precision(bcr_batch b, int precision) {
+  B_CHECK(b);
+  if (precision != BCR_PRECISION_FP64 && precision != BCR_PRECISION_MIXED)
+    return b->fail(BCR_BAD_ARGUMENT, fmt("bcr_batch_set_precision: unknown precision %d\n", precision));
+  b->release();
+  b->precision = precision;
+  return BCR_OK;
+}
+
+int bcr_batch_set_refinement(bcr_batch b, double tol, int max_iter) {
+  B_CHECK(b);
+  if (!(tol >= 0.0) || max_iter < 0)
+    return b->fail(BCR_BAD_ARGUMENT, fmt("bcr_batch_set_refinement: bad tolerance %g or iteration limit %d\n", tol, max_iter));
+  b->ir_tol = tol;
+  b->ir_max = max_iter;
+  return BCR_OK;
+}
+
+int bcr_batch_refinement_info(bcr_batch b, int* iters, double* worst) {
+  B_CHECK(b);
+  int rc = b->read_worst();
+  if (rc) return rc;
+  if (iters) *iters = b->mixed() ? b->ir_iters : 0;
+  if (worst) *worst = b->mixed() ? b->ir_worst : 0.0;
+  return BCR_OK;
 }
 
 int bcr_batch_check_status(bcr_batch b) {

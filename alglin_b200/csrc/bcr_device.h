@@ -17,6 +17,9 @@ struct DevState {
   int pair_kernel;  // PairKernel: AUTO, or a forced pair-kernel family
   double* bx;       // batch: right-hand side / solution of this system
   int bldx;         // batch: its leading dimension
+  double* bsol;     // batch, mixed path: the refined solution
+  const double* bb; // batch, mixed path: the right-hand side
+  double* bnrm;     // batch, mixed path: |A|, |r|, |x|, |b|
   // loaded matrix (reference layout), never modified on the device
   double *D0, *E0, *B0, *C0, *Cq, *F0, *H;
   // working blocks / factors
@@ -80,6 +83,7 @@ size_t panel_smem_per_warp(const Dims& d, int elem_bytes);
 struct BatchClass {
   int nsys = 0;
   int fam = PAIR_AUTO;   // PAIR_TC, PAIR_GRP or PAIR_ROWS
+  int mixed = 0;         // FP32 working blocks (refined by the caller)
   int chunk = 8;         // pairs per CTA of the factorization launches
   int n = 0, nrm = 0, nxm = 0, levels = 0, nrhs = 1;
   size_t last_smem = 0;
@@ -87,18 +91,23 @@ struct BatchClass {
   void* sf = nullptr;    // device SweepArgs<double>[nsys], forward layout
   void* sb = nullptr;    // device SweepArgs<double>[nsys], backward layout
   void* ld = nullptr;    // device last-block descriptors [nsys]
+  void* rd = nullptr;    // device residual descriptors [nsys] (mixed path)
   BatchCta* fmap = nullptr;  // device: factorization chunks of every level
   BatchCta* smap = nullptr;  // device: sweep chunks of every level
   std::vector<long> foff, fcnt, soff, scnt;
 };
 
 // the pair-kernel families a batch class may use for systems of shape d (LU)
-bool batch_family_ok(int fam, const Dims& d);
+bool batch_family_ok(int fam, const Dims& d, bool mixed);
 // tables and maps of one class; sys[i] holds the device pointers of system i
 // (x, ldx: its right-hand side; st: its status word)
 int batch_build(BatchClass& c, const std::vector<DevState>& sys, int nrhs);
 void batch_free(BatchClass& c);
 void batch_factorize(BatchClass& c, cudaStream_t st);
 void batch_solve(BatchClass& c, cudaStream_t st);
+// mixed path: r = b - A x_sol into the rhs slots, per-system norms, batch-worst
+// relative residual (|A| is measured when with_A); y += x over a packed region
+void batch_residual(BatchClass& c, int with_A, unsigned long long* worst, cudaStream_t st);
+void batch_axpy(double* y, const double* x, size_t len, cudaStream_t st);
 
 }  // namespace bcr

@@ -3260,7 +3260,8 @@ void launch_axpy(double* y, const double* x, long len, cudaStream_t st) {
 struct LastDesc {
   Dims d;
   const double *D0, *E0, *B0, *C0, *H, *Cq, *F0, *Fbuf, *XB;
-  double *D, *E, *B, *C, *Ffin, *Hl, *tau, *x;
+  void *Dw, *Ew, *Bw, *Cw;  // working blocks: FP64, or FP32 on the mixed path
+  double *Ffin, *Hl, *tau, *x;
   int* piv;
   int kind, ldx;
   StatusWords* st;
@@ -3268,28 +3269,34 @@ struct LastDesc {
 };
 
 // status reset and the blocks the first level does not touch (odd tail, C_N)
+template <typename T>
 __global__ void __launch_bounds__(256) kb_begin(const LastDesc* t) {
   const LastDesc& L = t[blockIdx.x];
   const Dims d = L.d;
   const int nb = d.nblock;
   const size_t nn = (size_t)d.n * d.n, nnx = (size_t)d.n * d.nx, nrn = (size_t)d.nr * d.n;
+  T* D = static_cast<T*>(L.Dw);
+  T* E = static_cast<T*>(L.Ew);
+  T* B = static_cast<T*>(L.Bw);
+  T* C = static_cast<T*>(L.Cw);
   if (threadIdx.x == 0) *L.st = StatusWords{0, 0, 0, 0, 0};
   if (nb % 2 == 1) {
     const size_t b = (size_t)(nb - 1);
     for (size_t e = threadIdx.x; e < nn; e += blockDim.x) {
-      L.D[b * nn + e] = L.D0[b * nn + e];
-      L.E[b * nn + e] = L.E0[b * nn + e];
+      D[b * nn + e] = T(L.D0[b * nn + e]);
+      E[b * nn + e] = T(L.E0[b * nn + e]);
     }
-    for (size_t e = threadIdx.x; e < nnx; e += blockDim.x) L.B[b * nnx + e] = L.B0[b * nnx + e];
-    for (size_t e = threadIdx.x; e < nrn; e += blockDim.x) L.C[b * nrn + e] = L.C0[b * nrn + e];
+    for (size_t e = threadIdx.x; e < nnx; e += blockDim.x) B[b * nnx + e] = T(L.B0[b * nnx + e]);
+    for (size_t e = threadIdx.x; e < nrn; e += blockDim.x) C[b * nrn + e] = T(L.C0[b * nrn + e]);
   }
-  for (size_t e = threadIdx.x; e < nrn; e += blockDim.x) L.C[(size_t)nb * nrn + e] = L.C0[(size_t)nb * nrn + e];
+  for (size_t e = threadIdx.x; e < nrn; e += blockDim.x) C[(size_t)nb * nrn + e] = T(L.C0[(size_t)nb * nrn + e]);
 }
 
 // C_jpp += dC_jpp for the pairs of each chunk (one writer per target block)
-__global__ void __launch_bounds__(128) kb_border_fix(const FactorArgs<double>* tab, const BatchCta* cmap, int k) {
+template <typename T>
+__global__ void __launch_bounds__(128) kb_border_fix(const FactorArgs<T>* tab, const BatchCta* cmap, int k) {
   const BatchCta c = cmap[blockIdx.x];
-  const FactorArgs<double>& a = tab[c.sys];
+  const FactorArgs<T>& a = tab[c.sys];
   const Dims d = a.d;
   const size_t nrn = (size_t)d.nr * d.n;
   for (long q = c.q0; q < c.q1; ++q) {
@@ -3308,10 +3315,11 @@ __global__ void __launch_bounds__(256) kb_reduce_F(const LastDesc* t) {
   reduce_tree_body(L.Fbuf, m, 1, cnt, m, cnt > 0 ? cnt : 1, (double*)nullptr, L.F0, d.nr, d.nr, L.Ffin, d.nr, 0);
 }
 
+template <typename T>
 __global__ void __launch_bounds__(256) kb_last_assemble(const LastDesc* t) {
   const LastDesc& L = t[blockIdx.x];
-  last_assemble_range(L.d, (const double*)L.D, (const double*)L.E, (const double*)L.B, (const double*)L.C,
-                      L.H, L.Cq, L.Ffin, L.Hl, (int)threadIdx.x, (int)blockDim.x);
+  last_assemble_range(L.d, static_cast<const T*>(L.Dw), static_cast<const T*>(L.Ew), static_cast<const T*>(L.Bw),
+                      static_cast<const T*>(L.Cw), L.H, L.Cq, L.Ffin, L.Hl, (int)threadIdx.x, (int)blockDim.x);
 }
 
 __global__ void __launch_bounds__(512) kb_last_factor(const LastDesc* t) {
@@ -3338,10 +3346,147 @@ __global__ void __launch_bounds__(256) kb_last_solve(const LastDesc* t, int nrhs
   last_solve_body<double>(L.d, L.lb, L.st, L.x, L.ldx, nrhs);
 }
 
-bool batch_family_ok(int fam, const Dims& d) {
+// ---------------------------------------------------------------------------
+// FP64 residual of the mixed batch path, one CTA per system:
+// r = b - A xs with the loaded matrix (add_Mv, cc:2118-2166), written into the
+// system's right-hand-side slot, and |r|, |xs|, |b| (and |A|_inf when asked)
+// into nrm[1..3] (nrm[0]); the worst |r|/(|A||x|+|b|) of the batch goes to
+// *worst (bits of a non-negative double, so an integer max orders them)
+// ---------------------------------------------------------------------------
+struct ResDesc {
+  Dims d;
+  const double *D0, *E0, *B0, *C0, *Cq, *F0, *H;
+  const double *xs, *b;
+  double *r, *nrm;
+};
+
+__device__ double block_max(double v, double* sv) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) sv[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < nw ? sv[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (lane == 0) sv[0] = v;
+  }
+  __syncthreads();
+  return sv[0];
+}
+
+__global__ void __launch_bounds__(256) kb_residual(const ResDesc* t, int with_A, unsigned long long* worst) {
+  __shared__ double sv[32];
+  const ResDesc& R = t[blockIdx.x];
+  const Dims d = R.d;
+  const int n = d.n, nb = d.nblock, nr = d.nr, nx = d.nx, qx = d.qx, m = n + d.qr, Nc = d.Nc;
+  const int tid = threadIdx.x, bs = blockDim.x;
+  const size_t nn = (size_t)n * n, nnx = (size_t)n * nx, nrn = (size_t)nr * n;
+  const size_t xN = (size_t)nb * n, xq = (size_t)(nb + 1) * n, xb = xq + qx;
+  const double* xs = R.xs;
+  double mr = 0.0, ma = 0.0;
+  // block rows
+  for (long e = tid; e < (long)nb * n; e += bs) {
+    const size_t k = (size_t)(e / n);
+    const int i = (int)(e % n);
+    const double* Dk = R.D0 + k * nn;
+    const double* Ek = R.E0 + k * nn;
+    const double* Bk = R.B0 + k * nnx;
+    double s = 0.0, sa = 0.0;
+    for (int c = 0; c < n; ++c) {
+      s = fma(Dk[(size_t)c * n + i], xs[k * n + c], s);
+      s = fma(Ek[(size_t)c * n + i], xs[(k + 1) * n + c], s);
+      if (with_A) sa += fabs(Dk[(size_t)c * n + i]) + fabs(Ek[(size_t)c * n + i]);
+    }
+    for (int c = 0; c < nx; ++c) {
+      s = fma(Bk[(size_t)c * n + i], xs[xb + c], s);
+      if (with_A) sa += fabs(Bk[(size_t)c * n + i]);
+    }
+    const double r = R.b[e] - s;
+    R.r[e] = r;
+    mr = fmax(mr, fabs(r));
+    ma = fmax(ma, sa);
+  }
+  // boundary rows (H)
+  for (int row = tid; row < m; row += bs) {
+    double s = 0.0, sa = 0.0;
+    for (int c = 0; c < Nc; ++c) {
+      const size_t xi = c < n ? (size_t)c : (c < 2 * n ? xN + (c - n) : xq + (c - 2 * n));
+      const double h = R.H[(size_t)c * m + row];
+      s = fma(h, xs[xi], s);
+      sa += fabs(h);
+    }
+    const size_t o = xN + row;
+    const double r = R.b[o] - s;
+    R.r[o] = r;
+    mr = fmax(mr, fabs(r));
+    ma = fmax(ma, with_A ? sa : 0.0);
+  }
+  // border rows: every block column, reduced over the CTA
+  for (int rr = 0; rr < nr; ++rr) {
+    double s = 0.0, sa = 0.0;
+    for (long e = tid; e < (long)(nb + 1) * n; e += bs) {
+      const size_t k = (size_t)(e / n);
+      const int c = (int)(e % n);
+      const double cv = R.C0[k * nrn + (size_t)c * nr + rr];
+      s = fma(cv, xs[k * n + c], s);
+      sa += fabs(cv);
+    }
+    for (int c = tid; c < qx; c += bs) { s = fma(R.Cq[(size_t)c * nr + rr], xs[xq + c], s); sa += fabs(R.Cq[(size_t)c * nr + rr]); }
+    for (int c = tid; c < nx; c += bs) { s = fma(R.F0[(size_t)c * nr + rr], xs[xb + c], s); sa += fabs(R.F0[(size_t)c * nr + rr]); }
+    s = block_sum(s, sv);
+    sa = block_sum(sa, sv);
+    if (tid == 0) {
+      const size_t o = xN + m + rr;
+      const double r = R.b[o] - s;
+      R.r[o] = r;
+      mr = fmax(mr, fabs(r));
+      ma = fmax(ma, with_A ? sa : 0.0);
+    }
+  }
+  const long nrows = (long)n * (nb + 1) + d.qr + nr;
+  const long ncols = (long)n * (nb + 1) + qx + nx;
+  double mx = 0.0, mb = 0.0;
+  for (long e = tid; e < ncols; e += bs) mx = fmax(mx, fabs(xs[e]));
+  for (long e = tid; e < nrows; e += bs) mb = fmax(mb, fabs(R.b[e]));
+  mr = block_max(mr, sv);
+  mx = block_max(mx, sv);
+  mb = block_max(mb, sv);
+  if (with_A) ma = block_max(ma, sv);
+  if (tid == 0) {
+    if (with_A) R.nrm[0] = ma;
+    R.nrm[1] = mr;
+    R.nrm[2] = mx;
+    R.nrm[3] = mb;
+    const double den = R.nrm[0] * mx + mb;
+    double rel = den > 0.0 ? mr / den : (mr > 0.0 ? INFINITY : 0.0);
+    if (rel != rel) rel = INFINITY;
+    atomicMax(worst, (unsigned long long)__double_as_longlong(rel));
+  }
+}
+
+__global__ void kb_axpy(double* y, const double* x, size_t len) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (size_t)gridDim.x * blockDim.x)
+    y[i] += x[i];
+}
+
+void batch_residual(BatchClass& c, int with_A, unsigned long long* worst, cudaStream_t st) {
+  if (c.nsys == 0) return;
+  kb_residual<<<c.nsys, 256, 0, st>>>(static_cast<const ResDesc*>(c.rd), with_A, worst);
+  check_launch("kb_residual");
+}
+
+void batch_axpy(double* y, const double* x, size_t len, cudaStream_t st) {
+  kb_axpy<<<grid_for((long)len, 256, 148 * 8), 256, 0, st>>>(y, x, len);
+  check_launch("kb_axpy");
+}
+
+bool batch_family_ok(int fam, const Dims& d, bool mixed) {
   if (d.nr > 8 || d.nx > 8) return false;
   switch (fam) {
-    case PAIR_TC: return d.n == 8 || d.n == 16;
+    case PAIR_TC: return !mixed && (d.n == 8 || d.n == 16);
     case PAIR_GRP: return d.n == 16 || d.n == 32;
     case PAIR_ROWS: return d.n <= 16 && d.nr <= 4 && d.nx <= 4;
     default: return false;
@@ -3378,26 +3523,29 @@ static int upload_table(void*& dst, const std::vector<X>& v) {
 }
 
 void batch_free(BatchClass& c) {
-  for (void** p : {&c.fa, &c.sf, &c.sb, &c.ld})
+  for (void** p : {&c.fa, &c.sf, &c.sb, &c.ld, &c.rd})
     if (*p) { cudaFree(*p); *p = nullptr; }
   if (c.fmap) { cudaFree(c.fmap); c.fmap = nullptr; }
   if (c.smap) { cudaFree(c.smap); c.smap = nullptr; }
   c.foff.clear(); c.fcnt.clear(); c.soff.clear(); c.scnt.clear();
 }
 
-int batch_build(BatchClass& c, const std::vector<DevState>& sys, int nrhs) {
-  batch_free(c);
+template <typename T>
+static int batch_build_t(BatchClass& c, const std::vector<DevState>& sys, int nrhs) {
   c.nsys = (int)sys.size();
   c.nrhs = nrhs;
   c.levels = 0;
   c.nrm = c.nxm = 0;
   size_t lmax = 0;
-  std::vector<FactorArgs<double>> fa(sys.size());
-  std::vector<SweepArgs<double>> sf(sys.size()), sb(sys.size());
+  std::vector<FactorArgs<T>> fa(sys.size());
+  std::vector<SweepArgs<T>> sf(sys.size()), sb(sys.size());
   std::vector<LastDesc> ld(sys.size());
+  std::vector<ResDesc> rd(sys.size());
+  T* tag = nullptr;
   for (size_t i = 0; i < sys.size(); ++i) {
-    const DevState& s = sys[i];
+    DevState s = sys[i];
     const Dims d = s.d;
+    const WorkSet<T> w = work_set(s, tag);
     c.n = d.n;
     c.nrm = std::max(c.nrm, d.nr);
     c.nxm = std::max(c.nxm, d.nx);
@@ -3405,36 +3553,43 @@ int batch_build(BatchClass& c, const std::vector<DevState>& sys, int nrhs) {
     while (K < d.nblock) { K *= 2; ++lev; }
     c.levels = std::max(c.levels, lev);
     lmax = std::max<size_t>(lmax, (size_t)std::max(d.Nr, d.Nc));
-    FactorArgs<double> a{};
+    FactorArgs<T> a{};
     a.d = d;
     a.D0 = s.D0; a.E0 = s.E0; a.B0 = s.B0; a.C0 = s.C0;
-    a.D = s.D; a.E = s.E; a.B = s.B; a.C = s.C; a.Tm = s.T; a.P = s.P;
-    a.Rbuf = s.Rbuf; a.Fbuf = s.Fbuf; a.st = s.st;
+    a.D = w.D; a.E = w.E; a.B = w.B; a.C = w.C; a.Tm = w.Tm; a.P = s.P;
+    a.Rbuf = w.Rbuf; a.Fbuf = s.Fbuf; a.st = s.st;
     a.ldw = odd_ld(2 * d.n + d.nr);
     a.x = nullptr; a.ldx = 0; a.nrf = 0; a.XB = s.XB;
     fa[i] = a;
-    SweepArgs<double> w{};
-    w.d = d;
-    w.D = s.D; w.E = s.E; w.B = s.B; w.C = s.C; w.Tm = s.T; w.P = s.P;
-    w.x = s.bx; w.ldx = s.bldx; w.nrhs = nrhs; w.XB = s.XB; w.sel = SEL_LU;
-    w.ldw = odd_ld(2 * d.n);
-    sf[i] = w;
-    w.ldw = d.n;
-    sb[i] = w;
+    SweepArgs<T> sw{};
+    sw.d = d;
+    sw.D = w.D; sw.E = w.E; sw.B = w.B; sw.C = w.C; sw.Tm = w.Tm; sw.P = s.P;
+    sw.x = s.bx; sw.ldx = s.bldx; sw.nrhs = nrhs; sw.XB = s.XB; sw.sel = SEL_LU;
+    sw.ldw = odd_ld(2 * d.n);
+    sf[i] = sw;
+    sw.ldw = d.n;
+    sb[i] = sw;
     LastDesc l{};
     l.d = d;
     l.D0 = s.D0; l.E0 = s.E0; l.B0 = s.B0; l.C0 = s.C0; l.H = s.H; l.Cq = s.Cq; l.F0 = s.F0;
     l.Fbuf = s.Fbuf; l.XB = s.XB;
-    l.D = s.D; l.E = s.E; l.B = s.B; l.C = s.C; l.Ffin = s.Ffin; l.Hl = s.Hl; l.tau = s.tau_l; l.x = s.bx;
+    l.Dw = w.D; l.Ew = w.E; l.Bw = w.B; l.Cw = w.C;
+    l.Ffin = s.Ffin; l.Hl = s.Hl; l.tau = s.tau_l; l.x = s.bx;
     l.piv = s.piv_l; l.kind = s.sel_last; l.ldx = s.bldx; l.st = s.st;
     l.lb = last_bufs(s);
     ld[i] = l;
+    ResDesc r{};
+    r.d = d;
+    r.D0 = s.D0; r.E0 = s.E0; r.B0 = s.B0; r.C0 = s.C0; r.Cq = s.Cq; r.F0 = s.F0; r.H = s.H;
+    r.xs = s.bsol; r.b = s.bb; r.r = s.bx; r.nrm = s.bnrm;
+    rd[i] = r;
   }
   c.last_smem = 2 * lmax * 8;
   std::vector<BatchCta> fmap, smap;
   build_map(sys, c.levels, c.chunk, fmap, c.foff, c.fcnt);
   build_map(sys, c.levels, 8, smap, c.soff, c.scnt);
-  int bad = upload_table(c.fa, fa) | upload_table(c.sf, sf) | upload_table(c.sb, sb) | upload_table(c.ld, ld);
+  int bad = upload_table(c.fa, fa) | upload_table(c.sf, sf) | upload_table(c.sb, sb) | upload_table(c.ld, ld) |
+            upload_table(c.rd, rd);
   void* m1 = nullptr;
   void* m2 = nullptr;
   bad |= upload_table(m1, fmap) | upload_table(m2, smap);
@@ -3443,120 +3598,143 @@ int batch_build(BatchClass& c, const std::vector<DevState>& sys, int nrhs) {
   return bad;
 }
 
+int batch_build(BatchClass& c, const std::vector<DevState>& sys, int nrhs) {
+  batch_free(c);
+  return c.mixed ? batch_build_t<float>(c, sys, nrhs) : batch_build_t<double>(c, sys, nrhs);
+}
+
 // one batched launch of the class's pair kernel at level `L`
+template <typename T>
 static void batch_pairs(BatchClass& c, int L, cudaStream_t st) {
   const long cnt = c.fcnt[L];
   if (cnt == 0) return;
-  FactorArgs<double> a0{};
+  FactorArgs<T> a0{};
   a0.k = 1 << L;
   a0.first = L == 0;
-  const FactorArgs<double>* tab = static_cast<const FactorArgs<double>*>(c.fa);
+  const FactorArgs<T>* tab = static_cast<const FactorArgs<T>*>(c.fa);
   const BatchCta* map = c.fmap + c.foff[L];
   const unsigned g = (unsigned)cnt;
-  if (c.fam == PAIR_TC) {
-    if (c.n == 16) {
-      const size_t sm = tc_smem_per_warp(16) * 4;
-      smem_limit_once(k_factor_lu_tc<16, true>, sm);
-      k_factor_lu_tc<16, true><<<g, 128, sm, st>>>(a0, tab, map);
-    } else {
-      const size_t sm = tc_smem_per_warp(8) * 4;
-      smem_limit_once(k_factor_lu_tc<8, true>, sm);
-      k_factor_lu_tc<8, true><<<g, 128, sm, st>>>(a0, tab, map);
+  if constexpr (sizeof(T) == 8) {
+    if (c.fam == PAIR_TC) {
+      if (c.n == 16) {
+        const size_t sm = tc_smem_per_warp(16) * 4;
+        smem_limit_once(k_factor_lu_tc<16, true>, sm);
+        k_factor_lu_tc<16, true><<<g, 128, sm, st>>>(a0, tab, map);
+      } else {
+        const size_t sm = tc_smem_per_warp(8) * 4;
+        smem_limit_once(k_factor_lu_tc<8, true>, sm);
+        k_factor_lu_tc<8, true><<<g, 128, sm, st>>>(a0, tab, map);
+      }
+      check_launch("batched pair kernel");
     }
-  } else if (c.fam == PAIR_GRP) {
+  }
+  if (c.fam == PAIR_GRP) {
     if (c.n == 32) {
-      smem_limit_once(k_factor_lu_grp<double, 32, true>, GrpShape<double, 32>::BYTES);
-      k_factor_lu_grp<double, 32, true><<<g, 96, GrpShape<double, 32>::BYTES, st>>>(a0, tab, map);
+      smem_limit_once(k_factor_lu_grp<T, 32, true>, GrpShape<T, 32>::BYTES);
+      k_factor_lu_grp<T, 32, true><<<g, 96, GrpShape<T, 32>::BYTES, st>>>(a0, tab, map);
     } else {
-      smem_limit_once(k_factor_lu_grp<double, 16, true>, GrpShape<double, 16>::BYTES);
-      k_factor_lu_grp<double, 16, true><<<g, 64, GrpShape<double, 16>::BYTES, st>>>(a0, tab, map);
+      smem_limit_once(k_factor_lu_grp<T, 16, true>, GrpShape<T, 16>::BYTES);
+      k_factor_lu_grp<T, 16, true><<<g, 64, GrpShape<T, 16>::BYTES, st>>>(a0, tab, map);
     }
-  } else {
-    if (c.n <= 4) k_factor_lu_rows<double, 4, 4, 4, true><<<g, 128, 0, st>>>(a0, tab, map);
-    else if (c.n <= 8) k_factor_lu_rows<double, 8, 4, 4, true><<<g, 128, 0, st>>>(a0, tab, map);
-    else k_factor_lu_rows<double, 16, 4, 4, true><<<g, 128, 0, st>>>(a0, tab, map);
+  } else if (c.fam == PAIR_ROWS) {
+    if (c.n <= 4) k_factor_lu_rows<T, 4, 4, 4, true><<<g, 128, 0, st>>>(a0, tab, map);
+    else if (c.n <= 8) k_factor_lu_rows<T, 8, 4, 4, true><<<g, 128, 0, st>>>(a0, tab, map);
+    else k_factor_lu_rows<T, 16, 4, 4, true><<<g, 128, 0, st>>>(a0, tab, map);
   }
   check_launch("batched pair kernel");
   if (c.nrm > 0) {
-    kb_border_fix<<<g, 128, 0, st>>>(tab, map, 1 << L);
+    kb_border_fix<T><<<g, 128, 0, st>>>(tab, map, 1 << L);
     check_launch("kb_border_fix");
   }
 }
 
-void batch_factorize(BatchClass& c, cudaStream_t st) {
-  if (c.nsys == 0) return;
+template <typename T>
+static void batch_factorize_t(BatchClass& c, cudaStream_t st) {
   const LastDesc* ld = static_cast<const LastDesc*>(c.ld);
-  kb_begin<<<c.nsys, 256, 0, st>>>(ld);
+  kb_begin<T><<<c.nsys, 256, 0, st>>>(ld);
   check_launch("kb_begin");
-  for (int L = 0; L < c.levels; ++L) batch_pairs(c, L, st);
+  for (int L = 0; L < c.levels; ++L) batch_pairs<T>(c, L, st);
   kb_reduce_F<<<c.nsys, 256, 0, st>>>(ld);
-  kb_last_assemble<<<c.nsys, 256, 0, st>>>(ld);
+  kb_last_assemble<T><<<c.nsys, 256, 0, st>>>(ld);
   kb_last_factor<<<c.nsys, 512, 0, st>>>(ld);
   check_launch("batched last block");
 }
 
-template <int N>
+void batch_factorize(BatchClass& c, cudaStream_t st) {
+  if (c.nsys == 0) return;
+  if (c.mixed) batch_factorize_t<float>(c, st);
+  else batch_factorize_t<double>(c, st);
+}
+
+template <typename T, int N>
 static void batch_sweeps_rows(BatchClass& c, cudaStream_t st, bool forward, int L) {
   const bool r4 = c.nrm <= 4, x4 = c.nxm <= 4;
   const BatchCta* map = c.smap + c.soff[L];
   const unsigned g = (unsigned)c.scnt[L];
-  SweepArgs<double> a0{};
+  SweepArgs<T> a0{};
   a0.k = 1 << L;
   if (forward) {
-    const SweepArgs<double>* tab = static_cast<const SweepArgs<double>*>(c.sf);
-    if (r4) k_forward_rows<double, N, 4, true, true><<<g, 256, 0, st>>>(a0, tab, map);
-    else k_forward_rows<double, N, 8, true, true><<<g, 256, 0, st>>>(a0, tab, map);
+    const SweepArgs<T>* tab = static_cast<const SweepArgs<T>*>(c.sf);
+    if (r4) k_forward_rows<T, N, 4, true, true><<<g, 256, 0, st>>>(a0, tab, map);
+    else k_forward_rows<T, N, 8, true, true><<<g, 256, 0, st>>>(a0, tab, map);
   } else {
-    const SweepArgs<double>* tab = static_cast<const SweepArgs<double>*>(c.sb);
-    if (x4) k_backward_rows<double, N, 4, true><<<g, 256, 0, st>>>(a0, tab, map);
-    else k_backward_rows<double, N, 8, true><<<g, 256, 0, st>>>(a0, tab, map);
+    const SweepArgs<T>* tab = static_cast<const SweepArgs<T>*>(c.sb);
+    if (x4) k_backward_rows<T, N, 4, true><<<g, 256, 0, st>>>(a0, tab, map);
+    else k_backward_rows<T, N, 8, true><<<g, 256, 0, st>>>(a0, tab, map);
   }
 }
 
+template <typename T>
 static void batch_sweep_level(BatchClass& c, cudaStream_t st, bool forward, int L) {
   if (c.scnt[L] == 0) return;
-  if (c.n <= 4) batch_sweeps_rows<4>(c, st, forward, L);
-  else if (c.n <= 8) batch_sweeps_rows<8>(c, st, forward, L);
-  else if (c.n <= 16) batch_sweeps_rows<16>(c, st, forward, L);
+  if (c.n <= 4) batch_sweeps_rows<T, 4>(c, st, forward, L);
+  else if (c.n <= 8) batch_sweeps_rows<T, 8>(c, st, forward, L);
+  else if (c.n <= 16) batch_sweeps_rows<T, 16>(c, st, forward, L);
   else if (c.n == 32) {
     const BatchCta* map = c.smap + c.soff[L];
     const unsigned g = (unsigned)c.scnt[L];
-    SweepArgs<double> a0{};
+    SweepArgs<T> a0{};
     a0.k = 1 << L;
     if (forward) {
-      const SweepArgs<double>* tab = static_cast<const SweepArgs<double>*>(c.sf);
-      if (c.nrm <= 4) k_forward_rows32<double, 4, true><<<g, 256, 0, st>>>(a0, tab, map);
-      else k_forward_rows32<double, 8, true><<<g, 256, 0, st>>>(a0, tab, map);
+      const SweepArgs<T>* tab = static_cast<const SweepArgs<T>*>(c.sf);
+      if (c.nrm <= 4) k_forward_rows32<T, 4, true><<<g, 256, 0, st>>>(a0, tab, map);
+      else k_forward_rows32<T, 8, true><<<g, 256, 0, st>>>(a0, tab, map);
     } else {
-      const SweepArgs<double>* tab = static_cast<const SweepArgs<double>*>(c.sb);
-      if (c.nxm <= 4) k_backward_rows32<double, 4, true><<<g, 256, 0, st>>>(a0, tab, map);
-      else k_backward_rows32<double, 8, true><<<g, 256, 0, st>>>(a0, tab, map);
+      const SweepArgs<T>* tab = static_cast<const SweepArgs<T>*>(c.sb);
+      if (c.nxm <= 4) k_backward_rows32<T, 4, true><<<g, 256, 0, st>>>(a0, tab, map);
+      else k_backward_rows32<T, 8, true><<<g, 256, 0, st>>>(a0, tab, map);
     }
   } else {
     const BatchCta* map = c.smap + c.soff[L];
     const unsigned g = (unsigned)c.scnt[L];
-    SweepArgs<double> a0{};
+    SweepArgs<T> a0{};
     a0.k = 1 << L;
     if (forward) {
       const size_t sm = (size_t)odd_ld(2 * c.n) * c.nrhs * 8 * WARPS_PANEL;
-      smem_limit_once(k_forward_level<double, true>, sm);
-      k_forward_level<double, true><<<g, WARPS_PANEL * 32, sm, st>>>(a0, static_cast<const SweepArgs<double>*>(c.sf), map);
+      smem_limit_once(k_forward_level<T, true>, sm);
+      k_forward_level<T, true><<<g, WARPS_PANEL * 32, sm, st>>>(a0, static_cast<const SweepArgs<T>*>(c.sf), map);
     } else {
       const size_t sm = (size_t)c.n * 8 * WARPS_PANEL;
-      k_backward_level<double, true><<<g, WARPS_PANEL * 32, sm, st>>>(a0, static_cast<const SweepArgs<double>*>(c.sb), map);
+      k_backward_level<T, true><<<g, WARPS_PANEL * 32, sm, st>>>(a0, static_cast<const SweepArgs<T>*>(c.sb), map);
     }
   }
   check_launch(forward ? "batched forward sweep" : "batched backward sweep");
 }
 
-void batch_solve(BatchClass& c, cudaStream_t st) {
-  if (c.nsys == 0) return;
+template <typename T>
+static void batch_solve_t(BatchClass& c, cudaStream_t st) {
   const LastDesc* ld = static_cast<const LastDesc*>(c.ld);
-  for (int L = 0; L < c.levels; ++L) batch_sweep_level(c, st, true, L);
+  for (int L = 0; L < c.levels; ++L) batch_sweep_level<T>(c, st, true, L);
   kb_reduce_xb<<<c.nsys, 256, 0, st>>>(ld, c.nrhs);
   kb_last_solve<<<c.nsys, 256, c.last_smem, st>>>(ld, c.nrhs);
-  for (int L = c.levels - 1; L >= 0; --L) batch_sweep_level(c, st, false, L);
+  for (int L = c.levels - 1; L >= 0; --L) batch_sweep_level<T>(c, st, false, L);
   check_launch("batched solve");
+}
+
+void batch_solve(BatchClass& c, cudaStream_t st) {
+  if (c.nsys == 0) return;
+  if (c.mixed) batch_solve_t<float>(c, st);
+  else batch_solve_t<double>(c, st);
 }
 
 }  // namespace bcr

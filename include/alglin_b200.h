@@ -269,6 +269,13 @@ int bcr_batch_check_status(bcr_batch b);
 void *bcr_batch_stream(bcr_batch b);
 int bcr_batch_synchronize(bcr_batch b);
 const char *bcr_batch_last_error(bcr_batch b);
+/* mixed precision for the whole batch (set before prepare): FP32 working
+   blocks, FP64 F, last block and vectors, FP64 refinement of every system until
+   the worst |b-Ax|/(|A||x|+|b|) of the batch is <= tol or after max_iter
+   corrections; the systems must be square */
+int bcr_batch_set_precision(bcr_batch b, int precision);
+int bcr_batch_set_refinement(bcr_batch b, double tol, int max_iter);
+int bcr_batch_refinement_info(bcr_batch b, int *iters, double *worst);
 
 #ifdef __cplusplus
 }

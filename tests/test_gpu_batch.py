@@ -162,3 +162,78 @@ def test_batch_rejects_unsupported():
     bt2 = B.Batch([h2])
     with pytest.raises(B.BCRError, match="internal LU"):
         bt2.prepare()
+
+
+def square_systems(nsys, lo, hi, seed):
+    """Uneven square systems (qr = qx = 0, nr = nx) of the batch workload."""
+    return make_systems(nsys, lo, hi, seed)
+
+
+def relres_each(systems, rhs, xs):
+    out = []
+    for s, b, x in zip(systems, rhs, xs):
+        o = po.Oracle(s, "LU", "LU")
+        out.append(relres(o, s, x, b))
+    return out
+
+
+@pytest.mark.parametrize("autotune", [False, True])
+def test_batch_mixed_refines_every_system(autotune):
+    """FP32 factors + FP64 refinement over the batch: every system reaches the
+    mixed bar (rel. residual <= 1e-12) and the forward error against the FP64
+    oracle is <= 1e-8."""
+    systems, rhs = square_systems(24, 1, 300, seed=17)
+    bt = B.Batch(handles_for(systems))
+    bt.set_precision(B.PRECISION_MIXED)
+    bt.set_refinement(1e-12, 10)
+    bt.prepare(autotune=autotune)
+    xs = [b.copy() for b in rhs]
+    assert bt.factorize_solve(xs), bt.last_error()
+    it, worst = bt.refinement_info()
+    assert 1 <= it <= 10 and worst <= 1e-12, (it, worst)
+    for i, rr in enumerate(relres_each(systems, rhs, xs)):
+        assert rr <= 1e-12, (i, rr)
+    for i, (s, b, x) in enumerate(zip(systems, rhs, xs)):
+        o = po.Oracle(s, "LU", "LU")
+        assert o.factorize()
+        xo = o.solve(b[None, :])[0]
+        assert fwd_err(x[:s.ncols], xo[:s.ncols]) <= 1e-8, i
+    # factorize once, solve again
+    ys = [b.copy() for b in rhs]
+    assert bt.solve(ys), bt.last_error()
+    assert bt.refinement_info()[1] <= 1e-12
+
+
+def test_batch_mixed_graph_replays_the_refinement():
+    torch = pytest.importorskip("torch")
+    systems, rhs = square_systems(11, 50, 400, seed=23)
+    bt = B.Batch(handles_for(systems))
+    bt.set_precision(B.PRECISION_MIXED)
+    bt.prepare()
+    bt.set_rhs(rhs)
+    bt.graph_capture()
+    it0, w0 = bt.refinement_info()
+    ys0 = [np.zeros_like(b) for b in rhs]
+    bt.get_x(ys0)
+    for _ in range(3):
+        bt.graph_launch()
+    bt.synchronize()
+    it, worst = bt.refinement_info()
+    assert it == it0 and worst <= 1e-12
+    ys = [np.zeros_like(b) for b in rhs]
+    bt.get_x(ys)
+    for a, c in zip(ys0, ys):
+        assert np.array_equal(a, c)
+    for i, rr in enumerate(relres_each(systems, rhs, ys)):
+        assert rr <= 1e-12, (i, rr)
+
+
+def test_batch_mixed_rejects_non_square():
+    s = synth.collocation(20, 8, 1, 0, 2, 2, seed=2)
+    h = B.BorderedCR()
+    h.load_system(s)
+    h.select_last("QR")
+    bt = B.Batch([h])
+    bt.set_precision(B.PRECISION_MIXED)
+    with pytest.raises(B.BCRError, match="square"):
+        bt.prepare()
