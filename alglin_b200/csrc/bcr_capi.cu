@@ -1292,12 +1292,13 @@ struct bcr_batch_s {
   // mixed path: FP32 working arrays, refined solutions, per-system norms
   int precision = BCR_PRECISION_FP64;
   double ir_tol = 1e-12;
-  int ir_max = 10;
+  int ir_max = 30;  // converged systems drop out, so a slow one costs little
   int ir_iters = 0;
   double ir_worst = 0.0;
   bool ir_pending = false;
   double* d_sol = nullptr;             // refined solutions, same packing as d_x
-  double* d_nrm = nullptr;             // 4 per system: |A|, |r|, |x|, |b|
+  double* d_nrm = nullptr;             // 5 per system: |A|, |r|, |x|, |b|, relative residual
+  int* d_done = nullptr;               // per system: refinement converged
   unsigned long long* d_worst = nullptr;
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph = nullptr;
@@ -1326,6 +1327,8 @@ struct bcr_batch_s {
     if (d_sol) cudaFree(d_sol);
     if (d_nrm) cudaFree(d_nrm);
     if (d_worst) cudaFree(d_worst);
+    if (d_done) cudaFree(d_done);
+    d_done = nullptr;
     d_sol = d_nrm = nullptr;
     d_worst = nullptr;
     ir_pending = false;
@@ -1400,12 +1403,13 @@ struct bcr_batch_s {
   // the batch-worst norm after each residual) or for exactly `fixed` steps;
   // the refined solutions end in the rhs region
   int solve_mixed(int fixed, bool with_A) {
+    cudaMemsetAsync(d_done, 0, hs.size() * sizeof(int), stream);  // every system solves x0
     enqueue_solve();
     cudaMemcpyAsync(d_sol, d_x, x_elems * 8, cudaMemcpyDeviceToDevice, stream);
     int it = 0;
     for (;;) {
       cudaMemsetAsync(d_worst, 0, 8, stream);
-      for (auto& c : cls) bcr::batch_residual(c, with_A && it == 0 ? 1 : 0, d_worst, stream);
+      for (auto& c : cls) bcr::batch_residual(c, with_A && it == 0 ? 1 : 0, ir_tol, d_worst, stream);
       ir_pending = true;
       if (fixed < 0) {
         int rc = read_worst();
@@ -1414,8 +1418,8 @@ struct bcr_batch_s {
       } else if (it >= fixed) {
         break;
       }
-      enqueue_solve();
-      bcr::batch_axpy(d_sol, d_x, x_elems, stream);
+      enqueue_solve();  // converged systems skip their sweeps
+      for (auto& c : cls) bcr::batch_correct(c, stream);
       ++it;
     }
     cudaMemcpyAsync(d_x, d_sol, x_elems * 8, cudaMemcpyDeviceToDevice, stream);
@@ -1524,7 +1528,8 @@ int bcr_batch_s::prepare(int autotune) {
   if (e == cudaSuccess) e = cudaMalloc(&d_b, std::max<size_t>(x_elems, 1) * 8);
   if (e == cudaSuccess) e = cudaMalloc(&d_st, ns * sizeof(bcr::StatusWords));
   if (e == cudaSuccess && mixed()) e = cudaMalloc(&d_sol, std::max<size_t>(x_elems, 1) * 8);
-  if (e == cudaSuccess && mixed()) e = cudaMalloc(&d_nrm, ns * 4 * sizeof(double));
+  if (e == cudaSuccess && mixed()) e = cudaMalloc(&d_nrm, ns * 5 * sizeof(double));
+  if (e == cudaSuccess && mixed()) e = cudaMalloc(&d_done, ns * sizeof(int));
   if (e == cudaSuccess && mixed()) e = cudaMalloc(&d_worst, 8);
   if (e == cudaSuccess && any_handle) e = cudaMallocHost(&h_in, in_bytes);
   if (e == cudaSuccess) e = cudaMallocHost(&h_x, std::max<size_t>(x_elems, 1) * 8);
@@ -1554,7 +1559,8 @@ int bcr_batch_s::prepare(int autotune) {
       s.Df = F(o.D); s.Ef = F(o.E); s.Bf = F(o.B); s.Cf = F(o.C); s.Tf = F(o.T); s.Rbuff = F(o.Rbuf);
       s.bsol = d_sol + x_off[i];
       s.bb = d_b + x_off[i];
-      s.bnrm = d_nrm + 4 * i;
+      s.bnrm = d_nrm + 5 * i;
+      s.bdone = d_done + i;
     } else {
       s.D = W(o.D); s.E = W(o.E); s.B = W(o.B); s.C = W(o.C); s.T = W(o.T);
       s.Rbuf = W(o.Rbuf);

@@ -19,7 +19,8 @@ struct DevState {
   int bldx;         // batch: its leading dimension
   double* bsol;     // batch, mixed path: the refined solution
   const double* bb; // batch, mixed path: the right-hand side
-  double* bnrm;     // batch, mixed path: |A|, |r|, |x|, |b|
+  double* bnrm;     // batch, mixed path: |A|, |r|, |x|, |b|, relative residual
+  int* bdone;       // batch, mixed path: refinement converged (null otherwise)
   // loaded matrix (reference layout), never modified on the device
   double *D0, *E0, *B0, *C0, *Cq, *F0, *H;
   // working blocks / factors
@@ -105,9 +106,11 @@ int batch_build(BatchClass& c, const std::vector<DevState>& sys, int nrhs);
 void batch_free(BatchClass& c);
 void batch_factorize(BatchClass& c, cudaStream_t st);
 void batch_solve(BatchClass& c, cudaStream_t st);
-// mixed path: r = b - A x_sol into the rhs slots, per-system norms, batch-worst
-// relative residual (|A| is measured when with_A); y += x over a packed region
-void batch_residual(BatchClass& c, int with_A, unsigned long long* worst, cudaStream_t st);
-void batch_axpy(double* y, const double* x, size_t len, cudaStream_t st);
+// mixed path: r = b - A x_sol into the rhs slots, per-system norms and
+// converged flags (relative residual <= tol), batch-worst relative residual
+// (|A| is measured when with_A)
+void batch_residual(BatchClass& c, int with_A, double tol, unsigned long long* worst, cudaStream_t st);
+// x_sol += d for the systems that have not converged
+void batch_correct(BatchClass& c, cudaStream_t st);
 
 }  // namespace bcr

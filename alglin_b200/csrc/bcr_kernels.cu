@@ -63,6 +63,11 @@ __device__ __forceinline__ T ldsrc(bool first, const double* orig, const T* work
 __device__ __forceinline__ void take_level(FactorArgs<float>& a, const FactorArgs<float>& a0) { a.k = a0.k; a.first = a0.first; }
 __device__ __forceinline__ void take_level(FactorArgs<double>& a, const FactorArgs<double>& a0) { a.k = a0.k; a.first = a0.first; }
 
+// a batch system whose refinement has converged skips the sweeps (the
+// SweepArgs overload below; found at instantiation)
+template <typename A>
+__device__ __forceinline__ bool system_active(const A&) { return true; }
+
 template <bool BATCH, typename A>
 __device__ __forceinline__ void pair_range(const A& a0, const A* tab, const BatchCta* cmap, int workers, int worker,
                                            A& a, long& q0, long& q1, long& qs) {
@@ -71,7 +76,7 @@ __device__ __forceinline__ void pair_range(const A& a0, const A* tab, const Batc
     a = tab[c.sys];
     take_level(a, a0);
     q0 = c.q0 + worker;
-    q1 = c.q1;
+    q1 = system_active(a) ? c.q1 : q0;
     qs = workers;
   } else {
     q0 = (long)blockIdx.x * workers + worker;
@@ -1901,7 +1906,11 @@ struct SweepArgs {
   int ldx, nrhs;
   double* XB;
   int k, ldw, sel;
+  const int* done;  // batch, mixed path: nonzero once this system's refinement converged
 };
+
+template <typename T>
+__device__ __forceinline__ bool system_active(const SweepArgs<T>& a) { return !(a.done && *a.done); }
 
 __device__ __forceinline__ void take_level(SweepArgs<float>& a, const SweepArgs<float>& a0) { a.k = a0.k; }
 __device__ __forceinline__ void take_level(SweepArgs<double>& a, const SweepArgs<double>& a0) { a.k = a0.k; }
@@ -3266,6 +3275,7 @@ struct LastDesc {
   int kind, ldx;
   StatusWords* st;
   LastBufs lb;
+  const int* done;  // mixed path: the system's refinement converged (skip its solve)
 };
 
 // status reset and the blocks the first level does not touch (odd tail, C_N)
@@ -3333,7 +3343,7 @@ __global__ void __launch_bounds__(512) kb_last_factor(const LastDesc* t) {
 __global__ void __launch_bounds__(256) kb_reduce_xb(const LastDesc* t, int nrhs) {
   const LastDesc& L = t[blockIdx.x];
   const Dims d = L.d;
-  if (d.nr == 0) return;
+  if (d.nr == 0 || (L.done && *L.done)) return;
   const int m = d.nr * nrhs;
   const long cnt = d.nblock - 1;
   double* xb = L.x + (size_t)(d.nblock + 1) * d.n + d.qr;
@@ -3343,6 +3353,7 @@ __global__ void __launch_bounds__(256) kb_reduce_xb(const LastDesc* t, int nrhs)
 
 __global__ void __launch_bounds__(256) kb_last_solve(const LastDesc* t, int nrhs) {
   const LastDesc& L = t[blockIdx.x];
+  if (L.done && *L.done) return;
   last_solve_body<double>(L.d, L.lb, L.st, L.x, L.ldx, nrhs);
 }
 
@@ -3356,8 +3367,10 @@ __global__ void __launch_bounds__(256) kb_last_solve(const LastDesc* t, int nrhs
 struct ResDesc {
   Dims d;
   const double *D0, *E0, *B0, *C0, *Cq, *F0, *H;
-  const double *xs, *b;
-  double *r, *nrm;
+  double* xs;          // the refined solution
+  const double* b;
+  double *r, *nrm;     // nrm: |A|, |r|, |x|, |b|, |r|/(|A||x|+|b|)
+  int* done;
 };
 
 __device__ double block_max(double v, double* sv) {
@@ -3377,9 +3390,14 @@ __device__ double block_max(double v, double* sv) {
   return sv[0];
 }
 
-__global__ void __launch_bounds__(256) kb_residual(const ResDesc* t, int with_A, unsigned long long* worst) {
+__global__ void __launch_bounds__(256) kb_residual(const ResDesc* t, int with_A, double tol,
+                                                   unsigned long long* worst) {
   __shared__ double sv[32];
   const ResDesc& R = t[blockIdx.x];
+  if (*R.done) {  // converged earlier: its last figure still counts for the batch
+    if (threadIdx.x == 0) atomicMax(worst, (unsigned long long)__double_as_longlong(R.nrm[4]));
+    return;
+  }
   const Dims d = R.d;
   const int n = d.n, nb = d.nblock, nr = d.nr, nx = d.nx, qx = d.qx, m = n + d.qr, Nc = d.Nc;
   const int tid = threadIdx.x, bs = blockDim.x;
@@ -3463,24 +3481,31 @@ __global__ void __launch_bounds__(256) kb_residual(const ResDesc* t, int with_A,
     const double den = R.nrm[0] * mx + mb;
     double rel = den > 0.0 ? mr / den : (mr > 0.0 ? INFINITY : 0.0);
     if (rel != rel) rel = INFINITY;
+    R.nrm[4] = rel;
+    if (rel <= tol) *R.done = 1;
     atomicMax(worst, (unsigned long long)__double_as_longlong(rel));
   }
 }
 
-__global__ void kb_axpy(double* y, const double* x, size_t len) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (size_t)gridDim.x * blockDim.x)
-    y[i] += x[i];
+// x_sol += d for the systems still refining (d was solved in place of r)
+__global__ void __launch_bounds__(256) kb_correct(const ResDesc* t) {
+  const ResDesc& R = t[blockIdx.x];
+  if (*R.done) return;
+  const Dims d = R.d;
+  const long ncols = (long)d.n * (d.nblock + 1) + d.qx + d.nx;
+  for (long i = threadIdx.x; i < ncols; i += blockDim.x) R.xs[i] += R.r[i];
 }
 
-void batch_residual(BatchClass& c, int with_A, unsigned long long* worst, cudaStream_t st) {
+void batch_residual(BatchClass& c, int with_A, double tol, unsigned long long* worst, cudaStream_t st) {
   if (c.nsys == 0) return;
-  kb_residual<<<c.nsys, 256, 0, st>>>(static_cast<const ResDesc*>(c.rd), with_A, worst);
+  kb_residual<<<c.nsys, 256, 0, st>>>(static_cast<const ResDesc*>(c.rd), with_A, tol, worst);
   check_launch("kb_residual");
 }
 
-void batch_axpy(double* y, const double* x, size_t len, cudaStream_t st) {
-  kb_axpy<<<grid_for((long)len, 256, 148 * 8), 256, 0, st>>>(y, x, len);
-  check_launch("kb_axpy");
+void batch_correct(BatchClass& c, cudaStream_t st) {
+  if (c.nsys == 0) return;
+  kb_correct<<<c.nsys, 256, 0, st>>>(static_cast<const ResDesc*>(c.rd));
+  check_launch("kb_correct");
 }
 
 bool batch_family_ok(int fam, const Dims& d, bool mixed) {
@@ -3565,6 +3590,7 @@ static int batch_build_t(BatchClass& c, const std::vector<DevState>& sys, int nr
     sw.d = d;
     sw.D = w.D; sw.E = w.E; sw.B = w.B; sw.C = w.C; sw.Tm = w.Tm; sw.P = s.P;
     sw.x = s.bx; sw.ldx = s.bldx; sw.nrhs = nrhs; sw.XB = s.XB; sw.sel = SEL_LU;
+    sw.done = s.bdone;
     sw.ldw = odd_ld(2 * d.n);
     sf[i] = sw;
     sw.ldw = d.n;
@@ -3577,11 +3603,12 @@ static int batch_build_t(BatchClass& c, const std::vector<DevState>& sys, int nr
     l.Ffin = s.Ffin; l.Hl = s.Hl; l.tau = s.tau_l; l.x = s.bx;
     l.piv = s.piv_l; l.kind = s.sel_last; l.ldx = s.bldx; l.st = s.st;
     l.lb = last_bufs(s);
+    l.done = s.bdone;
     ld[i] = l;
     ResDesc r{};
     r.d = d;
     r.D0 = s.D0; r.E0 = s.E0; r.B0 = s.B0; r.C0 = s.C0; r.Cq = s.Cq; r.F0 = s.F0; r.H = s.H;
-    r.xs = s.bsol; r.b = s.bb; r.r = s.bx; r.nrm = s.bnrm;
+    r.xs = s.bsol; r.b = s.bb; r.r = s.bx; r.nrm = s.bnrm; r.done = s.bdone;
     rd[i] = r;
   }
   c.last_smem = 2 * lmax * 8;

@@ -379,14 +379,16 @@ def variants(torch, bcr, synth, steps, warmup, rank):
     out["C_fp64"] = dict(f64, workload=wl)
     out["C_mixed"] = dict(mix, workload=wl)
     out["C_mixed_over_fp64"] = mix["value"] / f64["value"]
-    try:
-        out["D_batched_fp64"] = batched(torch, bcr, synth, rank)
-    except Exception as e:  # e.g. not enough device memory on a shared GPU
-        out["D_batched_fp64"] = {"unavailable": str(e)[:200]}
+    for name, prec in (("D_batched_fp64", bcr.PRECISION_FP64), ("D_batched_mixed", bcr.PRECISION_MIXED)):
+        try:
+            out[name] = batched(torch, bcr, synth, rank, prec)
+        except Exception as e:  # e.g. not enough device memory on a shared GPU
+            out[name] = {"unavailable": str(e)[:200]}
+        torch.cuda.empty_cache()
     return out
 
 
-def batched(torch, bcr, synth, rank, nsys=4096):
+def batched(torch, bcr, synth, rank, prec, nsys=4096):
     """4096 independent systems, nblock ~ U{64..4096}, n in {4,8,16,32},
     nr = nx in {0,2,4}: one CUDA graph per factorize + solve of the whole batch."""
     from cuda.bindings import runtime as rt
@@ -394,6 +396,7 @@ def batched(torch, bcr, synth, rank, nsys=4096):
     bt = bcr.Batch()
     for d in dims:
         bt.add_device(*d)
+    bt.set_precision(prec)
     bt.prepare()
     g = torch.Generator(device="cuda")
     g.manual_seed(7 + rank)
@@ -421,11 +424,13 @@ def batched(torch, bcr, synth, rank, nsys=4096):
         e1.synchronize()
         lat.append(e0.elapsed_time(e1))
     ok = bt.check_status()
+    iters, worst = bt.refinement_info()
     lat.sort()
     p50, p99 = lat[len(lat) // 2], lat[-1]
     unk = sum(n * (nb + 1) + nx for nb, n, _, _, _, nx in dims)
     return {"systems_per_s": nsys / (p50 * 1e-3), "unknowns_per_s": unk / (p50 * 1e-3),
             "p50_ms": p50, "p99_ms": p99, "nsys": nsys, "all_factorized": bool(ok),
+            "refinement_steps": iters, "worst_rel_residual": worst if prec else None,
             "classes": [{"n": c[0], "systems": c[1], "family": ["auto", "tc", "grp", "rows"][c[2]],
                          "pairs_per_cta": c[3]} for c in bt.classes()],
             "workload": "4096 systems, nblock U{64..4096}, n in {4,8,16,32}, nr=nx in {0,2,4}, "

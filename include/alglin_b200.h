@@ -272,7 +272,8 @@ const char *bcr_batch_last_error(bcr_batch b);
 /* mixed precision for the whole batch (set before prepare): FP32 working
    blocks, FP64 F, last block and vectors, FP64 refinement of every system until
    the worst |b-Ax|/(|A||x|+|b|) of the batch is <= tol or after max_iter
-   corrections; the systems must be square */
+   corrections (defaults 1e-12 and 30); a system that has converged drops out
+   of the later corrections; the systems must be square */
 int bcr_batch_set_precision(bcr_batch b, int precision);
 int bcr_batch_set_refinement(bcr_batch b, double tol, int max_iter);
 int bcr_batch_refinement_info(bcr_batch b, int *iters, double *worst);
