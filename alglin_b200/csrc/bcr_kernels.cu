@@ -2267,6 +2267,153 @@ __global__ void __launch_bounds__(256, 2) k_backward_rows32(SweepArgs<TF> a0, co
 }
 
 // ---------------------------------------------------------------------------
+// sweeps for large blocks (n > 32, n <= 128): one CTA per pair, the 2n
+// values of the pair in shared memory, the triangular solves blocked by 32
+// rows (one warp solves a diagonal block with shuffles, the CTA applies it to
+// the rows that follow)
+// ---------------------------------------------------------------------------
+constexpr int SWP_MAXN = 128;
+
+template <typename TF, bool BATCH = false>
+__global__ void __launch_bounds__(256) k_forward_cta(SweepArgs<TF> a0, const SweepArgs<TF>* tab,
+                                                     const BatchCta* cmap) {
+  constexpr unsigned FULL = 0xffffffffu;
+  __shared__ double w[2 * SWP_MAXN];
+  const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  SweepArgs<TF> ab;
+  long q0, q1, qs;
+  pair_range<BATCH>(a0, tab, cmap, 1, 0, ab, q0, q1, qs);
+  const SweepArgs<TF>& a = BATCH ? ab : a0;
+  const Dims d = a.d;
+  const int n = d.n, n2 = 2 * n, nr = d.nr, nrhs = a.nrhs, k = a.k;
+  for (long q = q0; q < q1; q += qs) {
+    const int j = k + (int)(2L * k * q), jp = j - k;
+    const TF* Tj = a.Tm + (size_t)j * szT(d);
+    const unsigned char* Pj = a.P + (size_t)j * szP(d);
+    const TF* Cj = a.C + (size_t)j * nr * n;
+    for (int col = 0; col < nrhs; ++col) {
+      double* xc = a.x + (size_t)col * a.ldx;
+      __syncthreads();  // w of the previous column / pair is no longer read
+      for (int pos = tid; pos < n2; pos += bs) {
+        const int r = Pj[pos];  // original row at this position
+        w[pos] = r < n ? xc[(size_t)jp * n + r] : xc[(size_t)j * n + (r - n)];
+      }
+      __syncthreads();
+      // unit lower L on positions [0, n), then the rows below: w -= T(:, c) w[c]
+      for (int cb = 0; cb < n; cb += 32) {
+        const int cw = n - cb < 32 ? n - cb : 32;
+        if (warp == 0) {
+          double v = lane < cw ? w[cb + lane] : 0.0;
+          for (int c = 0; c < cw; ++c) {
+            const double vc = __shfl_sync(FULL, v, c);
+            if (lane > c && lane < cw) v = fma(-double(Tj[(size_t)(cb + c) * n2 + cb + lane]), vc, v);
+          }
+          if (lane < cw) w[cb + lane] = v;
+        }
+        __syncthreads();
+        for (int r = cb + cw + tid; r < n2; r += bs) {
+          double s = w[r];
+          for (int c = 0; c < cw; ++c) s = fma(-double(Tj[(size_t)(cb + c) * n2 + r]), w[cb + c], s);
+          w[r] = s;
+        }
+        __syncthreads();
+      }
+      for (int pos = tid; pos < n2; pos += bs) {
+        if (pos < n) xc[(size_t)j * n + pos] = w[pos];
+        else xc[(size_t)jp * n + pos - n] = w[pos];
+      }
+      // xb contribution of this pair: -C'_j w[0, n)
+      for (int r = warp; r < nr; r += bs >> 5) {
+        double sr = 0.0;
+        for (int c = lane; c < n; c += 32) sr = fma(double(Cj[(size_t)c * nr + r]), w[c], sr);
+        sr = warp_sum(sr);
+        if (lane == 0) a.XB[(size_t)j * nr * nrhs + (size_t)col * nr + r] = -sr;
+      }
+    }
+  }
+}
+
+template <typename TF, bool BATCH = false>
+__global__ void __launch_bounds__(256) k_backward_cta(SweepArgs<TF> a0, const SweepArgs<TF>* tab,
+                                                      const BatchCta* cmap) {
+  constexpr unsigned FULL = 0xffffffffu;
+  __shared__ double xa[SWP_MAXN], xz[SWP_MAXN], y[SWP_MAXN];
+  __shared__ double part[256];
+  const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  SweepArgs<TF> ab;
+  long q0, q1, qs;
+  pair_range<BATCH>(a0, tab, cmap, 1, 0, ab, q0, q1, qs);
+  const SweepArgs<TF>& a = BATCH ? ab : a0;
+  const Dims d = a.d;
+  const int n = d.n, n2 = 2 * n, nx = d.nx, nb = d.nblock, nrhs = a.nrhs, k = a.k;
+  const bool qrp = a.sel == SEL_QRP;
+  const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
+  const size_t nn = (size_t)n * n;
+  const int G = bs / n;  // threads per row in the product (n <= 128: G >= 2)
+  for (long q = q0; q < q1; q += qs) {
+    const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
+    const TF* Dj = a.D + (size_t)j * nn;
+    const TF* Ej = a.E + (size_t)j * nn;
+    const TF* Bj = a.B + (size_t)j * n * nx;
+    const TF* Tj = a.Tm + (size_t)j * szT(d);
+    for (int col = 0; col < nrhs; ++col) {
+      double* xc = a.x + (size_t)col * a.ldx;
+      __syncthreads();
+      for (int i = tid; i < n; i += bs) {
+        xa[i] = xc[(size_t)jp * n + i];
+        xz[i] = xc[(size_t)jpp * n + i];
+      }
+      __syncthreads();
+      // y = x_j - D'_j x_jp - E'_j x_jpp - B'_j xb, G threads per row, fixed order
+      {
+        const int i = tid % n, g = tid / n;
+        double s = 0.0;
+        if (g < G) {
+          for (int c = g; c < n; c += G) {
+            s = fma(double(Dj[(size_t)c * n + i]), xa[c], s);
+            s = fma(double(Ej[(size_t)c * n + i]), xz[c], s);
+          }
+          for (int c = g; c < nx; c += G) s = fma(double(Bj[(size_t)c * n + i]), xc[xb_off + c], s);
+        }
+        part[tid] = s;
+        __syncthreads();
+        for (int i2 = tid; i2 < n; i2 += bs) {
+          double t = 0.0;
+          for (int g2 = 0; g2 < G; ++g2) t += part[g2 * n + i2];
+          y[i2] = xc[(size_t)j * n + i2] - t;
+        }
+        __syncthreads();
+      }
+      // U y = rhs, from the last block of 32 rows up
+      for (int rb = ((n - 1) / 32) * 32; rb >= 0; rb -= 32) {
+        const int rw = n - rb < 32 ? n - rb : 32;
+        if (warp == 0) {
+          double v = lane < rw ? y[rb + lane] : 0.0;
+          const double rdi = lane < rw ? 1.0 / double(Tj[(size_t)(rb + lane) * n2 + rb + lane]) : 0.0;
+          for (int ii = rw - 1; ii >= 0; --ii) {
+            const double xi = __shfl_sync(FULL, v * rdi, ii);
+            if (lane == ii) v = xi;
+            else if (lane < ii) v = fma(-double(Tj[(size_t)(rb + ii) * n2 + rb + lane]), xi, v);
+          }
+          if (lane < rw) y[rb + lane] = v;
+        }
+        __syncthreads();
+        for (int r = tid; r < rb; r += bs) {
+          double s = y[r];
+          for (int c = 0; c < rw; ++c) s = fma(-double(Tj[(size_t)(rb + c) * n2 + r]), y[rb + c], s);
+          y[r] = s;
+        }
+        __syncthreads();
+      }
+      for (int i = tid; i < n; i += bs) {
+        const int dst = qrp ? (int)a.P[(size_t)j * szP(d) + n2 + i] : i;
+        xc[(size_t)j * n + dst] = y[i];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // last block (load_and_factorize_last, cc:1281-1374; solve_last, cc:1385-1479)
 // one CTA; the Nr x Nc matrix lives in global memory (L2 resident)
 // ---------------------------------------------------------------------------
@@ -3059,6 +3206,8 @@ template <typename T>
 struct SweepPlan {
   void (*fwd)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*) = nullptr;
   void (*bwd)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*) = nullptr;
+  void (*fwd_cta)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*) = nullptr;  // CTA per pair (large n)
+  void (*bwd_cta)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*) = nullptr;
 };
 
 template <typename T>
@@ -3080,6 +3229,9 @@ static SweepPlan<T> plan_sweeps(const DevState& s) {
   if (n == 32) {
     if (s.sel == SEL_LU && d.nr <= 8) p.fwd = d.nr <= 4 ? k_forward_rows32<T, 4> : k_forward_rows32<T, 8>;
     if (d.nx <= 8) p.bwd = d.nx <= 4 ? k_backward_rows32<T, 4> : k_backward_rows32<T, 8>;
+  } else if (n > 16 && n <= SWP_MAXN) {
+    if (s.sel == SEL_LU) p.fwd_cta = k_forward_cta<T>;
+    p.bwd_cta = k_backward_cta<T>;
   }
   return p;
 }
@@ -3119,7 +3271,8 @@ static void forward_levels(DevState& s, const SweepPlan<T>& p, const WorkSet<T>&
   for (int K = 1; K < d.nblock; K *= 2) {
     a.k = K;
     const long np = pairs_at_level(d.nblock, K);
-    if (p.fwd) p.fwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a, nullptr, nullptr);
+    if (p.fwd_cta) p.fwd_cta<<<grid_for(np, 1, 148 * 8), 256, 0, st>>>(a, nullptr, nullptr);
+    else if (p.fwd) p.fwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a, nullptr, nullptr);
     else k_forward_level<T><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_f, st>>>(a, nullptr, nullptr);
     check_launch("k_forward_level");
   }
@@ -3139,7 +3292,8 @@ static void last_and_backward(DevState& s, const SweepPlan<T>& p, const WorkSet<
   for (int k = top_level(d.nblock); (k /= 2) > 0;) {
     a.k = k;
     const long np = pairs_at_level(d.nblock, k);
-    if (p.bwd) p.bwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a, nullptr, nullptr);
+    if (p.bwd_cta) p.bwd_cta<<<grid_for(np, 1, 148 * 8), 256, 0, st>>>(a, nullptr, nullptr);
+    else if (p.bwd) p.bwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a, nullptr, nullptr);
     else k_backward_level<T><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_b, st>>>(a, nullptr, nullptr);
     check_launch("k_backward_level");
   }
