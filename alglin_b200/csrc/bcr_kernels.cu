@@ -1292,10 +1292,12 @@ __global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
 constexpr int BLK_W = 32;
 constexpr int BLK_ROWS_MAX = 512;  // 2n + nr of the blocked kernel
 
-// W[c*R + r] -= sum_m L[m*LD + r] * W[c*R + k0 + m] for r in [r0, R), c in [c0, NC), m < w
-// L: the factored block in shared memory (column m, row r), U: rows [k0, k0+w) of W
+// W[c*R + rowp[r]] -= sum_m L[m*LD + r] * W[c*R + rowp[k0 + m]] for positions r in
+// [r0, R), c in [c0, NC), m < w; L: the factored block in shared memory (column m,
+// position r); rowp: position -> row of W
 template <typename T>
-__device__ void blk_update(T* W, int R, int NC, const T* Lsm, int LD, int k0, int w, int r0, int c0) {
+__device__ void blk_update(T* W, int R, int NC, const T* Lsm, int LD, int k0, int w, int r0, int c0,
+                           const int* rowp) {
   const int tid = threadIdx.x, bs = blockDim.x;
   const int rows = R - r0, cols = NC - c0;
   if (rows <= 0 || cols <= 0) return;
@@ -1315,7 +1317,7 @@ __device__ void blk_update(T* W, int R, int NC, const T* Lsm, int LD, int k0, in
 #pragma unroll
         for (int v = 0; v < 2; ++v) {
           const int c = cb + v * 8 + g;
-          bf[ks][v] = (m < w && c < NC) ? W[(size_t)c * R + k0 + m] : 0.0;
+          bf[ks][v] = (m < w && c < NC) ? W[(size_t)c * R + rowp[k0 + m]] : 0.0;
         }
       }
 #pragma unroll
@@ -1325,7 +1327,7 @@ __device__ void blk_update(T* W, int R, int NC, const T* Lsm, int LD, int k0, in
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const int r = rb + u * 8 + g, c = cb + v * 8 + 2 * q + h;
-            cv[u][v][h] = (r < R && c < NC) ? W[(size_t)c * R + r] : 0.0;
+            cv[u][v][h] = (r < R && c < NC) ? W[(size_t)c * R + rowp[r]] : 0.0;
           }
       double acc[2][2][2] = {};
 #pragma unroll
@@ -1349,7 +1351,7 @@ __device__ void blk_update(T* W, int R, int NC, const T* Lsm, int LD, int k0, in
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const int r = rb + u * 8 + g, c = cb + v * 8 + 2 * q + h;
-            if (r < R && c < NC) W[(size_t)c * R + r] = cv[u][v][h] - acc[u][v][h];
+            if (r < R && c < NC) W[(size_t)c * R + rowp[r]] = cv[u][v][h] - acc[u][v][h];
           }
     }
   } else {
@@ -1364,7 +1366,7 @@ __device__ void blk_update(T* W, int R, int NC, const T* Lsm, int LD, int k0, in
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           av[u] = rb + u < R ? Lsm[(size_t)m * LD + rb + u] : T(0);
-          bv[u] = cb + u < NC ? W[(size_t)(cb + u) * R + k0 + m] : T(0);
+          bv[u] = cb + u < NC ? W[(size_t)(cb + u) * R + rowp[k0 + m]] : T(0);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u)
@@ -1375,7 +1377,7 @@ __device__ void blk_update(T* W, int R, int NC, const T* Lsm, int LD, int k0, in
       for (int u = 0; u < 4; ++u)
 #pragma unroll
         for (int v = 0; v < 4; ++v)
-          if (rb + u < R && cb + v < NC) W[(size_t)(cb + v) * R + rb + u] -= acc[u][v];
+          if (rb + u < R && cb + v < NC) W[(size_t)(cb + v) * R + rowp[rb + u]] -= acc[u][v];
     }
   }
 }
@@ -1386,15 +1388,13 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
   __shared__ T sv[32];
   __shared__ int si[32];
   __shared__ int s_piv[256];
-  __shared__ int s_src[2 * BLK_W], s_dst[2 * BLK_W], s_cnt;
-  __shared__ int s_perm[BLK_ROWS_MAX];
+  __shared__ int s_perm[BLK_ROWS_MAX];  // position -> row of the slab (rows never move)
   const int tid = threadIdx.x, bs = blockDim.x;
   const Dims d = a.d;
   const int n = d.n, nr = d.nr, nx = d.nx, nb = d.nblock;
   const int n2 = 2 * n, R = n2 + nr, NC = 3 * n + nx;
   const size_t nn = (size_t)n * n, nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
   T* Pb = reinterpret_cast<T*>(smem_raw);  // [BLK_W][R] the current panel block, column-major
-  T* Sg = Pb + (size_t)BLK_W * R;           // [2*BLK_W][BLK_W] staging of interchanged rows
   T* W = slab + (size_t)blockIdx.x * slab_elems;
   const int k = a.k;
   const long np = pairs_at_level(nb, k);
@@ -1445,15 +1445,18 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
       const int r = idx % nr, c = idx / nr;
       W[(size_t)(3 * n + c) * R + n2 + r] = T(0);
     }
+    for (int r = tid; r < R; r += bs) s_perm[r] = r;
     __syncthreads();
     // ------------------------------------------------- blocked elimination
+    // the interchanges are kept as the position -> row map s_perm; a block is
+    // staged by position, so no row of the slab is ever moved
     int info = 0;
     for (int kb = 0; kb < n && info == 0; kb += BLK_W) {
       const int w = n - kb < BLK_W ? n - kb : BLK_W;
       // stage the block's columns (all rows) in shared memory
       for (int e = tid; e < w * R; e += bs) {
         const int r = e % R, c = e / R;
-        Pb[(size_t)c * R + r] = W[(size_t)(kb + c) * R + r];
+        Pb[(size_t)c * R + r] = W[(size_t)(kb + c) * R + s_perm[r]];
       }
       __syncthreads();
       for (int i = 0; i < w; ++i) {
@@ -1474,6 +1477,7 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
           T* col = Pb + (size_t)tid * R;
           const T t = col[gi]; col[gi] = col[bi]; col[bi] = t;
         }
+        if (bi != gi && tid == w) { const int t = s_perm[gi]; s_perm[gi] = s_perm[bi]; s_perm[bi] = t; }
         __syncthreads();
         // one thread per row below the pivot: its multiplier, then its update
         const T rinv = T(1) / pv;
@@ -1485,54 +1489,18 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
         __syncthreads();
       }
       if (info != 0) break;
-      // the factored block back to the slab, its interchanges on every other column
+      // the factored block back to the slab (by position)
       for (int e = tid; e < w * R; e += bs) {
         const int r = e % R, c = e / R;
-        W[(size_t)(kb + c) * R + r] = Pb[(size_t)c * R + r];
-      }
-      // the block's interchanges as one row permutation of the touched rows,
-      // applied to every other column through a staging buffer
-      for (int r = kb + tid; r < n2; r += bs) s_perm[r] = r;
-      __syncthreads();
-      if (tid == 0) {
-        for (int i = 0; i < w; ++i) {
-          const int p = s_piv[kb + i];
-          const int t = s_perm[kb + i]; s_perm[kb + i] = s_perm[p]; s_perm[p] = t;
-        }
-        int cnt = 0;
-        for (int r = kb; r < n2; ++r)
-          if (s_perm[r] != r) { s_dst[cnt] = r; s_src[cnt] = s_perm[r]; ++cnt; }
-        s_cnt = cnt;
+        W[(size_t)(kb + c) * R + s_perm[r]] = Pb[(size_t)c * R + r];
       }
       __syncthreads();
-      const int cnt = s_cnt;
-      if (cnt > 0) {
-        constexpr int CW = BLK_W;  // columns per stage
-        const int other = NC - w;
-        for (int c0 = 0; c0 < other; c0 += CW) {
-          const int cw = other - c0 < CW ? other - c0 : CW;
-          // consecutive threads take consecutive rows of one column (the rows
-          // [kb, kb+w) come first in the list, so most accesses coalesce)
-          for (int e = tid; e < cnt * cw; e += bs) {
-            const int t = e % cnt, cc = e / cnt;
-            const int col = c0 + cc < kb ? c0 + cc : c0 + cc + w;
-            Sg[cc * (2 * BLK_W) + t] = W[(size_t)col * R + s_src[t]];
-          }
-          __syncthreads();
-          for (int e = tid; e < cnt * cw; e += bs) {
-            const int t = e % cnt, cc = e / cnt;
-            const int col = c0 + cc < kb ? c0 + cc : c0 + cc + w;
-            W[(size_t)col * R + s_dst[t]] = Sg[cc * (2 * BLK_W) + t];
-          }
-          __syncthreads();
-        }
-      }
       // rows [kb, kb+w) of the columns right of the block: unit lower solve
       for (int c = kb + w + tid; c < NC; c += bs) {
-        T* col = W + (size_t)c * R + kb;
+        T* col = W + (size_t)c * R;
         T y[BLK_W];
 #pragma unroll
-        for (int r = 0; r < BLK_W; ++r) y[r] = r < w ? col[r] : T(0);
+        for (int r = 0; r < BLK_W; ++r) y[r] = r < w ? col[s_perm[kb + r]] : T(0);
 #pragma unroll
         for (int m = 0; m < BLK_W; ++m) {
 #pragma unroll
@@ -1541,11 +1509,11 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
         }
 #pragma unroll
         for (int r = 0; r < BLK_W; ++r)
-          if (r < w) col[r] = y[r];
+          if (r < w) col[s_perm[kb + r]] = y[r];
       }
       __syncthreads();
       // rows below the block: one product of depth w
-      blk_update<T>(W, R, NC, Pb, R, kb, w, kb + w, kb + w);
+      blk_update<T>(W, R, NC, Pb, R, kb, w, kb + w, kb + w, s_perm);
       __syncthreads();
     }
     if (info != 0) {
@@ -1560,7 +1528,7 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
 #pragma unroll
       for (int u = 0; u < UL; ++u) {
         const int idx = base + tid + u * bs;
-        v[u] = idx < (int)(2 * nn) ? W[(size_t)(idx / n2) * R + idx % n2] : T(0);
+        v[u] = idx < (int)(2 * nn) ? W[(size_t)(idx / n2) * R + s_perm[idx % n2]] : T(0);
       }
 #pragma unroll
       for (int u = 0; u < UL; ++u) {
@@ -1569,14 +1537,9 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
       }
     }
     unsigned char* Pj = a.P + (size_t)j * szP(d);
-    if (tid == 0) {
-      // row map (getrf order) from the interchange sequence
-      unsigned char mp[512];
-      for (int r = 0; r < n2; ++r) mp[r] = (unsigned char)r;
-      for (int i = 0; i < n; ++i) { const unsigned char t = mp[i]; mp[i] = mp[s_piv[i]]; mp[s_piv[i]] = t; }
-      for (int r = 0; r < n2; ++r) Pj[r] = mp[r];
-      for (int i = 0; i < n; ++i) Pj[n2 + i] = (unsigned char)i;
-    }
+    // row map (getrf order): the original row at each position
+    for (int r = tid; r < n2; r += bs) Pj[r] = (unsigned char)s_perm[r];
+    for (int i = tid; i < n; i += bs) Pj[n2 + i] = (unsigned char)i;
     for (int base = 0; base < (int)nn; base += bs * UL) {
       T v0[UL], v1[UL], v2[UL], v3[UL];
 #pragma unroll
@@ -1584,10 +1547,11 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
         const int idx = base + tid + u * bs;
         const int i = idx % n, c = idx / n;
         const bool in = idx < (int)nn;
-        v0[u] = in ? W[(size_t)(n + c) * R + i] : T(0);
-        v1[u] = in ? W[(size_t)(n2 + c) * R + i] : T(0);
-        v2[u] = in ? W[(size_t)(n + c) * R + n + i] : T(0);
-        v3[u] = in ? W[(size_t)(n2 + c) * R + n + i] : T(0);
+        const int pu = in ? s_perm[i] : 0, pr = in ? s_perm[n + i] : 0;
+        v0[u] = in ? W[(size_t)(n + c) * R + pu] : T(0);
+        v1[u] = in ? W[(size_t)(n2 + c) * R + pu] : T(0);
+        v2[u] = in ? W[(size_t)(n + c) * R + pr] : T(0);
+        v3[u] = in ? W[(size_t)(n2 + c) * R + pr] : T(0);
       }
 #pragma unroll
       for (int u = 0; u < UL; ++u) {
@@ -1602,8 +1566,8 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
     }
     for (int idx = tid; idx < (int)nnx; idx += bs) {
       const int i = idx % n, c = idx / n;
-      a.B[(size_t)j * nnx + idx] = W[(size_t)(3 * n + c) * R + i];
-      a.B[(size_t)jp * nnx + idx] = W[(size_t)(3 * n + c) * R + n + i];
+      a.B[(size_t)j * nnx + idx] = W[(size_t)(3 * n + c) * R + s_perm[i]];
+      a.B[(size_t)jp * nnx + idx] = W[(size_t)(3 * n + c) * R + s_perm[n + i]];
     }
     for (int idx = tid; idx < (int)nrn; idx += bs) {
       const int r = idx % nr, c = idx / nr;
@@ -3105,7 +3069,7 @@ static FactorPlan<T> plan_factor(const DevState& s) {
       (s.pair_kernel != PAIR_SMEM || !smem_fits)) {
     p.cta = s.sel == SEL_LU ? k_factor_cta<T, SEL_LU>
           : s.sel == SEL_QR ? k_factor_cta<T, SEL_QR> : k_factor_cta<T, SEL_QRP>;
-    const size_t bsm = ((size_t)BLK_W * (2 * n + d.nr) + 2 * BLK_W * BLK_W) * sizeof(T);
+    const size_t bsm = (size_t)BLK_W * (2 * n + d.nr) * sizeof(T);
     if (s.sel == SEL_LU && n <= 128 && 2 * n + d.nr <= BLK_ROWS_MAX && bsm <= SMEM_MAX) {
       p.blk = k_factor_lu_blocked<T>;
       p.blk_smem = bsm;
