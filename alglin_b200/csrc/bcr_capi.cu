@@ -346,6 +346,9 @@ struct bcr_handle_s {
     }
     if (st.code == bcr::DEV_LAST_SINGULAR || st.code == bcr::DEV_BAD_SHAPE)
       return fail(BCR_NUMERICAL, "BorderedCR<t_Value>::load_and_factorize_last failed\n");
+    if (st.code == bcr::DEV_TIMEOUT)
+      return fail(BCR_DEVICE_TIMEOUT, fmt("BorderedCR: tensor-core pipeline wait expired at block %d, level %d\n",
+                                      st.block, st.level));
     factorized = true;
     return BCR_OK;
   }
@@ -1202,7 +1205,7 @@ int bcr_graph_launch(bcr_handle h, int what) {
 
 int bcr_set_pair_kernel(bcr_handle h, int choice) {
   H_CHECK(h);
-  if (choice < BCR_PAIR_AUTO || choice > BCR_PAIR_SMEM)
+  if (choice < BCR_PAIR_AUTO || choice > BCR_PAIR_UMMA)
     return h->fail(BCR_BAD_ARGUMENT, fmt("bcr_set_pair_kernel: unknown choice %d\n", choice));
   h->s.pair_kernel = choice;
   h->drop_graphs();

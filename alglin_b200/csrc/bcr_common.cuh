@@ -23,7 +23,8 @@ enum LastKind : int { LAST_LU = 0, LAST_LUPQ = 1, LAST_QR = 2, LAST_QRP = 3,
                       LAST_SVD = 4, LAST_LSS = 5, LAST_LSY = 6, LAST_PINV = 7 };
 
 // pair-kernel choice of the factorization (PAIR_AUTO picks by shape)
-enum PairKernel : int { PAIR_AUTO = 0, PAIR_TC = 1, PAIR_GRP = 2, PAIR_ROWS = 3, PAIR_CTA = 4, PAIR_SMEM = 5 };
+enum PairKernel : int { PAIR_AUTO = 0, PAIR_TC = 1, PAIR_GRP = 2, PAIR_ROWS = 3, PAIR_CTA = 4, PAIR_SMEM = 5,
+                        PAIR_UMMA = 6 };
 
 // error codes written by kernels into the device status word
 enum DevStatus : int {
@@ -31,6 +32,7 @@ enum DevStatus : int {
   DEV_ZERO_PIVOT = 1,      // panel LU hit an exactly-zero pivot
   DEV_LAST_SINGULAR = 2,   // last block factorization failed
   DEV_BAD_SHAPE = 3,       // last block shape unsupported by the selected solver
+  DEV_TIMEOUT = 4,         // a bounded wait on the tensor-core pipeline expired
 };
 
 struct Dims {

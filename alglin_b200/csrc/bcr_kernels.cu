@@ -1585,6 +1585,8 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
   }
 }
 
+#include "bcr_umma.cuh"
+
 // ---------------------------------------------------------------------------
 // Large blocks: one CTA eliminates one pair; the (2n+nr) x (3n+nx) work
 // matrix lives in a global scratch slab of the CTA (column-major, ld = R),
@@ -3010,6 +3012,8 @@ struct FactorPlan {
   void (*cta)(FactorArgs<T>, T*, size_t) = nullptr;  // CTA per pair (large n)
   void (*blk)(FactorArgs<T>, T*, size_t) = nullptr;  // CTA per pair, blocked LU (large n)
   size_t blk_smem = 0;
+  void (*umma)(FactorArgs<T>, T*, size_t) = nullptr;  // CTA per pair, tcgen05 products (FP32, large n)
+  size_t umma_smem = 0;
   void (*tc)(FactorArgs<T>, const FactorArgs<T>*, const BatchCta*) = nullptr;               // tensor-core LU (FP64, n = 8, 16)
   size_t tc_smem = 0;
   void (*grp)(FactorArgs<T>, const FactorArgs<T>*, const BatchCta*) = nullptr;              // CTA of 2n threads per pair (n = 16, 32)
@@ -3075,6 +3079,13 @@ static FactorPlan<T> plan_factor(const DevState& s) {
       p.blk_smem = bsm;
       smem_limit_once(p.blk, bsm);
     }
+    if constexpr (sizeof(T) == 4) {
+      if (s.sel == SEL_LU && umma_fits(d) && (s.pair_kernel == PAIR_AUTO || s.pair_kernel == PAIR_UMMA)) {
+        p.umma = k_factor_lu_umma;
+        p.umma_smem = umma_layout(d).bytes;
+        smem_limit_once(p.umma, p.umma_smem);
+      }
+    }
   }
   return p;
 }
@@ -3114,7 +3125,8 @@ static void factor_levels(DevState& s, const FactorPlan<T>& p, const WorkSet<T>&
     a.k = k;
     a.first = (k == 1);
     const long np = pairs_at_level(nb, k);
-    if (p.blk) p.blk<<<grid_for(np, 1, s.slab_ctas), 256, p.blk_smem, st>>>(a, w.slab, s.slab_elems);
+    if (p.umma) p.umma<<<grid_for(np, 1, 148), UM_NT, p.umma_smem, st>>>(a, w.slab, s.slab_elems);
+    else if (p.blk) p.blk<<<grid_for(np, 1, s.slab_ctas), 256, p.blk_smem, st>>>(a, w.slab, s.slab_elems);
     else if (p.cta) p.cta<<<grid_for(np, 1, s.slab_ctas), 256, 0, st>>>(a, w.slab, s.slab_elems);
     else if (p.grp) p.grp<<<grid_for(np, 1, p.grp_ctas), p.grp_threads, p.grp_smem, st>>>(a, nullptr, nullptr);
     else if (p.tc) p.tc<<<grid_for(np, 4, 148 * 16), 128, p.tc_smem, st>>>(a, nullptr, nullptr);

@@ -1,0 +1,596 @@
+// ---------------------------------------------------------------------------
+// Large blocks, FP32 working precision, LU: one CTA per pair with the trailing
+// products on the 5th-generation tensor cores (tcgen05.mma, kind::tf32, FP32
+// accumulators in tensor memory) as 3xTF32 split products.
+//
+// The pair is eliminated in three steps (the same algebra as buildT/applyT,
+// BABD_BorderedCR.cc:845-982, with the border rows of factorize_block,
+// cc:1107-1154):
+//
+//   1. panel LU: the (2n + nr) x n panel [E_jp; D_j; C_j] is factored in
+//      shared memory with the getrf pivot rule (largest |a| among the 2n
+//      candidate rows, first position on ties), in column blocks of 32.
+//      Every thread owns one row of the block in registers; one block barrier
+//      per pivot step (the warps post their candidate rows, every thread
+//      picks the winner); the block's U rows are solved with its unit lower
+//      triangle and the rows below get one product of depth 32.  Row
+//      interchanges are a position map, no row moves.
+//   2. Z = L11^-1 (the inverse of the unit lower triangle of the n pivot rows),
+//      by 32 x 32 diagonal inverses and block forward substitution.
+//   3. with Xt the n pivot rows and Xb the other n rows of the trailing
+//      columns X = [D_jp 0 B_jp; 0 E_j B_j] (2n + nx columns):
+//        U12 = Z Xt                 (tensor cores: the U-row D'_j E'_j B'_j)
+//        Xb' = Xb - L21 U12         (tensor cores: the reduced row)
+//        border = -Lc U12           (CUDA cores: dC_jp, dC_jpp, dF)
+//      Operands are split as a = hi + lo with hi the TF32 part of a and lo
+//      the FP32 remainder; each product is hi*hi + lo*hi + hi*lo accumulated
+//      in FP32 (the products' error is about that of FP32 arithmetic).
+//
+// Shared memory operands use the K-major layout without swizzle: 8-row x
+// 16-byte core matrices, 8-row groups 128 bytes apart (SBO), 4-element K
+// groups LBO bytes apart.  The K loop of each product is staged 16 deep in two
+// buffers; tcgen05.commit arrives on the buffer's mbarrier when the MMAs that
+// read it are done.  Every wait on an mbarrier is bounded (about a second):
+// on expiry the kernel reports DEV_TIMEOUT, frees its tensor memory and ends.
+// ---------------------------------------------------------------------------
+constexpr int UM_NT = 384;              // threads per CTA
+constexpr int UM_NW = UM_NT / 32;
+constexpr int UM_NMAX = 128, UM_NRMAX = 16, UM_NXMAX = 16;
+constexpr int UM_TMEM_COLS = 512;
+
+struct UmmaLayout {
+  int R, NP, LDP, Kpad, Nc, Npad, N0, N1, LBO_B;
+  unsigned szAhalf, offB, szBhalf, offZ, offLc, offSlot, bytes;
+};
+
+__host__ __device__ inline UmmaLayout umma_layout(const Dims& d) {
+  UmmaLayout L;
+  const int n = d.n;
+  L.R = 2 * n + d.nr;
+  L.NP = (n + 31) / 32 * 32;
+  L.LDP = L.NP + 4;  // rows 16-byte aligned, 8 consecutive rows on distinct banks
+  L.Kpad = (n + 15) / 16 * 16;
+  L.Nc = 2 * n + d.nx;
+  L.Npad = (L.Nc + 15) / 16 * 16;
+  if (L.Npad <= 256) { L.N0 = L.Npad; L.N1 = 0; }
+  else { L.N0 = (L.Npad / 2 + 15) / 16 * 16; L.N1 = L.Npad - L.N0; }
+  int lbo = L.Npad * 16;
+  while ((lbo / 4) % 32 != 8) lbo += 16;  // the 4 K groups of a stage on distinct banks
+  L.LBO_B = lbo;
+  L.szAhalf = (unsigned)(L.Kpad / 4) * 2048u;      // 128 rows x Kpad, one of hi / lo
+  L.offB = 2 * L.szAhalf;
+  L.szBhalf = 4u * (unsigned)lbo;                  // Npad rows x 16, one of hi / lo
+  const unsigned endB = L.offB + 4 * L.szBhalf;    // two stages of (hi, lo)
+  // Z is read while the A operand is written, and Lc is read between the two
+  // products: neither may overlap the operand regions
+  L.offZ = ((unsigned)(L.R * L.LDP * 4) + 15u) & ~15u;
+  if (L.offZ < L.offB) L.offZ = L.offB;
+  L.offLc = L.offZ + (unsigned)(L.NP * L.LDP * 4);
+  if (L.offLc < endB) L.offLc = endB;
+  L.offSlot = (L.offLc + (unsigned)(d.nr * n * 4) + 15u) & ~15u;
+  const unsigned endS = L.offSlot + 2u * UM_NW * 36u * 4u;
+  L.bytes = endB > endS ? endB : endS;
+  return L;
+}
+
+// ---- sm_100a primitives ----------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// completion of the phase with the given parity; false after about a second
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > (2LL << 30)) return false;
+  return true;
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// smem matrix descriptor, K-major, no swizzle
+__device__ __forceinline__ uint64_t umma_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+         (1ull << 46);
+}
+// instruction descriptor: D f32, A and B tf32, both K-major, M x N
+__host__ __device__ constexpr uint32_t umma_idesc_tf32(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+__device__ __forceinline__ void umma_tf32(uint32_t dt, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(dt),
+      "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+// 16 consecutive FP32 columns of this thread's tensor-memory lane
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ float tf32_hi(float v) { return __uint_as_float(__float_as_uint(v) & 0xFFFFE000u); }
+
+// A operand element (row i of 128, K index k): byte offset in one of hi / lo
+__device__ __forceinline__ uint32_t umma_a_off(int i, int k) {
+  return (uint32_t)((k >> 2) * 2048 + (i >> 3) * 128 + (i & 7) * 16 + (k & 3) * 4);
+}
+// B stage element (N index c, K index m within the 16-deep stage)
+__device__ __forceinline__ uint32_t umma_b_off(int c, int m, int lbo) {
+  return (uint32_t)((m >> 2) * lbo + (c >> 3) * 128 + (c & 7) * 16 + (m & 3) * 4);
+}
+
+// One product D[128 x Npad] = A[128 x Kpad] * B[Kpad x Npad] with the B operand
+// staged 16 K-rows at a time by all threads from src(c, m) (m the K index).
+// A (hi, lo) must be in shared memory and fenced.  Returns false on a timeout.
+template <typename Src>
+__device__ bool umma_product(const UmmaLayout& L, unsigned char* sm, uint64_t* bars, uint32_t (&par)[2],
+                             uint32_t tmem, Src src) {
+  const int tid = threadIdx.x;
+  const int S = L.Kpad / 16;
+  const uint32_t sA = smem_u32(sm);
+  const int cnt = 16 * L.Npad;
+  bool ok = true;
+  for (int s = 0; s < S; ++s) {
+    const int b = s & 1;
+    if (s >= 2) {  // the MMAs of stage s-2 read this buffer
+      ok = mbar_wait_bounded(&bars[b], par[b]);
+      par[b] ^= 1u;
+    }
+    if (ok) {
+      unsigned char* bh = sm + L.offB + (unsigned)b * 2u * L.szBhalf;
+      unsigned char* bl = bh + L.szBhalf;
+      for (int e = tid; e < cnt; e += UM_NT) {
+        const int m = e & 15, c = e >> 4;
+        const float v = src(c, 16 * s + m);
+        const float h = tf32_hi(v);
+        const uint32_t o = umma_b_off(c, m, L.LBO_B);
+        *reinterpret_cast<float*>(bh + o) = h;
+        *reinterpret_cast<float*>(bl + o) = v - h;
+      }
+    }
+    fence_async_smem();
+    if (__syncthreads_or(!ok)) return false;
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t sB = smem_u32(sm + L.offB + (unsigned)b * 2u * L.szBhalf);
+#pragma unroll
+      for (int ks = 0; ks < 2; ++ks) {
+        const int kg = 16 * s + 8 * ks;
+        const uint32_t ao = (uint32_t)(kg >> 2) * 2048u;
+        const uint64_t ah = umma_sdesc(sA + ao, 2048, 128);
+        const uint64_t al = umma_sdesc(sA + L.szAhalf + ao, 2048, 128);
+        const uint32_t bo = (uint32_t)(2 * ks) * (uint32_t)L.LBO_B;
+        for (int ch = 0; ch < 2; ++ch) {
+          const int nw = ch ? L.N1 : L.N0;
+          if (nw == 0) continue;
+          const int c0 = ch ? L.N0 : 0;
+          const uint32_t co = (uint32_t)(c0 >> 3) * 128u;
+          const uint64_t bdh = umma_sdesc(sB + bo + co, (uint32_t)L.LBO_B, 128);
+          const uint64_t bdl = umma_sdesc(sB + L.szBhalf + bo + co, (uint32_t)L.LBO_B, 128);
+          const uint32_t id = umma_idesc_tf32(128, nw);
+          const uint32_t dt = tmem + (uint32_t)c0;
+          umma_tf32(dt, ah, bdh, id, (s > 0 || ks > 0) ? 1u : 0u);
+          umma_tf32(dt, al, bdh, id, 1u);
+          umma_tf32(dt, ah, bdl, id, 1u);
+        }
+      }
+      umma_commit(&bars[b]);
+    }
+  }
+  // the last (up to) two commits: every commit is waited exactly once
+  for (int s = S - 2 < 0 ? 0 : S - 2; s < S; ++s) {
+    const int b = s & 1;
+    if (ok) ok = mbar_wait_bounded(&bars[b], par[b]);
+    par[b] ^= 1u;
+  }
+  tc_fence_after();
+  return !__syncthreads_or(!ok);
+}
+
+// A operand (hi, lo) from a(i, k), i < 128, k < Kpad
+template <typename Src>
+__device__ void umma_stage_a(const UmmaLayout& L, unsigned char* sm, Src a) {
+  const int cnt = 128 * L.Kpad;
+  for (int e = threadIdx.x; e < cnt; e += UM_NT) {
+    const int kl = e & 3, i = (e >> 2) & 127, kg = e >> 9;
+    const int k = 4 * kg + kl;
+    const float v = a(i, k);
+    const float h = tf32_hi(v);
+    const uint32_t o = umma_a_off(i, k);
+    *reinterpret_cast<float*>(sm + o) = h;
+    *reinterpret_cast<float*>(sm + L.szAhalf + o) = v - h;
+  }
+  fence_async_smem();
+}
+
+__global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a, float* slab, size_t slab_elems) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_perm[2 * UM_NMAX + UM_NRMAX];  // position -> row
+  __shared__ int s_pos[2 * UM_NMAX];              // row -> position
+  __shared__ int s_pivrow[UM_NMAX];               // pivot step -> row
+  __shared__ __align__(8) uint64_t s_bar[2];
+  __shared__ uint32_t s_taddr;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const Dims d = a.d;
+  const int n = d.n, nr = d.nr, nb = d.nblock, n2 = 2 * n;
+  const UmmaLayout L = umma_layout(d);
+  const int R = L.R, LDP = L.LDP, NP = L.NP, Nc = L.Nc;
+  const int nwr = (R + 31) / 32;  // warps that own panel rows
+  const size_t nn = (size_t)n * n, nnx = (size_t)n * d.nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * d.nx;
+  float* P = reinterpret_cast<float*>(smem_raw);
+  float* Zf = reinterpret_cast<float*>(smem_raw + L.offZ);
+  float* Lc = reinterpret_cast<float*>(smem_raw + L.offLc);
+  float* slot = reinterpret_cast<float*>(smem_raw + L.offSlot);
+  float* Xs = slab + (size_t)blockIdx.x * slab_elems;  // [col][position], 2n x Nc
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_taddr)),
+                 "r"(UM_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_taddr;
+  uint32_t par[2] = {0u, 0u};
+
+  const int k = a.k;
+  const long np = pairs_at_level(nb, k);
+  const bool first = a.first != 0;
+  for (long q = blockIdx.x; q < np; q += gridDim.x) {
+    const int j = k + (int)(2L * k * q), jp = j - k;
+    const size_t oj = (size_t)j * nn, ojp = (size_t)jp * nn;
+    // ------------------------------------------------------------ panel load
+    for (int e = tid; e < R * n; e += UM_NT) {
+      const int r = e % R, c = e / R;
+      float v;
+      if (r < n) v = ldg_src(first, a.E0, a.E, ojp + r + (size_t)c * n);
+      else if (r < n2) v = ldsrc(first, a.D0, a.D, oj + (r - n) + (size_t)c * n);  // D'_j is written here later
+      else v = ldsrc(first, a.C0, a.C, (size_t)j * nrn + (r - n2) + (size_t)c * nr);
+      P[r * LDP + c] = v;
+    }
+    __syncthreads();
+    // --------------------------------------------------------------- panel LU
+    int pos = tid, done = 0, info = 0;
+    float rv[32];
+    for (int kb = 0; kb < n && info == 0; kb += 32) {
+      const int w = n - kb < 32 ? n - kb : 32;
+      if (tid < R) {
+        const float4* src = reinterpret_cast<const float4*>(P + tid * LDP + kb);
+#pragma unroll
+        for (int q4 = 0; q4 < 8; ++q4) {
+          const float4 t = src[q4];
+          rv[4 * q4] = t.x; rv[4 * q4 + 1] = t.y; rv[4 * q4 + 2] = t.z; rv[4 * q4 + 3] = t.w;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 32; ++i) {
+        if (i < w) {
+          const int gi = kb + i;
+          const bool cand = tid < n2 && !done;
+          const uint32_t key = (cand && rv[i] == rv[i]) ? __float_as_uint(fabsf(rv[i])) : 0u;
+          const uint32_t cpos = cand ? (uint32_t)pos : 0xFFFFu;
+          const uint32_t kmax = __reduce_max_sync(0xFFFFFFFFu, key);
+          const uint32_t pmin = __reduce_min_sync(0xFFFFFFFFu, key == kmax ? cpos : 0xFFFFu);
+          float* sl = slot + ((gi & 1) * UM_NW + warp) * 36;
+          if (warp < nwr) {
+            if (cand && key == kmax && cpos == pmin) {
+              float4* d4 = reinterpret_cast<float4*>(sl);
+#pragma unroll
+              for (int q4 = 0; q4 < 8; ++q4)
+                d4[q4] = make_float4(rv[4 * q4], rv[4 * q4 + 1], rv[4 * q4 + 2], rv[4 * q4 + 3]);
+              reinterpret_cast<uint32_t*>(sl)[32] = kmax;
+              reinterpret_cast<uint32_t*>(sl)[33] = pmin;
+              reinterpret_cast<int*>(sl)[34] = tid;
+            } else if (lane == 0 && pmin == 0xFFFFu) {
+              reinterpret_cast<uint32_t*>(sl)[32] = 0u;
+              reinterpret_cast<uint32_t*>(sl)[33] = 0xFFFFu;
+              reinterpret_cast<int*>(sl)[34] = -1;
+            }
+          }
+          __syncthreads();
+          uint32_t bk = 0u, bp = 0xFFFFu;
+          int bw = 0;
+          for (int ww = 0; ww < nwr; ++ww) {
+            const uint32_t* s2 = reinterpret_cast<const uint32_t*>(slot + ((gi & 1) * UM_NW + ww) * 36);
+            const uint32_t k2 = s2[32], p2 = s2[33];
+            if (k2 > bk || (k2 == bk && p2 < bp)) { bk = k2; bp = p2; bw = ww; }
+          }
+          const float* win = slot + ((gi & 1) * UM_NW + bw) * 36;
+          const int wt = reinterpret_cast<const int*>(win)[34];
+          const float pv = win[i];
+          if (pv == 0.0f || wt < 0) { info = gi + 1; break; }
+          if (tid == 0) s_pivrow[gi] = wt;
+          if (pos == gi) pos = (int)bp;
+          if (tid == wt) { pos = gi; done = 1; }
+          if (tid < R && !done) {
+            const float l = rv[i] * (1.0f / pv);
+            rv[i] = l;
+#pragma unroll
+            for (int jj = i + 1; jj < 32; ++jj) rv[jj] = fmaf(-l, win[jj], rv[jj]);
+          }
+        }
+      }
+      if (info != 0) break;
+      if (tid < R) {
+        float4* dst = reinterpret_cast<float4*>(P + tid * LDP + kb);
+#pragma unroll
+        for (int q4 = 0; q4 < 8; ++q4)
+          dst[q4] = make_float4(rv[4 * q4], rv[4 * q4 + 1], rv[4 * q4 + 2], rv[4 * q4 + 3]);
+      }
+      __syncthreads();
+      if (kb + 32 < n) {  // w == 32 here
+        int ro[32];
+#pragma unroll
+        for (int m = 0; m < 32; ++m) ro[m] = s_pivrow[kb + m] * LDP;
+        // the block's U rows in the panel columns right of it: unit lower solve
+        for (int c = kb + 32 + tid; c < n; c += UM_NT) {
+          float y[32];
+#pragma unroll
+          for (int r = 0; r < 32; ++r) y[r] = P[ro[r] + c];
+#pragma unroll
+          for (int m = 0; m < 32; ++m)
+#pragma unroll
+            for (int r = m + 1; r < 32; ++r) y[r] = fmaf(-P[ro[r] + kb + m], y[m], y[r]);
+#pragma unroll
+          for (int r = 0; r < 32; ++r) P[ro[r] + c] = y[r];
+        }
+        __syncthreads();
+        // the rows that are not pivots yet: one product of depth 32
+        if (tid < R && !done) {
+          float* row = P + tid * LDP;
+          for (int c = kb + 32; c < n; c += 4) {
+            float4 acc = *reinterpret_cast<float4*>(row + c);
+#pragma unroll
+            for (int m = 0; m < 32; ++m) {
+              const float4 u = *reinterpret_cast<const float4*>(P + ro[m] + c);
+              acc.x = fmaf(-rv[m], u.x, acc.x);
+              acc.y = fmaf(-rv[m], u.y, acc.y);
+              acc.z = fmaf(-rv[m], u.z, acc.z);
+              acc.w = fmaf(-rv[m], u.w, acc.w);
+            }
+            *reinterpret_cast<float4*>(row + c) = acc;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    if (info != 0) {
+      if (tid == 0) report(a.st, DEV_ZERO_PIVOT, j, info, k);
+      __syncthreads();
+      continue;
+    }
+    if (tid < R) s_perm[pos] = tid;
+    if (tid < n2) s_pos[tid] = pos;
+    __syncthreads();
+    // ------------------------------------- factors out; X staged by position
+    float* Tj = a.Tm + (size_t)j * szT(d);
+    for (int e = tid; e < n2 * n; e += UM_NT) {
+      const int p = e % n2, c = e / n2;
+      Tj[e] = P[s_perm[p] * LDP + c];
+    }
+    unsigned char* Pj = a.P + (size_t)j * szP(d);
+    for (int r = tid; r < n2; r += UM_NT) Pj[r] = (unsigned char)s_perm[r];
+    for (int i = tid; i < n; i += UM_NT) Pj[n2 + i] = (unsigned char)i;
+    for (int e = tid; e < nr * n; e += UM_NT) {
+      const int r = e % nr, c = e / nr;
+      const float v = P[(n2 + r) * LDP + c];
+      a.C[(size_t)j * nrn + e] = v;
+      Lc[c * nr + r] = v;
+    }
+    // X = [D_jp 0 B_jp; 0 E_j B_j] by position: Xs[col * 2n + pos]
+    for (int e = tid; e < n2 * Nc; e += UM_NT) {
+      const int r = e % n2, c = e / n2;
+      float v = 0.0f;
+      if (c >= n2) {
+        const size_t o = (size_t)(r < n ? jp : j) * nnx + (r % n) + (size_t)(c - n2) * n;
+        v = ldsrc(first, a.B0, a.B, o);
+      } else if (r < n) {
+        if (c < n) v = ldg_src(first, a.D0, a.D, ojp + r + (size_t)c * n);
+      } else if (c >= n) {
+        v = ldsrc(first, a.E0, a.E, oj + (r - n) + (size_t)(c - n) * n);  // E'_j is written here later
+      }
+      Xs[(size_t)c * n2 + s_pos[r]] = v;
+    }
+    // ---------------------------------------------------- Z = L11^-1 (FP32)
+    for (int e = tid; e < NP * NP; e += UM_NT) {
+      const int r = e / NP, c = e % NP;
+      if ((c >> 5) > (r >> 5)) Zf[r * LDP + c] = 0.0f;
+    }
+    if (warp < NP / 32) {  // diagonal 32 x 32 inverses, one column per lane
+      const int a32 = warp * 32, c = lane;
+      float z[32];
+#pragma unroll
+      for (int r = 0; r < 32; ++r) {
+        const int gr = a32 + r;
+        float v = 0.0f;
+        if (gr < n) {
+          v = (r == c) ? 1.0f : 0.0f;
+          const float* Lr = P + s_perm[gr] * LDP + a32;
+#pragma unroll
+          for (int m = 0; m < r; ++m) v = fmaf(-Lr[m], z[m], v);
+        }
+        z[r] = v;
+      }
+#pragma unroll
+      for (int r = 0; r < 32; ++r) Zf[(a32 + r) * LDP + a32 + c] = z[r];
+    }
+    __syncthreads();
+    for (int r0 = 32; r0 < NP; r0 += 32) {
+      // Zf[r0:r0+32, 0:r0] = L[r0:r0+32, 0:r0] * Z[0:r0, 0:r0]  (2 rows x 4 columns per thread)
+      for (int t = tid; t < 16 * (r0 / 4); t += UM_NT) {
+        const int rr = 2 * (t % 16), cc = 4 * (t / 16);
+        const int g0 = r0 + rr, g1 = g0 + 1;
+        const float* L0 = g0 < n ? P + s_perm[g0] * LDP : nullptr;
+        const float* L1 = g1 < n ? P + s_perm[g1] * LDP : nullptr;
+        float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0;
+        for (int m = cc; m < r0; ++m) {  // Z[m][cc..cc+3] = 0 for m < cc
+          const float4 zv = *reinterpret_cast<const float4*>(Zf + m * LDP + cc);
+          const float l0 = L0 ? L0[m] : 0.0f, l1 = L1 ? L1[m] : 0.0f;
+          s0.x = fmaf(l0, zv.x, s0.x); s0.y = fmaf(l0, zv.y, s0.y);
+          s0.z = fmaf(l0, zv.z, s0.z); s0.w = fmaf(l0, zv.w, s0.w);
+          s1.x = fmaf(l1, zv.x, s1.x); s1.y = fmaf(l1, zv.y, s1.y);
+          s1.z = fmaf(l1, zv.z, s1.z); s1.w = fmaf(l1, zv.w, s1.w);
+        }
+        *reinterpret_cast<float4*>(Zf + g0 * LDP + cc) = s0;
+        *reinterpret_cast<float4*>(Zf + g1 * LDP + cc) = s1;
+      }
+      __syncthreads();
+      // Zf[r0:r0+32, 0:r0] = -Z_bb * (that), in place, one column per thread
+      for (int c = tid; c < r0; c += UM_NT) {
+        float y[32];
+#pragma unroll
+        for (int r = 0; r < 32; ++r) y[r] = Zf[(r0 + r) * LDP + c];
+#pragma unroll
+        for (int r = 31; r >= 0; --r) {
+          const float* Zr = Zf + (r0 + r) * LDP + r0;
+          float s = 0.0f;
+#pragma unroll
+          for (int m = 0; m <= r; ++m) s = fmaf(Zr[m], y[m], s);
+          y[r] = -s;
+        }
+#pragma unroll
+        for (int r = 0; r < 32; ++r) Zf[(r0 + r) * LDP + c] = y[r];
+      }
+      __syncthreads();
+    }
+    // ------------------------------------------------ U12 = Z Xt (tensor cores)
+    umma_stage_a(L, smem_raw, [&](int i, int kk) {
+      return (i < n && kk < n) ? Zf[i * LDP + kk] : 0.0f;
+    });
+    __syncthreads();
+    bool ok = umma_product(L, smem_raw, s_bar, par, tmem, [&](int c, int m) {
+      return (m < n && c < Nc) ? Xs[(size_t)c * n2 + m] : 0.0f;
+    });
+    if (!ok) {
+      if (tid == 0) report(a.st, DEV_TIMEOUT, j, 0, k);
+      break;
+    }
+    // U-row out: D'_j, E'_j, B'_j
+    {
+      const int qd = warp & 3, grp = warp >> 2, m = 32 * qd + lane;
+      for (int pc = grp; pc < L.Npad / 16; pc += UM_NW / 4) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(16 * pc), v);
+        if (m < n) {
+#pragma unroll
+          for (int jj = 0; jj < 16; ++jj) {
+            const int c = 16 * pc + jj;
+            if (c < n) a.D[oj + m + (size_t)c * n] = v[jj];
+            else if (c < n2) a.E[oj + m + (size_t)(c - n) * n] = v[jj];
+            else if (c < Nc) a.B[(size_t)j * nnx + m + (size_t)(c - n2) * n] = v[jj];
+          }
+        }
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+    // border rows: -Lc U12 (CUDA cores), one trailing column per thread
+    if (nr > 0) {
+      for (int c = tid; c < Nc; c += UM_NT) {
+        const float* u = c < n ? a.D + oj + (size_t)c * n
+                       : c < n2 ? a.E + oj + (size_t)(c - n) * n : a.B + (size_t)j * nnx + (size_t)(c - n2) * n;
+        float acc[UM_NRMAX];
+#pragma unroll
+        for (int r = 0; r < UM_NRMAX; ++r) acc[r] = 0.0f;
+        for (int m = 0; m < n; ++m) {
+          const float um = u[m];
+#pragma unroll
+          for (int r = 0; r < UM_NRMAX; ++r)
+            if (r < nr) acc[r] = fmaf(Lc[m * nr + r], um, acc[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < UM_NRMAX; ++r) {
+          if (r < nr) {
+            if (c < n) {
+              const size_t oc = (size_t)jp * nrn + r + (size_t)c * nr;
+              const float cjp = first ? float(a.C0[oc]) : a.C[oc];
+              a.C[oc] = cjp - acc[r];
+            } else if (c < n2) {
+              a.Rbuf[(size_t)j * nrn + r + (size_t)(c - n) * nr] = -acc[r];
+            } else {
+              a.Fbuf[(size_t)j * nrnx + r + (size_t)(c - n2) * nr] = -(double)acc[r];
+            }
+          }
+        }
+      }
+    }
+    // ------------------------------------------- Xb - L21 U12 (tensor cores)
+    umma_stage_a(L, smem_raw, [&](int i, int kk) {
+      return (i < n && kk < n) ? Tj[(size_t)kk * n2 + n + i] : 0.0f;
+    });
+    __syncthreads();
+    ok = umma_product(L, smem_raw, s_bar, par, tmem, [&](int c, int m) {
+      if (m >= n || c >= Nc) return 0.0f;
+      return c < n ? a.D[oj + m + (size_t)c * n]
+           : c < n2 ? a.E[oj + m + (size_t)(c - n) * n] : a.B[(size_t)j * nnx + m + (size_t)(c - n2) * n];
+    });
+    if (!ok) {
+      if (tid == 0) report(a.st, DEV_TIMEOUT, j, 1, k);
+      break;
+    }
+    // reduced row out: D'_jp, E'_jp, B'_jp
+    {
+      const int qd = warp & 3, grp = warp >> 2, i = 32 * qd + lane;
+      for (int pc = grp; pc < L.Npad / 16; pc += UM_NW / 4) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(16 * pc), v);
+        if (i < n) {
+#pragma unroll
+          for (int jj = 0; jj < 16; ++jj) {
+            const int c = 16 * pc + jj;
+            if (c >= Nc) continue;
+            const float y = Xs[(size_t)c * n2 + n + i] - v[jj];
+            if (c < n) a.D[ojp + i + (size_t)c * n] = y;
+            else if (c < n2) a.E[ojp + i + (size_t)(c - n) * n] = y;
+            else a.B[(size_t)jp * nnx + i + (size_t)(c - n2) * n] = y;
+          }
+        }
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(UM_TMEM_COLS) : "memory");
+}
+
+__host__ inline bool umma_fits(const Dims& d) {
+  return d.n > 32 && d.n <= UM_NMAX && d.nr <= UM_NRMAX && d.nx <= UM_NXMAX &&
+         umma_layout(d).bytes + 4096 <= 227u * 1024u;  // with the static shared memory
+}

@@ -116,13 +116,17 @@ int bcr_set_precision(bcr_handle h, int precision);      /* extension: FP64 / mi
 /* Pair-kernel family of the factorization (extension, no reference
    counterpart; for tuning and tests).  AUTO picks by block size, selection and
    precision; a forced family that does not apply to the shape falls back to
-   the next one that does (TC -> GRP -> ROWS -> CTA -> SMEM). */
+   the next one that does (TC -> GRP -> ROWS -> CTA -> SMEM).  UMMA is the
+   FP32 (mixed-precision) large-block LU kernel with tcgen05 tensor-core
+   products (33 <= n <= 128, nr <= 16, nx <= 16); under AUTO it is the choice
+   for those shapes, and CTA selects the CUDA-core blocked kernel instead. */
 #define BCR_PAIR_AUTO 0
 #define BCR_PAIR_TC 1
 #define BCR_PAIR_GRP 2
 #define BCR_PAIR_ROWS 3
 #define BCR_PAIR_CTA 4
 #define BCR_PAIR_SMEM 5
+#define BCR_PAIR_UMMA 6
 int bcr_set_pair_kernel(bcr_handle h, int choice);
 
 /* Iterative refinement of the mixed path (extension, no reference counterpart):

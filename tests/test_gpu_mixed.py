@@ -161,3 +161,39 @@ def test_mixed_full_size_config_C(kappa):
     assert rr <= RELRES_BAR, (kappa, it, rr)
     o = po.Oracle(s, "LU", "LU")
     assert relres(o, s, x, b[0]) <= RELRES_BAR
+
+
+# shapes of the FP32 large-block kernel with tcgen05 tensor-core products
+# (33 <= n <= 128, nr <= 16, nx <= 16): one and two N chunks of the product
+# (2n + nx above 256 at n = 128), K and N padding, n not a multiple of 32
+UMMA_DIMS = [(5, 128, 4, 4, 16, 16), (33, 128, 4, 4, 16, 16), (17, 100, 2, 2, 16, 16),
+             (9, 48, 1, 1, 4, 4), (8, 67, 0, 2, 5, 3), (6, 40, 0, 0, 0, 0), (12, 33, 1, 1, 2, 2),
+             (7, 96, 3, 3, 8, 8)]
+
+
+@pytest.mark.parametrize("dims", UMMA_DIMS)
+def test_mixed_tensor_core_large_blocks(dims):
+    """The tcgen05 3xTF32 pair kernel: its unrefined FP32 solve is FP32-accurate
+    (within 100x of the CUDA-core FP32 kernel's residual), and refinement
+    reaches the mixed bar with the forward error of the FP64 oracle."""
+    s = synth.collocation(*dims, seed=sum(dims))
+    assert s.nrows == s.ncols
+    b = synth.rhs(s, nrhs=1, seed=4)
+    o, xo = oracle_solution(s, b)
+    unref = {}
+    for pk in (B.PAIR_CTA, B.PAIR_UMMA):
+        h = mixed_solver(s, max_iter=0)
+        h.set_pair_kernel(pk)
+        assert h.factorize(), h.last_error()
+        x = np.array(b[0], copy=True)
+        assert h.solve(x), h.last_error()
+        unref[pk] = h.refinement_info()[1]
+    assert unref[B.PAIR_UMMA] < 1e-5 and unref[B.PAIR_UMMA] <= 100 * unref[B.PAIR_CTA] + 1e-12, unref
+    h = mixed_solver(s)
+    assert h.factorize(), h.last_error()
+    x = np.array(b[0], copy=True)
+    assert h.solve(x), h.last_error()
+    it, rr = h.refinement_info()
+    assert it <= 3 and rr <= RELRES_BAR, (dims, it, rr)
+    assert relres(o, s, x, b[0]) <= RELRES_BAR
+    assert fwd_err(x[:s.ncols], xo[0, :s.ncols]) <= FWD_BAR
