@@ -67,7 +67,7 @@ __host__ __device__ inline UmmaLayout umma_layout(const Dims& d) {
   if (L.offZ < L.offB) L.offZ = L.offB;
   L.offLc = L.offZ + (unsigned)(L.NP * L.LDP * 4);
   if (L.offLc < endB) L.offLc = endB;
-  L.offSlot = (L.offLc + (unsigned)(d.nr * n * 4) + 15u) & ~15u;
+  L.offSlot = (L.offLc + (unsigned)(UM_NRMAX * n * 4) + 15u) & ~15u;
   const unsigned endS = L.offSlot + 2u * UM_NW * 36u * 4u;
   L.bytes = endB > endS ? endB : endS;
   return L;
@@ -146,12 +146,33 @@ __device__ __forceinline__ uint32_t umma_b_off(int c, int m, int lbo) {
   return (uint32_t)((m >> 2) * lbo + (c >> 3) * 128 + (c & 7) * 16 + (m & 3) * 4);
 }
 
+// cnt elements read by ld(e) and written by st(e, v), the reads of a thread
+// issued in groups of 16 before their writes (a CTA per SM keeps few loads in
+// flight otherwise)
+template <typename Ld, typename St>
+__device__ __forceinline__ void um_batched(int cnt, Ld ld, St st) {
+  constexpr int U = 16;
+  for (int base = threadIdx.x; base < cnt; base += U * UM_NT) {
+    float v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int e = base + u * UM_NT;
+      v[u] = e < cnt ? ld(e) : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int e = base + u * UM_NT;
+      if (e < cnt) st(e, v[u]);
+    }
+  }
+}
+
 // One product D[128 x Npad] = A[128 x Kpad] * B[Kpad x Npad] with the B operand
 // staged 16 K-rows at a time by all threads from src(c, m) (m the K index).
 // A (hi, lo) must be in shared memory and fenced.  Returns false on a timeout.
-template <typename Src>
+template <typename Src, typename Obs>
 __device__ bool umma_product(const UmmaLayout& L, unsigned char* sm, uint64_t* bars, uint32_t (&par)[2],
-                             uint32_t tmem, Src src) {
+                             uint32_t tmem, Src src, Obs obs) {
   const int tid = threadIdx.x;
   const int S = L.Kpad / 16;
   const uint32_t sA = smem_u32(sm);
@@ -166,14 +187,12 @@ __device__ bool umma_product(const UmmaLayout& L, unsigned char* sm, uint64_t* b
     if (ok) {
       unsigned char* bh = sm + L.offB + (unsigned)b * 2u * L.szBhalf;
       unsigned char* bl = bh + L.szBhalf;
-      for (int e = tid; e < cnt; e += UM_NT) {
-        const int m = e & 15, c = e >> 4;
-        const float v = src(c, 16 * s + m);
+      um_batched(cnt, [&](int e) { return src(e >> 4, 16 * s + (e & 15)); }, [&](int e, float v) {
         const float h = tf32_hi(v);
-        const uint32_t o = umma_b_off(c, m, L.LBO_B);
+        const uint32_t o = umma_b_off(e >> 4, e & 15, L.LBO_B);
         *reinterpret_cast<float*>(bh + o) = h;
         *reinterpret_cast<float*>(bl + o) = v - h;
-      }
+      });
     }
     fence_async_smem();
     if (__syncthreads_or(!ok)) return false;
@@ -203,6 +222,8 @@ __device__ bool umma_product(const UmmaLayout& L, unsigned char* sm, uint64_t* b
       }
       umma_commit(&bars[b]);
     }
+    // CUDA-core work on the staged rows while the tensor cores run
+    obs(s, sm + L.offB + (unsigned)b * 2u * L.szBhalf);
   }
   // the last (up to) two commits: every commit is waited exactly once
   for (int s = S - 2 < 0 ? 0 : S - 2; s < S; ++s) {
@@ -217,23 +238,45 @@ __device__ bool umma_product(const UmmaLayout& L, unsigned char* sm, uint64_t* b
 // A operand (hi, lo) from a(i, k), i < 128, k < Kpad
 template <typename Src>
 __device__ void umma_stage_a(const UmmaLayout& L, unsigned char* sm, Src a) {
-  const int cnt = 128 * L.Kpad;
-  for (int e = threadIdx.x; e < cnt; e += UM_NT) {
-    const int kl = e & 3, i = (e >> 2) & 127, kg = e >> 9;
-    const int k = 4 * kg + kl;
-    const float v = a(i, k);
-    const float h = tf32_hi(v);
-    const uint32_t o = umma_a_off(i, k);
-    *reinterpret_cast<float*>(sm + o) = h;
-    *reinterpret_cast<float*>(sm + L.szAhalf + o) = v - h;
-  }
+  um_batched(128 * L.Kpad, [&](int e) { return a((e >> 2) & 127, 4 * (e >> 9) + (e & 3)); },
+             [&](int e, float v) {
+               const float h = tf32_hi(v);
+               const uint32_t o = umma_a_off((e >> 2) & 127, 4 * (e >> 9) + (e & 3));
+               *reinterpret_cast<float*>(sm + o) = h;
+               *reinterpret_cast<float*>(sm + L.szAhalf + o) = v - h;
+             });
   fence_async_smem();
+}
+
+// one row of cnt elements, element c at src[c * stride], into dst[0, round_up(cnt, 16))
+// (16-byte aligned; zero past cnt), the 16 loads of a group issued together
+template <typename S>
+__device__ __forceinline__ void um_load_row(const S* src, int stride, int cnt, float* dst) {
+  for (int c0 = 0; c0 < cnt; c0 += 16) {
+    float v[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) v[u] = c0 + u < cnt ? float(src[(size_t)(c0 + u) * stride]) : 0.0f;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      *reinterpret_cast<float4*>(dst + c0 + 4 * u) = make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
+  }
+}
+// cnt elements src[c * stride] (zeros when src is null) to dst[c * dstride]
+template <typename S>
+__device__ __forceinline__ void um_copy_col(const S* src, int stride, int cnt, float* dst, int dstride) {
+  for (int c0 = 0; c0 < cnt; c0 += 16) {
+    float v[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) v[u] = (src && c0 + u < cnt) ? float(src[(size_t)(c0 + u) * stride]) : 0.0f;
+#pragma unroll
+    for (int u = 0; u < 16; ++u)
+      if (c0 + u < cnt) dst[(size_t)(c0 + u) * dstride] = v[u];
+  }
 }
 
 __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a, float* slab, size_t slab_elems) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_perm[2 * UM_NMAX + UM_NRMAX];  // position -> row
-  __shared__ int s_pos[2 * UM_NMAX];              // row -> position
   __shared__ int s_pivrow[UM_NMAX];               // pivot step -> row
   __shared__ __align__(8) uint64_t s_bar[2];
   __shared__ uint32_t s_taddr;
@@ -246,7 +289,7 @@ __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a
   const size_t nn = (size_t)n * n, nnx = (size_t)n * d.nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * d.nx;
   float* P = reinterpret_cast<float*>(smem_raw);
   float* Zf = reinterpret_cast<float*>(smem_raw + L.offZ);
-  float* Lc = reinterpret_cast<float*>(smem_raw + L.offLc);
+  float* Lc = reinterpret_cast<float*>(smem_raw + L.offLc);  // [m][UM_NRMAX], zero past nr
   float* slot = reinterpret_cast<float*>(smem_raw + L.offSlot);
   float* Xs = slab + (size_t)blockIdx.x * slab_elems;  // [col][position], 2n x Nc
 
@@ -273,14 +316,23 @@ __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a
   for (long q = blockIdx.x; q < np; q += gridDim.x) {
     const int j = k + (int)(2L * k * q), jp = j - k;
     const size_t oj = (size_t)j * nn, ojp = (size_t)jp * nn;
+    float* const Dj = a.D + oj;
+    float* const Ej = a.E + oj;
+    float* const Bj = a.B + (size_t)j * nnx;
+    // column c of the pair's U-row [D'_j E'_j B'_j] (n rows)
+    auto ucol = [&](int c) -> float* { return c < n ? Dj + (size_t)c * n : c < n2 ? Ej + (size_t)(c - n) * n : Bj + (size_t)(c - n2) * n; };
     // ------------------------------------------------------------ panel load
-    for (int e = tid; e < R * n; e += UM_NT) {
-      const int r = e % R, c = e / R;
-      float v;
-      if (r < n) v = ldg_src(first, a.E0, a.E, ojp + r + (size_t)c * n);
-      else if (r < n2) v = ldsrc(first, a.D0, a.D, oj + (r - n) + (size_t)c * n);  // D'_j is written here later
-      else v = ldsrc(first, a.C0, a.C, (size_t)j * nrn + (r - n2) + (size_t)c * nr);
-      P[r * LDP + c] = v;
+    // row t of [E_jp; D_j; C_j] by thread t
+    if (tid < R) {
+      float* dst = P + tid * LDP;
+      if (tid < n) {
+        if (first) um_load_row(a.E0 + ojp + tid, n, n, dst); else um_load_row(a.E + ojp + tid, n, n, dst);
+      } else if (tid < n2) {
+        if (first) um_load_row(a.D0 + oj + (tid - n), n, n, dst); else um_load_row(Dj + (tid - n), n, n, dst);
+      } else {
+        const size_t o = (size_t)j * nrn + (tid - n2);
+        if (first) um_load_row(a.C0 + o, nr, n, dst); else um_load_row(a.C + o, nr, n, dst);
+      }
     }
     __syncthreads();
     // --------------------------------------------------------------- panel LU
@@ -298,49 +350,58 @@ __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a
       }
 #pragma unroll
       for (int i = 0; i < 32; ++i) {
-        if (i < w) {
+        if (i < w && info == 0) {
           const int gi = kb + i;
-          const bool cand = tid < n2 && !done;
-          const uint32_t key = (cand && rv[i] == rv[i]) ? __float_as_uint(fabsf(rv[i])) : 0u;
-          const uint32_t cpos = cand ? (uint32_t)pos : 0xFFFFu;
-          const uint32_t kmax = __reduce_max_sync(0xFFFFFFFFu, key);
-          const uint32_t pmin = __reduce_min_sync(0xFFFFFFFFu, key == kmax ? cpos : 0xFFFFu);
-          float* sl = slot + ((gi & 1) * UM_NW + warp) * 36;
+          float* slb = slot + (gi & 1) * UM_NW * 36;  // this step's candidate bank
           if (warp < nwr) {
+            // the warp's candidate: largest |a|, then first position
+            const bool cand = tid < n2 && !done;
+            const uint32_t key = (cand && rv[i] == rv[i]) ? __float_as_uint(fabsf(rv[i])) : 0u;
+            const uint32_t cpos = cand ? (uint32_t)pos : 0xFFFFu;
+            const uint32_t kmax = __reduce_max_sync(0xFFFFFFFFu, key);
+            const uint32_t pmin = __reduce_min_sync(0xFFFFFFFFu, key == kmax ? cpos : 0xFFFFu);
+            float* sl = slb + warp * 36;
             if (cand && key == kmax && cpos == pmin) {
               float4* d4 = reinterpret_cast<float4*>(sl);
 #pragma unroll
               for (int q4 = 0; q4 < 8; ++q4)
                 d4[q4] = make_float4(rv[4 * q4], rv[4 * q4 + 1], rv[4 * q4 + 2], rv[4 * q4 + 3]);
-              reinterpret_cast<uint32_t*>(sl)[32] = kmax;
-              reinterpret_cast<uint32_t*>(sl)[33] = pmin;
-              reinterpret_cast<int*>(sl)[34] = tid;
+              *reinterpret_cast<uint4*>(sl + 32) = make_uint4(kmax, pmin, (uint32_t)tid, 0u);
             } else if (lane == 0 && pmin == 0xFFFFu) {
-              reinterpret_cast<uint32_t*>(sl)[32] = 0u;
-              reinterpret_cast<uint32_t*>(sl)[33] = 0xFFFFu;
-              reinterpret_cast<int*>(sl)[34] = -1;
+              *reinterpret_cast<uint4*>(sl + 32) = make_uint4(0u, 0xFFFFu, 0xFFFFFFFFu, 0u);
             }
           }
           __syncthreads();
-          uint32_t bk = 0u, bp = 0xFFFFu;
-          int bw = 0;
-          for (int ww = 0; ww < nwr; ++ww) {
-            const uint32_t* s2 = reinterpret_cast<const uint32_t*>(slot + ((gi & 1) * UM_NW + ww) * 36);
-            const uint32_t k2 = s2[32], p2 = s2[33];
-            if (k2 > bk || (k2 == bk && p2 < bp)) { bk = k2; bp = p2; bw = ww; }
+          // the winner over the warps' candidates, one lane per warp slot
+          uint32_t k2 = 0u, p2 = 0xFFFFu;
+          if (lane < nwr) {
+            const uint4 t = *reinterpret_cast<const uint4*>(slb + lane * 36 + 32);
+            k2 = t.x; p2 = t.y;
           }
-          const float* win = slot + ((gi & 1) * UM_NW + bw) * 36;
+          const uint32_t kw = __reduce_max_sync(0xFFFFFFFFu, k2);
+          const uint32_t pw = __reduce_min_sync(0xFFFFFFFFu, k2 == kw ? p2 : 0xFFFFu);
+          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, lane < nwr && k2 == kw && p2 == pw);
+          const float* win = slb + (bal ? __ffs(bal) - 1 : 0) * 36;
           const int wt = reinterpret_cast<const int*>(win)[34];
           const float pv = win[i];
-          if (pv == 0.0f || wt < 0) { info = gi + 1; break; }
-          if (tid == 0) s_pivrow[gi] = wt;
-          if (pos == gi) pos = (int)bp;
-          if (tid == wt) { pos = gi; done = 1; }
-          if (tid < R && !done) {
-            const float l = rv[i] * (1.0f / pv);
-            rv[i] = l;
+          if (pv == 0.0f || wt < 0 || pw == 0xFFFFu) {
+            info = gi + 1;
+          } else {
+            if (tid == 0) s_pivrow[gi] = wt;
+            if (pos == gi) pos = (int)pw;
+            if (tid == wt) { pos = gi; done = 1; }
+            if (tid < R && !done) {
+              const float l = rv[i] * __frcp_rn(pv);
+              rv[i] = l;
 #pragma unroll
-            for (int jj = i + 1; jj < 32; ++jj) rv[jj] = fmaf(-l, win[jj], rv[jj]);
+              for (int q4 = (i + 1) / 4; q4 < 8; ++q4) {
+                const float4 u4 = *reinterpret_cast<const float4*>(win + 4 * q4);
+                if (4 * q4 > i) rv[4 * q4] = fmaf(-l, u4.x, rv[4 * q4]);
+                if (4 * q4 + 1 > i) rv[4 * q4 + 1] = fmaf(-l, u4.y, rv[4 * q4 + 1]);
+                if (4 * q4 + 2 > i) rv[4 * q4 + 2] = fmaf(-l, u4.z, rv[4 * q4 + 2]);
+                if (4 * q4 + 3 > i) rv[4 * q4 + 3] = fmaf(-l, u4.w, rv[4 * q4 + 3]);
+              }
+            }
           }
         }
       }
@@ -394,41 +455,45 @@ __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a
       continue;
     }
     if (tid < R) s_perm[pos] = tid;
-    if (tid < n2) s_pos[tid] = pos;
     __syncthreads();
     // ------------------------------------- factors out; X staged by position
     float* Tj = a.Tm + (size_t)j * szT(d);
-    for (int e = tid; e < n2 * n; e += UM_NT) {
-      const int p = e % n2, c = e / n2;
-      Tj[e] = P[s_perm[p] * LDP + c];
-    }
-    unsigned char* Pj = a.P + (size_t)j * szP(d);
-    for (int r = tid; r < n2; r += UM_NT) Pj[r] = (unsigned char)s_perm[r];
-    for (int i = tid; i < n; i += UM_NT) Pj[n2 + i] = (unsigned char)i;
-    for (int e = tid; e < nr * n; e += UM_NT) {
-      const int r = e % nr, c = e / nr;
-      const float v = P[(n2 + r) * LDP + c];
-      a.C[(size_t)j * nrn + e] = v;
-      Lc[c * nr + r] = v;
-    }
-    // X = [D_jp 0 B_jp; 0 E_j B_j] by position: Xs[col * 2n + pos]
-    for (int e = tid; e < n2 * Nc; e += UM_NT) {
-      const int r = e % n2, c = e / n2;
-      float v = 0.0f;
-      if (c >= n2) {
-        const size_t o = (size_t)(r < n ? jp : j) * nnx + (r % n) + (size_t)(c - n2) * n;
-        v = ldsrc(first, a.B0, a.B, o);
-      } else if (r < n) {
-        if (c < n) v = ldg_src(first, a.D0, a.D, ojp + r + (size_t)c * n);
-      } else if (c >= n) {
-        v = ldsrc(first, a.E0, a.E, oj + (r - n) + (size_t)(c - n) * n);  // E'_j is written here later
+    if (tid < n2) {  // T in getrf order, column-major 2n x n: one position per thread
+      const float* prow = P + s_perm[tid] * LDP;
+      for (int c0 = 0; c0 < n; c0 += 4) {
+        const float4 v = *reinterpret_cast<const float4*>(prow + c0);
+        Tj[(size_t)c0 * n2 + tid] = v.x;
+        if (c0 + 1 < n) Tj[(size_t)(c0 + 1) * n2 + tid] = v.y;
+        if (c0 + 2 < n) Tj[(size_t)(c0 + 2) * n2 + tid] = v.z;
+        if (c0 + 3 < n) Tj[(size_t)(c0 + 3) * n2 + tid] = v.w;
       }
-      Xs[(size_t)c * n2 + s_pos[r]] = v;
+      a.P[(size_t)j * szP(d) + tid] = (unsigned char)s_perm[tid];
+      if (tid < n) a.P[(size_t)j * szP(d) + n2 + tid] = (unsigned char)tid;
+      // X = [D_jp 0 B_jp; 0 E_j B_j], row tid, to Xs[col * 2n + pos]
+      float* xd = Xs + pos;
+      const int r = tid % n;
+      if (tid < n) {
+        if (first) um_copy_col(a.D0 + ojp + r, n, n, xd, n2); else um_copy_col(a.D + ojp + r, n, n, xd, n2);
+        um_copy_col((const float*)nullptr, n, n, xd + (size_t)n * n2, n2);
+      } else {
+        um_copy_col((const float*)nullptr, n, n, xd, n2);
+        // E'_j is written here later: plain loads
+        if (first) um_copy_col(a.E0 + oj + r, n, n, xd + (size_t)n * n2, n2); else um_copy_col(Ej + r, n, n, xd + (size_t)n * n2, n2);
+      }
+      const size_t ob = (size_t)(tid < n ? jp : j) * nnx + r;
+      if (first) um_copy_col(a.B0 + ob, n, d.nx, xd + (size_t)n2 * n2, n2);
+      else um_copy_col(a.B + ob, n, d.nx, xd + (size_t)n2 * n2, n2);
+    }
+    for (int e = tid; e < n * UM_NRMAX; e += UM_NT) {  // border multipliers C_j U^-1
+      const int r = e & (UM_NRMAX - 1), c = e / UM_NRMAX;
+      const float v = r < nr ? P[(n2 + r) * LDP + c] : 0.0f;
+      Lc[e] = v;
+      if (r < nr) a.C[(size_t)j * nrn + r + (size_t)c * nr] = v;
     }
     // ---------------------------------------------------- Z = L11^-1 (FP32)
-    for (int e = tid; e < NP * NP; e += UM_NT) {
-      const int r = e / NP, c = e % NP;
-      if ((c >> 5) > (r >> 5)) Zf[r * LDP + c] = 0.0f;
+    if (tid < NP) {  // zero above the diagonal blocks
+      for (int c = 32 * (tid / 32 + 1); c < NP; c += 4)
+        *reinterpret_cast<float4*>(Zf + tid * LDP + c) = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     if (warp < NP / 32) {  // diagonal 32 x 32 inverses, one column per lane
       const int a32 = warp * 32, c = lane;
@@ -452,7 +517,7 @@ __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a
     for (int r0 = 32; r0 < NP; r0 += 32) {
       // Zf[r0:r0+32, 0:r0] = L[r0:r0+32, 0:r0] * Z[0:r0, 0:r0]  (2 rows x 4 columns per thread)
       for (int t = tid; t < 16 * (r0 / 4); t += UM_NT) {
-        const int rr = 2 * (t % 16), cc = 4 * (t / 16);
+        const int rr = 2 * (t & 15), cc = 4 * (t >> 4);
         const int g0 = r0 + rr, g1 = g0 + 1;
         const float* L0 = g0 < n ? P + s_perm[g0] * LDP : nullptr;
         const float* L1 = g1 < n ? P + s_perm[g1] * LDP : nullptr;
@@ -494,7 +559,7 @@ __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a
     __syncthreads();
     bool ok = umma_product(L, smem_raw, s_bar, par, tmem, [&](int c, int m) {
       return (m < n && c < Nc) ? Xs[(size_t)c * n2 + m] : 0.0f;
-    });
+    }, [](int, const unsigned char*) {});
     if (!ok) {
       if (tid == 0) report(a.st, DEV_TIMEOUT, j, 0, k);
       break;
@@ -509,74 +574,94 @@ __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a
 #pragma unroll
           for (int jj = 0; jj < 16; ++jj) {
             const int c = 16 * pc + jj;
-            if (c < n) a.D[oj + m + (size_t)c * n] = v[jj];
-            else if (c < n2) a.E[oj + m + (size_t)(c - n) * n] = v[jj];
-            else if (c < Nc) a.B[(size_t)j * nnx + m + (size_t)(c - n2) * n] = v[jj];
+            if (c < Nc) ucol(c)[m] = v[jj];
           }
         }
       }
     }
     tc_fence_before();
     __syncthreads();
-    // border rows: -Lc U12 (CUDA cores), one trailing column per thread
-    if (nr > 0) {
-      for (int c = tid; c < Nc; c += UM_NT) {
-        const float* u = c < n ? a.D + oj + (size_t)c * n
-                       : c < n2 ? a.E + oj + (size_t)(c - n) * n : a.B + (size_t)j * nnx + (size_t)(c - n2) * n;
-        float acc[UM_NRMAX];
-#pragma unroll
-        for (int r = 0; r < UM_NRMAX; ++r) acc[r] = 0.0f;
-        for (int m = 0; m < n; ++m) {
-          const float um = u[m];
-#pragma unroll
-          for (int r = 0; r < UM_NRMAX; ++r)
-            if (r < nr) acc[r] = fmaf(Lc[m * nr + r], um, acc[r]);
-        }
-#pragma unroll
-        for (int r = 0; r < UM_NRMAX; ++r) {
-          if (r < nr) {
-            if (c < n) {
-              const size_t oc = (size_t)jp * nrn + r + (size_t)c * nr;
-              const float cjp = first ? float(a.C0[oc]) : a.C[oc];
-              a.C[oc] = cjp - acc[r];
-            } else if (c < n2) {
-              a.Rbuf[(size_t)j * nrn + r + (size_t)(c - n) * nr] = -acc[r];
-            } else {
-              a.Fbuf[(size_t)j * nrnx + r + (size_t)(c - n2) * nr] = -(double)acc[r];
-            }
-          }
-        }
-      }
-    }
     // ------------------------------------------- Xb - L21 U12 (tensor cores)
     umma_stage_a(L, smem_raw, [&](int i, int kk) {
       return (i < n && kk < n) ? Tj[(size_t)kk * n2 + n + i] : 0.0f;
     });
     __syncthreads();
+    // the border rows' -Lc U12 on the CUDA cores from the staged U12 rows, one
+    // trailing column per thread
+    float bacc[UM_NRMAX];
+#pragma unroll
+    for (int r = 0; r < UM_NRMAX; ++r) bacc[r] = 0.0f;
     ok = umma_product(L, smem_raw, s_bar, par, tmem, [&](int c, int m) {
-      if (m >= n || c >= Nc) return 0.0f;
-      return c < n ? a.D[oj + m + (size_t)c * n]
-           : c < n2 ? a.E[oj + m + (size_t)(c - n) * n] : a.B[(size_t)j * nnx + m + (size_t)(c - n2) * n];
+      return (m < n && c < Nc) ? ucol(c)[m] : 0.0f;
+    }, [&](int s, const unsigned char* bh) {
+      if (nr == 0 || tid >= Nc) return;
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {
+        const uint32_t o = umma_b_off(tid, 4 * g, L.LBO_B);
+        const float4 h4 = *reinterpret_cast<const float4*>(bh + o);
+        const float4 l4 = *reinterpret_cast<const float4*>(bh + L.szBhalf + o);
+        const float u[4] = {h4.x + l4.x, h4.y + l4.y, h4.z + l4.z, h4.w + l4.w};
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int m = 16 * s + 4 * g + t;
+          if (m < n) {
+            const float4* l4p = reinterpret_cast<const float4*>(Lc + m * UM_NRMAX);
+#pragma unroll
+            for (int r4 = 0; r4 < UM_NRMAX / 4; ++r4) {
+              const float4 lc = l4p[r4];
+              bacc[4 * r4] = fmaf(lc.x, u[t], bacc[4 * r4]);
+              bacc[4 * r4 + 1] = fmaf(lc.y, u[t], bacc[4 * r4 + 1]);
+              bacc[4 * r4 + 2] = fmaf(lc.z, u[t], bacc[4 * r4 + 2]);
+              bacc[4 * r4 + 3] = fmaf(lc.w, u[t], bacc[4 * r4 + 3]);
+            }
+          }
+        }
+      }
     });
     if (!ok) {
       if (tid == 0) report(a.st, DEV_TIMEOUT, j, 1, k);
       break;
     }
+    if (nr > 0 && tid < Nc) {
+      const int c = tid;
+#pragma unroll
+      for (int r = 0; r < UM_NRMAX; ++r) {
+        if (r < nr) {
+          if (c < n) {
+            const size_t oc = (size_t)jp * nrn + r + (size_t)c * nr;
+            const float cjp = first ? float(a.C0[oc]) : a.C[oc];
+            a.C[oc] = cjp - bacc[r];
+          } else if (c < n2) {
+            a.Rbuf[(size_t)j * nrn + r + (size_t)(c - n) * nr] = -bacc[r];
+          } else {
+            a.Fbuf[(size_t)j * nrnx + r + (size_t)(c - n2) * nr] = -(double)bacc[r];
+          }
+        }
+      }
+    }
     // reduced row out: D'_jp, E'_jp, B'_jp
     {
+      float* const Djp = a.D + ojp;
+      float* const Ejp = a.E + ojp;
+      float* const Bjp = a.B + (size_t)jp * nnx;
       const int qd = warp & 3, grp = warp >> 2, i = 32 * qd + lane;
       for (int pc = grp; pc < L.Npad / 16; pc += UM_NW / 4) {
         float v[16];
+        float xb[16];
+#pragma unroll
+        for (int jj = 0; jj < 16; ++jj) {
+          const int c = 16 * pc + jj;
+          xb[jj] = (i < n && c < Nc) ? Xs[(size_t)c * n2 + n + i] : 0.0f;
+        }
         tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(16 * pc), v);
         if (i < n) {
 #pragma unroll
           for (int jj = 0; jj < 16; ++jj) {
             const int c = 16 * pc + jj;
             if (c >= Nc) continue;
-            const float y = Xs[(size_t)c * n2 + n + i] - v[jj];
-            if (c < n) a.D[ojp + i + (size_t)c * n] = y;
-            else if (c < n2) a.E[ojp + i + (size_t)(c - n) * n] = y;
-            else a.B[(size_t)jp * nnx + i + (size_t)(c - n2) * n] = y;
+            const float y = xb[jj] - v[jj];
+            float* col = c < n ? Djp + (size_t)c * n : c < n2 ? Ejp + (size_t)(c - n) * n : Bjp + (size_t)(c - n2) * n;
+            col[i] = y;
           }
         }
       }
