@@ -9,11 +9,13 @@
 //
 //   1. panel LU: the (2n + nr) x n panel [E_jp; D_j; C_j] is factored in
 //      shared memory with the getrf pivot rule (largest |a| among the 2n
-//      candidate rows, first position on ties), in column blocks of 32.
-//      Every thread owns one row of the block in registers; one block barrier
-//      per pivot step (the warps post their candidate rows, every thread
-//      picks the winner); the block's U rows are solved with its unit lower
-//      triangle and the rows below get one product of depth 32.  Row
+//      candidate rows, first position on ties), in column blocks of UM_BW.
+//      Every thread owns one row of the block in registers.  Per pivot step
+//      each warp with candidate rows posts its best row and a shared 64-bit
+//      atomicMax of (|a|, first position, warp) picks the winner; one barrier
+//      over those warps per step (border-only warps apply the block's
+//      eliminations afterwards); the block's U rows are solved with its unit lower
+//      triangle and the rows below get one product of depth UM_BW.  Row
 //      interchanges are a position map, no row moves.
 //   2. Z = L11^-1 (the inverse of the unit lower triangle of the n pivot rows),
 //      by 32 x 32 diagonal inverses and block forward substitution.
@@ -37,10 +39,11 @@ constexpr int UM_NT = 384;              // threads per CTA
 constexpr int UM_NW = UM_NT / 32;
 constexpr int UM_NMAX = 128, UM_NRMAX = 16, UM_NXMAX = 16;
 constexpr int UM_TMEM_COLS = 512;
+constexpr int UM_BW = 16;  // panel column block of the LU (registers per row)
 
 struct UmmaLayout {
   int R, NP, LDP, Kpad, Nc, Npad, N0, N1, LBO_B;
-  unsigned szAhalf, offB, szBhalf, offZ, offLc, offSlot, bytes;
+  unsigned szAhalf, offB, szBhalf, offZ, offLc, bytes;
 };
 
 __host__ __device__ inline UmmaLayout umma_layout(const Dims& d) {
@@ -67,8 +70,7 @@ __host__ __device__ inline UmmaLayout umma_layout(const Dims& d) {
   if (L.offZ < L.offB) L.offZ = L.offB;
   L.offLc = L.offZ + (unsigned)(L.NP * L.LDP * 4);
   if (L.offLc < endB) L.offLc = endB;
-  L.offSlot = (L.offLc + (unsigned)(UM_NRMAX * n * 4) + 15u) & ~15u;
-  const unsigned endS = L.offSlot + 2u * UM_NW * 36u * 4u;
+  const unsigned endS = L.offLc + (unsigned)(UM_NRMAX * n * 4);
   L.bytes = endB > endS ? endB : endS;
   return L;
 }
@@ -280,17 +282,20 @@ __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a
   __shared__ int s_pivrow[UM_NMAX];               // pivot step -> row
   __shared__ __align__(8) uint64_t s_bar[2];
   __shared__ uint32_t s_taddr;
+  __shared__ int s_info;
+  __shared__ unsigned long long s_best[UM_BW];  // per pivot step: key | first position | warp
+  __shared__ int s_pivw[UM_BW];                 // per pivot step: the winning warp
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const Dims d = a.d;
   const int n = d.n, nr = d.nr, nb = d.nblock, n2 = 2 * n;
   const UmmaLayout L = umma_layout(d);
   const int R = L.R, LDP = L.LDP, NP = L.NP, Nc = L.Nc;
-  const int nwr = (R + 31) / 32;  // warps that own panel rows
+  const int nwc = (n2 + 31) / 32;  // warps that own pivot candidates
   const size_t nn = (size_t)n * n, nnx = (size_t)n * d.nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * d.nx;
   float* P = reinterpret_cast<float*>(smem_raw);
   float* Zf = reinterpret_cast<float*>(smem_raw + L.offZ);
   float* Lc = reinterpret_cast<float*>(smem_raw + L.offLc);  // [m][UM_NRMAX], zero past nr
-  float* slot = reinterpret_cast<float*>(smem_raw + L.offSlot);
+  float* slot = Zf;  // during the LU: [step][warp][UM_BW values, winner row]
   float* Xs = slab + (size_t)blockIdx.x * slab_elems;  // [col][position], 2n x Nc
 
   if (warp == 0) {
@@ -322,6 +327,8 @@ __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a
     // column c of the pair's U-row [D'_j E'_j B'_j] (n rows)
     auto ucol = [&](int c) -> float* { return c < n ? Dj + (size_t)c * n : c < n2 ? Ej + (size_t)(c - n) * n : Bj + (size_t)(c - n2) * n; };
     // ------------------------------------------------------------ panel load
+    if (tid == 0) s_info = 0;
+    if (tid < UM_BW) s_best[tid] = 0ull;
     // row t of [E_jp; D_j; C_j] by thread t
     if (tid < R) {
       float* dst = P + tid * LDP;
@@ -337,106 +344,129 @@ __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a
     __syncthreads();
     // --------------------------------------------------------------- panel LU
     int pos = tid, done = 0, info = 0;
-    float rv[32];
-    for (int kb = 0; kb < n && info == 0; kb += 32) {
-      const int w = n - kb < 32 ? n - kb : 32;
+    float rv[UM_BW];
+    for (int kb = 0; kb < n && info == 0; kb += UM_BW) {
+      const int w = n - kb < UM_BW ? n - kb : UM_BW;
       if (tid < R) {
         const float4* src = reinterpret_cast<const float4*>(P + tid * LDP + kb);
 #pragma unroll
-        for (int q4 = 0; q4 < 8; ++q4) {
+        for (int q4 = 0; q4 < UM_BW / 4; ++q4) {
           const float4 t = src[q4];
           rv[4 * q4] = t.x; rv[4 * q4 + 1] = t.y; rv[4 * q4 + 2] = t.z; rv[4 * q4 + 3] = t.w;
         }
       }
+      // pivot steps: only the warps with candidate rows take part (named barrier 1)
+      if (warp < nwc) {
 #pragma unroll
-      for (int i = 0; i < 32; ++i) {
-        if (i < w && info == 0) {
-          const int gi = kb + i;
-          float* slb = slot + (gi & 1) * UM_NW * 36;  // this step's candidate bank
-          if (warp < nwr) {
-            // the warp's candidate: largest |a|, then first position
-            const bool cand = tid < n2 && !done;
-            const uint32_t key = (cand && rv[i] == rv[i]) ? __float_as_uint(fabsf(rv[i])) : 0u;
-            const uint32_t cpos = cand ? (uint32_t)pos : 0xFFFFu;
-            const uint32_t kmax = __reduce_max_sync(0xFFFFFFFFu, key);
-            const uint32_t pmin = __reduce_min_sync(0xFFFFFFFFu, key == kmax ? cpos : 0xFFFFu);
-            float* sl = slb + warp * 36;
-            if (cand && key == kmax && cpos == pmin) {
-              float4* d4 = reinterpret_cast<float4*>(sl);
+        for (int i = 0; i < UM_BW; ++i) {
+          if (i < w && info == 0) {
+            const int gi = kb + i;
+            {
+              // the warp's candidate: largest |a|, then first position
+              const bool cand = tid < n2 && !done;
+              const uint32_t key = (cand && rv[i] == rv[i]) ? __float_as_uint(fabsf(rv[i])) : 0u;
+              const uint32_t kmax = __reduce_max_sync(0xFFFFFFFFu, key);
+              uint32_t bal = __ballot_sync(0xFFFFFFFFu, cand && key == kmax);
+              if (__popc(bal) > 1) {  // tie: the first position among them
+                const uint32_t pmin = __reduce_min_sync(0xFFFFFFFFu, (cand && key == kmax) ? (uint32_t)pos : 0xFFFFu);
+                bal = __ballot_sync(0xFFFFFFFFu, cand && key == kmax && (uint32_t)pos == pmin);
+              }
+              if (bal != 0u && lane == __ffs(bal) - 1) {
+                float* sl = slot + (i * UM_NW + warp) * (UM_BW + 4);
 #pragma unroll
-              for (int q4 = 0; q4 < 8; ++q4)
-                d4[q4] = make_float4(rv[4 * q4], rv[4 * q4 + 1], rv[4 * q4 + 2], rv[4 * q4 + 3]);
-              *reinterpret_cast<uint4*>(sl + 32) = make_uint4(kmax, pmin, (uint32_t)tid, 0u);
-            } else if (lane == 0 && pmin == 0xFFFFu) {
-              *reinterpret_cast<uint4*>(sl + 32) = make_uint4(0u, 0xFFFFu, 0xFFFFFFFFu, 0u);
+                for (int q4 = 0; q4 < UM_BW / 4; ++q4)
+                  reinterpret_cast<float4*>(sl)[q4] = make_float4(rv[4 * q4], rv[4 * q4 + 1], rv[4 * q4 + 2], rv[4 * q4 + 3]);
+                reinterpret_cast<int*>(sl)[UM_BW] = tid;
+                atomicMax(&s_best[i], ((unsigned long long)kmax << 32) |
+                                          ((unsigned long long)(0xFFFFu - (uint32_t)pos) << 16) | (unsigned)warp);
+              }
             }
-          }
-          __syncthreads();
-          // the winner over the warps' candidates, one lane per warp slot
-          uint32_t k2 = 0u, p2 = 0xFFFFu;
-          if (lane < nwr) {
-            const uint4 t = *reinterpret_cast<const uint4*>(slb + lane * 36 + 32);
-            k2 = t.x; p2 = t.y;
-          }
-          const uint32_t kw = __reduce_max_sync(0xFFFFFFFFu, k2);
-          const uint32_t pw = __reduce_min_sync(0xFFFFFFFFu, k2 == kw ? p2 : 0xFFFFu);
-          const uint32_t bal = __ballot_sync(0xFFFFFFFFu, lane < nwr && k2 == kw && p2 == pw);
-          const float* win = slb + (bal ? __ffs(bal) - 1 : 0) * 36;
-          const int wt = reinterpret_cast<const int*>(win)[34];
-          const float pv = win[i];
-          if (pv == 0.0f || wt < 0 || pw == 0xFFFFu) {
-            info = gi + 1;
-          } else {
-            if (tid == 0) s_pivrow[gi] = wt;
-            if (pos == gi) pos = (int)pw;
-            if (tid == wt) { pos = gi; done = 1; }
-            if (tid < R && !done) {
-              const float l = rv[i] * __frcp_rn(pv);
-              rv[i] = l;
+            asm volatile("bar.sync 1, %0;" ::"r"(nwc * 32) : "memory");
+            const unsigned long long bst = *reinterpret_cast<volatile unsigned long long*>(&s_best[i]);
+            const int bw = (int)(bst & 0xFFFFu);
+            const float* win = slot + (i * UM_NW + bw) * (UM_BW + 4);
+            const int wt = reinterpret_cast<const int*>(win)[UM_BW];
+            const float pv = win[i];
+            if (bst == 0ull || pv == 0.0f) {
+              info = gi + 1;
+            } else {
+              if (tid == 0) { s_pivrow[gi] = wt; s_pivw[i] = bw; }
+              if (pos == gi) pos = (int)(0xFFFFu - (uint32_t)((bst >> 16) & 0xFFFFu));
+              if (tid == wt) { pos = gi; done = 1; }
+              if (tid < R && !done) {
+                float rinv;
+                asm("rcp.approx.f32 %0, %1;" : "=f"(rinv) : "f"(pv));
+                const float l = rv[i] * rinv;
+                rv[i] = l;
 #pragma unroll
-              for (int q4 = (i + 1) / 4; q4 < 8; ++q4) {
-                const float4 u4 = *reinterpret_cast<const float4*>(win + 4 * q4);
-                if (4 * q4 > i) rv[4 * q4] = fmaf(-l, u4.x, rv[4 * q4]);
-                if (4 * q4 + 1 > i) rv[4 * q4 + 1] = fmaf(-l, u4.y, rv[4 * q4 + 1]);
-                if (4 * q4 + 2 > i) rv[4 * q4 + 2] = fmaf(-l, u4.z, rv[4 * q4 + 2]);
-                if (4 * q4 + 3 > i) rv[4 * q4 + 3] = fmaf(-l, u4.w, rv[4 * q4 + 3]);
+                for (int q4 = (i + 1) / 4; q4 < UM_BW / 4; ++q4) {
+                  const float4 u4 = *reinterpret_cast<const float4*>(win + 4 * q4);
+                  if (4 * q4 > i) rv[4 * q4] = fmaf(-l, u4.x, rv[4 * q4]);
+                  if (4 * q4 + 1 > i) rv[4 * q4 + 1] = fmaf(-l, u4.y, rv[4 * q4 + 1]);
+                  if (4 * q4 + 2 > i) rv[4 * q4 + 2] = fmaf(-l, u4.z, rv[4 * q4 + 2]);
+                  if (4 * q4 + 3 > i) rv[4 * q4 + 3] = fmaf(-l, u4.w, rv[4 * q4 + 3]);
+                }
               }
             }
           }
         }
+        if (tid == 0) s_info = info;
       }
-      if (info != 0) break;
+      __syncthreads();
+      info = s_info;
+      // border rows of warps without candidates: the block's eliminations in order
+      if (warp >= nwc && tid < R && info == 0) {
+#pragma unroll
+        for (int i = 0; i < UM_BW; ++i) {
+          if (i < w) {
+            const float* win = slot + (i * UM_NW + s_pivw[i]) * (UM_BW + 4);
+            float rinv;
+            asm("rcp.approx.f32 %0, %1;" : "=f"(rinv) : "f"(win[i]));
+            const float l = rv[i] * rinv;
+            rv[i] = l;
+#pragma unroll
+            for (int q4 = (i + 1) / 4; q4 < UM_BW / 4; ++q4) {
+              const float4 u4 = *reinterpret_cast<const float4*>(win + 4 * q4);
+              if (4 * q4 > i) rv[4 * q4] = fmaf(-l, u4.x, rv[4 * q4]);
+              if (4 * q4 + 1 > i) rv[4 * q4 + 1] = fmaf(-l, u4.y, rv[4 * q4 + 1]);
+              if (4 * q4 + 2 > i) rv[4 * q4 + 2] = fmaf(-l, u4.z, rv[4 * q4 + 2]);
+              if (4 * q4 + 3 > i) rv[4 * q4 + 3] = fmaf(-l, u4.w, rv[4 * q4 + 3]);
+            }
+          }
+        }
+      }
       if (tid < R) {
         float4* dst = reinterpret_cast<float4*>(P + tid * LDP + kb);
 #pragma unroll
-        for (int q4 = 0; q4 < 8; ++q4)
+        for (int q4 = 0; q4 < UM_BW / 4; ++q4)
           dst[q4] = make_float4(rv[4 * q4], rv[4 * q4 + 1], rv[4 * q4 + 2], rv[4 * q4 + 3]);
       }
+      if (tid < UM_BW) s_best[tid] = 0ull;  // read by every candidate warp before the barrier above
       __syncthreads();
-      if (kb + 32 < n) {  // w == 32 here
-        int ro[32];
+      if (kb + UM_BW < n) {  // w == UM_BW here
+        int ro[UM_BW];
 #pragma unroll
-        for (int m = 0; m < 32; ++m) ro[m] = s_pivrow[kb + m] * LDP;
+        for (int m = 0; m < UM_BW; ++m) ro[m] = s_pivrow[kb + m] * LDP;
         // the block's U rows in the panel columns right of it: unit lower solve
-        for (int c = kb + 32 + tid; c < n; c += UM_NT) {
-          float y[32];
+        for (int c = kb + UM_BW + tid; c < n; c += UM_NT) {
+          float y[UM_BW];
 #pragma unroll
-          for (int r = 0; r < 32; ++r) y[r] = P[ro[r] + c];
+          for (int r = 0; r < UM_BW; ++r) y[r] = P[ro[r] + c];
 #pragma unroll
-          for (int m = 0; m < 32; ++m)
+          for (int m = 0; m < UM_BW; ++m)
 #pragma unroll
-            for (int r = m + 1; r < 32; ++r) y[r] = fmaf(-P[ro[r] + kb + m], y[m], y[r]);
+            for (int r = m + 1; r < UM_BW; ++r) y[r] = fmaf(-P[ro[r] + kb + m], y[m], y[r]);
 #pragma unroll
-          for (int r = 0; r < 32; ++r) P[ro[r] + c] = y[r];
+          for (int r = 0; r < UM_BW; ++r) P[ro[r] + c] = y[r];
         }
         __syncthreads();
-        // the rows that are not pivots yet: one product of depth 32
+        // the rows that are not pivots yet: one product of depth UM_BW
         if (tid < R && !done) {
           float* row = P + tid * LDP;
-          for (int c = kb + 32; c < n; c += 4) {
+          for (int c = kb + UM_BW; c < n; c += 4) {
             float4 acc = *reinterpret_cast<float4*>(row + c);
 #pragma unroll
-            for (int m = 0; m < 32; ++m) {
+            for (int m = 0; m < UM_BW; ++m) {
               const float4 u = *reinterpret_cast<const float4*>(P + ro[m] + c);
               acc.x = fmaf(-rv[m], u.x, acc.x);
               acc.y = fmaf(-rv[m], u.y, acc.y);
