@@ -12,8 +12,10 @@ Workload (one "step" = factorize + solve of one system):
 
   variants: the mixed path (FP32 factors + FP64 refinement to rel. residual
           <= 1e-12) on the same workload; FP64 and mixed on n=32, nblock=65536,
-          nr=nx=8; and a batch of 4096 uneven systems (systems/s, p50/p99 of the
-          batch latency), each through its own CUDA graph, device-timed.
+          nr=nx=8 and on n=128, nblock=8192, qr=qx=4, nr=nx=16 (the mixed pair
+          kernel there runs its products on the tcgen05 tensor cores); and a
+          batch of 4096 uneven systems (systems/s, p50/p99 of the batch
+          latency), each through its own CUDA graph, device-timed.
 
 The matrix (0.65 GB) is larger than L2 (126 MB), so no L2 flush is needed
 between steps.  Multi-GPU: one process per GPU, each solving its own system
@@ -359,7 +361,7 @@ def graph_step_time(torch, bcr, h, s, b, steps, warmup, prec):
 
 def variants(torch, bcr, synth, steps, warmup, rank):
     """The other measured paths: the mixed path on this workload, both paths on
-    the n=32 workload, and the batch of 4096 uneven systems."""
+    the n=32 and n=128 workloads, and the batch of 4096 uneven systems."""
     out = {}
     sB = synth.collocation(**CFG, seed=rank)
     bB = synth.rhs(sB, 1, seed=1 + rank)[0]
@@ -379,6 +381,18 @@ def variants(torch, bcr, synth, steps, warmup, rank):
     out["C_fp64"] = dict(f64, workload=wl)
     out["C_mixed"] = dict(mix, workload=wl)
     out["C_mixed_over_fp64"] = mix["value"] / f64["value"]
+    cE = dict(synth.CONFIGS["E"])
+    sE = synth.collocation(**cE, seed=rank)
+    bE = synth.rhs(sE, 1, seed=1 + rank)[0]
+    hE = bcr.BorderedCR()
+    hE.load_system(sE)
+    f64 = graph_step_time(torch, bcr, hE, sE, bE, steps, warmup, bcr.PRECISION_FP64)
+    mix = graph_step_time(torch, bcr, hE, sE, bE, steps, warmup, bcr.PRECISION_MIXED)
+    del hE, sE
+    wl = "trapezoid-collocation BABD n=128 nblock=8192 qr=qx=4 nr=nx=16, 1 rhs"
+    out["E_fp64"] = dict(f64, workload=wl, pair_kernel="FP64 blocked LU, DMMA products")
+    out["E_mixed"] = dict(mix, workload=wl, pair_kernel="FP32 LU, tcgen05 3xTF32 products")
+    out["E_mixed_over_fp64"] = mix["value"] / f64["value"]
     for name, prec in (("D_batched_fp64", bcr.PRECISION_FP64), ("D_batched_mixed", bcr.PRECISION_MIXED)):
         try:
             out[name] = batched(torch, bcr, synth, rank, prec)
