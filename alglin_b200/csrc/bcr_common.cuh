@@ -55,7 +55,10 @@ struct BatchCta {
 };
 
 // factorization of the last block actually in use (written by the device)
-enum LastFact : int { FACT_LU = 0, FACT_LUPQ = 1, FACT_QR = 2, FACT_QRP = 3, FACT_SVD = 4, FACT_SVD_T = 5 };
+// FACT_LU_ROWS: getrf factors with the rows left in place, piv[pos] = the row
+// holding position pos of L\U (the blocked last-block LU)
+enum LastFact : int { FACT_LU = 0, FACT_LUPQ = 1, FACT_QR = 2, FACT_QRP = 3, FACT_SVD = 4, FACT_SVD_T = 5,
+                      FACT_LU_ROWS = 6 };
 
 // status layout: [0] code, [1] block index, [2] LAPACK-style info, [3] level,
 // [4] LastFact of the last block

@@ -1291,6 +1291,7 @@ __global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
 // ---------------------------------------------------------------------------
 constexpr int BLK_W = 32;
 constexpr int BLK_ROWS_MAX = 512;  // 2n + nr of the blocked kernel
+constexpr int LAST_BLOCKED_MIN = 64;  // last blocks of this order and above: blocked LU
 
 // W[c*R + rowp[r]] -= sum_m L[m*LD + r] * W[c*R + rowp[k0 + m]] for positions r in
 // [r0, R), c in [c0, NC), m < w; L: the factored block in shared memory (column m,
@@ -1382,12 +1383,90 @@ __device__ void blk_update(T* W, int R, int NC, const T* Lsm, int LD, int k0, in
   }
 }
 
+// Blocked right-looking LU of the first npiv columns of the R x NC column-major
+// matrix W (ld R) by one CTA: the getrf pivot rule among positions [i, ncand)
+// (rows at positions >= ncand are eliminated but never pivots), the
+// interchanges kept in the position -> row map s_perm (rows of W never move;
+// s_perm holds the identity on entry), each block of BLK_W columns factored in
+// shared memory Pb (BLK_W x R), the block's rows of the columns right of it
+// solved with its unit lower triangle, the rows below updated with one product
+// of depth BLK_W.  Returns the LAPACK info: 0, or the first zero pivot + 1.
+template <typename T>
+__device__ int blk_eliminate(T* W, int R, int NC, int npiv, int ncand, T* Pb, int* s_perm, T* sv, int* si) {
+  const int tid = threadIdx.x, bs = blockDim.x;
+  int info = 0;
+  for (int kb = 0; kb < npiv && info == 0; kb += BLK_W) {
+    const int w = npiv - kb < BLK_W ? npiv - kb : BLK_W;
+    // stage the block's columns (all rows) in shared memory
+    for (int e = tid; e < w * R; e += bs) {
+      const int r = e % R, c = e / R;
+      Pb[(size_t)c * R + r] = W[(size_t)(kb + c) * R + s_perm[r]];
+    }
+    __syncthreads();
+    for (int i = 0; i < w; ++i) {
+      const int gi = kb + i;
+      T* ci = Pb + (size_t)i * R;
+      T best = T(-1);
+      int bi = gi;  // stays in range even when every candidate is NaN
+      for (int r = gi + tid; r < ncand; r += bs) {
+        const T v = dev_abs(ci[r]);
+        if (v > best) { best = v; bi = r; }
+      }
+      block_argmax(best, bi, sv, si);
+      const T pv = ci[bi];
+      __syncthreads();  // every thread holds the pivot before the rows are swapped
+      if (pv == T(0)) { info = gi + 1; break; }
+      if (bi != gi && tid < w) {
+        T* col = Pb + (size_t)tid * R;
+        const T t = col[gi]; col[gi] = col[bi]; col[bi] = t;
+      }
+      if (bi != gi && tid == w) { const int t = s_perm[gi]; s_perm[gi] = s_perm[bi]; s_perm[bi] = t; }
+      __syncthreads();
+      // one thread per row below the pivot: its multiplier, then its update
+      const T rinv = T(1) / pv;
+      for (int r = gi + 1 + tid; r < R; r += bs) {
+        const T l = ci[r] * rinv;
+        ci[r] = l;
+        for (int c = i + 1; c < w; ++c) Pb[(size_t)c * R + r] -= l * Pb[(size_t)c * R + gi];
+      }
+      __syncthreads();
+    }
+    if (info != 0) break;
+    // the factored block back to the slab (by position)
+    for (int e = tid; e < w * R; e += bs) {
+      const int r = e % R, c = e / R;
+      W[(size_t)(kb + c) * R + s_perm[r]] = Pb[(size_t)c * R + r];
+    }
+    __syncthreads();
+    // rows [kb, kb+w) of the columns right of the block: unit lower solve
+    for (int c = kb + w + tid; c < NC; c += bs) {
+      T* col = W + (size_t)c * R;
+      T y[BLK_W];
+#pragma unroll
+      for (int r = 0; r < BLK_W; ++r) y[r] = r < w ? col[s_perm[kb + r]] : T(0);
+#pragma unroll
+      for (int m = 0; m < BLK_W; ++m) {
+#pragma unroll
+        for (int r = m + 1; r < BLK_W; ++r)
+          if (r < w) y[r] = fma(-Pb[(size_t)m * R + kb + r], y[m], y[r]);
+      }
+#pragma unroll
+      for (int r = 0; r < BLK_W; ++r)
+        if (r < w) col[s_perm[kb + r]] = y[r];
+    }
+    __syncthreads();
+    // rows below the block: one product of depth w
+    blk_update<T>(W, R, NC, Pb, R, kb, w, kb + w, kb + w, s_perm);
+    __syncthreads();
+  }
+  return info;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T* slab, size_t slab_elems) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ T sv[32];
   __shared__ int si[32];
-  __shared__ int s_piv[256];
   __shared__ int s_perm[BLK_ROWS_MAX];  // position -> row of the slab (rows never move)
   const int tid = threadIdx.x, bs = blockDim.x;
   const Dims d = a.d;
@@ -1448,74 +1527,7 @@ __global__ void __launch_bounds__(256, 2) k_factor_lu_blocked(FactorArgs<T> a, T
     for (int r = tid; r < R; r += bs) s_perm[r] = r;
     __syncthreads();
     // ------------------------------------------------- blocked elimination
-    // the interchanges are kept as the position -> row map s_perm; a block is
-    // staged by position, so no row of the slab is ever moved
-    int info = 0;
-    for (int kb = 0; kb < n && info == 0; kb += BLK_W) {
-      const int w = n - kb < BLK_W ? n - kb : BLK_W;
-      // stage the block's columns (all rows) in shared memory
-      for (int e = tid; e < w * R; e += bs) {
-        const int r = e % R, c = e / R;
-        Pb[(size_t)c * R + r] = W[(size_t)(kb + c) * R + s_perm[r]];
-      }
-      __syncthreads();
-      for (int i = 0; i < w; ++i) {
-        const int gi = kb + i;
-        T* ci = Pb + (size_t)i * R;
-        T best = T(-1);
-        int bi = gi;  // stays in range even when every candidate is NaN
-        for (int r = gi + tid; r < n2; r += bs) {
-          const T v = dev_abs(ci[r]);
-          if (v > best) { best = v; bi = r; }
-        }
-        block_argmax(best, bi, sv, si);
-        if (tid == 0) s_piv[gi] = bi;
-        const T pv = ci[bi];
-        __syncthreads();  // every thread holds the pivot before the rows are swapped
-        if (pv == T(0)) { info = gi + 1; break; }
-        if (bi != gi && tid < w) {
-          T* col = Pb + (size_t)tid * R;
-          const T t = col[gi]; col[gi] = col[bi]; col[bi] = t;
-        }
-        if (bi != gi && tid == w) { const int t = s_perm[gi]; s_perm[gi] = s_perm[bi]; s_perm[bi] = t; }
-        __syncthreads();
-        // one thread per row below the pivot: its multiplier, then its update
-        const T rinv = T(1) / pv;
-        for (int r = gi + 1 + tid; r < R; r += bs) {
-          const T l = ci[r] * rinv;
-          ci[r] = l;
-          for (int c = i + 1; c < w; ++c) Pb[(size_t)c * R + r] -= l * Pb[(size_t)c * R + gi];
-        }
-        __syncthreads();
-      }
-      if (info != 0) break;
-      // the factored block back to the slab (by position)
-      for (int e = tid; e < w * R; e += bs) {
-        const int r = e % R, c = e / R;
-        W[(size_t)(kb + c) * R + s_perm[r]] = Pb[(size_t)c * R + r];
-      }
-      __syncthreads();
-      // rows [kb, kb+w) of the columns right of the block: unit lower solve
-      for (int c = kb + w + tid; c < NC; c += bs) {
-        T* col = W + (size_t)c * R;
-        T y[BLK_W];
-#pragma unroll
-        for (int r = 0; r < BLK_W; ++r) y[r] = r < w ? col[s_perm[kb + r]] : T(0);
-#pragma unroll
-        for (int m = 0; m < BLK_W; ++m) {
-#pragma unroll
-          for (int r = m + 1; r < BLK_W; ++r)
-            if (r < w) y[r] = fma(-Pb[(size_t)m * R + kb + r], y[m], y[r]);
-        }
-#pragma unroll
-        for (int r = 0; r < BLK_W; ++r)
-          if (r < w) col[s_perm[kb + r]] = y[r];
-      }
-      __syncthreads();
-      // rows below the block: one product of depth w
-      blk_update<T>(W, R, NC, Pb, R, kb, w, kb + w, kb + w, s_perm);
-      __syncthreads();
-    }
+    const int info = blk_eliminate<T>(W, R, NC, n, n2, Pb, s_perm, sv, si);
     if (info != 0) {
       if (tid == 0) report(a.st, DEV_ZERO_PIVOT, j, info, k);
       __syncthreads();
@@ -2779,6 +2791,16 @@ __device__ void last_solve_body(Dims d, LastBufs lb, const StatusWords* st, T* x
           for (int r = i + 1 + tid; r < N; r += bs) b[r] -= A[(size_t)i * N + r] * bi;
           __syncthreads();
         }
+      } else if (kind == FACT_LU_ROWS) {
+        for (int r = tid; r < N; r += bs) tmp[r] = b[piv[r]];
+        __syncthreads();
+        for (int r = tid; r < N; r += bs) b[r] = tmp[r];
+        __syncthreads();
+        for (int i = 0; i < N; ++i) {
+          const T bi = b[i];
+          for (int r = i + 1 + tid; r < N; r += bs) b[r] -= A[(size_t)i * N + piv[r]] * bi;
+          __syncthreads();
+        }
       } else {
         for (int i = 0; i < N; ++i) {
           const T* v = A + (size_t)i * M;
@@ -2792,12 +2814,13 @@ __device__ void last_solve_body(Dims d, LastBufs lb, const StatusWords* st, T* x
           __syncthreads();
         }
       }
-      const int lda = (kind == FACT_LU || kind == FACT_LUPQ) ? N : M;
+      const int lda = (kind == FACT_LU || kind == FACT_LUPQ || kind == FACT_LU_ROWS) ? N : M;
+      const bool rows = kind == FACT_LU_ROWS;  // row of position r: piv[r]
       for (int i = N - 1; i >= 0; --i) {
-        const T xi = b[i] / A[(size_t)i * lda + i];
+        const T xi = b[i] / A[(size_t)i * lda + (rows ? piv[i] : i)];
         __syncthreads();
         if (tid == 0) b[i] = xi;
-        for (int r = tid; r < i; r += bs) b[r] -= A[(size_t)i * lda + r] * xi;
+        for (int r = tid; r < i; r += bs) b[r] -= A[(size_t)i * lda + (rows ? piv[r] : r)] * xi;
         __syncthreads();
       }
       if (kind == FACT_LUPQ) {
@@ -2825,6 +2848,31 @@ __device__ void last_solve_body(Dims d, LastBufs lb, const StatusWords* st, T* x
 template <typename T>
 __global__ void k_last_factor(Dims d, LastBufs b, int sel_last, StatusWords* st) {
   last_factor_body<T>(d, b, sel_last, st);
+}
+
+// load_and_factorize_last with LU for larger blocks (cc:1319-1346, getrf): the
+// blocked elimination of the pair kernels on the whole block, FP64 tensor-core
+// products, rows left in place (kind FACT_LU_ROWS, piv[pos] = row)
+__global__ void __launch_bounds__(256, 1) k_last_lu_blocked(Dims d, LastBufs b, StatusWords* st) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double sv[32];
+  __shared__ int si[32];
+  __shared__ int s_perm[BLK_ROWS_MAX];
+  const int N = d.Nc, tid = threadIdx.x;
+  if (d.Nr != N || N > BLK_ROWS_MAX) {
+    if (tid == 0) report(st, DEV_BAD_SHAPE, -1, 0, -1);
+    return;
+  }
+  for (int r = tid; r < N; r += blockDim.x) s_perm[r] = r;
+  __syncthreads();
+  double* Pb = reinterpret_cast<double*>(smem_raw);
+  const int info = blk_eliminate<double>(b.A, N, N, N, N, Pb, s_perm, sv, si);
+  if (info != 0) {
+    if (tid == 0) report(st, DEV_LAST_SINGULAR, -1, info, -1);
+    return;
+  }
+  for (int r = tid; r < N; r += blockDim.x) b.piv[r] = s_perm[r];
+  if (tid == 0) st->kind = FACT_LU_ROWS;
 }
 
 __global__ void k_last_fallback(Dims d, LastBufs b, StatusWords* st) { last_fallback_body(d, b, st); }
@@ -3155,8 +3203,15 @@ static void factor_last(DevState& s, const WorkSet<T>& w, cudaStream_t st) {
     cudaMemcpyAsync(s.Al, s.Hl, (size_t)d.Nr * d.Nc * 8, cudaMemcpyDeviceToDevice, st);
   }
   const LastBufs lb = last_bufs(s);
-  k_last_factor<double><<<1, 512, 0, st>>>(d, lb, s.sel_last, s.st);
-  check_launch("k_last_factor");
+  if (s.sel_last == LAST_LU && d.Nr == d.Nc && d.Nc >= LAST_BLOCKED_MIN && d.Nc <= BLK_ROWS_MAX) {
+    const size_t sm = (size_t)BLK_W * d.Nc * sizeof(double);
+    smem_limit_once(k_last_lu_blocked, sm);
+    k_last_lu_blocked<<<1, 256, sm, st>>>(d, lb, s.st);
+    check_launch("k_last_lu_blocked");
+  } else {
+    k_last_factor<double><<<1, 512, 0, st>>>(d, lb, s.sel_last, s.st);
+    check_launch("k_last_factor");
+  }
   if (s.sel_last2) {
     k_last_fallback<<<1, 512, 0, st>>>(d, lb, s.st);
     check_launch("k_last_fallback");

@@ -285,3 +285,43 @@ def test_gpu_fallback_not_used_when_primary_succeeds():
     h2 = gpu_solver(s, "LU", "LU", "PINV")
     assert h1.factorize() and h2.factorize()
     assert np.array_equal(gpu_solve(h1, b), gpu_solve(h2, b))
+
+
+@pytest.mark.parametrize("dims", [(6, 30, 2, 2, 1, 1), (6, 31, 1, 1, 1, 1), (9, 40, 3, 3, 4, 4),
+                                  (5, 128, 4, 4, 16, 16)])
+def test_gpu_blocked_last_block_lu(dims):
+    """Last blocks of order 64 and above are factored by the blocked LU (rows
+    left in place); 63 stays on the unblocked one: both against the oracle."""
+    s = synth.collocation(*dims, seed=sum(dims) + 7)
+    assert s.Nr == s.Nc
+    b = synth.rhs(s, nrhs=2, seed=6)
+    o = po.Oracle(s, "LU", "LU")
+    assert o.factorize(), o.last_error()
+    xo = o.solve(b)
+    h = gpu_solver(s, "LU", "LU")
+    assert h.factorize(), h.last_error()
+    xg = gpu_solve(h, b)
+    for c in range(2):
+        assert fwd_err(xg[c, :s.ncols], xo[c, :s.ncols]) < 1e-10
+        assert relres(o, s, xg[c], b[c]) <= 1e-13
+
+
+def test_gpu_blocked_last_block_singular_falls_back():
+    """A singular last block of order 66 (zero boundary rows): LU reports it, and
+    with select_last2 the minimum-norm solution matches the oracle's."""
+    s = synth.collocation(9, 32, 0, 0, 2, 2, seed=5)
+    s.H[:] = 0.0
+    assert s.Nr == 66
+    h = gpu_solver(s, "LU", "LU", "NONE")
+    assert not h.factorize()
+    assert "load_and_factorize_last" in h.last_error()
+    o = po.Oracle(s, "LU", "LU", "PINV")
+    assert o.factorize(), o.last_error()
+    xref = synth.rhs(s, nrhs=1, seed=9)[0][:s.ncols]
+    b = np.zeros((1, s.nrows))
+    b[0] = o.mv(xref)
+    xo = o.solve(b)[0]
+    h2 = gpu_solver(s, "LU", "LU", "PINV")
+    assert h2.factorize(), h2.last_error()
+    xg = gpu_solve(h2, b)[0]
+    assert fwd_err(xg[:s.ncols], xo[:s.ncols]) < 1e-8
