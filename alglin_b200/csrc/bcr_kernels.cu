@@ -2257,6 +2257,7 @@ __global__ void __launch_bounds__(256) k_forward_cta(SweepArgs<TF> a0, const Swe
                                                      const BatchCta* cmap) {
   constexpr unsigned FULL = 0xffffffffu;
   __shared__ double w[2 * SWP_MAXN];
+  __shared__ double tb[32][33];  // diagonal 32 x 32 block of the triangle
   const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5;
   SweepArgs<TF> ab;
   long q0, q1, qs;
@@ -2280,18 +2281,31 @@ __global__ void __launch_bounds__(256) k_forward_cta(SweepArgs<TF> a0, const Swe
       // unit lower L on positions [0, n), then the rows below: w -= T(:, c) w[c]
       for (int cb = 0; cb < n; cb += 32) {
         const int cw = n - cb < 32 ? n - cb : 32;
+        // the diagonal block of L through shared memory (one coalesced load)
+        for (int e = tid; e < cw * 32; e += bs) {
+          const int c = e >> 5, r = e & 31;
+          tb[c][r] = r < cw ? double(Tj[(size_t)(cb + c) * n2 + cb + r]) : 0.0;
+        }
+        __syncthreads();
         if (warp == 0) {
           double v = lane < cw ? w[cb + lane] : 0.0;
           for (int c = 0; c < cw; ++c) {
             const double vc = __shfl_sync(FULL, v, c);
-            if (lane > c && lane < cw) v = fma(-double(Tj[(size_t)(cb + c) * n2 + cb + lane]), vc, v);
+            if (lane > c && lane < cw) v = fma(-tb[c][lane], vc, v);
           }
           if (lane < cw) w[cb + lane] = v;
         }
         __syncthreads();
         for (int r = cb + cw + tid; r < n2; r += bs) {
           double s = w[r];
-          for (int c = 0; c < cw; ++c) s = fma(-double(Tj[(size_t)(cb + c) * n2 + r]), w[cb + c], s);
+          for (int c0 = 0; c0 < cw; c0 += 8) {  // 8 loads in flight
+            double tv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) tv[u] = c0 + u < cw ? double(Tj[(size_t)(cb + c0 + u) * n2 + r]) : 0.0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+              if (c0 + u < cw) s = fma(-tv[u], w[cb + c0 + u], s);
+          }
           w[r] = s;
         }
         __syncthreads();
@@ -2317,6 +2331,7 @@ __global__ void __launch_bounds__(256) k_backward_cta(SweepArgs<TF> a0, const Sw
   constexpr unsigned FULL = 0xffffffffu;
   __shared__ double xa[SWP_MAXN], xz[SWP_MAXN], y[SWP_MAXN];
   __shared__ double part[256];
+  __shared__ double tb[32][33];  // diagonal 32 x 32 block of the triangle
   const int tid = threadIdx.x, bs = blockDim.x, lane = tid & 31, warp = tid >> 5;
   SweepArgs<TF> ab;
   long q0, q1, qs;
@@ -2347,9 +2362,22 @@ __global__ void __launch_bounds__(256) k_backward_cta(SweepArgs<TF> a0, const Sw
         const int i = tid % n, g = tid / n;
         double s = 0.0;
         if (g < G) {
-          for (int c = g; c < n; c += G) {
-            s = fma(double(Dj[(size_t)c * n + i]), xa[c], s);
-            s = fma(double(Ej[(size_t)c * n + i]), xz[c], s);
+          for (int c0 = g; c0 < n; c0 += 4 * G) {  // 8 loads in flight
+            double dv[4], ev[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int c = c0 + u * G;
+              dv[u] = c < n ? double(Dj[(size_t)c * n + i]) : 0.0;
+              ev[u] = c < n ? double(Ej[(size_t)c * n + i]) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int c = c0 + u * G;
+              if (c < n) {
+                s = fma(dv[u], xa[c], s);
+                s = fma(ev[u], xz[c], s);
+              }
+            }
           }
           for (int c = g; c < nx; c += G) s = fma(double(Bj[(size_t)c * n + i]), xc[xb_off + c], s);
         }
@@ -2365,20 +2393,33 @@ __global__ void __launch_bounds__(256) k_backward_cta(SweepArgs<TF> a0, const Sw
       // U y = rhs, from the last block of 32 rows up
       for (int rb = ((n - 1) / 32) * 32; rb >= 0; rb -= 32) {
         const int rw = n - rb < 32 ? n - rb : 32;
+        // the diagonal block of U through shared memory (one coalesced load)
+        for (int e = tid; e < rw * 32; e += bs) {
+          const int c = e >> 5, r = e & 31;
+          tb[c][r] = r < rw ? double(Tj[(size_t)(rb + c) * n2 + rb + r]) : 0.0;
+        }
+        __syncthreads();
         if (warp == 0) {
           double v = lane < rw ? y[rb + lane] : 0.0;
-          const double rdi = lane < rw ? 1.0 / double(Tj[(size_t)(rb + lane) * n2 + rb + lane]) : 0.0;
+          const double rdi = lane < rw ? 1.0 / tb[lane][lane] : 0.0;
           for (int ii = rw - 1; ii >= 0; --ii) {
             const double xi = __shfl_sync(FULL, v * rdi, ii);
             if (lane == ii) v = xi;
-            else if (lane < ii) v = fma(-double(Tj[(size_t)(rb + ii) * n2 + rb + lane]), xi, v);
+            else if (lane < ii) v = fma(-tb[ii][lane], xi, v);
           }
           if (lane < rw) y[rb + lane] = v;
         }
         __syncthreads();
         for (int r = tid; r < rb; r += bs) {
           double s = y[r];
-          for (int c = 0; c < rw; ++c) s = fma(-double(Tj[(size_t)(rb + c) * n2 + r]), y[rb + c], s);
+          for (int c0 = 0; c0 < rw; c0 += 8) {  // 8 loads in flight
+            double tv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) tv[u] = c0 + u < rw ? double(Tj[(size_t)(rb + c0 + u) * n2 + r]) : 0.0;
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+              if (c0 + u < rw) s = fma(-tv[u], y[rb + c0 + u], s);
+          }
           y[r] = s;
         }
         __syncthreads();
