@@ -40,6 +40,7 @@ constexpr int UM_NW = UM_NT / 32;
 constexpr int UM_NMAX = 128, UM_NRMAX = 16, UM_NXMAX = 16;
 constexpr int UM_TMEM_COLS = 512;
 constexpr int UM_BW = 16;  // panel column block of the LU (registers per row)
+constexpr int UM_PF = 12;  // B-operand elements per thread and stage: 16 * (2n + nx) <= UM_PF * UM_NT
 
 struct UmmaLayout {
   int R, NP, LDP, Kpad, Nc, Npad, N0, N1, LBO_B;
@@ -178,7 +179,17 @@ __device__ bool umma_product(const UmmaLayout& L, unsigned char* sm, uint64_t* b
   const int tid = threadIdx.x;
   const int S = L.Kpad / 16;
   const uint32_t sA = smem_u32(sm);
-  const int cnt = 16 * L.Npad;
+  const int cnt = 16 * L.Npad;  // <= UM_PF * UM_NT
+  // the next stage's elements are loaded one stage ahead, into registers
+  float pv[UM_PF];
+  auto load_stage = [&](int s) {
+#pragma unroll
+    for (int u = 0; u < UM_PF; ++u) {
+      const int e = tid + u * UM_NT;
+      pv[u] = e < cnt ? src(e >> 4, 16 * s + (e & 15)) : 0.0f;
+    }
+  };
+  load_stage(0);
   bool ok = true;
   for (int s = 0; s < S; ++s) {
     const int b = s & 1;
@@ -189,15 +200,20 @@ __device__ bool umma_product(const UmmaLayout& L, unsigned char* sm, uint64_t* b
     if (ok) {
       unsigned char* bh = sm + L.offB + (unsigned)b * 2u * L.szBhalf;
       unsigned char* bl = bh + L.szBhalf;
-      um_batched(cnt, [&](int e) { return src(e >> 4, 16 * s + (e & 15)); }, [&](int e, float v) {
-        const float h = tf32_hi(v);
-        const uint32_t o = umma_b_off(e >> 4, e & 15, L.LBO_B);
-        *reinterpret_cast<float*>(bh + o) = h;
-        *reinterpret_cast<float*>(bl + o) = v - h;
-      });
+#pragma unroll
+      for (int u = 0; u < UM_PF; ++u) {
+        const int e = tid + u * UM_NT;
+        if (e < cnt) {
+          const float h = tf32_hi(pv[u]);
+          const uint32_t o = umma_b_off(e >> 4, e & 15, L.LBO_B);
+          *reinterpret_cast<float*>(bh + o) = h;
+          *reinterpret_cast<float*>(bl + o) = pv[u] - h;
+        }
+      }
     }
     fence_async_smem();
     if (__syncthreads_or(!ok)) return false;
+    if (s + 1 < S) load_stage(s + 1);
     if (tid == 0) {
       tc_fence_after();
       const uint32_t sB = smem_u32(sm + L.offB + (unsigned)b * 2u * L.szBhalf);
@@ -525,8 +541,8 @@ __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a
       for (int c = 32 * (tid / 32 + 1); c < NP; c += 4)
         *reinterpret_cast<float4*>(Zf + tid * LDP + c) = make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    if (warp < NP / 32) {  // diagonal 32 x 32 inverses, one column per lane
-      const int a32 = warp * 32, c = lane;
+    if (warp >= UM_NW - NP / 32) {  // diagonal 32 x 32 inverses, one column per lane, on the
+      const int a32 = (warp - (UM_NW - NP / 32)) * 32, c = lane;  // warps the position copy leaves idle
       float z[32];
 #pragma unroll
       for (int r = 0; r < 32; ++r) {
@@ -601,10 +617,16 @@ __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a
         float v[16];
         tmem_ld16(tmem + ((uint32_t)(32 * qd) << 16) + (uint32_t)(16 * pc), v);
         if (m < n) {
+          if ((n & 15) == 0 && 16 * pc + 16 <= Nc) {  // the piece lies in one of D'_j, E'_j, B'_j
+            float* col = ucol(16 * pc) + m;
 #pragma unroll
-          for (int jj = 0; jj < 16; ++jj) {
-            const int c = 16 * pc + jj;
-            if (c < Nc) ucol(c)[m] = v[jj];
+            for (int jj = 0; jj < 16; ++jj) col[(size_t)jj * n] = v[jj];
+          } else {
+#pragma unroll
+            for (int jj = 0; jj < 16; ++jj) {
+              const int c = 16 * pc + jj;
+              if (c < Nc) ucol(c)[m] = v[jj];
+            }
           }
         }
       }
@@ -707,5 +729,6 @@ __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a
 
 __host__ inline bool umma_fits(const Dims& d) {
   return d.n > 32 && d.n <= UM_NMAX && d.nr <= UM_NRMAX && d.nx <= UM_NXMAX &&
+         16 * umma_layout(d).Npad <= UM_PF * UM_NT &&
          umma_layout(d).bytes + 4096 <= 227u * 1024u;  // with the static shared memory
 }
