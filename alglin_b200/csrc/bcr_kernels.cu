@@ -2768,6 +2768,7 @@ __device__ void last_solve_body(Dims d, LastBufs lb, const StatusWords* st, T* x
   T* b = reinterpret_cast<T*>(smem_raw);
   T* tmp = b + L;
   __shared__ T sv[32];
+  __shared__ T lt[32][33];  // a diagonal 32 x 32 block of the blocked LU's factors
   const int kind = st->kind;
   const T* A = lb.A;
   const int* piv = lb.piv;
@@ -2837,9 +2838,39 @@ __device__ void last_solve_body(Dims d, LastBufs lb, const StatusWords* st, T* x
         __syncthreads();
         for (int r = tid; r < N; r += bs) b[r] = tmp[r];
         __syncthreads();
-        for (int i = 0; i < N; ++i) {
-          const T bi = b[i];
-          for (int r = i + 1 + tid; r < N; r += bs) b[r] -= A[(size_t)i * N + piv[r]] * bi;
+        // unit lower L by blocks of 32 rows: the diagonal block staged in shared
+        // memory and solved by one warp, the rows below updated with 8 loads in
+        // flight (same operation order as one column at a time)
+        const int lane = tid & 31, warp = tid >> 5;
+        for (int kb = 0; kb < N; kb += 32) {
+          const int w = N - kb < 32 ? N - kb : 32;
+          for (int e = tid; e < 32 * 32; e += bs) {
+            const int c = e >> 5, r = e & 31;
+            lt[c][r] = (c < w && r < w) ? A[(size_t)(kb + c) * N + piv[kb + r]] : T(0);
+          }
+          __syncthreads();
+          if (warp == 0) {
+            T v = lane < w ? b[kb + lane] : T(0);
+            for (int c = 0; c < w; ++c) {
+              const T vc = __shfl_sync(0xffffffffu, v, c);
+              if (lane > c && lane < w) v = fma(-lt[c][lane], vc, v);
+            }
+            if (lane < w) b[kb + lane] = v;
+          }
+          __syncthreads();
+          for (int r = kb + w + tid; r < N; r += bs) {
+            const int pr = piv[r];
+            T sr = b[r];
+            for (int c0 = 0; c0 < w; c0 += 8) {
+              T av[8];
+#pragma unroll
+              for (int u = 0; u < 8; ++u) av[u] = c0 + u < w ? A[(size_t)(kb + c0 + u) * N + pr] : T(0);
+#pragma unroll
+              for (int u = 0; u < 8; ++u)
+                if (c0 + u < w) sr = fma(-av[u], b[kb + c0 + u], sr);
+            }
+            b[r] = sr;
+          }
           __syncthreads();
         }
       } else {
@@ -2855,14 +2886,52 @@ __device__ void last_solve_body(Dims d, LastBufs lb, const StatusWords* st, T* x
           __syncthreads();
         }
       }
-      const int lda = (kind == FACT_LU || kind == FACT_LUPQ || kind == FACT_LU_ROWS) ? N : M;
-      const bool rows = kind == FACT_LU_ROWS;  // row of position r: piv[r]
-      for (int i = N - 1; i >= 0; --i) {
-        const T xi = b[i] / A[(size_t)i * lda + (rows ? piv[i] : i)];
-        __syncthreads();
-        if (tid == 0) b[i] = xi;
-        for (int r = tid; r < i; r += bs) b[r] -= A[(size_t)i * lda + (rows ? piv[r] : r)] * xi;
-        __syncthreads();
+      const int lda = (kind == FACT_LU || kind == FACT_LUPQ) ? N : M;
+      if (kind == FACT_LU_ROWS) {
+        // U by blocks of 32 rows from the bottom (row of position r: piv[r]), the
+        // same operation order as one column at a time
+        const int lane = tid & 31, warp = tid >> 5;
+        for (int rb = ((N - 1) / 32) * 32; rb >= 0; rb -= 32) {
+          const int w = N - rb < 32 ? N - rb : 32;
+          for (int e = tid; e < 32 * 32; e += bs) {
+            const int c = e >> 5, r = e & 31;
+            lt[c][r] = (c < w && r < w) ? A[(size_t)(rb + c) * N + piv[rb + r]] : T(0);
+          }
+          __syncthreads();
+          if (warp == 0) {
+            T v = lane < w ? b[rb + lane] : T(0);
+            const T dl = lane < w ? lt[lane][lane] : T(1);
+            for (int ii = w - 1; ii >= 0; --ii) {
+              const T xi = __shfl_sync(0xffffffffu, v / dl, ii);
+              if (lane == ii) v = xi;
+              else if (lane < ii) v = fma(-lt[ii][lane], xi, v);
+            }
+            if (lane < w) b[rb + lane] = v;
+          }
+          __syncthreads();
+          for (int r = tid; r < rb; r += bs) {
+            const int pr = piv[r];
+            T sr = b[r];
+            for (int c1 = w; c1 > 0; c1 -= 8) {  // columns rb + w - 1 down to rb
+              T av[8];
+#pragma unroll
+              for (int u = 0; u < 8; ++u) av[u] = c1 - 1 - u >= 0 ? A[(size_t)(rb + c1 - 1 - u) * N + pr] : T(0);
+#pragma unroll
+              for (int u = 0; u < 8; ++u)
+                if (c1 - 1 - u >= 0) sr = fma(-av[u], b[rb + c1 - 1 - u], sr);
+            }
+            b[r] = sr;
+          }
+          __syncthreads();
+        }
+      } else {
+        for (int i = N - 1; i >= 0; --i) {
+          const T xi = b[i] / A[(size_t)i * lda + i];
+          __syncthreads();
+          if (tid == 0) b[i] = xi;
+          for (int r = tid; r < i; r += bs) b[r] -= A[(size_t)i * lda + r] * xi;
+          __syncthreads();
+        }
       }
       if (kind == FACT_LUPQ) {
         if (tid == 0)

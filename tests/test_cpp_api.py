@@ -1,6 +1,7 @@
-"""The C++ drop-in (include/alglin_b200/BorderedCR.hh): a reference-style
-program (tests/cpp/test_bcr_cpp.cc, the checks of src_tests/test7-BorderedCR.cc)
-compiles against it on CPU and runs on the GPU."""
+"""The C++ drop-ins (include/alglin_b200/BorderedCR.hh, include/alglin_b200/BABD.hh):
+reference-style programs (tests/cpp/test_bcr_cpp.cc, the checks of
+src_tests/test7-BorderedCR.cc; tests/cpp/test_babd_cpp.cc, the BABD wrapper's
+cyclic-reduction choices) compile against them on CPU and run on the GPU."""
 import os
 import subprocess
 
@@ -11,11 +12,15 @@ SRC = os.path.join(ROOT, "tests", "cpp", "test_bcr_cpp.cc")
 EXE = os.path.join(ROOT, "tests", "cpp", "test_bcr_cpp")
 
 
-def build_exe():
-    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), SRC,
+def build_exe(src=SRC, exe=EXE):
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"), src,
                     "-L", os.path.join(ROOT, "alglin_b200"), "-lalglin_b200",
-                    "-Wl,-rpath," + os.path.join(ROOT, "alglin_b200"), "-o", EXE], check=True)
-    return EXE
+                    "-Wl,-rpath," + os.path.join(ROOT, "alglin_b200"), "-o", exe], check=True)
+    return exe
+
+
+BABD_SRC = os.path.join(ROOT, "tests", "cpp", "test_babd_cpp.cc")
+BABD_EXE = os.path.join(ROOT, "tests", "cpp", "test_babd_cpp")
 
 
 def test_cpp_dropin_compiles():
@@ -29,3 +34,17 @@ def test_cpp_dropin_runs_test7_workload():
     assert r.returncode == 0, r.stdout + r.stderr
     assert "C++ drop-in ok" in r.stdout
     assert "CyclicReduction+LU" in r.stdout
+
+
+def test_cpp_babd_wrapper_compiles():
+    assert os.path.exists(build_exe(BABD_SRC, BABD_EXE))
+
+
+@pytest.mark.gpu
+def test_cpp_babd_wrapper_runs():
+    exe = build_exe(BABD_SRC, BABD_EXE)
+    r = subprocess.run([exe, "2000"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "BABD drop-in ok" in r.stdout
+    for name in ("CyclicReduction+LU", "CyclicReduction+QR", "CyclicReduction+QRP"):
+        assert name in r.stdout
