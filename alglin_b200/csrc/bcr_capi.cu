@@ -286,12 +286,9 @@ struct bcr_handle_s {
     return BCR_OK;
   }
 
-  // the factorization kernels; the mixed path also measures |A|_inf (FP64)
-  void enqueue_factorize() {
-    if (s.mixed)
-      bcr::launch_norm_A(s, dRow, reinterpret_cast<unsigned long long*>(dNorm), stream);
-    bcr::launch_factorize(s, stream);
-  }
+  // the factorization kernels (the mixed path measures |A|_inf in the first
+  // residual of each solve)
+  void enqueue_factorize() { bcr::launch_factorize(s, stream); }
 
   int factorize_launch() {
     factorized = false;
@@ -396,8 +393,11 @@ struct bcr_handle_s {
     ir_nrhs = nrhs;
     int it = 0;
     for (;;) {
-      for (int c = 0; c < nrhs; ++c)
-        bcr::launch_residual(s, dB + c * Lx, dx + (size_t)c * ld, dR + c * Lx, norms + 1 + 3 * c, stream);
+      for (int c = 0; c < nrhs; ++c) {
+        const bool with_A = it == 0 && c == 0;  // |A|_inf into norms[0] from this pass
+        bcr::launch_residual(s, dB + c * Lx, dx + (size_t)c * ld, dR + c * Lx, norms + 1 + 3 * c, stream,
+                             with_A ? dRow : nullptr, with_A ? norms : nullptr);
+      }
       if (fixed < 0) {
         ir_pending = true;
         if ((rc = read_refinement())) return rc;

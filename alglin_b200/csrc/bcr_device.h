@@ -66,11 +66,11 @@ bool factorize_solve_fuses(const DevState& s, int nrhs);
 void launch_mv(DevState& s, double alpha, const double* x, double beta, double* res,
                cudaStream_t st);
 
-// iterative-refinement helpers (FP64): ||A||_inf, r = b - A x with the norms
-// |r|, |x|, |b| (as non-negative doubles stored in unsigned 64-bit words), y += x
-void launch_norm_A(DevState& s, double* rowsum, unsigned long long* out, cudaStream_t st);
+// iterative-refinement helpers (FP64): r = b - A x with the norms |r|, |x|, |b|
+// (as non-negative doubles stored in unsigned 64-bit words) and, when rowsum is
+// given, ||A||_inf from the same pass over the matrix; y += x
 void launch_residual(DevState& s, const double* b, const double* x, double* r, unsigned long long* out,
-                     cudaStream_t st);
+                     cudaStream_t st, double* rowsum = nullptr, unsigned long long* normA = nullptr);
 void launch_axpy(double* y, const double* x, long len, cudaStream_t st);
 
 // smem bytes needed by one warp of the panel kernel; 0 if it does not fit

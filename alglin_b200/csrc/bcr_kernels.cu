@@ -3001,10 +3001,11 @@ static LastBufs last_bufs(const DevState& s) {
 // ---------------------------------------------------------------------------
 // Mv with the loaded matrix (add_Mv, cc:2118-2166): res = alpha*A*x + beta*res
 // ---------------------------------------------------------------------------
-// ABS: |A| * 1 (row sums of absolute values, for ||A||_inf); x is not read
+// ABS: |A| * 1 (row sums of absolute values, for ||A||_inf); x is not read.
+// Otherwise, with rowsum non-null, the same pass also writes |A| * 1 there.
 template <bool ABS>
 __global__ void k_mv_rows(Dims d, const double* D, const double* E, const double* B, double alpha,
-                          const double* x, double beta, double* res) {
+                          const double* x, double beta, double* res, double* rowsum = nullptr) {
   const int n = d.n, nx = d.nx;
   const size_t rows = (size_t)d.nblock * n;
   const size_t xb_off = (size_t)(d.nblock + 1) * n + d.qx;
@@ -3020,6 +3021,25 @@ __global__ void k_mv_rows(Dims d, const double* D, const double* E, const double
       for (int c = 0; c < n; ++c) s += fabs(Dk[(size_t)c * n + i]) + fabs(Ek[(size_t)c * n + i]);
       for (int c = 0; c < nx; ++c) s += fabs(Bk[(size_t)c * n + i]);
       res[e] = s;
+    } else if (rowsum) {
+      double sa = 0;
+      for (int c = 0; c < n; ++c) {
+        const double a = Dk[(size_t)c * n + i];
+        s += a * x[k * n + c];
+        sa += fabs(a);
+      }
+      for (int c = 0; c < n; ++c) {
+        const double a = Ek[(size_t)c * n + i];
+        s += a * x[(k + 1) * n + c];
+        sa += fabs(a);
+      }
+      for (int c = 0; c < nx; ++c) {
+        const double a = Bk[(size_t)c * n + i];
+        s += a * x[xb_off + c];
+        sa += fabs(a);
+      }
+      res[e] = (beta == 0.0 ? 0.0 : beta * res[e]) + alpha * s;
+      rowsum[e] = sa;
     } else {
       for (int c = 0; c < n; ++c) s += Dk[(size_t)c * n + i] * x[k * n + c];
       for (int c = 0; c < n; ++c) s += Ek[(size_t)c * n + i] * x[(k + 1) * n + c];
@@ -3488,12 +3508,16 @@ bool factorize_solve_fuses(const DevState& s, int nrhs) {
   return fusable_rhs(s, plan_factor<double>(s), nrhs) == nrhs;
 }
 
+// rowsum (value pass only): the block rows' |A| * 1 from the same reads;
+// skip_rows (ABS pass only): the block rows are already done
 template <bool ABS>
-static void mv_t(DevState& s, double alpha, const double* x, double beta, double* res, cudaStream_t st) {
+static void mv_t(DevState& s, double alpha, const double* x, double beta, double* res, cudaStream_t st,
+                 double* rowsum = nullptr, bool skip_rows = false) {
   const Dims d = s.d;
   const long rows = (long)d.nblock * d.n;
-  if (rows > 0) {
-    k_mv_rows<ABS><<<grid_for(rows, 256, 148 * 8), 256, 0, st>>>(d, s.D0, s.E0, s.B0, alpha, x, beta, res);
+  if (rows > 0 && !skip_rows) {
+    k_mv_rows<ABS><<<grid_for(rows, 256, 148 * 8), 256, 0, st>>>(d, s.D0, s.E0, s.B0, alpha, x, beta, res,
+                                                                  rowsum);
     check_launch("k_mv_rows");
   }
   const int nr = d.nr;
@@ -3528,24 +3552,21 @@ __global__ void k_axpy(double* y, const double* x, long len) {
     y[i] += x[i];
 }
 
-// ||A||_inf of the loaded matrix into norms[0]; scratch: ncols-long buffer
-void launch_norm_A(DevState& s, double* rowsum, unsigned long long* out, cudaStream_t st) {
-  const Dims d = s.d;
-  const long nrows = (long)d.n * (d.nblock + 1) + d.qr + d.nr;
-  mv_t<true>(s, 1.0, nullptr, 0.0, rowsum, st);
-  cudaMemsetAsync(out, 0, sizeof(unsigned long long), st);
-  k_absmax<<<grid_for(nrows, 256, 148 * 2), 256, 0, st>>>(rowsum, nrows, out);
-  check_launch("k_absmax");
-}
-
-// r = b - A x and the three inf-norms |r|, |x|, |b| into out[0..2]
+// r = b - A x and the three inf-norms |r|, |x|, |b| into out[0..2]; with rowsum
+// (an nrows-long scratch) non-null, also ||A||_inf into *normA, the block rows'
+// |A| sums taken from the residual's own reads of the matrix
 void launch_residual(DevState& s, const double* b, const double* x, double* r, unsigned long long* out,
-                     cudaStream_t st) {
+                     cudaStream_t st, double* rowsum, unsigned long long* normA) {
   const Dims d = s.d;
   const long nrows = (long)d.n * (d.nblock + 1) + d.qr + d.nr;
   const long ncols = (long)d.n * (d.nblock + 1) + d.qx + d.nx;
   cudaMemcpyAsync(r, b, (size_t)nrows * 8, cudaMemcpyDeviceToDevice, st);
-  mv_t<false>(s, -1.0, x, 1.0, r, st);
+  mv_t<false>(s, -1.0, x, 1.0, r, st, rowsum);
+  if (rowsum) {
+    mv_t<true>(s, 1.0, nullptr, 0.0, rowsum, st, nullptr, true);  // border and last rows
+    cudaMemsetAsync(normA, 0, sizeof(unsigned long long), st);
+    k_absmax<<<grid_for(nrows, 256, 148 * 2), 256, 0, st>>>(rowsum, nrows, normA);
+  }
   cudaMemsetAsync(out, 0, 3 * sizeof(unsigned long long), st);
   k_absmax<<<grid_for(nrows, 256, 148 * 2), 256, 0, st>>>(r, nrows, out);
   k_absmax<<<grid_for(ncols, 256, 148 * 2), 256, 0, st>>>(x, ncols, out + 1);
