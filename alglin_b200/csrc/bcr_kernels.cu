@@ -3403,6 +3403,7 @@ static SweepArgs<T> sweep_args(DevState& s, const WorkSet<T>& w, double* x, int 
   a.d = s.d;
   a.D = w.D; a.E = w.E; a.B = w.B; a.C = w.C; a.Tm = w.Tm; a.P = s.P;
   a.x = x; a.ldx = ldx; a.nrhs = nrhs; a.XB = s.XB; a.sel = s.sel;
+  a.done = nullptr;
   return a;
 }
 
