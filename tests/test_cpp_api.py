@@ -48,3 +48,17 @@ def test_cpp_babd_wrapper_runs():
     assert "BABD drop-in ok" in r.stdout
     for name in ("CyclicReduction+LU", "CyclicReduction+QR", "CyclicReduction+QRP"):
         assert name in r.stdout
+
+
+def test_umma_layout_invariants():
+    """The tcgen05 pair kernel's shared-memory layout (bcr_umma_layout.cuh) for
+    every accepted shape: no overlap of regions live at the same time, 16-byte
+    aligned operands, tiles inside their regions, within one CTA's limit."""
+    src = os.path.join(ROOT, "tests", "cpp", "umma_layout_check.cu")
+    exe = os.path.join(ROOT, "tests", "cpp", "umma_layout_check")
+    subprocess.run(["nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+                    "-I", os.path.join(ROOT, "alglin_b200", "csrc"), "-I", os.path.join(ROOT, "include"),
+                    src, "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "0 failures" in r.stdout
