@@ -56,9 +56,12 @@ def test_umma_layout_invariants():
     aligned operands, tiles inside their regions, within one CTA's limit."""
     src = os.path.join(ROOT, "tests", "cpp", "umma_layout_check.cu")
     exe = os.path.join(ROOT, "tests", "cpp", "umma_layout_check")
-    subprocess.run(["nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+    subprocess.run(["nvcc", "-std=c++17", "-cudart", "shared", "-gencode", "arch=compute_100a,code=sm_100a",
                     "-I", os.path.join(ROOT, "alglin_b200", "csrc"), "-I", os.path.join(ROOT, "include"),
                     src, "-o", exe], check=True)
-    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    try:
+        r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    finally:
+        os.remove(exe)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "0 failures" in r.stdout
