@@ -325,3 +325,23 @@ def test_gpu_blocked_last_block_singular_falls_back():
     assert h2.factorize(), h2.last_error()
     xg = gpu_solve(h2, b)[0]
     assert fwd_err(xg[:s.ncols], xo[:s.ncols]) < 1e-8
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gpu_singular_panel_large_blocks(precision):
+    """A zero first column in the panel of pair (0, 1) at n=40: the blocked FP64
+    kernel and the FP32 tensor-core kernel both stop with getrf's INFO = 1."""
+    s = synth.collocation(6, 40, 0, 0, 2, 2, seed=1)
+    s.E[0][0, :] = 0.0  # column 0 (blocks are held column by column)
+    s.D[1][0, :] = 0.0
+    h = gpu_solver(s)
+    if precision == "mixed":
+        h.set_precision(B.PRECISION_MIXED)
+    assert not h.factorize()
+    assert "getrf(M=80,N=40,A,LDA=80,iperm)::INFO = 1" in h.last_error()
+    # the handle recovers: a regular system factors afterwards
+    s2 = synth.collocation(6, 40, 0, 0, 2, 2, seed=2)
+    h2 = gpu_solver(s2)
+    if precision == "mixed":
+        h2.set_precision(B.PRECISION_MIXED)
+    assert h2.factorize(), h2.last_error()
