@@ -498,67 +498,72 @@ __global__ void __launch_bounds__(UM_NT, 1) k_factor_lu_umma(FactorArgs<float> a
       if (r < nr) a.C[(size_t)j * nrn + r + (size_t)c * nr] = v;
     }
     // ---------------------------------------------------- Z = L11^-1 (FP32)
-    if (tid < NP) {  // zero above the diagonal blocks
-      for (int c = 32 * (tid / 32 + 1); c < NP; c += 4)
-        *reinterpret_cast<float4*>(Zf + tid * LDP + c) = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    if (warp >= UM_NW - NP / 32) {  // diagonal 32 x 32 inverses, one column per lane, on the
-      const int a32 = (warp - (UM_NW - NP / 32)) * 32, c = lane;  // warps the position copy leaves idle
-      float z[32];
-#pragma unroll
-      for (int r = 0; r < 32; ++r) {
-        const int gr = a32 + r;
-        float v = 0.0f;
-        if (gr < n) {
-          v = (r == c) ? 1.0f : 0.0f;
-          const float* Lr = P + s_perm[gr] * LDP + a32;
-#pragma unroll
-          for (int m = 0; m < r; ++m) v = fmaf(-Lr[m], z[m], v);
-        }
-        z[r] = v;
+    // on the last four warps (named barrier 2), while warps 0..7 copy X above
+    if (warp >= UM_NW - 4) {
+      const int zt = tid - (UM_NT - 128);  // 0..127
+      if (zt < NP) {  // zero above the diagonal blocks
+        for (int c = 32 * (zt / 32 + 1); c < NP; c += 4)
+          *reinterpret_cast<float4*>(Zf + zt * LDP + c) = make_float4(0.f, 0.f, 0.f, 0.f);
       }
+      if (zt < NP) {  // diagonal 32 x 32 inverses, one column per lane
+        const int a32 = (zt >> 5) * 32, c = lane;
+        float z[32];
 #pragma unroll
-      for (int r = 0; r < 32; ++r) Zf[(a32 + r) * LDP + a32 + c] = z[r];
+        for (int r = 0; r < 32; ++r) {
+          const int gr = a32 + r;
+          float v = 0.0f;
+          if (gr < n) {
+            v = (r == c) ? 1.0f : 0.0f;
+            const float* Lr = P + s_perm[gr] * LDP + a32;
+#pragma unroll
+            for (int m = 0; m < r; ++m) v = fmaf(-Lr[m], z[m], v);
+          }
+          z[r] = v;
+        }
+#pragma unroll
+        for (int r = 0; r < 32; ++r) Zf[(a32 + r) * LDP + a32 + c] = z[r];
+      }
+      asm volatile("bar.sync 2, 128;" ::: "memory");
+      for (int r0 = 32; r0 < NP; r0 += 32) {
+        // Zf[r0:r0+32, 0:r0] = L[r0:r0+32, 0:r0] * Z[0:r0, 0:r0]  (2 rows x 4 columns per thread)
+        for (int t = zt; t < 16 * (r0 / 4); t += 128) {
+          const int rr = 2 * (t & 15), cc = 4 * (t >> 4);
+          const int g0 = r0 + rr, g1 = g0 + 1;
+          const float* L0 = g0 < n ? P + s_perm[g0] * LDP : nullptr;
+          const float* L1 = g1 < n ? P + s_perm[g1] * LDP : nullptr;
+          float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0;
+          for (int m = cc; m < r0; ++m) {  // Z[m][cc..cc+3] = 0 for m < cc
+            const float4 zv = *reinterpret_cast<const float4*>(Zf + m * LDP + cc);
+            const float l0 = L0 ? L0[m] : 0.0f, l1 = L1 ? L1[m] : 0.0f;
+            s0.x = fmaf(l0, zv.x, s0.x); s0.y = fmaf(l0, zv.y, s0.y);
+            s0.z = fmaf(l0, zv.z, s0.z); s0.w = fmaf(l0, zv.w, s0.w);
+            s1.x = fmaf(l1, zv.x, s1.x); s1.y = fmaf(l1, zv.y, s1.y);
+            s1.z = fmaf(l1, zv.z, s1.z); s1.w = fmaf(l1, zv.w, s1.w);
+          }
+          *reinterpret_cast<float4*>(Zf + g0 * LDP + cc) = s0;
+          *reinterpret_cast<float4*>(Zf + g1 * LDP + cc) = s1;
+        }
+        asm volatile("bar.sync 2, 128;" ::: "memory");
+        // Zf[r0:r0+32, 0:r0] = -Z_bb * (that), in place, one column per thread
+        for (int c = zt; c < r0; c += 128) {
+          float y[32];
+#pragma unroll
+          for (int r = 0; r < 32; ++r) y[r] = Zf[(r0 + r) * LDP + c];
+#pragma unroll
+          for (int r = 31; r >= 0; --r) {
+            const float* Zr = Zf + (r0 + r) * LDP + r0;
+            float s = 0.0f;
+#pragma unroll
+            for (int m = 0; m <= r; ++m) s = fmaf(Zr[m], y[m], s);
+            y[r] = -s;
+          }
+#pragma unroll
+          for (int r = 0; r < 32; ++r) Zf[(r0 + r) * LDP + c] = y[r];
+        }
+        asm volatile("bar.sync 2, 128;" ::: "memory");
+      }
     }
     __syncthreads();
-    for (int r0 = 32; r0 < NP; r0 += 32) {
-      // Zf[r0:r0+32, 0:r0] = L[r0:r0+32, 0:r0] * Z[0:r0, 0:r0]  (2 rows x 4 columns per thread)
-      for (int t = tid; t < 16 * (r0 / 4); t += UM_NT) {
-        const int rr = 2 * (t & 15), cc = 4 * (t >> 4);
-        const int g0 = r0 + rr, g1 = g0 + 1;
-        const float* L0 = g0 < n ? P + s_perm[g0] * LDP : nullptr;
-        const float* L1 = g1 < n ? P + s_perm[g1] * LDP : nullptr;
-        float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0;
-        for (int m = cc; m < r0; ++m) {  // Z[m][cc..cc+3] = 0 for m < cc
-          const float4 zv = *reinterpret_cast<const float4*>(Zf + m * LDP + cc);
-          const float l0 = L0 ? L0[m] : 0.0f, l1 = L1 ? L1[m] : 0.0f;
-          s0.x = fmaf(l0, zv.x, s0.x); s0.y = fmaf(l0, zv.y, s0.y);
-          s0.z = fmaf(l0, zv.z, s0.z); s0.w = fmaf(l0, zv.w, s0.w);
-          s1.x = fmaf(l1, zv.x, s1.x); s1.y = fmaf(l1, zv.y, s1.y);
-          s1.z = fmaf(l1, zv.z, s1.z); s1.w = fmaf(l1, zv.w, s1.w);
-        }
-        *reinterpret_cast<float4*>(Zf + g0 * LDP + cc) = s0;
-        *reinterpret_cast<float4*>(Zf + g1 * LDP + cc) = s1;
-      }
-      __syncthreads();
-      // Zf[r0:r0+32, 0:r0] = -Z_bb * (that), in place, one column per thread
-      for (int c = tid; c < r0; c += UM_NT) {
-        float y[32];
-#pragma unroll
-        for (int r = 0; r < 32; ++r) y[r] = Zf[(r0 + r) * LDP + c];
-#pragma unroll
-        for (int r = 31; r >= 0; --r) {
-          const float* Zr = Zf + (r0 + r) * LDP + r0;
-          float s = 0.0f;
-#pragma unroll
-          for (int m = 0; m <= r; ++m) s = fmaf(Zr[m], y[m], s);
-          y[r] = -s;
-        }
-#pragma unroll
-        for (int r = 0; r < 32; ++r) Zf[(r0 + r) * LDP + c] = y[r];
-      }
-      __syncthreads();
-    }
     // ------------------------------------------------ U12 = Z Xt (tensor cores)
     umma_stage_a(L, smem_raw, [&](int i, int kk) {
       return (i < n && kk < n) ? Zf[i * LDP + kk] : 0.0f;
