@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(HERE, "libalglin_b200.so")
 
 BCR_OK, BCR_NUMERICAL, BCR_BAD_ARGUMENT, BCR_CUDA_ERROR, BCR_DEVICE_TIMEOUT = range(5)
 PRECISION_FP64, PRECISION_MIXED = 0, 1
-PAIR_AUTO, PAIR_TC, PAIR_GRP, PAIR_ROWS, PAIR_CTA, PAIR_SMEM, PAIR_UMMA = range(7)
+PAIR_AUTO, PAIR_TC, PAIR_GRP, PAIR_ROWS, PAIR_CTA, PAIR_SMEM, PAIR_UMMA, PAIR_TREE = range(8)
 
 _dp = ct.POINTER(ct.c_double)
 _ip = ct.POINTER(ct.c_int)
@@ -333,7 +333,8 @@ class BorderedCR:
     def set_precision(self, p): self._check(self.L.bcr_set_precision(self.h, p))
 
     def set_pair_kernel(self, choice: int):
-        """Force a pair-kernel family (PAIR_AUTO, PAIR_TC, PAIR_GRP, PAIR_ROWS, PAIR_CTA, PAIR_SMEM, PAIR_UMMA)."""
+        """Force a pair-kernel family (PAIR_AUTO, PAIR_TC, PAIR_GRP, PAIR_ROWS, PAIR_CTA, PAIR_SMEM, PAIR_UMMA,
+        PAIR_TREE)."""
         self._check(self.L.bcr_set_pair_kernel(self.h, int(choice)))
 
     def set_refinement(self, tol: float = 1e-12, max_iter: int = 10):

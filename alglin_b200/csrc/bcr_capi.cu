@@ -134,7 +134,7 @@ struct bcr_handle_s {
     dfree(z.D0); dfree(z.E0); dfree(z.B0); dfree(z.C0); dfree(z.Cq); dfree(z.F0); dfree(z.H);
     dfree(z.D); dfree(z.E); dfree(z.B); dfree(z.C); dfree(z.T); dfree(z.P);
     dfree(z.Rbuf); dfree(z.Fbuf); dfree(z.XB); dfree(z.part); dfree(z.Ffin); dfree(z.Hl);
-    dfree(z.tau_l); dfree(z.piv_l); dfree(z.st); dfree(z.mv_part); dfree(z.slab);
+    dfree(z.tau_l); dfree(z.piv_l); dfree(z.st); dfree(z.mv_part); dfree(z.slab); dfree(z.tree_cnt);
     dfree(z.Ul); dfree(z.Vl); dfree(z.Sl); dfree(z.Al);
     dfree(z.Df); dfree(z.Ef); dfree(z.Bf); dfree(z.Cf); dfree(z.Tf); dfree(z.Rbuff);
     dfree(dX); dfree(dY); dfree(dB); dfree(dR); dfree(dNorm); dfree(dRow);
@@ -190,6 +190,7 @@ struct bcr_handle_s {
     A(dalloc(z.Ul, Lmax * Lmax)); A(dalloc(z.Vl, Lmax * Lmax)); A(dalloc(z.Sl, Lmax));
     A(dalloc(z.Al, (size_t)d.Nr * d.Nc));
     A(dalloc(z.st, 1)); A(dalloc(z.mv_part, (nb + 2) * nr));
+    A(dalloc(z.tree_cnt, nb + 1));
     z.slab_elems = bcr::cta_slab_elems(d);
     z.slab_ctas = 148 * 2;  // the CTA-per-pair kernel may be chosen for any n
     if (z.slab_ctas) {
@@ -1205,7 +1206,7 @@ int bcr_graph_launch(bcr_handle h, int what) {
 
 int bcr_set_pair_kernel(bcr_handle h, int choice) {
   H_CHECK(h);
-  if (choice < BCR_PAIR_AUTO || choice > BCR_PAIR_UMMA)
+  if (choice < BCR_PAIR_AUTO || choice > BCR_PAIR_TREE)
     return h->fail(BCR_BAD_ARGUMENT, fmt("bcr_set_pair_kernel: unknown choice %d\n", choice));
   h->s.pair_kernel = choice;
   h->drop_graphs();

@@ -40,6 +40,8 @@ struct DevState {
   int sel_last2;        // fallback solver (0: none, else the SVD family)
   StatusWords* st;      // device status
   double* mv_part;      // Mv border partials ((nblock+1) x nr)
+  int* tree_cnt;        // tree schedule: arrival counter per node + leaf counter (nblock+1);
+                        // null where the tree schedule is not used (batches)
   // mixed precision: FP32 working blocks and factors (the loaded matrix, F,
   // the last block, the vectors and the residual stay FP64)
   int mixed;

@@ -41,6 +41,7 @@ struct FactorArgs {
   unsigned char* P;
   T* Rbuf;
   double* Fbuf;  // the F Schur updates are accumulated in FP64 in every precision
+  const double* F0;  // loaded F (read by the tree schedule's root)
   StatusWords* st;
   int k, first, ldw;
   // right-hand sides eliminated together with the factorization (forward
@@ -593,18 +594,27 @@ size_t tc_smem_per_warp(int n) {
   return n == 16 ? TcShape<16>::BYTES : n == 8 ? TcShape<8>::BYTES : 0;
 }
 
-template <int N, bool BATCH = false>
-__global__ void __launch_bounds__(128, 4) k_factor_lu_tc(FactorArgs<double> a0, const FactorArgs<double>* tab,
-                                                       const BatchCta* cmap) {
+// Per-pair extras of the tree-scheduled factorization (k_factor_tree_tc):
+// gather = the C_jpp contributions of earlier levels are added to C_j at load
+// (Rbuf[j - K'] for K' = 1, 2, ..., gather; 0 in the level-by-level launches,
+// where k_border_fix adds them after each level); c1, c2 = the nodes whose F
+// and xb partial sums are added to this pair's own (0: none).
+struct TcTree {
+  int gather, c1, c2;
+};
+
+// Coherent load of an element that another warp of the same launch may have
+// written (tree schedule): bypasses L1, served by L2.
+__device__ __forceinline__ double ldw(const double* p) { return __ldcg(p); }
+
+// Eliminates x_j from the pair (jp = j - k, j); see the comment above.
+// Returns false (after reporting) when the panel has an exactly-zero pivot; the
+// outputs of that pair are then not written.
+template <int N>
+__device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int k, bool first, double* Wt,
+                                        int lane, const TcTree& tr) {
   using S = TcShape<N>;
   constexpr unsigned FULL = 0xffffffffu;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  FactorArgs<double> ab;  // this CTA's system (batch only)
-  long q0, q1, qs;
-  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
-  const FactorArgs<double>& a = BATCH ? ab : a0;
-  double* Wt = reinterpret_cast<double*>(smem_raw + (size_t)warp * S::BYTES);
   double* Gs = Wt + S::WS;
   double* bc = Gs + S::GS;                        // pivot row + its reciprocal
   int* rowof = reinterpret_cast<int*>(bc + N + 2);
@@ -615,200 +625,201 @@ __global__ void __launch_bounds__(128, 4) k_factor_lu_tc(FactorArgs<double> a0, 
   const size_t nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
   const int nrf = a.nrf;             // fused right-hand sides
   const int NT = n2 + nx + nrf;      // live trailing columns
-  const int k = a.k;
-  const bool first = a.first != 0;
+  const bool act = lane < n2, top = lane < n;
+  const int ri = top ? lane : lane - n;
+  const int g = lane >> 2, t = lane & 3;
+  const int jp = j - k;
   const double* srcD = first ? a.D0 : a.D;
   const double* srcE = first ? a.E0 : a.E;
   const double* srcB = first ? a.B0 : a.B;
   const double* srcC = first ? a.C0 : a.C;
-  const bool act = lane < n2, top = lane < n;
-  const int ri = top ? lane : lane - n;
-  const int g = lane >> 2, t = lane & 3;
-
-  for (long q = q0; q < q1; q += qs) {
-    const int j = k + (int)(2L * k * q), jp = j - k;
-    // ------------------------------------------------------------ load
-    double rowA[N], rowC[N];
-    {
-      const double* Pm = top ? srcE + (size_t)jp * nn : srcD + (size_t)j * nn;
+  // ------------------------------------------------------------ load
+  double rowA[N], rowC[N];
+  {
+    const double* Pm = top ? srcE + (size_t)jp * nn : srcD + (size_t)j * nn;
 #pragma unroll
-      for (int c = 0; c < N; ++c) rowA[c] = act ? Pm[(size_t)c * n + ri] : 0.0;
+    for (int c = 0; c < N; ++c) rowA[c] = act ? ldw(Pm + (size_t)c * n + ri) : 0.0;
 #pragma unroll
-      for (int c = 0; c < N; ++c) rowC[c] = 0.0;
-      if (lane < nr) {
-        const double* Cj = srcC + (size_t)j * nrn + lane;
+    for (int c = 0; c < N; ++c) rowC[c] = 0.0;
+    if (lane < nr) {
+      const double* Cj = srcC + (size_t)j * nrn + lane;
 #pragma unroll
-        for (int c = 0; c < N; ++c) rowC[c] = Cj[(size_t)c * nr];
+      for (int c = 0; c < N; ++c) rowC[c] = ldw(Cj + (size_t)c * nr);
+      // C_jpp contributions of the pairs (j - 2K', j - K') of earlier levels
+      for (int kk = 1; kk <= tr.gather; kk *= 2) {
+        const double* R = a.Rbuf + (size_t)(j - kk) * nrn + lane;
+#pragma unroll
+        for (int c = 0; c < N; ++c) rowC[c] += ldw(R + (size_t)c * nr);
       }
-      // trailing columns in the original row order: TOP [D_jp 0 B_jp], BOTTOM [0 E_j B_j]
-      // compile-time trip counts: every load of the pair is issued before the
-      // first one is consumed, so a lone pair pays one memory latency
-      const double* Djp = srcD + (size_t)jp * nn;
-      const double* Ej = srcE + (size_t)j * nn;
+    }
+    // trailing columns in the original row order: TOP [D_jp 0 B_jp], BOTTOM [0 E_j B_j]
+    // compile-time trip counts: every load of the pair is issued before the
+    // first one is consumed, so a lone pair pays one memory latency
+    const double* Djp = srcD + (size_t)jp * nn;
+    const double* Ej = srcE + (size_t)j * nn;
 #pragma unroll
-      for (int it = 0; it < (int)(nn / 32); ++it) {
-        const int idx = lane + 32 * it;
+    for (int it = 0; it < (int)(nn / 32); ++it) {
+      const int idx = lane + 32 * it;
+      const int r = idx % n, c = idx / n;
+      Wt[r * S::LDW + c] = ldw(Djp + idx);
+      Wt[(n + r) * S::LDW + c] = ldw(Ej + idx);
+    }
+    const double* Bjp = srcB + (size_t)jp * nnx;
+    const double* Bj = srcB + (size_t)j * nnx;
+#pragma unroll
+    for (int it = 0; it < (8 * N + 31) / 32; ++it) {
+      const int idx = lane + 32 * it;
+      if (idx < (int)nnx) {
         const int r = idx % n, c = idx / n;
-        Wt[r * S::LDW + c] = Djp[idx];
-        Wt[(n + r) * S::LDW + c] = Ej[idx];
-      }
-      const double* Bjp = srcB + (size_t)jp * nnx;
-      const double* Bj = srcB + (size_t)j * nnx;
-#pragma unroll
-      for (int it = 0; it < (8 * N + 31) / 32; ++it) {
-        const int idx = lane + 32 * it;
-        if (idx < (int)nnx) {
-          const int r = idx % n, c = idx / n;
-          Wt[r * S::LDW + n + c] = Bjp[idx];
-          Wt[(n + r) * S::LDW + n + c] = Bj[idx];
-        }
-      }
-      // fused right-hand sides: TOP rows hold x_jp, BOTTOM rows x_j
-      for (int idx = lane; idx < n2 * nrf; idx += 32) {
-        const int r = idx % n2, c = idx / n2;
-        const double* xc = a.x + (size_t)c * a.ldx;
-        Wt[r * S::LDW + n + nx + c] = r < n ? xc[(size_t)jp * n + r] : xc[(size_t)j * n + r - n];
-      }
-      // zero the padding columns of the live rows (they feed padding outputs only,
-      // but keep them finite)
-      for (int idx = lane; idx < n2 * (S::NTP - NT); idx += 32) {
-        const int r = idx % n2, c = NT + idx / n2;
-        Wt[r * S::LDW + c - n] = 0.0;
+        Wt[r * S::LDW + n + c] = ldw(Bjp + idx);
+        Wt[(n + r) * S::LDW + n + c] = ldw(Bj + idx);
       }
     }
-    // --------------------------------------------------- phase 1: panel LU
-    int mypos = lane, mykey = 0, info = 0;
-    bool done = !act;
-#pragma unroll
-    for (int i = 0; i < N; ++i) {
-      // every lane forms the reciprocal of its own candidate while the pivot is
-      // searched; the pivot lane publishes its value with the pivot row
-      const double rc = __drcp_rn(rowA[i]);
-      // pivot: max |a| over rows not yet used, ties to the smaller position
-      const double av = fabs(rowA[i]);
-      const unsigned long long bits = (unsigned long long)__double_as_longlong(av);
-      unsigned hi = (unsigned)(bits >> 32) + 1u;
-      if (done) hi = 0u;
-      else if (av != av) hi = 1u;  // NaN loses against every number
-      const unsigned hmax = __reduce_max_sync(FULL, hi);
-      unsigned m = __ballot_sync(FULL, hi == hmax && !done);
-      unsigned pmin;
-      if (__popc(m) == 1) {  // unique maximum in the upper word: the usual case
-        pmin = (unsigned)__shfl_sync(FULL, mypos, __ffs(m) - 1);
-      } else {               // exact tie handling: lower word, then smallest position
-        const unsigned lo = (hi == hmax) ? (unsigned)bits : 0u;
-        const unsigned lmax = __reduce_max_sync(FULL, lo);
-        const bool cand = (hi == hmax) && (lo == lmax) && !done;
-        pmin = __reduce_min_sync(FULL, cand ? (unsigned)mypos : 0xffffffffu);
-        m = __ballot_sync(FULL, cand && (unsigned)mypos == pmin);
-      }
-      const int p = __ffs(m) - 1;
-      if (lane == i) mykey = (int)pmin;
-      if (!done && mypos == i && lane != p) mypos = (int)pmin;
-      if (lane == p) {
-        mypos = i;
-#pragma unroll
-        for (int c = (i & ~1); c < N; c += 2)
-          *reinterpret_cast<double2*>(&bc[c]) = make_double2(rowA[c], rowA[c + 1]);
-        bc[N] = rc;
-      }
-      __syncwarp();
-      const double piv = bc[i];
-      if (piv == 0.0 && info == 0) info = i + 1;
-      const double rinv = piv != 0.0 ? bc[N] : 0.0;
-      double u[N];
-#pragma unroll
-      for (int c = (i + 1) & ~1; c < N; c += 2) {
-        const double2 v2 = *reinterpret_cast<const double2*>(&bc[c]);
-        u[c] = v2.x;
-        u[c + 1] = v2.y;
-      }
-      if (!done && lane != p) {
-        const double l = rowA[i] * rinv;
-        rowA[i] = l;
-#pragma unroll
-        for (int c = i + 1; c < N; ++c) rowA[c] = fma(-l, u[c], rowA[c]);
-      }
-      if (lane < nr) {
-        const double l = rowC[i] * rinv;
-        rowC[i] = l;
-#pragma unroll
-        for (int c = i + 1; c < N; ++c) rowC[c] = fma(-l, u[c], rowC[c]);
-      }
-      if (lane == p) done = true;
-      __syncwarp();
+    // fused right-hand sides: TOP rows hold x_jp, BOTTOM rows x_j
+    for (int idx = lane; idx < n2 * nrf; idx += 32) {
+      const int r = idx % n2, c = idx / n2;
+      const double* xc = a.x + (size_t)c * a.ldx;
+      Wt[r * S::LDW + n + nx + c] = r < n ? ldw(xc + (size_t)jp * n + r) : ldw(xc + (size_t)j * n + r - n);
     }
-    if (info != 0) {
-      if (lane == 0) report(a.st, DEV_ZERO_PIVOT, j, info, k);
-      continue;
+    // zero the padding columns of the live rows (they feed padding outputs only,
+    // but keep them finite)
+    for (int idx = lane; idx < n2 * (S::NTP - NT); idx += 32) {
+      const int r = idx % n2, c = NT + idx / n2;
+      Wt[r * S::LDW + c - n] = 0.0;
     }
-    // panel factors T_j (L\U and M in getrf row order), pivots, C_j U^-1
-    {
-      double* Tj = a.Tm + (size_t)j * szT(d);
-      if (act) {
+  }
+  // --------------------------------------------------- phase 1: panel LU
+  int mypos = lane, info = 0;
+  bool done = !act;
 #pragma unroll
-        for (int c = 0; c < N; ++c) Tj[(size_t)mypos + (size_t)c * n2] = rowA[c];
-        rowof[mypos] = lane;
-      }
-      if (act) a.P[(size_t)j * szP(d) + mypos] = (unsigned char)lane;
-      if (lane < nr) {
-        double* Cj = a.C + (size_t)j * nrn + lane;
+  for (int i = 0; i < N; ++i) {
+    // every lane forms the reciprocal of its own candidate while the pivot is
+    // searched; the pivot lane publishes its value with the pivot row
+    const double rc = __drcp_rn(rowA[i]);
+    // pivot: max |a| over rows not yet used, ties to the smaller position
+    const double av = fabs(rowA[i]);
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(av);
+    unsigned hi = (unsigned)(bits >> 32) + 1u;
+    if (done) hi = 0u;
+    else if (av != av) hi = 1u;  // NaN loses against every number
+    const unsigned hmax = __reduce_max_sync(FULL, hi);
+    unsigned m = __ballot_sync(FULL, hi == hmax && !done);
+    unsigned pmin;
+    if (__popc(m) == 1) {  // unique maximum in the upper word: the usual case
+      pmin = (unsigned)__shfl_sync(FULL, mypos, __ffs(m) - 1);
+    } else {               // exact tie handling: lower word, then smallest position
+      const unsigned lo = (hi == hmax) ? (unsigned)bits : 0u;
+      const unsigned lmax = __reduce_max_sync(FULL, lo);
+      const bool cand = (hi == hmax) && (lo == lmax) && !done;
+      pmin = __reduce_min_sync(FULL, cand ? (unsigned)mypos : 0xffffffffu);
+      m = __ballot_sync(FULL, cand && (unsigned)mypos == pmin);
+    }
+    const int p = __ffs(m) - 1;
+    if (!done && mypos == i && lane != p) mypos = (int)pmin;
+    if (lane == p) {
+      mypos = i;
 #pragma unroll
-        for (int c = 0; c < N; ++c) Cj[(size_t)c * nr] = rowC[c];
-      }
-      // rows of L (row m contiguous) for the triangular solve
-      if (act && mypos < n) {
-#pragma unroll
-        for (int c = 0; c < N; c += 2)
-          *reinterpret_cast<double2*>(&Gs[mypos * S::LDG + c]) = make_double2(rowA[c], rowA[c + 1]);
-      }
+      for (int c = (i & ~1); c < N; c += 2)
+        *reinterpret_cast<double2*>(&bc[c]) = make_double2(rowA[c], rowA[c + 1]);
+      bc[N] = rc;
     }
     __syncwarp();
-    // ------------------------------------ phase 2: operator G (X L = R)
-    // R rows: identity for U-row positions, -M for reduced positions, -C' for border rows
-    {
-      double x[N];
+    const double piv = bc[i];
+    if (piv == 0.0 && info == 0) info = i + 1;
+    const double rinv = piv != 0.0 ? bc[N] : 0.0;
+    double u[N];
 #pragma unroll
-      for (int c = 0; c < N; ++c) x[c] = (mypos < n) ? (c == mypos ? 1.0 : 0.0) : -rowA[c];
+    for (int c = (i + 1) & ~1; c < N; c += 2) {
+      const double2 v2 = *reinterpret_cast<const double2*>(&bc[c]);
+      u[c] = v2.x;
+      u[c + 1] = v2.y;
+    }
+    if (!done && lane != p) {
+      const double l = rowA[i] * rinv;
+      rowA[i] = l;
 #pragma unroll
-      for (int c = 0; c < N; ++c) rowC[c] = -rowC[c];
-      // right-looking: once x[mm] is final, update every x[c], c < mm (the
-      // updates of one step are independent, so the dependent chain is N long)
+      for (int c = i + 1; c < N; ++c) rowA[c] = fma(-l, u[c], rowA[c]);
+    }
+    if (lane < nr) {
+      const double l = rowC[i] * rinv;
+      rowC[i] = l;
 #pragma unroll
-      for (int mm = N - 1; mm > 0; --mm) {
-        const double xm = x[mm], cm = rowC[mm];
-        const double* Lrow = Gs + mm * S::LDG;  // L(mm, 0..mm-1)
+      for (int c = i + 1; c < N; ++c) rowC[c] = fma(-l, u[c], rowC[c]);
+    }
+    if (lane == p) done = true;
+    __syncwarp();
+  }
+  if (info != 0) {
+    if (lane == 0) report(a.st, DEV_ZERO_PIVOT, j, info, k);
+    return false;
+  }
+  // panel factors T_j (L\U and M in getrf row order), pivots, C_j U^-1
+  {
+    double* Tj = a.Tm + (size_t)j * szT(d);
+    if (act) {
 #pragma unroll
-        for (int c = 0; c < mm; c += 2) {
-          const double2 l2 = *reinterpret_cast<const double2*>(&Lrow[c]);
-          x[c] = fma(-xm, l2.x, x[c]);
-          rowC[c] = fma(-cm, l2.x, rowC[c]);
-          if (c + 1 < mm) {
-            x[c + 1] = fma(-xm, l2.y, x[c + 1]);
-            rowC[c + 1] = fma(-cm, l2.y, rowC[c + 1]);
-          }
-        }
-      }
-      __syncwarp();
-      if (act) {
+      for (int c = 0; c < N; ++c) Tj[(size_t)mypos + (size_t)c * n2] = rowA[c];
+      rowof[mypos] = lane;
+    }
+    if (act) a.P[(size_t)j * szP(d) + mypos] = (unsigned char)lane;
+    if (lane < nr) {
+      double* Cj = a.C + (size_t)j * nrn + lane;
 #pragma unroll
-        for (int c = 0; c < N; c += 2)
-          *reinterpret_cast<double2*>(&Gs[mypos * S::LDG + c]) = make_double2(x[c], x[c + 1]);
-      }
-      if (lane < 8) {  // border rows (zero when lane >= nr)
+      for (int c = 0; c < N; ++c) Cj[(size_t)c * nr] = rowC[c];
+    }
+    // rows of L (row m contiguous) for the triangular solve
+    if (act && mypos < n) {
 #pragma unroll
-        for (int c = 0; c < N; c += 2) {
-          const bool live = lane < nr;
-          *reinterpret_cast<double2*>(&Gs[(n2 + lane) * S::LDG + c]) =
-              make_double2(live ? rowC[c] : 0.0, live ? rowC[c + 1] : 0.0);
+      for (int c = 0; c < N; c += 2)
+        *reinterpret_cast<double2*>(&Gs[mypos * S::LDG + c]) = make_double2(rowA[c], rowA[c + 1]);
+    }
+  }
+  __syncwarp();
+  // ------------------------------------ phase 2: operator G (X L = R)
+  // R rows: identity for U-row positions, -M for reduced positions, -C' for border rows
+  {
+    double x[N];
+#pragma unroll
+    for (int c = 0; c < N; ++c) x[c] = (mypos < n) ? (c == mypos ? 1.0 : 0.0) : -rowA[c];
+#pragma unroll
+    for (int c = 0; c < N; ++c) rowC[c] = -rowC[c];
+    // right-looking: once x[mm] is final, update every x[c], c < mm (the
+    // updates of one step are independent, so the dependent chain is N long)
+#pragma unroll
+    for (int mm = N - 1; mm > 0; --mm) {
+      const double xm = x[mm], cm = rowC[mm];
+      const double* Lrow = Gs + mm * S::LDG;  // L(mm, 0..mm-1)
+#pragma unroll
+      for (int c = 0; c < mm; c += 2) {
+        const double2 l2 = *reinterpret_cast<const double2*>(&Lrow[c]);
+        x[c] = fma(-xm, l2.x, x[c]);
+        rowC[c] = fma(-cm, l2.x, rowC[c]);
+        if (c + 1 < mm) {
+          x[c + 1] = fma(-xm, l2.y, x[c + 1]);
+          rowC[c + 1] = fma(-cm, l2.y, rowC[c + 1]);
         }
       }
     }
     __syncwarp();
-    // ----------------------------------------- phase 3: tensor-core GEMM
-    // two passes over the column tiles keep the accumulators within budget
+    if (act) {
 #pragma unroll
-    for (int pass = 0; pass < 2; ++pass) {
+      for (int c = 0; c < N; c += 2)
+        *reinterpret_cast<double2*>(&Gs[mypos * S::LDG + c]) = make_double2(x[c], x[c + 1]);
+    }
+    if (lane < 8) {  // border rows (zero when lane >= nr)
+#pragma unroll
+      for (int c = 0; c < N; c += 2) {
+        const bool live = lane < nr;
+        *reinterpret_cast<double2*>(&Gs[(n2 + lane) * S::LDG + c]) =
+            make_double2(live ? rowC[c] : 0.0, live ? rowC[c + 1] : 0.0);
+      }
+    }
+  }
+  __syncwarp();
+  // ----------------------------------------- phase 3: tensor-core GEMM
+  // two passes over the column tiles keep the accumulators within budget
+#pragma unroll
+  for (int pass = 0; pass < 2; ++pass) {
     constexpr int PC = S::PC;
     double acc[S::MTILES][PC][2];
 #pragma unroll
@@ -872,21 +883,167 @@ __global__ void __launch_bounds__(128, 4) k_factor_lu_tc(FactorArgs<double> a0, 
               if (rr < nr) {
                 if (col < n) {
                   const size_t o = (size_t)jp * nrn + (size_t)col * nr + rr;
-                  a.C[o] = srcC[o] + v;
+                  a.C[o] = ldw(srcC + o) + v;
                 } else if (col < n2) {
                   a.Rbuf[(size_t)j * nrn + (size_t)(col - n) * nr + rr] = v;
                 } else if (col < n2 + nx) {
-                  a.Fbuf[(size_t)j * nrnx + (size_t)(col - n2) * nr + rr] = v;
+                  // own F update plus the partial sums of the child nodes (tree)
+                  const size_t e = (size_t)(col - n2) * nr + rr;
+                  double s = v;
+                  if (tr.c1) s += ldw(a.Fbuf + (size_t)tr.c1 * nrnx + e);
+                  if (tr.c2) s += ldw(a.Fbuf + (size_t)tr.c2 * nrnx + e);
+                  a.Fbuf[(size_t)j * nrnx + e] = s;
                 } else if (col < NT) {
-                  a.XB[(size_t)j * nr * nrf + (size_t)(col - n2 - nx) * nr + rr] = v;
+                  const size_t e = (size_t)(col - n2 - nx) * nr + rr, nrr = (size_t)nr * nrf;
+                  double s = v;
+                  if (tr.c1) s += ldw(a.XB + (size_t)tr.c1 * nrr + e);
+                  if (tr.c2) s += ldw(a.XB + (size_t)tr.c2 * nrr + e);
+                  a.XB[(size_t)j * nrr + e] = s;
                 }
               }
             }
           }
       }
     }
-    }  // pass
-    __syncwarp();
+  }  // pass
+  __syncwarp();
+  return true;
+}
+
+template <int N, bool BATCH = false>
+__global__ void __launch_bounds__(128, 4) k_factor_lu_tc(FactorArgs<double> a0, const FactorArgs<double>* tab,
+                                                       const BatchCta* cmap) {
+  using S = TcShape<N>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  FactorArgs<double> ab;  // this CTA's system (batch only)
+  long q0, q1, qs;
+  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
+  const FactorArgs<double>& a = BATCH ? ab : a0;
+  double* Wt = reinterpret_cast<double*>(smem_raw + (size_t)warp * S::BYTES);
+  const TcTree none{0, 0, 0};
+  for (long q = q0; q < q1; q += qs) {
+    const int j = a.k + (int)(2L * a.k * q);
+    tc_pair<N>(a, j, a.k, a.first != 0, Wt, lane, none);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The whole cyclic reduction of one system in one launch (tree schedule).
+//
+// Node j >= 1 is the pair (j - K, j) of level K = lowbit(j).  Its TOP row
+// jp = j - K is final once the pair (jp, jp + K/2) -- node j - K/2 -- is done
+// (K >= 2); its BOTTOM row j once the last pair of row j's own chain, node
+// j + k'' (k'' the largest power of two below K with j + k'' < nblock), is
+// done.  So each node waits for at most two children, and each node has one
+// parent: the next pair of row jp's chain (node jp + 2K, when jp is a multiple
+// of 4K and jp + 2K < nblock), otherwise the pair that eliminates row jp
+// (node jp); node jp = 0 is the root.  Warps take the level-1 nodes (the
+// leaves) from a counter; a warp that finishes a node adds one to its
+// parent's arrival counter, and the warp that brings the count to the
+// parent's number of children carries on with the parent.  No warp ever
+// waits for another: the schedule needs no grid barrier and cannot stall.
+//
+// The border bookkeeping of the level-by-level schedule moves into the tree:
+// the C_jpp updates a pair leaves in Rbuf[j] are gathered by the node that
+// eliminates that block (or, for C_nblock, by the root), and the F and xb
+// updates are summed up the tree (each node adds its children's partial sums
+// to its own, in a fixed order), so results are bit-reproducible run to run.
+// ---------------------------------------------------------------------------
+__host__ __device__ inline int lowbit(int v) { return v & -v; }
+
+// parent node of node j, 0 for the root
+__host__ __device__ inline int tree_parent(int j, int nb) {
+  const int K = lowbit(j), jp = j - K;
+  if ((jp & (4 * K - 1)) == 0 && jp + 2 * K < nb) return jp + 2 * K;
+  return jp;
+}
+// children of node j (0: none): the TOP child, then the BOTTOM child
+__host__ __device__ inline void tree_children(int j, int nb, int& c1, int& c2) {
+  const int K = lowbit(j);
+  c1 = K >= 2 ? j - K / 2 : 0;
+  c2 = 0;
+  if (K >= 2 && j + 1 < nb) {
+    int kk = K / 2;
+    while (j + kk >= nb) kk >>= 1;
+    c2 = j + kk;
+  }
+}
+
+struct TreeArgs {
+  int* cnt;         // [nblock] arrival counters (zero at launch)
+  int* leaf;        // next level-1 node to take (zero at launch)
+  double* Ffin;     // out: F0 + all F updates (nr x nx, FP64)
+  double* xb;       // fused solve: rows of xb in x (+= sum of the xb updates), or null
+};
+
+// Work of the root: C_nblock with the C_jpp updates of the pairs whose jpp is
+// nblock (one per level at most, in level order), F = F0 + sum of every F
+// update, xb += sum of every xb update.
+template <int N>
+__device__ void tree_root(const FactorArgs<double>& a, const TreeArgs& ta, int root, int lane) {
+  const Dims d = a.d;
+  const int nb = d.nblock, nr = d.nr, nx = d.nx;
+  const size_t nrn = (size_t)nr * N, nrnx = (size_t)nr * nx;
+  for (size_t e = lane; e < nrn; e += 32) {
+    double s = ldw(a.C + (size_t)nb * nrn + e);
+    for (int K = 1; K < nb; K *= 2) {
+      const long np = pairs_at_level(nb, K);
+      const int jl = (int)(K * (2 * np - 1));
+      if (np > 0 && jl + K >= nb) s += ldw(a.Rbuf + (size_t)jl * nrn + e);
+    }
+    a.C[(size_t)nb * nrn + e] = s;
+  }
+  for (size_t e = lane; e < nrnx; e += 32) {
+    const int r = (int)(e % nr), c = (int)(e / nr);
+    ta.Ffin[e] = a.F0[(size_t)c * nr + r] + ldw(a.Fbuf + (size_t)root * nrnx + e);
+  }
+  if (ta.xb) {
+    for (int e = lane; e < nr * a.nrf; e += 32) {
+      const int r = e % nr, c = e / nr;
+      ta.xb[(size_t)c * a.ldx + r] += ldw(a.XB + (size_t)root * nr * a.nrf + e);
+    }
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(128, 4) k_factor_tree_tc(FactorArgs<double> a, TreeArgs ta) {
+  using S = TcShape<N>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* Wt = reinterpret_cast<double*>(smem_raw + (size_t)warp * S::BYTES);
+  const int nb = a.d.nblock;
+  const long leaves = pairs_at_level(nb, 1);
+  for (;;) {
+    int q = 0;
+    if (lane == 0) q = atomicAdd(ta.leaf, 1);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (q >= leaves) break;
+    int j = 2 * q + 1;
+    for (;;) {
+      const int K = lowbit(j);
+      TcTree tr;
+      tr.gather = K / 2;
+      tree_children(j, nb, tr.c1, tr.c2);
+      tc_pair<N>(a, j, K, K == 1, Wt, lane, tr);
+      const int par = tree_parent(j, nb);
+      if (par == 0) {  // the root: every pair is done
+        __threadfence();
+        tree_root<N>(a, ta, j, lane);
+        break;
+      }
+      // publish this node's results, then count the arrival at the parent
+      __threadfence();
+      int old = 0;
+      if (lane == 0) old = atomicAdd(ta.cnt + par, 1);
+      old = __shfl_sync(0xffffffffu, old, 0);
+      int c1, c2;
+      tree_children(par, nb, c1, c2);
+      const int expected = (c1 != 0) + (c2 != 0);
+      if (old + 1 < expected) break;  // the other child's warp will carry on
+      __threadfence();                // acquire: the children's results are visible
+      j = par;
+    }
   }
 }
 
@@ -3194,6 +3351,8 @@ struct FactorPlan {
   size_t umma_smem = 0;
   void (*tc)(FactorArgs<T>, const FactorArgs<T>*, const BatchCta*) = nullptr;               // tensor-core LU (FP64, n = 8, 16)
   size_t tc_smem = 0;
+  void (*tree)(FactorArgs<double>, TreeArgs) = nullptr;  // tc pairs, whole reduction in one launch
+  int tree_ctas = 0;
   void (*grp)(FactorArgs<T>, const FactorArgs<T>*, const BatchCta*) = nullptr;              // CTA of 2n threads per pair (n = 16, 32)
   size_t grp_smem = 0;
   int grp_threads = 0, grp_ctas = 0;
@@ -3219,10 +3378,16 @@ static FactorPlan<T> plan_factor(const DevState& s) {
   if (p.smem <= SMEM_MAX) smem_limit_once(p.smem_k, p.smem);
   if constexpr (sizeof(T) == 8) {
     if (s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 && (n == 16 || n == 8) && s.use_tc &&
-        (s.pair_kernel == PAIR_AUTO || s.pair_kernel == PAIR_TC)) {
+        (s.pair_kernel == PAIR_AUTO || s.pair_kernel == PAIR_TC || s.pair_kernel == PAIR_TREE)) {
       p.tc_smem = tc_smem_per_warp(n) * 4;
       if (n == 16) { p.tc = k_factor_lu_tc<16>; smem_limit_once(k_factor_lu_tc<16>, p.tc_smem); p.tc_cols = TcShape<16>::NTP; }
       else { p.tc = k_factor_lu_tc<8>; smem_limit_once(k_factor_lu_tc<8>, p.tc_smem); p.tc_cols = TcShape<8>::NTP; }
+      // the tree schedule (single systems with at least one pair)
+      if (s.pair_kernel != PAIR_TC && s.tree_cnt && d.nblock >= 2) {
+        p.tree = n == 16 ? k_factor_tree_tc<16> : k_factor_tree_tc<8>;
+        smem_limit_once(p.tree, p.tc_smem);
+        p.tree_ctas = 148 * resident_ctas(p.tree, 128, p.tc_smem);
+      }
     }
   }
   const bool grp_ok = s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 &&
@@ -3275,9 +3440,11 @@ static int fusable_rhs(const DevState& s, const FactorPlan<T>& p, int nrhs) {
   return 2 * s.d.n + s.d.nx + nrhs <= p.tc_cols ? nrhs : 0;
 }
 
-// every CR level: pair eliminations and the C_jpp border fix-up
+// every CR level: pair eliminations and the C_jpp border fix-up.  Returns true
+// when the tree schedule ran, which also leaves F (s.Ffin), C_nblock and, for
+// fused right-hand sides, xb complete.
 template <typename T>
-static void factor_levels(DevState& s, const FactorPlan<T>& p, const WorkSet<T>& w, double* x, int ldx,
+static bool factor_levels(DevState& s, const FactorPlan<T>& p, const WorkSet<T>& w, double* x, int ldx,
                           int nrf, cudaStream_t st) {
   const Dims d = s.d;
   const int n = d.n, nb = d.nblock;
@@ -3299,6 +3466,21 @@ static void factor_levels(DevState& s, const FactorPlan<T>& p, const WorkSet<T>&
   a.Tm = w.Tm; a.P = s.P; a.Rbuf = w.Rbuf; a.Fbuf = s.Fbuf; a.st = s.st;
   a.ldw = odd_ld(2 * n + d.nr);
   a.x = x; a.ldx = ldx; a.nrf = nrf; a.XB = s.XB;
+  if constexpr (sizeof(T) == 8) {
+    if (p.tree) {
+      a.F0 = s.F0;
+      TreeArgs ta;
+      ta.cnt = s.tree_cnt;
+      ta.leaf = s.tree_cnt + nb;
+      ta.Ffin = s.Ffin;
+      ta.xb = (nrf > 0 && d.nr > 0) ? x + (size_t)(nb + 1) * n + d.qr : nullptr;
+      cudaMemsetAsync(s.tree_cnt, 0, (size_t)(nb + 1) * sizeof(int), st);
+      const long leaves = pairs_at_level(nb, 1);
+      p.tree<<<grid_for(leaves, 4, p.tree_ctas), 128, p.tc_smem, st>>>(a, ta);
+      check_launch("k_factor_tree_tc");
+      return true;
+    }
+  }
   for (int k = 1; k < nb; k *= 2) {
     a.k = k;
     a.first = (k == 1);
@@ -3317,14 +3499,15 @@ static void factor_levels(DevState& s, const FactorPlan<T>& p, const WorkSet<T>&
       check_launch("k_border_fix");
     }
   }
+  return false;
 }
 
 // F = F0 + sum of the Schur updates (FP64); assemble and factor the last block (FP64)
 template <typename T>
-static void factor_last(DevState& s, const WorkSet<T>& w, cudaStream_t st) {
+static void factor_last(DevState& s, const WorkSet<T>& w, cudaStream_t st, bool f_done = false) {
   const Dims d = s.d;
   const int nrnx = d.nr * d.nx;
-  if (nrnx > 0)
+  if (nrnx > 0 && !f_done)
     reduce_blocks(s, s.Fbuf, 1, d.nblock - 1, nrnx, d.nr, s.F0, d.nr, s.Ffin, d.nr, st);
   k_last_assemble<T><<<grid_for((long)d.Nr * d.Nc, 256, 64), 256, 0, st>>>(
       d, w.D, w.E, w.B, w.C, s.H, s.Cq, s.Ffin, s.Hl);
@@ -3353,8 +3536,8 @@ static void factorize_t(DevState& s, cudaStream_t st) {
   T* tag = nullptr;
   const WorkSet<T> w = work_set(s, tag);
   const FactorPlan<T> p = plan_factor<T>(s);
-  factor_levels(s, p, w, nullptr, 0, 0, st);
-  factor_last(s, w, st);
+  const bool tree = factor_levels(s, p, w, nullptr, 0, 0, st);
+  factor_last(s, w, st, tree);
 }
 
 void launch_factorize(DevState& s, cudaStream_t st) {
@@ -3498,9 +3681,9 @@ void launch_factorize_solve(DevState& s, double* x, int ldx, int nrhs, cudaStrea
     launch_solve(s, x, ldx, nrhs, st);
     return;
   }
-  factor_levels(s, fp, w, x, ldx, nrf, st);
-  reduce_xb(s, x, ldx, nrf, st);
-  factor_last(s, w, st);
+  const bool tree = factor_levels(s, fp, w, x, ldx, nrf, st);
+  if (!tree) reduce_xb(s, x, ldx, nrf, st);
+  factor_last(s, w, st, tree);
   last_and_backward(s, plan_sweeps<double>(s), w, x, ldx, nrf, st);
 }
 

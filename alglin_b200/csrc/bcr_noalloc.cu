@@ -17,6 +17,7 @@
 // process exits.  Each call writes every scratch slot it later reads, so
 // nothing has to start at zero; all calls share the array, so calls that
 // overlap on the GPU (for example on two streams at once) race on it.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -36,6 +37,38 @@ static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_MAX_PARTS * NO
 constexpr int MAX_DEVICES = 64;
 std::mutex g_setup_mutex;
 double* g_scratch_ptr[MAX_DEVICES] = {};
+// the context each cached address belongs to: after a device reset the module
+// is loaded again in a new context and the array may move
+unsigned long long g_scratch_ctx[MAX_DEVICES] = {};
+
+// driver entry points for the current context's unique id (taken through the
+// runtime, so the library needs no link to libcuda)
+using PfnCtxGetCurrent = CUresult (*)(CUcontext*);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long*);
+
+// unique id of the calling thread's current context, 0 when unknown
+unsigned long long current_ctx_id() {
+  static PfnCtxGetCurrent get_current = nullptr;
+  static PfnCtxGetId get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<PfnCtxGetCurrent>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<PfnCtxGetId>(f);
+    looked_up = true;
+  }
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current && get_id && get_current(&ctx) == CUDA_SUCCESS && ctx && get_id(ctx, &id) == CUDA_SUCCESS)
+    return id;
+  return 0;
+}
 
 void set_err(char* buf, int len, const char* msg) {
   if (buf && len > 0) snprintf(buf, (size_t)len, "%s", msg);
@@ -129,12 +162,22 @@ extern "C" int bcr_mv_noalloc(int nblock, int n, int qr, int qx, int nr, int nx,
     set_err(errbuf, errlen, "bcr_mv_noalloc: a required device pointer is NULL");
     return BCR_BAD_ARGUMENT;
   }
-  // Set-up, once per device with that device current: the address of the
-  // scratch array on this device (the array's host-side name is not a device
-  // address).  The first call on each device does this look-up, so it should
-  // come before any stream capture.
+  // An error left pending by earlier work on this thread belongs to its owner:
+  // report it without clearing it, and launch nothing.
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess) {
+    char msg[200];
+    snprintf(msg, sizeof msg, "bcr_mv_noalloc: a CUDA error was already pending before the call: %s",
+             cudaGetErrorString(e));
+    set_err(errbuf, errlen, msg);
+    return BCR_CUDA_ERROR;
+  }
+  // Set-up, once per device (and again if the device's context was reset),
+  // with that device current: the address of the scratch array on this device
+  // (the array's host-side name is not a device address).  The first call on
+  // each device does this look-up, so it should come before any stream capture.
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) {
     set_err(errbuf, errlen, "bcr_mv_noalloc: no usable CUDA device");
     return BCR_CUDA_ERROR;
@@ -142,7 +185,8 @@ extern "C" int bcr_mv_noalloc(int nblock, int n, int qr, int qx, int nr, int nx,
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev]) {
+    const unsigned long long ctx = current_ctx_id();
+    if (!g_scratch_ptr[dev] || ctx == 0 || ctx != g_scratch_ctx[dev]) {
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess || !p) {
@@ -150,6 +194,7 @@ extern "C" int bcr_mv_noalloc(int nblock, int n, int qr, int qx, int nr, int nx,
         return BCR_CUDA_ERROR;
       }
       g_scratch_ptr[dev] = static_cast<double*>(p);
+      g_scratch_ctx[dev] = current_ctx_id();
     }
     scratch = g_scratch_ptr[dev];
   }
@@ -170,7 +215,7 @@ extern "C" int bcr_mv_noalloc(int nblock, int n, int qr, int qx, int nr, int nx,
     k_noalloc_border_parts<<<parts, NOALLOC_THREADS, 0, st>>>(d, C, x, chunk, scratch);
   }
   k_noalloc_tail<<<1, NOALLOC_THREADS, 0, st>>>(d, H, Cq, F, scratch, parts, alpha, x, beta, res);
-  e = cudaGetLastError();
+  e = cudaGetLastError();  // nothing was pending at entry: an error here is this call's
   if (e != cudaSuccess) {
     set_err(errbuf, errlen, cudaGetErrorString(e));
     return BCR_CUDA_ERROR;

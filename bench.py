@@ -10,12 +10,22 @@ Workload (one "step" = factorize + solve of one system):
           (bcr_factorize uploads the matrix from pinned host memory,
            bcr_solve copies the right-hand side in and the solution out)
 
-  variants: the mixed path (FP32 factors + FP64 refinement to rel. residual
-          <= 1e-12) on the same workload; FP64 and mixed on n=32, nblock=65536,
-          nr=nx=8 and on n=128, nblock=8192, qr=qx=4, nr=nx=16 (the mixed pair
-          kernel there runs its products on the tcgen05 tensor cores); and a
-          batch of 4096 uneven systems (systems/s, p50/p99 of the batch
-          latency), each through its own CUDA graph, device-timed.
+  variants: every other workload of the benchmark plan, each through its own
+          CUDA graph, device-timed: n=8 nblock=1000 (the CPU-sized case); this
+          workload with the QR panel, with 8 right-hand sides and on the mixed
+          path (FP32 factors + FP64 refinement to rel. residual <= 1e-12); FP64
+          and mixed on n=32, nblock=65536, nr=nx=8 at kappa = 1, 10, 100 and on
+          n=128, nblock=8192, qr=qx=4, nr=nx=16 (the mixed pair kernel there
+          runs its products on the tcgen05 tensor cores); a batch of 4096
+          uneven systems (systems/s, p50/p99 of the batch latency); and the
+          reference's own BorderedCR<float> (unrefined FP32) on this workload.
+
+  accuracy: every entry carries its relative residual
+          ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf), with A x taken by
+          the reference's own Mv on the host, and its forward error
+          ||x - x_ref||_inf / ||x_ref||_inf against the reference BorderedCR's
+          solution of the same seeded system (oracle/_ref, the unmodified
+          reference sources), whose host-core time is reported beside it.
 
 The matrix (0.65 GB) is larger than L2 (126 MB), so no L2 flush is needed
 between steps.  Multi-GPU: one process per GPU, each solving its own system
@@ -152,11 +162,14 @@ def launches_per_step(nblock, nr, nx):
     return fact + solve
 
 
-def cpu_reference_run(s, b, steps, warmup, threads):
-    """The reference's own BorderedCR (oracle/_ref) on the host cores."""
+def cpu_reference_run(s, b, steps, warmup, threads, internal="LU"):
+    """The reference's own BorderedCR (oracle/_ref) on the host cores with its
+    own thread pool: `warmup` untimed and `steps` timed factorize + solve runs,
+    each on a fresh copy of the matrix.  Returns (times, x, the object holding
+    the unfactored matrix)."""
     from oracle import pyoracle as po
-    src = po.RefBCR(s, "LU", "LU", "NONE", nthreads=threads, npb=threads)
-    work = po.RefBCR(s, "LU", "LU", "NONE", nthreads=threads, npb=threads)
+    src = po.RefBCR(s, internal, "LU", "NONE", nthreads=threads, npb=threads)
+    work = po.RefBCR(s, internal, "LU", "NONE", nthreads=threads, npb=threads)
     work.set_threads(True, True)
     times = []
     x = None
@@ -164,13 +177,45 @@ def cpu_reference_run(s, b, steps, warmup, threads):
         t, x = work.time_factor_solve(src, b)
         if i >= warmup:
             times.append(t)
-    return times, x
+    return times, x, src
 
 
-def rel_residual_host(h, s, x, b):
-    """||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) with the device Mv."""
-    r = h.mv(x[:s.ncols])[:s.nrows] - b[:s.nrows]
-    return float(np.abs(r).max() / (s.norm_inf() * np.abs(x[:s.ncols]).max() + np.abs(b[:s.nrows]).max()))
+def accuracy(s, x, b, ref_src=None, x_ref=None):
+    """Relative residual ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) with
+    A x from the reference's own Mv (ref_src, an unfactored RefBCR; the C
+    oracle's Mv when the reference is not built) and the forward error
+    ||x - x_ref||_inf / ||x_ref||_inf against the reference solution.  x, b
+    may hold several right-hand sides (rows); the worst column is reported."""
+    from oracle import pyoracle as po
+    mv = ref_src.mv if ref_src is not None else po.Oracle(s).mv
+    X = np.atleast_2d(x)
+    Bm = np.atleast_2d(b)
+    nA = s.norm_inf()
+    rel = 0.0
+    for c in range(X.shape[0]):
+        r = Bm[c, :s.nrows] - mv(X[c, :s.ncols])
+        rel = max(rel, float(np.abs(r).max() / (nA * np.abs(X[c, :s.ncols]).max() + np.abs(Bm[c, :s.nrows]).max())))
+    out = {"rel_residual": rel, "residual_mv": "reference" if ref_src is not None else "oracle"}
+    if x_ref is not None:
+        XR = np.atleast_2d(x_ref)
+        fe = max(float(np.abs(X[c, :s.ncols] - XR[c, :s.ncols]).max() / np.abs(XR[c, :s.ncols]).max())
+                 for c in range(X.shape[0]))
+        out["fwd_err"] = fe
+        out["fwd_err_vs"] = "reference BorderedCR (oracle/_ref)"
+    return out
+
+
+def reference_point(s, b, threads, internal="LU", runs=1):
+    """The reference BorderedCR's time and solution for system s (None when
+    oracle/_ref is not built)."""
+    from oracle import pyoracle as po
+    if not po.ref_available():
+        return None
+    times, x, src = cpu_reference_run(s, b, runs, 0, threads, internal)
+    t = statistics.median(times)
+    return {"t": t, "x": x, "src": src,
+            "json": {"ms": t * 1e3, "value": s.ncols / t, "unit": "unknowns/s", "cores": threads,
+                     "kind": "reference", "runs": runs}}
 
 
 def run_reference(args):
@@ -185,18 +230,19 @@ def run_reference(args):
     s = synth.collocation(**CFG, seed=0)
     b = synth.rhs(s, 1, seed=1)[0]
     threads = os.cpu_count() or 1
-    steps = max(1, min(args.steps, 5))
-    warm = max(1, min(args.warmup, 1))
-    times, x = cpu_reference_run(s, b, steps, warm, threads)
+    steps, warm = args.steps, args.warmup
+    times, x, src = cpu_reference_run(s, b, steps, warm, threads)
     t = statistics.median(times)
     v = s.ncols / t
     line = {"metric": METRIC, "value": v, "unit": "unknowns/s", "n_gpus": args.gpus, "steps": steps,
             "warmup": warm, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": workload_config({"threads": threads}),
+            "config": workload_config(), "cpu_threads": threads,
             "cpu_baseline": {"value": v, "unit": "unknowns/s", "cores": threads, "kind": "reference",
-                             "sample": "full workload, median of %d factorize+solve runs" % steps},
+                             "sample": "full workload, median of %d factorize+solve runs after %d "
+                                       "untimed" % (steps, warm)},
             "e2e": {"value": v, "unit": "unknowns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line.update(accuracy(s, x, b, src))
     print(json.dumps(line))
     return 0
 
@@ -261,17 +307,15 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = world * s.ncols / (ms * 1e-3)
-
-    # accuracy of the timed result
     x = x_dev.cpu().numpy()
-    relres = rel_residual_host(h, s, x, b)
 
+    if args.no_e2e:
+        acc = accuracy(s, x, b)
+        print(json.dumps({"value": value, "ms_per_step": ms, "phases_ms": {"factorize": fact_ms, "solve": solve_ms},
+                          "nblock": CFG["nblock"], "clocks": clocks, **acc}))
+        return 0
     # end to end through the C ABI with host buffers: factorize + solve in one
     # call (the matrix is uploaded from the pinned host copy every step)
-    if args.no_e2e:
-        print(json.dumps({"value": value, "ms_per_step": ms, "phases_ms": {"factorize": fact_ms, "solve": solve_ms},
-                          "rel_residual": relres, "nblock": CFG["nblock"], "clocks": clocks}))
-        return 0
     xh = b.copy()
     for _ in range(2):
         assert h.factorize_solve(1, xh, L), h.last_error()
@@ -295,18 +339,17 @@ def run_ours(args):
     achieved = fact_b / (fact_ms * 1e-3) / 1e9
     line = None
     if rank == 0:
-        cpu = None
+        cpu, ref = None, None
         if world == 1 and not args.no_cpu:
-            cpu = cpu_baseline(s, b)
+            cpu, ref = cpu_baseline(s, b, args.steps, args.warmup)
         line = {
             "metric": METRIC, "value": value, "unit": "unknowns/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "ours",
-            "config": workload_config({"parallelism": f"replicas x{world}"}),
+            "config": workload_config(), "parallelism": f"replicas x{world}",
             "phases_ms": {"factorize": fact_ms, "solve": solve_ms},
-            "rel_residual": relres,
-            "roofline": {"bound": "hbm", "kernel": "factorize (all CR level launches)",
+            "roofline": {"bound": "hbm", "kernel": "factorize (tree-scheduled CR launch + last block)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": FACT_DRAM_BYTES_PER_BLOCK * CFG["nblock"],
@@ -319,10 +362,13 @@ def run_ours(args):
             "gpu_launches": launches_per_step(CFG["nblock"], CFG["nr"], CFG["nx"]) * args.steps,
             "clocks": clocks,
         }
+        line.update(accuracy(s, x, b, ref["src"] if ref else None, ref["x"] if ref else None))
         if cpu:
             line["cpu_baseline"] = cpu
         if not args.no_variants and world == 1:
-            line["variants"] = variants(torch, bcr, synth, min(args.steps, 10), 3, rank)
+            threads = os.cpu_count() or 1
+            line["variants"] = variants(torch, bcr, synth, min(args.steps, 10), 3, rank, threads,
+                                        s, b, ref, h)
         print(json.dumps(line))
     if dist:
         dist.barrier()
@@ -330,16 +376,19 @@ def run_ours(args):
     return 0
 
 
-def graph_step_time(torch, bcr, h, s, b, steps, warmup, prec):
-    """Device time of one factorize + solve graph step of system s on handle h."""
+def graph_step_time(torch, bcr, h, s, b, steps, warmup, prec, nrhs=1):
+    """Device time of one factorize + solve graph step of system s on handle h
+    (b: one right-hand side, or nrhs of them as rows).  Returns the timing
+    entry and the solution."""
     L = max(s.nrows, s.ncols)
     h.set_precision(prec)
     h.upload()
-    b_dev = torch.from_numpy(b).cuda()
+    bb = np.ascontiguousarray(np.atleast_2d(b)[:, :L])
+    b_dev = torch.from_numpy(bb).cuda()
     x_dev = torch.empty_like(b_dev)
     torch.cuda.synchronize()
     stream = torch.cuda.ExternalStream(h.stream())
-    h.graph_capture(bcr.GRAPH_STEP, 1, x_dev.data_ptr(), L, b_dev.data_ptr())
+    h.graph_capture(bcr.GRAPH_STEP, nrhs, x_dev.data_ptr(), L, b_dev.data_ptr())
     for _ in range(warmup):
         h.graph_launch(bcr.GRAPH_STEP)
     h.synchronize()
@@ -354,58 +403,117 @@ def graph_step_time(torch, bcr, h, s, b, steps, warmup, prec):
     assert h.factorize_status(), h.last_error()
     it, rr = h.refinement_info()
     x = x_dev.cpu().numpy()
-    relres = rel_residual_host(h, s, x, b)
     return {"value": s.ncols / (ms * 1e-3), "unit": "unknowns/s", "ms_per_step": ms,
-            "rel_residual": relres, "refinement_steps": it if prec else 0}
+            "refinement_steps": it if prec else 0}, (x if nrhs > 1 else x[0])
 
 
-def variants(torch, bcr, synth, steps, warmup, rank):
-    """The other measured paths: the mixed path on this workload, both paths on
-    the n=32 and n=128 workloads, and the batch of 4096 uneven systems."""
+def _entry(timing, s, x, b, ref, **extra):
+    e = dict(timing)
+    e.update(accuracy(s, x, b, ref["src"] if ref else None, ref["x"] if ref else None))
+    if ref:
+        e["reference"] = ref["json"]
+    e.update(extra)
+    return e
+
+
+def variants(torch, bcr, synth, steps, warmup, rank, threads, sB, bB, refB, hB):
+    """The other measured paths (see the module docstring), each with its
+    residual and forward error against the reference BorderedCR's solution of
+    the same system and the reference's time on the host cores."""
+    from oracle import pyoracle as po
     out = {}
-    sB = synth.collocation(**CFG, seed=rank)
-    bB = synth.rhs(sB, 1, seed=1 + rank)[0]
-    h = bcr.BorderedCR()
-    h.load_system(sB)
-    out["B_mixed"] = graph_step_time(torch, bcr, h, sB, bB, steps, warmup, bcr.PRECISION_MIXED)
-    del h
+    # n=8 nblock=1000: the reference's CPU-runnable case
+    cA = dict(synth.CONFIGS["A"])
+    sA = synth.collocation(**cA, seed=rank)
+    bA = synth.rhs(sA, 1, seed=1 + rank)[0]
+    hA = bcr.BorderedCR()
+    hA.load_system(sA)
+    tA, xA = graph_step_time(torch, bcr, hA, sA, bA, steps, warmup, bcr.PRECISION_FP64)
+    refA = reference_point(sA, bA, threads, runs=5)
+    out["A_fp64"] = _entry(tA, sA, xA, bA, refA, workload="trapezoid-collocation BABD n=8 nblock=1000 nr=nx=2, 1 rhs")
+    del hA
+    wlB = "trapezoid-collocation BABD n=16 nblock=100000 qr=qx=2 nr=nx=4"
+    # mixed path on the headline system
+    hB.select("LU")
+    t, x = graph_step_time(torch, bcr, hB, sB, bB, steps, warmup, bcr.PRECISION_MIXED)
+    out["B_mixed"] = _entry(t, sB, x, bB, refB, workload=wlB + ", 1 rhs")
+    # 8 right-hand sides: factorize + solve(8, ...)
+    b8 = synth.rhs(sB, 8, seed=11 + rank)
+    t, x8 = graph_step_time(torch, bcr, hB, sB, b8, steps, warmup, bcr.PRECISION_FP64, nrhs=8)
+    ref8 = None
+    if refB:
+        tt, xr8, _ = cpu_reference_run(sB, b8, 1, 0, threads)
+        ref8 = {"x": xr8, "src": refB["src"],
+                "json": {"ms": tt[0] * 1e3, "value": sB.ncols / tt[0], "unit": "unknowns/s", "cores": threads,
+                         "kind": "reference", "runs": 1}}
+    t["solutions_per_s"] = 8 * 1e3 / t["ms_per_step"]
+    out["B_fp64_rhs8"] = _entry(t, sB, x8, b8, ref8, workload=wlB + ", factorize + solve(8, X, ld)")
+    # QR panels
+    hB.select("QR")
+    t, x = graph_step_time(torch, bcr, hB, sB, bB, steps, warmup, bcr.PRECISION_FP64)
+    refQ = reference_point(sB, bB, threads, internal="QR")
+    out["B_fp64_QR"] = _entry(t, sB, x, bB, refQ, workload=wlB + ", internal QR, 1 rhs")
+    hB.select("LU")
+    del refQ
+    # the reference's own BorderedCR<float> (no refinement) on the host cores
+    if po.ref_available():
+        tf, xf = po.ref_f32_factor_solve(sB, bB, threads, threads)
+        out["B_reference_f32_cpu"] = _entry({"value": sB.ncols / tf, "unit": "unknowns/s", "ms_per_step": tf * 1e3,
+                                             "cores": threads}, sB, xf, bB, refB,
+                                            workload=wlB + ", reference BorderedCR<float> on the host cores, "
+                                                           "unrefined FP32")
+    # n=32 nblock=65536 at three condition levels
     cC = dict(synth.CONFIGS["C"])
-    sC = synth.collocation(**cC, kappa=1.0, seed=rank)
-    bC = synth.rhs(sC, 1, seed=1 + rank)[0]
-    hC = bcr.BorderedCR()
-    hC.load_system(sC)
-    f64 = graph_step_time(torch, bcr, hC, sC, bC, steps, warmup, bcr.PRECISION_FP64)
-    mix = graph_step_time(torch, bcr, hC, sC, bC, steps, warmup, bcr.PRECISION_MIXED)
-    del hC
-    wl = "trapezoid-collocation BABD n=32 nblock=65536 nr=nx=8 kappa=1, 1 rhs"
-    out["C_fp64"] = dict(f64, workload=wl)
-    out["C_mixed"] = dict(mix, workload=wl)
-    out["C_mixed_over_fp64"] = mix["value"] / f64["value"]
+    for kappa in (1.0, 10.0, 100.0):
+        sC = synth.collocation(**cC, kappa=kappa, seed=rank)
+        bC = synth.rhs(sC, 1, seed=1 + rank)[0]
+        hC = bcr.BorderedCR()
+        hC.load_system(sC)
+        refC = reference_point(sC, bC, threads)
+        f64, x64 = graph_step_time(torch, bcr, hC, sC, bC, steps, warmup, bcr.PRECISION_FP64)
+        mix, xmx = graph_step_time(torch, bcr, hC, sC, bC, steps, warmup, bcr.PRECISION_MIXED)
+        wl = "trapezoid-collocation BABD n=32 nblock=65536 nr=nx=8 kappa=%g, 1 rhs" % kappa
+        k = "%g" % kappa
+        out["C_fp64_k" + k] = _entry(f64, sC, x64, bC, refC, workload=wl)
+        out["C_mixed_k" + k] = _entry(mix, sC, xmx, bC, refC, workload=wl)
+        out["C_mixed_over_fp64_k" + k] = mix["value"] / f64["value"]
+        del hC, sC, refC
+    # n=128 nblock=8192: tcgen05 split-precision pair kernel on the mixed path
     cE = dict(synth.CONFIGS["E"])
     sE = synth.collocation(**cE, seed=rank)
     bE = synth.rhs(sE, 1, seed=1 + rank)[0]
     hE = bcr.BorderedCR()
     hE.load_system(sE)
-    f64 = graph_step_time(torch, bcr, hE, sE, bE, steps, warmup, bcr.PRECISION_FP64)
-    mix = graph_step_time(torch, bcr, hE, sE, bE, steps, warmup, bcr.PRECISION_MIXED)
-    del hE, sE
+    f64, x64 = graph_step_time(torch, bcr, hE, sE, bE, steps, warmup, bcr.PRECISION_FP64)
+    mix, xmx = graph_step_time(torch, bcr, hE, sE, bE, steps, warmup, bcr.PRECISION_MIXED)
+    del hE
+    refE = reference_point(sE, bE, threads)
     wl = "trapezoid-collocation BABD n=128 nblock=8192 qr=qx=4 nr=nx=16, 1 rhs"
-    out["E_fp64"] = dict(f64, workload=wl, pair_kernel="FP64 blocked LU, DMMA products")
-    out["E_mixed"] = dict(mix, workload=wl, pair_kernel="FP32 LU, tcgen05 3xTF32 products")
+    out["E_fp64"] = _entry(f64, sE, x64, bE, refE, workload=wl, pair_kernel="FP64 blocked LU, DMMA products")
+    out["E_mixed"] = _entry(mix, sE, xmx, bE, refE, workload=wl, pair_kernel="FP32 LU, tcgen05 3xTF32 products")
     out["E_mixed_over_fp64"] = mix["value"] / f64["value"]
+    del sE, refE
     for name, prec in (("D_batched_fp64", bcr.PRECISION_FP64), ("D_batched_mixed", bcr.PRECISION_MIXED)):
         try:
-            out[name] = batched(torch, bcr, synth, rank, prec)
+            out[name] = batched(torch, bcr, synth, rank, prec, threads)
         except Exception as e:  # e.g. not enough device memory on a shared GPU
             out[name] = {"unavailable": str(e)[:200]}
         torch.cuda.empty_cache()
     return out
 
 
-def batched(torch, bcr, synth, rank, prec, nsys=4096):
+def batched(torch, bcr, synth, rank, prec, threads, nsys=4096, sample_every=32):
     """4096 independent systems, nblock ~ U{64..4096}, n in {4,8,16,32},
-    nr = nx in {0,2,4}: one CUDA graph per factorize + solve of the whole batch."""
+    nr = nx in {0,2,4}: one CUDA graph per factorize + solve of the whole batch.
+    Every 32nd system (128 in all) is also copied to the host: its GPU solution
+    is checked against the reference BorderedCR (residual with the reference's
+    Mv, forward error), and the reference solves those 128 systems with one
+    BorderedCR object per system (npb = 1) spread over the host cores, which
+    gives the reference's systems/s on the same mix."""
+    from concurrent.futures import ThreadPoolExecutor
+
     from cuda.bindings import runtime as rt
+    from oracle import pyoracle as po
     dims = synth.batch_dims(nsys, 64, 4096, seed=rank)
     bt = bcr.Batch()
     for d in dims:
@@ -414,6 +522,7 @@ def batched(torch, bcr, synth, rank, prec, nsys=4096):
     bt.prepare()
     g = torch.Generator(device="cuda")
     g.manual_seed(7 + rank)
+    kept = {}
     for i, d in enumerate(dims):
         ts = synth.collocation_torch(torch, *d, seed=i + nsys * rank)
         r, c = bt.system_size(i)
@@ -422,6 +531,10 @@ def batched(torch, bcr, synth, rank, prec, nsys=4096):
         torch.cuda.synchronize()  # the blocks and rhs are complete before they are copied
         bt.load_device(i, *[t.data_ptr() if t.numel() else 0 for t in ts])
         rt.cudaMemcpy(bt.device_b(i), rhs.data_ptr(), max(r, c) * 8, rt.cudaMemcpyKind.cudaMemcpyDeviceToDevice)
+        if i % sample_every == 0:
+            arr = [t.cpu().numpy() for t in ts]
+            kept[i] = (synth.BABD(*d, D=arr[0], E=arr[1], B=arr[2], C=arr[3], Cq=arr[4], F=arr[5], H=arr[6]),
+                       rhs.cpu().numpy())
     bt.autotune()
     bt.graph_capture()
     stream = torch.cuda.ExternalStream(bt.stream())
@@ -442,31 +555,67 @@ def batched(torch, bcr, synth, rank, prec, nsys=4096):
     lat.sort()
     p50, p99 = lat[len(lat) // 2], lat[-1]
     unk = sum(n * (nb + 1) + nx for nb, n, _, _, _, nx in dims)
-    return {"systems_per_s": nsys / (p50 * 1e-3), "unknowns_per_s": unk / (p50 * 1e-3),
-            "p50_ms": p50, "p99_ms": p99, "nsys": nsys, "all_factorized": bool(ok),
-            "refinement_steps": iters, "worst_rel_residual": worst if prec else None,
-            "classes": [{"n": c[0], "systems": c[1], "family": ["auto", "tc", "grp", "rows"][c[2]],
-                         "pairs_per_cta": c[3]} for c in bt.classes()],
-            "workload": "4096 systems, nblock U{64..4096}, n in {4,8,16,32}, nr=nx in {0,2,4}, "
-                        "collocation blocks drawn on the device"}
+    out = {"systems_per_s": nsys / (p50 * 1e-3), "unknowns_per_s": unk / (p50 * 1e-3),
+           "p50_ms": p50, "p99_ms": p99, "nsys": nsys, "all_factorized": bool(ok),
+           "refinement_steps": iters, "worst_rel_residual_device": worst if prec else None,
+           "classes": [{"n": c[0], "systems": c[1], "family": ["auto", "tc", "grp", "rows"][c[2]],
+                        "pairs_per_cta": c[3]} for c in bt.classes()],
+           "workload": "4096 systems, nblock U{64..4096}, n in {4,8,16,32}, nr=nx in {0,2,4}, "
+                       "collocation blocks drawn on the device"}
+    # the sampled systems' solutions, checked against the reference
+    xs = {}
+    for i, (s, _) in kept.items():
+        xh = np.zeros(max(s.nrows, s.ncols))
+        rt.cudaMemcpy(xh.ctypes.data, bt.device_x(i), xh.nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+        xs[i] = xh
+    if po.ref_available():
+        def ref_one(i):
+            s, rhs = kept[i]
+            src = po.RefBCR(s, "LU", "LU", "NONE", nthreads=0)
+            work = po.RefBCR(s, "LU", "LU", "NONE", nthreads=0)
+            t, xr = work.time_factor_solve(src, rhs)
+            return i, t, xr, src
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            res = list(ex.map(ref_one, sorted(kept)))
+        wall = time.perf_counter() - t0
+        worst_r, worst_f = 0.0, 0.0
+        for i, t, xr, src in res:
+            s, rhs = kept[i]
+            a = accuracy(s, xs[i], rhs, src, xr)
+            worst_r = max(worst_r, a["rel_residual"])
+            worst_f = max(worst_f, a["fwd_err"])
+        out["rel_residual"] = worst_r
+        out["fwd_err"] = worst_f
+        out["accuracy_sample"] = "%d systems (every %dth), worst over the sample, reference Mv and solution" % (
+            len(kept), sample_every)
+        out["reference"] = {"systems_per_s": len(kept) / wall, "cores": threads, "kind": "reference",
+                            "sample": "the same %d systems, one BorderedCR object per system (npb=1) on a "
+                                      "pool of %d host threads, factorize + solve" % (len(kept), threads)}
+    return out
 
 
-def cpu_baseline(s, b):
+def cpu_baseline(s, b, steps, warmup):
+    """The reference arm's measurement, run inside this arm: the reference
+    BorderedCR on the host cores, `warmup` untimed then `steps` timed
+    factorize + solve runs (median).  Returns (cpu_baseline entry, reference
+    point with the solution)."""
     from oracle import pyoracle as po
     threads = os.cpu_count() or 1
     if po.ref_available():
-        times, _ = cpu_reference_run(s, b, 3, 1, threads)
+        times, x, src = cpu_reference_run(s, b, steps, warmup, threads)
         t = statistics.median(times)
-        return {"value": s.ncols / t, "unit": "unknowns/s", "cores": threads, "kind": "reference",
-                "sample": "full workload, median of 3 factorize+solve runs of the reference "
-                          "BorderedCR with its own thread pool"}
+        return ({"value": s.ncols / t, "unit": "unknowns/s", "cores": threads, "kind": "reference",
+                 "sample": "full workload, median of %d factorize+solve runs after %d untimed, reference "
+                           "BorderedCR with its own thread pool" % (steps, warmup)},
+                {"x": x, "src": src, "json": {"ms": t * 1e3, "value": s.ncols / t, "cores": threads}})
     o = po.Oracle(s, "LU", "LU")
     t0 = time.perf_counter()
     o.factorize()
     o.solve(b)
     t = time.perf_counter() - t0
-    return {"value": s.ncols / t, "unit": "unknowns/s", "cores": 1, "kind": "port",
-            "sample": "full workload, one factorize+solve of the C oracle"}
+    return ({"value": s.ncols / t, "unit": "unknowns/s", "cores": 1, "kind": "port",
+             "sample": "full workload, one factorize+solve of the C oracle"}, None)
 
 
 def run_once(args):

@@ -127,6 +127,7 @@ int bcr_set_precision(bcr_handle h, int precision);      /* extension: FP64 / mi
 #define BCR_PAIR_CTA 4
 #define BCR_PAIR_SMEM 5
 #define BCR_PAIR_UMMA 6
+#define BCR_PAIR_TREE 7
 int bcr_set_pair_kernel(bcr_handle h, int choice);
 
 /* Iterative refinement of the mixed path (extension, no reference counterpart):
@@ -200,19 +201,20 @@ int bcr_graph_capture(bcr_handle h, int what, int nrhs, double *d_x, int ld, con
 int bcr_graph_launch(bcr_handle h, int what);
 
 /* --- allocation-free product ------------------------------------------------
- * No counterpart in the reference (whose Mv, cc:2111-2166, works on the
- * solver's own arrays).  res = alpha*A*x + beta*res for a matrix whose blocks
+ * No counterpart in the reference.  res = alpha*A*x + beta*res for a matrix whose blocks
  * (reference layout, see bcr_block_data), x and res are all caller-owned
  * DEVICE memory; for callers that cannot allocate device memory where they
  * need the product (a fixed memory budget owned by the host application, or a
  * loop that must not call into the CUDA allocator).  The library allocates
  * nothing: its only scratch is a fixed 512 KiB array in device memory, so nr
  * is limited to 64 border rows (larger nr is rejected with BCR_BAD_ARGUMENT).
- * The first call on each device looks the array up (cudaGetSymbolAddress);
- * make that first call before any stream capture.  All calls share the
- * array: calls that overlap on the GPU race.  Enqueued on `stream` (a
- * cudaStream_t, NULL for the legacy stream); errbuf (may be NULL) receives the
- * reason of a failure. */
+ * The first call on each device looks the array up (cudaGetSymbolAddress),
+ * and looks it up again after the device's context was reset; make that
+ * first call before any stream capture.  All calls share the array: calls
+ * that overlap on the GPU race.  A CUDA error already pending on the calling
+ * thread is reported (BCR_CUDA_ERROR) and left pending for its owner, and
+ * nothing is launched.  Enqueued on `stream` (a cudaStream_t, NULL for the
+ * legacy stream); errbuf (may be NULL) receives the reason of a failure. */
 int bcr_mv_noalloc(int nblock, int n, int qr, int qx, int nr, int nx,
                    const double *D, const double *E, const double *B, const double *C,
                    const double *Cq, const double *F, const double *H,

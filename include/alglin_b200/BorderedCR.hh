@@ -10,9 +10,16 @@
 //     Utils::Runtime_Error, which derives from std::runtime_error);
 //   * the element accessors B(nbl,i,j) ... H(i,j) return references into the
 //     handle's host copy of the matrix.
-// The constructor takes the thread count and the number of parallel blocks of
-// the reference's thread pool; they only affect info(), because the
-// factorization runs on the GPU.
+// The constructor has the reference's signature, BorderedCR( TP, npb ) with
+// TP a Utils::ThreadPoolBase* (hxx:373-384): the pool's thread count and npb
+// only affect info(), because the factorization runs on the GPU.  A program
+// that has the real UtilsLite pool defines ALGLIN_B200_EXTERNAL_UTILS and
+// includes it first; otherwise this header supplies a minimal Utils namespace
+// (ThreadPoolBase with thread_count(), ThreadPool0, ThreadPool1) so that the
+// reference's `Utils::ThreadPool1 TP(n); BorderedCR<double> BCR(&TP);`
+// compiles unchanged.  The class derives from LinearSystemSolver<double>, the
+// base whose factorize/solve/t_solve overloads the reference class overrides
+// (hxx:105, 362-364).
 //
 // With ALGLIN_B200_AS_ALGLIN defined, the class is also visible as
 // alglin::BorderedCR so that existing code switches by changing its include.
@@ -27,6 +34,29 @@
 #include <vector>
 
 #include "../alglin_b200.h"
+
+#ifndef ALGLIN_B200_EXTERNAL_UTILS
+// Thread-pool types of the reference's Utils library, reduced to what the
+// BorderedCR constructor reads (the thread count).  Tasks never run here.
+namespace Utils {
+  class ThreadPoolBase {
+  public:
+    virtual ~ThreadPoolBase() = default;
+    virtual unsigned thread_count() const = 0;
+  };
+  class ThreadPool0 : public ThreadPoolBase {
+  public:
+    explicit ThreadPool0( unsigned = 1 ) {}
+    unsigned thread_count() const override { return 1; }
+  };
+  class ThreadPool1 : public ThreadPoolBase {
+    unsigned m_n;
+  public:
+    explicit ThreadPool1( unsigned n ) : m_n( n < 1 ? 1 : n ) {}
+    unsigned thread_count() const override { return m_n; }
+  };
+}
+#endif
 
 namespace alglin_b200 {
 
@@ -50,10 +80,28 @@ namespace alglin_b200 {
     T const & operator () ( integer i, integer j ) const { return m_data[i + j * m_ld]; }
   };
 
+  // Base of the reference's BorderedCR (LapackWrapper's LinearSystemSolver,
+  // which the reference does not vendor): the factorize/solve/t_solve virtuals
+  // and the MatrixWrapper forms of solve/t_solve (used by the reference tests,
+  // test18:1018).
+  template <typename t_Value>
+  class LinearSystemSolver {
+  public:
+    using real_type = t_Value;
+    virtual ~LinearSystemSolver() = default;
+    virtual bool factorize() = 0;
+    virtual bool solve( t_Value x[] ) const = 0;
+    virtual bool solve( integer nrhs, t_Value rhs[], integer ldRhs ) const = 0;
+    virtual bool t_solve( t_Value x[] ) const = 0;
+    virtual bool t_solve( integer nrhs, t_Value rhs[], integer ldRhs ) const = 0;
+    bool solve( MatrixWrapper<t_Value> & M ) const { return this->solve( M.ncols(), M.data(), M.ldim() ); }
+    bool t_solve( MatrixWrapper<t_Value> & M ) const { return this->t_solve( M.ncols(), M.data(), M.ldim() ); }
+  };
+
   template <typename t_Value> class BorderedCR;
 
   template <>
-  class BorderedCR<double> {
+  class BorderedCR<double> : public LinearSystemSolver<double> {
   public:
     using real_type = double;
     using MatW      = MatrixWrapper<double>;
@@ -83,12 +131,23 @@ namespace alglin_b200 {
     BorderedCR( BorderedCR const & ) = delete;
     BorderedCR const & operator = ( BorderedCR const & ) = delete;
 
-    // BorderedCR( ThreadPoolBase * TP, integer npb )  hxx:373-384
+    using LinearSystemSolver<double>::solve;
+    using LinearSystemSolver<double>::t_solve;
+
+    // BorderedCR( Utils::ThreadPoolBase * TP, integer num_parallel_block = 0 )
+    // (hxx:373-384): with a pool, npb = its thread count, or the smaller of
+    // the two when npb > 0; without one (TP == nullptr), a single block
+    explicit BorderedCR( Utils::ThreadPoolBase * TP, integer num_parallel_block = 0 ) {
+      integer const nth = TP != nullptr ? integer( TP->thread_count() ) : 0;
+      if ( bcr_create( &m_h, nth, nth > 0 ? num_parallel_block : 0 ) != BCR_OK )
+        throw std::runtime_error( "alglin_b200: bcr_create failed" );
+    }
+    // the same from a thread count (no pool object needed)
     explicit BorderedCR( integer num_threads = 0, integer num_parallel_block = 0 ) {
       if ( bcr_create( &m_h, num_threads, num_parallel_block ) != BCR_OK )
         throw std::runtime_error( "alglin_b200: bcr_create failed" );
     }
-    ~BorderedCR() { bcr_destroy( m_h ); }
+    ~BorderedCR() override { bcr_destroy( m_h ); }
 
     bcr_handle handle() const { return m_h; }
 
@@ -247,13 +306,11 @@ namespace alglin_b200 {
     double & H( integer i, integer j )  { return bcr_block_data( m_h, 'H', 0 )[ i + j * ( block_size() + dim_qr() ) ]; }
 
     // --------------------------------------------------- factorize, solve
-    bool factorize() { return ok_or_false( bcr_factorize( m_h ) ); }
-    bool solve( real_type x[] ) const { return ok_or_false( bcr_solve( m_h, x ) ); }
-    bool solve( integer nrhs, real_type rhs[], integer ldRhs ) const { return ok_or_false( bcr_solve_n( m_h, nrhs, rhs, ldRhs ) ); }
-    bool solve( MatW & M ) const { return solve( M.ncols(), M.data(), M.ldim() ); }
-    bool t_solve( real_type x[] ) const { chk( bcr_t_solve( m_h, x ) ); return false; }
-    bool t_solve( integer nrhs, real_type rhs[], integer ld ) const { chk( bcr_t_solve_n( m_h, nrhs, rhs, ld ) ); return false; }
-    bool t_solve( MatW & M ) const { return t_solve( M.ncols(), M.data(), M.ldim() ); }
+    bool factorize() override { return ok_or_false( bcr_factorize( m_h ) ); }
+    bool solve( real_type x[] ) const override { return ok_or_false( bcr_solve( m_h, x ) ); }
+    bool solve( integer nrhs, real_type rhs[], integer ldRhs ) const override { return ok_or_false( bcr_solve_n( m_h, nrhs, rhs, ldRhs ) ); }
+    bool t_solve( real_type x[] ) const override { chk( bcr_t_solve( m_h, x ) ); return false; }
+    bool t_solve( integer nrhs, real_type rhs[], integer ld ) const override { chk( bcr_t_solve_n( m_h, nrhs, rhs, ld ) ); return false; }
 
     void Mv( real_type const x[], real_type res[] ) const { chk( bcr_mv( m_h, x, res ) ); }
     void add_Mv( real_type alpha, real_type const x[], real_type res[] ) const { chk( bcr_add_mv( m_h, alpha, x, res ) ); }
@@ -293,6 +350,7 @@ namespace alglin_b200 {
 #ifdef ALGLIN_B200_AS_ALGLIN
 namespace alglin {
   using alglin_b200::BorderedCR;
+  using alglin_b200::LinearSystemSolver;
   using alglin_b200::MatrixWrapper;
   using integer = alglin_b200::integer;
 }

@@ -24,9 +24,17 @@ LAST2 = {"NONE": 0, "SVD": 1, "LSS": 2, "LSY": 3, "PINV": 4}
 _dp = ct.POINTER(ct.c_double)
 
 
+_ip = ct.POINTER(ct.c_int)
+
+
 def _ptr(a: np.ndarray):
     assert a.dtype == np.float64 and a.flags.c_contiguous
     return a.ctypes.data_as(_dp)
+
+
+def _iptr(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_ip)
 
 
 def _load(path):
@@ -88,6 +96,11 @@ def ref_lib():
         L.ref_info.argtypes = [ct.c_void_p]
         L.ref_nrows.argtypes = [ct.c_void_p]
         L.ref_ncols.argtypes = [ct.c_void_p]
+        L.ref_sparse_nnz.argtypes = [ct.c_void_p]
+        L.ref_sparse_pattern.argtypes = [ct.c_void_p, _ip, _ip, ct.c_int]
+        L.ref_sparse_values.argtypes = [ct.c_void_p, _dp]
+        L.ref_f32_factor_solve.restype = ct.c_double
+        L.ref_f32_factor_solve.argtypes = [ct.c_int] * 8 + [_dp] * 8 + [ct.POINTER(ct.c_int)]
         L.ref_time_factor_solve.restype = ct.c_double
         L.ref_time_factor_solve.argtypes = [ct.c_void_p, ct.c_void_p, ct.c_int, _dp, ct.c_int,
                                             ct.POINTER(ct.c_int)]
@@ -145,6 +158,20 @@ class Oracle:
         return res[:self.s.nrows]
 
 
+def ref_f32_factor_solve(s, b, nthreads=0, npb=0):
+    """The reference's BorderedCR<float> (LU, last block LU) on system s with
+    every entry rounded to float: returns (seconds of factorize + solve, x)
+    with x converted back to double.  No refinement."""
+    L = ref_lib()
+    x = np.array(b, dtype=np.float64, order="C", copy=True)
+    arrs = _arrays(s)
+    ok = ct.c_int(0)
+    t = L.ref_f32_factor_solve(nthreads, npb, *s.dims(), *[_ptr(a) for a in arrs], _ptr(x), ct.byref(ok))
+    if not ok.value:
+        raise RuntimeError("reference BorderedCR<float> factor/solve failed")
+    return t, x
+
+
 class RefBCR:
     """The reference alglin::BorderedCR<double>, compiled from its own sources."""
 
@@ -195,6 +222,18 @@ class RefBCR:
         res = np.zeros(max(self.s.nrows, self.s.ncols))
         self.L.ref_mv(self.h, _ptr(x), _ptr(res))
         return res[:self.s.nrows]
+
+    def sparse(self):
+        """(I, J, V) of the reference's sparse_pattern(offs=0) / sparse_values."""
+        nnz = self.L.ref_sparse_nnz(self.h)
+        I = np.zeros(nnz, dtype=np.int32)
+        J = np.zeros(nnz, dtype=np.int32)
+        V = np.zeros(nnz)
+        if not self.L.ref_sparse_pattern(self.h, _iptr(I), _iptr(J), 0):
+            raise RuntimeError(self.last_error())
+        if not self.L.ref_sparse_values(self.h, _ptr(V)):
+            raise RuntimeError(self.last_error())
+        return I, J, V
 
     def time_factor_solve(self, src: "RefBCR", b: np.ndarray):
         """Factorize a fresh copy of ``src``'s matrix into this object and solve

@@ -8,6 +8,8 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <vector>
+#include <algorithm>
 
 namespace {
   struct RefHandle {
@@ -149,6 +151,68 @@ double ref_time_factor_solve( void * work, void * src, int nrhs, double * x, int
     *ok = good ? 1 : 0;
     return std::chrono::duration<double>( t1 - t0 ).count();
   } catch ( std::exception const & e ) { fail( w, e ); return -1; }
+}
+
+// sparse export of the loaded matrix (hxx:1079-1097, cc:2316-2413)
+int ref_sparse_nnz( void * p ) { return static_cast<RefHandle*>(p)->bcr->sparse_nnz(); }
+int ref_sparse_pattern( void * p, int * I, int * J, int offs ) {
+  auto * h = static_cast<RefHandle*>(p);
+  try { h->bcr->sparse_pattern( I, J, offs ); } catch ( std::exception const & e ) { return fail( h, e ); }
+  return 1;
+}
+int ref_sparse_values( void * p, double * V ) {
+  auto * h = static_cast<RefHandle*>(p);
+  try { h->bcr->sparse_values( V ); } catch ( std::exception const & e ) { return fail( h, e ); }
+  return 1;
+}
+
+// The reference's BorderedCR<float> (explicitly instantiated at cc:2663) on
+// the same system, loaded through its public loaders after rounding every
+// entry to float: an unrefined FP32 factorize + solve, timed like
+// ref_time_factor_solve (load excluded).  x (double, length >= max(nrows,
+// ncols)) holds the right-hand side on entry and the solution on return.
+double ref_f32_factor_solve( int nthreads, int npb, int nblock, int n, int qr, int qx, int nr, int nx,
+                             double const * D, double const * E, double const * B, double const * C,
+                             double const * Cq, double const * F, double const * H, double * x, int * ok ) {
+  *ok = 0;
+  try {
+    std::unique_ptr<Utils::ThreadPool1> tp;
+    std::unique_ptr<alglin::BorderedCR<float>> bcr;
+    if ( nthreads > 0 ) {
+      tp.reset( new Utils::ThreadPool1( unsigned(nthreads) ) );
+      bcr.reset( new alglin::BorderedCR<float>( tp.get(), npb ) );
+    } else {
+      bcr.reset( new alglin::BorderedCR<float>( nullptr ) );
+    }
+    auto & b = *bcr;
+    b.allocate( nblock, n, qr, qx, nr, nx );
+    b.fill_zero();
+    b.set_factorize_use_thread( nthreads > 0 );
+    b.set_solve_use_thread( nthreads > 0 );
+    b.select_LU();
+    b.select_last_LU();
+    auto cvt = []( double const * a, size_t len ) { return std::vector<float>( a, a + len ); };
+    for ( int k = 0; k < nblock; ++k ) {
+      b.load_D( k, cvt( D + size_t(k)*n*n, size_t(n)*n ).data(), n );
+      b.load_E( k, cvt( E + size_t(k)*n*n, size_t(n)*n ).data(), n );
+      if ( nx > 0 ) b.load_B( k, cvt( B + size_t(k)*n*nx, size_t(n)*nx ).data(), n );
+    }
+    if ( nr > 0 ) {
+      for ( int k = 0; k <= nblock; ++k ) b.load_C( k, cvt( C + size_t(k)*nr*n, size_t(nr)*n ).data(), nr );
+      if ( qx > 0 ) b.load_Cq( cvt( Cq, size_t(nr)*qx ).data(), nr );
+      if ( nx > 0 ) b.load_F( cvt( F, size_t(nr)*nx ).data(), nr );
+    }
+    b.load_bottom( cvt( H, size_t(n+qr)*(2*n+qx+nx) ).data(), n + qr );
+    size_t const L = size_t( std::max( b.nrows(), b.ncols() ) );
+    std::vector<float> xf( x, x + L );
+    auto t0 = std::chrono::steady_clock::now();
+    bool good = b.factorize();
+    if ( good ) good = b.solve( xf.data() );
+    auto t1 = std::chrono::steady_clock::now();
+    for ( size_t i = 0; i < L; ++i ) x[i] = double( xf[i] );
+    *ok = good ? 1 : 0;
+    return std::chrono::duration<double>( t1 - t0 ).count();
+  } catch ( std::exception const & ) { return -1; }
 }
 
 } // extern "C"

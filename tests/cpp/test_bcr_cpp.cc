@@ -17,7 +17,10 @@ static double rnd( double a, double b ) { return a + ( b - a ) * double( gen() )
 int main( int argc, char ** argv ) {
   int nblock = argc > 1 ? std::atoi( argv[1] ) : 10000;
   int const n = 8, qx = 4, qr = 4, nx = 1, nr = 1;
-  alglin::BorderedCR<double> BCR( 4 ), SAVED( 4 );
+  // the reference's own construction (test7-BorderedCR.cc:114-116)
+  Utils::ThreadPool1         TP( 4 );
+  alglin::BorderedCR<double> BCR( &TP );
+  alglin::BorderedCR<double> SAVED( &TP );
   BCR.allocate( nblock, n, qr, qx, nr, nx );
   BCR.fill_zero();
   double const diag = 1.01 * n;
@@ -62,6 +65,15 @@ int main( int argc, char ** argv ) {
   for ( int c = 0; c < 2; ++c )
     for ( int i = 0; i < N; ++i ) err = std::max( err, std::abs( x[c * N + i] - xref[i] ) );
   if ( !( err < 1e-8 ) ) { std::printf( "two rhs error %g\n", err ); return 1; }
+  // the same through the LinearSystemSolver base and its MatrixWrapper form
+  std::copy( rhs.begin(), rhs.begin() + N, x.begin() );
+  std::copy( rhs.begin(), rhs.begin() + N, x.begin() + N );
+  alglin::LinearSystemSolver<double> & base = BCR;
+  alglin::MatrixWrapper<double> XW( x.data(), N, 2, N );
+  if ( !base.solve( XW ) ) { std::printf( "solve(MatW) failed\n" ); return 1; }
+  for ( int c = 0; c < 2; ++c )
+    for ( int i = 0; i < N; ++i ) err = std::max( err, std::abs( x[c * N + i] - xref[i] ) );
+  if ( !( err < 1e-8 ) ) { std::printf( "solve(MatW) error %g\n", err ); return 1; }
   std::copy( rhs.begin(), rhs.begin() + N, x.begin() );
   BCR.solve( x.data() );
   for ( int i = 0; i < N; ++i ) resid[i] = -rhs[i];
@@ -70,6 +82,9 @@ int main( int argc, char ** argv ) {
   for ( double v : resid ) r2 += v * v;
   if ( !( std::sqrt( r2 ) < 1e-6 ) ) { std::printf( "residual %g\n", std::sqrt( r2 ) ); return 1; }
   std::printf( "%s", BCR.info().c_str() );
+  if ( BCR.info().find( "treads = 4/nblk:4/" ) == std::string::npos ) {
+    std::printf( "info() does not show the pool's 4 threads\n" ); return 1;
+  }
   std::printf( "C++ drop-in ok: max error %.3e, residual %.3e\n", err, std::sqrt( r2 ) );
   return 0;
 }

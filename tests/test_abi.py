@@ -12,6 +12,7 @@ import pytest
 
 from alglin_b200 import bcr as B
 from alglin_b200 import synth
+from oracle import pyoracle as po
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -109,6 +110,27 @@ def test_sparse_roundtrip_matches_dense():
     with pytest.raises(B.BCRError):
         g.sparse_load(np.array([1.0]), np.array([0]), 0, np.array([s.ncols - 1 - s.nx - 1]), 0)
     assert "out of pattern" in g.last_error()
+
+
+@pytest.mark.parametrize("dims", [(7, 3, 2, 1, 2, 2), (5, 4, 0, 0, 0, 0), (6, 2, 1, 3, 0, 2),
+                                  (4, 3, 0, 2, 3, 0), (9, 16, 2, 2, 4, 4)])
+def test_sparse_export_bit_exact_vs_reference(dims):
+    """sparse_pattern / sparse_values agree element by element (same order,
+    same indices, same values) with the reference's own export
+    (BABD_BorderedCR.cc:2316-2413, compiled in oracle/_ref)."""
+    if not po.ref_available():
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    s = synth.dominant(*dims, seed=5)
+    h = B.BorderedCR()
+    h.load_system(s)
+    I, J = h.sparse_pattern(0)
+    V = h.sparse_values()
+    Ir, Jr, Vr = po.RefBCR(s).sparse()
+    assert h.sparse_nnz() == len(Vr)
+    assert np.array_equal(I, Ir) and np.array_equal(J, Jr)
+    assert np.array_equal(V, Vr)
+    I1, J1 = h.sparse_pattern(1)
+    assert np.array_equal(I1, Ir + 1) and np.array_equal(J1, Jr + 1)
 
 
 def test_check_matrix_and_tsolve():
