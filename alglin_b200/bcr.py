@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(HERE, "libalglin_b200.so")
 
 BCR_OK, BCR_NUMERICAL, BCR_BAD_ARGUMENT, BCR_CUDA_ERROR, BCR_DEVICE_TIMEOUT = range(5)
 PRECISION_FP64, PRECISION_MIXED = 0, 1
-PAIR_AUTO, PAIR_TC, PAIR_GRP, PAIR_ROWS, PAIR_CTA, PAIR_SMEM, PAIR_UMMA, PAIR_TREE = range(8)
+PAIR_AUTO, PAIR_TC, PAIR_GRP, PAIR_ROWS, PAIR_CTA, PAIR_SMEM, PAIR_UMMA, PAIR_TREE, PAIR_TC_GATHER = range(9)
 
 _dp = ct.POINTER(ct.c_double)
 _ip = ct.POINTER(ct.c_int)

@@ -1206,7 +1206,7 @@ int bcr_graph_launch(bcr_handle h, int what) {
 
 int bcr_set_pair_kernel(bcr_handle h, int choice) {
   H_CHECK(h);
-  if (choice < BCR_PAIR_AUTO || choice > BCR_PAIR_TREE)
+  if (choice < BCR_PAIR_AUTO || choice > BCR_PAIR_TC_GATHER)
     return h->fail(BCR_BAD_ARGUMENT, fmt("bcr_set_pair_kernel: unknown choice %d\n", choice));
   h->s.pair_kernel = choice;
   h->drop_graphs();

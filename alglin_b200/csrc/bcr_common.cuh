@@ -24,7 +24,7 @@ enum LastKind : int { LAST_LU = 0, LAST_LUPQ = 1, LAST_QR = 2, LAST_QRP = 3,
 
 // pair-kernel choice of the factorization (PAIR_AUTO picks by shape)
 enum PairKernel : int { PAIR_AUTO = 0, PAIR_TC = 1, PAIR_GRP = 2, PAIR_ROWS = 3, PAIR_CTA = 4, PAIR_SMEM = 5,
-                        PAIR_UMMA = 6, PAIR_TREE = 7 };
+                        PAIR_UMMA = 6, PAIR_TREE = 7, PAIR_TC_GATHER = 8 };
 
 // error codes written by kernels into the device status word
 enum DevStatus : int {

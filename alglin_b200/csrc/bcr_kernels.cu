@@ -594,6 +594,9 @@ size_t tc_smem_per_warp(int n) {
   return n == 16 ? TcShape<16>::BYTES : n == 8 ? TcShape<8>::BYTES : 0;
 }
 
+__host__ __device__ inline int lowbit(int v) { return v & -v; }
+__host__ __device__ inline void tree_children(int j, int nb, int& c1, int& c2);
+
 // Per-pair extras of the tree-scheduled factorization (k_factor_tree_tc):
 // gather = the C_jpp contributions of earlier levels are added to C_j at load
 // (Rbuf[j - K'] for K' = 1, 2, ..., gather; 0 in the level-by-level launches,
@@ -610,7 +613,12 @@ __device__ __forceinline__ double ldw(const double* p) { return __ldcg(p); }
 // Eliminates x_j from the pair (jp = j - k, j); see the comment above.
 // Returns false (after reporting) when the panel has an exactly-zero pivot; the
 // outputs of that pair are then not written.
-template <int N>
+//
+// The nr <= NRM border rows are spread over the whole warp: lane = r * LPR +
+// cg holds columns cg*CPL .. cg*CPL + CPL - 1 of border row r (LPR = 32 / NRM
+// lanes per row), so their eliminations (C_j U^-1, then -C' L^-1) run in the
+// same instructions as everyone else instead of on nr lanes alone.
+template <int N, int NRM>
 __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int k, bool first, double* Wt,
                                         int lane, const TcTree& tr) {
   using S = TcShape<N>;
@@ -634,22 +642,49 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
   const double* srcB = first ? a.B0 : a.B;
   const double* srcC = first ? a.C0 : a.C;
   // ------------------------------------------------------------ load
-  double rowA[N], rowC[N];
+  constexpr int LPR = 32 / NRM, CPL = N / LPR;   // border layout (see above)
+  const int br = lane / LPR, bc0 = (lane % LPR) * CPL;
+  const bool blive = br < nr;
+  double rowA[N], cb[CPL];
+  double cs1[2] = {0.0, 0.0}, cs2[2] = {0.0, 0.0};  // children's F / xb sums (tree)
   {
     const double* Pm = top ? srcE + (size_t)jp * nn : srcD + (size_t)j * nn;
 #pragma unroll
     for (int c = 0; c < N; ++c) rowA[c] = act ? ldw(Pm + (size_t)c * n + ri) : 0.0;
 #pragma unroll
-    for (int c = 0; c < N; ++c) rowC[c] = 0.0;
-    if (lane < nr) {
-      const double* Cj = srcC + (size_t)j * nrn + lane;
+    for (int q = 0; q < CPL; ++q) cb[q] = blive ? ldw(srcC + (size_t)j * nrn + (size_t)(bc0 + q) * nr + br) : 0.0;
+    // C_jpp contributions of the pairs (j - 2K', j - K') of earlier levels,
+    // K' = 1, 2, ..., gather: loaded eight levels at a time so that their
+    // latencies overlap, then added in level order
+    for (int e0 = 0; e0 < 31 && (1 << e0) <= tr.gather; e0 += 8) {
+      double v[8][CPL];
 #pragma unroll
-      for (int c = 0; c < N; ++c) rowC[c] = ldw(Cj + (size_t)c * nr);
-      // C_jpp contributions of the pairs (j - 2K', j - K') of earlier levels
-      for (int kk = 1; kk <= tr.gather; kk *= 2) {
-        const double* R = a.Rbuf + (size_t)(j - kk) * nrn + lane;
+      for (int e = 0; e < 8; ++e) {
+        const int kk = e0 + e < 31 ? 1 << (e0 + e) : 0;
+        const bool on = blive && kk != 0 && kk <= tr.gather;
 #pragma unroll
-        for (int c = 0; c < N; ++c) rowC[c] += ldw(R + (size_t)c * nr);
+        for (int q = 0; q < CPL; ++q)
+          v[e][q] = on ? ldw(a.Rbuf + (size_t)(j - kk) * nrn + (size_t)(bc0 + q) * nr + br) : 0.0;
+      }
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+#pragma unroll
+        for (int q = 0; q < CPL; ++q) cb[q] += v[e][q];
+    }
+    // the children's F / xb partial sums of the two border-tile elements this
+    // lane holds in the product (row 2N + g, columns 2N + 2t + {0, 1})
+    if ((tr.c1 | tr.c2) && g < nr) {
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        const int cl = 2 * t + hh;
+        const double* base = nullptr;
+        size_t stride = 0, e = 0;
+        if (cl < nx) { base = a.Fbuf; stride = nrnx; e = (size_t)cl * nr + g; }
+        else if (cl < nx + nrf) { base = a.XB; stride = (size_t)nr * nrf; e = (size_t)(cl - nx) * nr + g; }
+        if (base) {
+          if (tr.c1) cs1[hh] = ldw(base + (size_t)tr.c1 * stride + e);
+          if (tr.c2) cs2[hh] = ldw(base + (size_t)tr.c2 * stride + e);
+        }
       }
     }
     // trailing columns in the original row order: TOP [D_jp 0 B_jp], BOTTOM [0 E_j B_j]
@@ -740,11 +775,15 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
 #pragma unroll
       for (int c = i + 1; c < N; ++c) rowA[c] = fma(-l, u[c], rowA[c]);
     }
-    if (lane < nr) {
-      const double l = rowC[i] * rinv;
-      rowC[i] = l;
+    {  // border rows: multiplier from the lane holding column i of the row
+      const double ci = __shfl_sync(FULL, cb[i % CPL], (lane & ~(LPR - 1)) | (i / CPL));
+      const double l = ci * rinv;
 #pragma unroll
-      for (int c = i + 1; c < N; ++c) rowC[c] = fma(-l, u[c], rowC[c]);
+      for (int q = 0; q < CPL; ++q) {
+        const int c = bc0 + q;
+        if (c == i) cb[q] = l;
+        else if (c > i) cb[q] = fma(-l, bc[c], cb[q]);
+      }
     }
     if (lane == p) done = true;
     __syncwarp();
@@ -762,10 +801,9 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
       rowof[mypos] = lane;
     }
     if (act) a.P[(size_t)j * szP(d) + mypos] = (unsigned char)lane;
-    if (lane < nr) {
-      double* Cj = a.C + (size_t)j * nrn + lane;
+    if (blive) {
 #pragma unroll
-      for (int c = 0; c < N; ++c) Cj[(size_t)c * nr] = rowC[c];
+      for (int q = 0; q < CPL; ++q) a.C[(size_t)j * nrn + (size_t)(bc0 + q) * nr + br] = cb[q];
     }
     // rows of L (row m contiguous) for the triangular solve
     if (act && mypos < n) {
@@ -782,23 +820,23 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
 #pragma unroll
     for (int c = 0; c < N; ++c) x[c] = (mypos < n) ? (c == mypos ? 1.0 : 0.0) : -rowA[c];
 #pragma unroll
-    for (int c = 0; c < N; ++c) rowC[c] = -rowC[c];
+    for (int q = 0; q < CPL; ++q) cb[q] = -cb[q];
     // right-looking: once x[mm] is final, update every x[c], c < mm (the
     // updates of one step are independent, so the dependent chain is N long)
 #pragma unroll
     for (int mm = N - 1; mm > 0; --mm) {
-      const double xm = x[mm], cm = rowC[mm];
+      const double xm = x[mm];
+      const double cm = __shfl_sync(FULL, cb[mm % CPL], (lane & ~(LPR - 1)) | (mm / CPL));
       const double* Lrow = Gs + mm * S::LDG;  // L(mm, 0..mm-1)
 #pragma unroll
       for (int c = 0; c < mm; c += 2) {
         const double2 l2 = *reinterpret_cast<const double2*>(&Lrow[c]);
         x[c] = fma(-xm, l2.x, x[c]);
-        rowC[c] = fma(-cm, l2.x, rowC[c]);
-        if (c + 1 < mm) {
-          x[c + 1] = fma(-xm, l2.y, x[c + 1]);
-          rowC[c + 1] = fma(-cm, l2.y, rowC[c + 1]);
-        }
+        if (c + 1 < mm) x[c + 1] = fma(-xm, l2.y, x[c + 1]);
       }
+#pragma unroll
+      for (int q = 0; q < CPL; ++q)
+        if (bc0 + q < mm) cb[q] = fma(-cm, Lrow[bc0 + q], cb[q]);
     }
     __syncwarp();
     if (act) {
@@ -806,13 +844,11 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
       for (int c = 0; c < N; c += 2)
         *reinterpret_cast<double2*>(&Gs[mypos * S::LDG + c]) = make_double2(x[c], x[c + 1]);
     }
-    if (lane < 8) {  // border rows (zero when lane >= nr)
+    // border rows of G (zero for rows >= nr, and rows NRM..7 of the tile)
 #pragma unroll
-      for (int c = 0; c < N; c += 2) {
-        const bool live = lane < nr;
-        *reinterpret_cast<double2*>(&Gs[(n2 + lane) * S::LDG + c]) =
-            make_double2(live ? rowC[c] : 0.0, live ? rowC[c + 1] : 0.0);
-      }
+    for (int q = 0; q < CPL; ++q) {
+      Gs[(n2 + br) * S::LDG + bc0 + q] = blive ? cb[q] : 0.0;
+      if constexpr (NRM < 8) Gs[(n2 + NRM + br) * S::LDG + bc0 + q] = 0.0;
     }
   }
   __syncwarp();
@@ -889,16 +925,10 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
                 } else if (col < n2 + nx) {
                   // own F update plus the partial sums of the child nodes (tree)
                   const size_t e = (size_t)(col - n2) * nr + rr;
-                  double s = v;
-                  if (tr.c1) s += ldw(a.Fbuf + (size_t)tr.c1 * nrnx + e);
-                  if (tr.c2) s += ldw(a.Fbuf + (size_t)tr.c2 * nrnx + e);
-                  a.Fbuf[(size_t)j * nrnx + e] = s;
+                  a.Fbuf[(size_t)j * nrnx + e] = v + cs1[hh] + cs2[hh];
                 } else if (col < NT) {
                   const size_t e = (size_t)(col - n2 - nx) * nr + rr, nrr = (size_t)nr * nrf;
-                  double s = v;
-                  if (tr.c1) s += ldw(a.XB + (size_t)tr.c1 * nrr + e);
-                  if (tr.c2) s += ldw(a.XB + (size_t)tr.c2 * nrr + e);
-                  a.XB[(size_t)j * nrr + e] = s;
+                  a.XB[(size_t)j * nrr + e] = v + cs1[hh] + cs2[hh];
                 }
               }
             }
@@ -910,7 +940,12 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
   return true;
 }
 
-template <int N, bool BATCH = false>
+// BOOK: the border bookkeeping of the tree schedule (see k_factor_tree_tc)
+// in level-by-level launches: every pair gathers the C_j updates of the lower
+// levels and adds its children's F / xb partial sums, so no border fix-up or
+// reduction launch is needed between or after the levels (k_tree_root
+// finishes C_nblock, F and xb after the last level).
+template <int N, bool BATCH = false, bool BOOK = false, int NRM = 8>
 __global__ void __launch_bounds__(128, 4) k_factor_lu_tc(FactorArgs<double> a0, const FactorArgs<double>* tab,
                                                        const BatchCta* cmap) {
   using S = TcShape<N>;
@@ -921,10 +956,14 @@ __global__ void __launch_bounds__(128, 4) k_factor_lu_tc(FactorArgs<double> a0, 
   pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
   const FactorArgs<double>& a = BATCH ? ab : a0;
   double* Wt = reinterpret_cast<double*>(smem_raw + (size_t)warp * S::BYTES);
-  const TcTree none{0, 0, 0};
+  TcTree tr{0, 0, 0};
   for (long q = q0; q < q1; q += qs) {
     const int j = a.k + (int)(2L * a.k * q);
-    tc_pair<N>(a, j, a.k, a.first != 0, Wt, lane, none);
+    if constexpr (BOOK) {
+      tr.gather = a.k / 2;
+      tree_children(j, a.d.nblock, tr.c1, tr.c2);
+    }
+    tc_pair<N, NRM>(a, j, a.k, a.first != 0, Wt, lane, tr);
   }
 }
 
@@ -950,8 +989,6 @@ __global__ void __launch_bounds__(128, 4) k_factor_lu_tc(FactorArgs<double> a0, 
 // updates are summed up the tree (each node adds its children's partial sums
 // to its own, in a fixed order), so results are bit-reproducible run to run.
 // ---------------------------------------------------------------------------
-__host__ __device__ inline int lowbit(int v) { return v & -v; }
-
 // parent node of node j, 0 for the root
 __host__ __device__ inline int tree_parent(int j, int nb) {
   const int K = lowbit(j), jp = j - K;
@@ -985,13 +1022,23 @@ __device__ void tree_root(const FactorArgs<double>& a, const TreeArgs& ta, int r
   const Dims d = a.d;
   const int nb = d.nblock, nr = d.nr, nx = d.nx;
   const size_t nrn = (size_t)nr * N, nrnx = (size_t)nr * nx;
+  // the contributing pair of each level (0: none), found before any load so
+  // that every load is in flight at once
+  int src[31];
+#pragma unroll
+  for (int lev = 0; lev < 31; ++lev) {
+    const int K = 1 << lev;
+    const long np = K < nb ? pairs_at_level(nb, K) : 0;
+    const int jl = np > 0 ? (int)(K * (2 * np - 1)) : 0;
+    src[lev] = (np > 0 && jl + K >= nb) ? jl : 0;
+  }
   for (size_t e = lane; e < nrn; e += 32) {
+    double v[31];
+#pragma unroll
+    for (int lev = 0; lev < 31; ++lev) v[lev] = src[lev] ? ldw(a.Rbuf + (size_t)src[lev] * nrn + e) : 0.0;
     double s = ldw(a.C + (size_t)nb * nrn + e);
-    for (int K = 1; K < nb; K *= 2) {
-      const long np = pairs_at_level(nb, K);
-      const int jl = (int)(K * (2 * np - 1));
-      if (np > 0 && jl + K >= nb) s += ldw(a.Rbuf + (size_t)jl * nrn + e);
-    }
+#pragma unroll
+    for (int lev = 0; lev < 31; ++lev) s += v[lev];
     a.C[(size_t)nb * nrn + e] = s;
   }
   for (size_t e = lane; e < nrnx; e += 32) {
@@ -1006,7 +1053,13 @@ __device__ void tree_root(const FactorArgs<double>& a, const TreeArgs& ta, int r
   }
 }
 
+// the root work after level-by-level launches with the tree bookkeeping
 template <int N>
+__global__ void __launch_bounds__(32) k_tree_root(FactorArgs<double> a, TreeArgs ta, int root) {
+  tree_root<N>(a, ta, root, threadIdx.x);
+}
+
+template <int N, int NRM>
 __global__ void __launch_bounds__(128, 4) k_factor_tree_tc(FactorArgs<double> a, TreeArgs ta) {
   using S = TcShape<N>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1025,7 +1078,7 @@ __global__ void __launch_bounds__(128, 4) k_factor_tree_tc(FactorArgs<double> a,
       TcTree tr;
       tr.gather = K / 2;
       tree_children(j, nb, tr.c1, tr.c2);
-      tc_pair<N>(a, j, K, K == 1, Wt, lane, tr);
+      tc_pair<N, NRM>(a, j, K, K == 1, Wt, lane, tr);
       const int par = tree_parent(j, nb);
       if (par == 0) {  // the root: every pair is done
         __threadfence();
@@ -2264,10 +2317,12 @@ __global__ void __launch_bounds__(256, 2) k_backward_rows(SweepArgs<TF> a0, cons
     for (int c = 0; c < N; ++c) u[c] = (!hi && rowok && c < n) ? Tj[(size_t)c * n2 + i] : 0.0;
 #pragma unroll
     for (int c = 0; c < NXM; ++c) bb[c] = (!hi && rowok && c < nx) ? Bj[(size_t)c * n + i] : 0.0;
-    double rdi = 0.0;  // 1 / U(i,i)
+    // 1 / U(i,i): pick the diagonal element first, then one division per lane
+    double ud = 1.0;
 #pragma unroll
     for (int c = 0; c < N; ++c)
-      if (c == i) rdi = (!hi && rowok) ? 1.0 / u[c] : 0.0;
+      if (c == i) ud = u[c];
+    const double rdi = (!hi && rowok) ? 1.0 / ud : 0.0;
     const int dst = (qrp && !hi && rowok) ? (int)a.P[(size_t)j * szP(d) + n2 + i] : i;
     for (int col = 0; col < nrhs; ++col) {
       double* xc = a.x + (size_t)col * a.ldx;
@@ -3353,6 +3408,9 @@ struct FactorPlan {
   size_t tc_smem = 0;
   void (*tree)(FactorArgs<double>, TreeArgs) = nullptr;  // tc pairs, whole reduction in one launch
   int tree_ctas = 0;
+  // tc pairs level by level with the tree's border bookkeeping (single systems)
+  void (*tcb)(FactorArgs<double>, const FactorArgs<double>*, const BatchCta*) = nullptr;
+  void (*root)(FactorArgs<double>, TreeArgs, int) = nullptr;
   void (*grp)(FactorArgs<T>, const FactorArgs<T>*, const BatchCta*) = nullptr;              // CTA of 2n threads per pair (n = 16, 32)
   size_t grp_smem = 0;
   int grp_threads = 0, grp_ctas = 0;
@@ -3378,13 +3436,27 @@ static FactorPlan<T> plan_factor(const DevState& s) {
   if (p.smem <= SMEM_MAX) smem_limit_once(p.smem_k, p.smem);
   if constexpr (sizeof(T) == 8) {
     if (s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 && (n == 16 || n == 8) && s.use_tc &&
-        (s.pair_kernel == PAIR_AUTO || s.pair_kernel == PAIR_TC || s.pair_kernel == PAIR_TREE)) {
+        (s.pair_kernel == PAIR_AUTO || s.pair_kernel == PAIR_TC || s.pair_kernel == PAIR_TREE ||
+         s.pair_kernel == PAIR_TC_GATHER)) {
       p.tc_smem = tc_smem_per_warp(n) * 4;
-      if (n == 16) { p.tc = k_factor_lu_tc<16>; smem_limit_once(k_factor_lu_tc<16>, p.tc_smem); p.tc_cols = TcShape<16>::NTP; }
-      else { p.tc = k_factor_lu_tc<8>; smem_limit_once(k_factor_lu_tc<8>, p.tc_smem); p.tc_cols = TcShape<8>::NTP; }
-      // the tree schedule (single systems with at least one pair)
-      if (s.pair_kernel != PAIR_TC && s.tree_cnt && d.nblock >= 2) {
-        p.tree = n == 16 ? k_factor_tree_tc<16> : k_factor_tree_tc<8>;
+      // border rows spread over the warp: 8 lanes per row when nr <= 4, else 4
+      const bool r4 = d.nr <= 4;
+      if (n == 16) p.tc = r4 ? k_factor_lu_tc<16, false, false, 4> : k_factor_lu_tc<16, false, false, 8>;
+      else p.tc = r4 ? k_factor_lu_tc<8, false, false, 4> : k_factor_lu_tc<8, false, false, 8>;
+      smem_limit_once(p.tc, p.tc_smem);
+      p.tc_cols = n == 16 ? TcShape<16>::NTP : TcShape<8>::NTP;
+      if (s.pair_kernel == PAIR_TC_GATHER && s.tree_cnt && d.nblock >= 2) {
+        if (n == 16) p.tcb = r4 ? k_factor_lu_tc<16, false, true, 4> : k_factor_lu_tc<16, false, true, 8>;
+        else p.tcb = r4 ? k_factor_lu_tc<8, false, true, 4> : k_factor_lu_tc<8, false, true, 8>;
+        p.root = n == 16 ? k_tree_root<16> : k_tree_root<8>;
+        smem_limit_once(p.tcb, p.tc_smem);
+      }
+      // the tree schedule (single systems with at least one pair), on request:
+      // its top levels run one pair per warp along a serial chain, which costs
+      // more than the level-by-level launches save at the sizes measured
+      if (s.pair_kernel == PAIR_TREE && s.tree_cnt && d.nblock >= 2) {
+        if (n == 16) p.tree = r4 ? k_factor_tree_tc<16, 4> : k_factor_tree_tc<16, 8>;
+        else p.tree = r4 ? k_factor_tree_tc<8, 4> : k_factor_tree_tc<8, 8>;
         smem_limit_once(p.tree, p.tc_smem);
         p.tree_ctas = 148 * resident_ctas(p.tree, 128, p.tc_smem);
       }
@@ -3467,17 +3539,30 @@ static bool factor_levels(DevState& s, const FactorPlan<T>& p, const WorkSet<T>&
   a.ldw = odd_ld(2 * n + d.nr);
   a.x = x; a.ldx = ldx; a.nrf = nrf; a.XB = s.XB;
   if constexpr (sizeof(T) == 8) {
-    if (p.tree) {
+    if (p.tree || p.tcb) {
       a.F0 = s.F0;
       TreeArgs ta;
       ta.cnt = s.tree_cnt;
       ta.leaf = s.tree_cnt + nb;
       ta.Ffin = s.Ffin;
       ta.xb = (nrf > 0 && d.nr > 0) ? x + (size_t)(nb + 1) * n + d.qr : nullptr;
-      cudaMemsetAsync(s.tree_cnt, 0, (size_t)(nb + 1) * sizeof(int), st);
-      const long leaves = pairs_at_level(nb, 1);
-      p.tree<<<grid_for(leaves, 4, p.tree_ctas), 128, p.tc_smem, st>>>(a, ta);
-      check_launch("k_factor_tree_tc");
+      if (p.tree) {
+        cudaMemsetAsync(s.tree_cnt, 0, (size_t)(nb + 1) * sizeof(int), st);
+        const long leaves = pairs_at_level(nb, 1);
+        p.tree<<<grid_for(leaves, 4, p.tree_ctas), 128, p.tc_smem, st>>>(a, ta);
+        check_launch("k_factor_tree_tc");
+        return true;
+      }
+      int root = 1;
+      for (int k = 1; k < nb; k *= 2) {
+        a.k = k;
+        a.first = (k == 1);
+        root = k;  // the pair (0, k) of the top level
+        p.tcb<<<grid_for(pairs_at_level(nb, k), 4, 148 * 16), 128, p.tc_smem, st>>>(a, nullptr, nullptr);
+        check_launch("k_factor_lu_tc");
+      }
+      p.root<<<1, 32, 0, st>>>(a, ta, root);
+      check_launch("k_tree_root");
       return true;
     }
   }

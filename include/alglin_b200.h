@@ -128,6 +128,7 @@ int bcr_set_precision(bcr_handle h, int precision);      /* extension: FP64 / mi
 #define BCR_PAIR_SMEM 5
 #define BCR_PAIR_UMMA 6
 #define BCR_PAIR_TREE 7
+#define BCR_PAIR_TC_GATHER 8
 int bcr_set_pair_kernel(bcr_handle h, int choice);
 
 /* Iterative refinement of the mixed path (extension, no reference counterpart):

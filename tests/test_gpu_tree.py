@@ -1,5 +1,7 @@
-"""GPU tests of the tree-scheduled factorization (k_factor_tree_tc: the whole
-cyclic reduction of one system in one launch, FP64 LU, n = 8 or 16).
+"""GPU tests of the tree bookkeeping of the n = 8 / 16 FP64 LU factorization:
+the tree schedule (k_factor_tree_tc: the whole cyclic reduction of one system
+in one launch) and the level-by-level launches that gather the border
+updates instead of running fix-up launches (PAIR_TC_GATHER).
 
 Every number of blocks whose tree has a ragged edge (odd counts, one above and
 one below a power of two) is compared with the CPU oracle (forward error
@@ -50,27 +52,28 @@ def test_tree_matches_oracle_and_level_schedule(nb, n, border):
     o = po.Oracle(s, "LU", _last(s))
     assert o.factorize(), o.last_error()
     xo = o.solve(b)
-    ht = _solver(s, B.PAIR_TREE)
-    assert ht.factorize(), ht.last_error()
-    xt = _solve(ht, b)
     hl = _solver(s, B.PAIR_TC)
     assert hl.factorize(), hl.last_error()
     xl = _solve(hl, b)
-    for c in range(2):
-        assert fwd_err(xt[c, :s.ncols], xo[c, :s.ncols]) < 1e-10, (nb, n, border, c)
-        assert fwd_err(xt[c, :s.ncols], xl[c, :s.ncols]) < 1e-12, (nb, n, border, c)
-        if s.Nr == s.Nc:
-            r = b[c, :s.nrows] - o.mv(xt[c, :s.ncols])
-            rel = np.abs(r).max() / (block_norm_inf(s) * np.abs(xt[c, :s.ncols]).max() +
-                                     np.abs(b[c, :s.nrows]).max())
-            assert rel < 1e-13, (nb, n, border, rel)
-    # the same factors again, and the fused factorize+solve of the tree path
-    X = b.copy()
-    assert ht.factorize_solve(2, X, X.shape[1]), ht.last_error()
-    assert fwd_err(X[:, :s.ncols], xo[:, :s.ncols]) < 1e-10
-    # bit-identical run to run
-    assert ht.factorize(), ht.last_error()
-    assert np.array_equal(_solve(ht, b), xt)
+    for fam in (B.PAIR_TREE, B.PAIR_TC_GATHER):
+        ht = _solver(s, fam)
+        assert ht.factorize(), ht.last_error()
+        xt = _solve(ht, b)
+        for c in range(2):
+            assert fwd_err(xt[c, :s.ncols], xo[c, :s.ncols]) < 1e-10, (fam, nb, n, border, c)
+            assert fwd_err(xt[c, :s.ncols], xl[c, :s.ncols]) < 1e-12, (fam, nb, n, border, c)
+            if s.Nr == s.Nc:
+                r = b[c, :s.nrows] - o.mv(xt[c, :s.ncols])
+                rel = np.abs(r).max() / (block_norm_inf(s) * np.abs(xt[c, :s.ncols]).max() +
+                                         np.abs(b[c, :s.nrows]).max())
+                assert rel < 1e-13, (fam, nb, n, border, rel)
+        # the same factors again, and the fused factorize+solve
+        X = b.copy()
+        assert ht.factorize_solve(2, X, X.shape[1]), ht.last_error()
+        assert fwd_err(X[:, :s.ncols], xo[:, :s.ncols]) < 1e-10
+        # bit-identical run to run
+        assert ht.factorize(), ht.last_error()
+        assert np.array_equal(_solve(ht, b), xt)
 
 
 @pytest.mark.parametrize("nrhs", [1, 3])
@@ -82,10 +85,11 @@ def test_tree_fused_rhs_full_width(nrhs):
     o = po.Oracle(s, "LU", "LU")
     assert o.factorize(), o.last_error()
     xo = o.solve(b)
-    h = _solver(s, B.PAIR_AUTO)
-    X = b.copy()
-    assert h.factorize_solve(nrhs, X, X.shape[1]), h.last_error()
-    assert fwd_err(X[:, :s.ncols], xo[:, :s.ncols]) < 1e-10
+    for fam in (B.PAIR_TREE, B.PAIR_TC_GATHER):
+        h = _solver(s, fam)
+        X = b.copy()
+        assert h.factorize_solve(nrhs, X, X.shape[1]), h.last_error()
+        assert fwd_err(X[:, :s.ncols], xo[:, :s.ncols]) < 1e-10
 
 
 def test_tree_singular_panel_reports_like_reference():
