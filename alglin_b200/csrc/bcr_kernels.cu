@@ -1053,6 +1053,36 @@ __device__ void tree_root(const FactorArgs<double>& a, const TreeArgs& ta, int r
   }
 }
 
+// The top levels of the cyclic reduction (at most TOP_WARPS pairs each) in one
+// launch of one CTA: each level's pairs go one per warp, then the CTA applies
+// the level's C_jpp updates (k_border_fix's work) before the next level; one
+// launch replaces two per level, whose fixed cost dominates there.
+constexpr int TOP_WARPS = 16;
+
+template <int N, int NRM>
+__global__ void __launch_bounds__(TOP_WARPS * 32, 1) k_factor_top_tc(FactorArgs<double> a, int k_first) {
+  using S = TcShape<N>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* Wt = reinterpret_cast<double*>(smem_raw + (size_t)warp * S::BYTES);
+  const TcTree none{0, 0, 0};
+  const int nb = a.d.nblock;
+  const size_t nrn = (size_t)a.d.nr * N;
+  for (int k = k_first; k < nb; k *= 2) {
+    const long np = pairs_at_level(nb, k);
+    for (long q = warp; q < np; q += TOP_WARPS)
+      tc_pair<N, NRM>(a, k + (int)(2L * k * q), k, k == 1, Wt, lane, none);
+    __syncthreads();
+    for (size_t e = threadIdx.x; e < (size_t)np * nrn; e += blockDim.x) {
+      const long q = (long)(e / nrn);
+      const size_t idx = e % nrn;
+      const int j = k + (int)(2L * k * q), jpp = min(j + k, nb);
+      a.C[(size_t)jpp * nrn + idx] += ldw(a.Rbuf + (size_t)j * nrn + idx);
+    }
+    __syncthreads();
+  }
+}
+
 // the root work after level-by-level launches with the tree bookkeeping
 template <int N>
 __global__ void __launch_bounds__(32) k_tree_root(FactorArgs<double> a, TreeArgs ta, int root) {
@@ -2822,6 +2852,67 @@ __device__ void last_svd(Dims d, const double* A, LastBufs b, StatusWords* st) {
 // load_and_factorize_last (cc:1281-1374) with the reference's last-block
 // solvers: LU (getrf), LUPQ (complete pivoting), QR (geqrf), QRP (geqp3: the
 // column of largest remaining 2-norm first), and the SVD family
+// Last blocks of order <= LAST_SMALL (configs with n <= 16 and small borders):
+// LU and the LU solves run in shared memory on one warp (lane = rows lane and
+// lane + 32) instead of the CTA-wide loops over global memory, which cost a few
+// barriers and a global round trip per column.  Same pivot rule (largest |a|,
+// first row on ties, NaN never chosen), same operation order.
+constexpr int LAST_SMALL = 64;
+
+template <typename T>
+__device__ void last_lu_small(Dims d, LastBufs b, StatusWords* st) {
+  __shared__ T As[LAST_SMALL * (LAST_SMALL + 1)];
+  __shared__ int s_bad;
+  const int N = d.Nc, ld = N + 1, tid = threadIdx.x, bs = blockDim.x;
+  T* A = b.A;
+  for (int e = tid; e < N * N; e += bs) As[(e / N) * ld + e % N] = A[e];
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+  if (tid < 32) {
+    const int lane = tid, r0 = lane, r1 = lane + 32;
+    const bool in0 = r0 < N, in1 = r1 < N;
+    for (int i = 0; i < N; ++i) {
+      // pivot of column i: rows >= i, |a| (NaN counts as -1: never chosen)
+      T v0 = T(-2), v1 = T(-2);
+      int i0 = 0x7fffffff, i1 = 0x7fffffff;
+      if (in0 && r0 >= i) { const T v = dev_abs(As[i * ld + r0]); v0 = v > T(-1) ? v : T(-1); i0 = r0; }
+      if (in1 && r1 >= i) { const T v = dev_abs(As[i * ld + r1]); v1 = v > T(-1) ? v : T(-1); i1 = r1; }
+      T best = v0;
+      int p = i0;
+      if (v1 > v0) { best = v1; p = i1; }
+      warp_argmax(best, p);
+      const T pv = As[i * ld + p];
+      if (pv == T(0)) {
+        if (lane == 0) { report(st, DEV_LAST_SINGULAR, -1, i + 1, -1); s_bad = 1; }
+        break;
+      }
+      if (lane == 0) b.piv[i] = p;
+      if (p != i)
+        for (int c = lane; c < N; c += 32) {
+          const T t = As[c * ld + i]; As[c * ld + i] = As[c * ld + p]; As[c * ld + p] = t;
+        }
+      __syncwarp();
+      const T rinv = T(1) / pv;
+      const bool u0 = in0 && r0 > i, u1 = in1 && r1 > i;
+      if (u0) As[i * ld + r0] *= rinv;
+      if (u1) As[i * ld + r1] *= rinv;
+      __syncwarp();
+      const T m0 = u0 ? As[i * ld + r0] : T(0), m1 = u1 ? As[i * ld + r1] : T(0);
+#pragma unroll 8
+      for (int c = i + 1; c < N; ++c) {
+        const T a = As[c * ld + i];
+        if (u0) As[c * ld + r0] = fma(-m0, a, As[c * ld + r0]);
+        if (u1) As[c * ld + r1] = fma(-m1, a, As[c * ld + r1]);
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  if (s_bad) return;
+  for (int e = tid; e < N * N; e += bs) A[e] = As[(e / N) * ld + e % N];
+  if (tid == 0) st->kind = FACT_LU;
+}
+
 template <typename T>
 __device__ void last_factor_body(Dims d, LastBufs b, int sel_last, StatusWords* st) {
   __shared__ T sv[32];
@@ -2833,6 +2924,10 @@ __device__ void last_factor_body(Dims d, LastBufs b, int sel_last, StatusWords* 
   T* tau = b.tau;
   if (kind == FACT_SVD || kind == FACT_SVD_T) {
     last_svd(d, A, b, st);
+    return;
+  }
+  if (kind == FACT_LU && M == N && N <= LAST_SMALL) {
+    last_lu_small<T>(d, b, st);
     return;
   }
   if (kind == FACT_LU) {
@@ -2980,8 +3075,16 @@ __device__ void last_solve_body(Dims d, LastBufs lb, const StatusWords* st, T* x
   T* b = reinterpret_cast<T*>(smem_raw);
   T* tmp = b + L;
   __shared__ T sv[32];
-  __shared__ T lt[32][33];  // a diagonal 32 x 32 block of the blocked LU's factors
+  // a diagonal 32 x 32 block of the blocked LU's factors, or the whole L\U of a
+  // small last block (order <= LAST_SMALL, ld order + 1)
+  __shared__ T big[LAST_SMALL * (LAST_SMALL + 1)];
+  T (*lt)[33] = reinterpret_cast<T (*)[33]>(big);
   const int kind = st->kind;
+  const bool small_lu = kind == FACT_LU && M == N && N <= LAST_SMALL;
+  if (small_lu) {
+    for (int e = tid; e < N * N; e += bs) big[(e / N) * (N + 1) + e % N] = lb.A[e];
+    __syncthreads();
+  }
   const T* A = lb.A;
   const int* piv = lb.piv;
   const T* tau = lb.tau;
@@ -3030,6 +3133,34 @@ __device__ void last_solve_body(Dims d, LastBufs lb, const StatusWords* st, T* x
         for (int j = 0; j < Np; ++j)
           s = fma(trn ? lb.U[(size_t)j * Mp + i] : lb.V[(size_t)j * Np + i], tmp[j], s);
         b[i] = s;
+      }
+      __syncthreads();
+    } else if (small_lu) {
+      // row interchanges, unit-lower and upper solves on one warp, the values in
+      // registers (lane = rows lane and lane + 32) and L\U in shared memory
+      if (tid < 32) {
+        const int lane = tid, r0 = lane, r1 = lane + 32, ld = N + 1;
+        if (lane == 0)
+          for (int i = 0; i < N; ++i) {
+            const int p = piv[i];
+            if (p != i) { T t = b[i]; b[i] = b[p]; b[p] = t; }
+          }
+        __syncwarp();
+        T x0 = r0 < N ? b[r0] : T(0), x1 = r1 < N ? b[r1] : T(0);
+        for (int i = 0; i < N; ++i) {
+          const T bi = __shfl_sync(0xffffffffu, i < 32 ? x0 : x1, i & 31);
+          if (r0 > i && r0 < N) x0 = fma(-big[i * ld + r0], bi, x0);
+          if (r1 > i && r1 < N) x1 = fma(-big[i * ld + r1], bi, x1);
+        }
+        for (int i = N - 1; i >= 0; --i) {
+          const T xi = __shfl_sync(0xffffffffu, i < 32 ? x0 : x1, i & 31) / big[i * ld + i];
+          if (r0 == i) x0 = xi;
+          else if (r0 < i) x0 = fma(-big[i * ld + r0], xi, x0);
+          if (r1 == i) x1 = xi;
+          else if (r1 < i) x1 = fma(-big[i * ld + r1], xi, x1);
+        }
+        if (r0 < N) b[r0] = x0;
+        if (r1 < N) b[r1] = x1;
       }
       __syncthreads();
     } else {
@@ -3410,6 +3541,7 @@ struct FactorPlan {
   int tree_ctas = 0;
   // tc pairs level by level with the tree's border bookkeeping (single systems)
   void (*tcb)(FactorArgs<double>, const FactorArgs<double>*, const BatchCta*) = nullptr;
+  void (*top)(FactorArgs<double>, int) = nullptr;  // the top levels in one CTA (single systems)
   void (*root)(FactorArgs<double>, TreeArgs, int) = nullptr;
   void (*grp)(FactorArgs<T>, const FactorArgs<T>*, const BatchCta*) = nullptr;              // CTA of 2n threads per pair (n = 16, 32)
   size_t grp_smem = 0;
@@ -3445,6 +3577,11 @@ static FactorPlan<T> plan_factor(const DevState& s) {
       else p.tc = r4 ? k_factor_lu_tc<8, false, false, 4> : k_factor_lu_tc<8, false, false, 8>;
       smem_limit_once(p.tc, p.tc_smem);
       p.tc_cols = n == 16 ? TcShape<16>::NTP : TcShape<8>::NTP;
+      if (s.tree_cnt) {  // single systems (batches keep their own level loop)
+        if (n == 16) p.top = r4 ? k_factor_top_tc<16, 4> : k_factor_top_tc<16, 8>;
+        else p.top = r4 ? k_factor_top_tc<8, 4> : k_factor_top_tc<8, 8>;
+        smem_limit_once(p.top, tc_smem_per_warp(n) * TOP_WARPS);
+      }
       if (s.pair_kernel == PAIR_TC_GATHER && s.tree_cnt && d.nblock >= 2) {
         if (n == 16) p.tcb = r4 ? k_factor_lu_tc<16, false, true, 4> : k_factor_lu_tc<16, false, true, 8>;
         else p.tcb = r4 ? k_factor_lu_tc<8, false, true, 4> : k_factor_lu_tc<8, false, true, 8>;
@@ -3558,7 +3695,9 @@ static bool factor_levels(DevState& s, const FactorPlan<T>& p, const WorkSet<T>&
         a.k = k;
         a.first = (k == 1);
         root = k;  // the pair (0, k) of the top level
-        p.tcb<<<grid_for(pairs_at_level(nb, k), 4, 148 * 16), 128, p.tc_smem, st>>>(a, nullptr, nullptr);
+        // level 1 has no gathers and no children: the plain instantiation
+        (k == 1 ? p.tc : p.tcb)<<<grid_for(pairs_at_level(nb, k), 4, 148 * 16), 128, p.tc_smem, st>>>(
+            a, nullptr, nullptr);
         check_launch("k_factor_lu_tc");
       }
       p.root<<<1, 32, 0, st>>>(a, ta, root);
@@ -3570,6 +3709,13 @@ static bool factor_levels(DevState& s, const FactorPlan<T>& p, const WorkSet<T>&
     a.k = k;
     a.first = (k == 1);
     const long np = pairs_at_level(nb, k);
+    if constexpr (sizeof(T) == 8) {
+      if (p.tc && p.top && np <= TOP_WARPS) {  // this level and every one above it
+        p.top<<<1, TOP_WARPS * 32, tc_smem_per_warp(n) * TOP_WARPS, st>>>(a, k);
+        check_launch("k_factor_top_tc");
+        break;
+      }
+    }
     if (p.umma) p.umma<<<grid_for(np, 1, 148), UM_NT, p.umma_smem, st>>>(a, w.slab, s.slab_elems);
     else if (p.blk) p.blk<<<grid_for(np, 1, s.slab_ctas), 256, p.blk_smem, st>>>(a, w.slab, s.slab_elems);
     else if (p.cta) p.cta<<<grid_for(np, 1, s.slab_ctas), 256, 0, st>>>(a, w.slab, s.slab_elems);

@@ -155,17 +155,63 @@ def test_gpu_deterministic():
     assert np.array_equal(x1, x2)
 
 
+def _reference_solution(s, b, internal="LU"):
+    """The reference BorderedCR's own solution (oracle/_ref, its thread pool)
+    and the object that keeps the unfactored matrix for its Mv."""
+    import os
+    th = os.cpu_count() or 1
+    src = po.RefBCR(s, internal, "LU", "NONE", nthreads=th, npb=th)
+    work = po.RefBCR(s, internal, "LU", "NONE", nthreads=th, npb=th)
+    work.set_threads(True, True)
+    _, x = work.time_factor_solve(src, b)
+    return x, src
+
+
+def _ref_relres(src, s, x, b):
+    r = b[:s.nrows] - src.mv(x[:s.ncols])
+    return np.abs(r).max() / (block_norm_inf(s) * np.abs(x[:s.ncols]).max() + np.abs(b[:s.nrows]).max())
+
+
 @pytest.mark.parametrize("internal", ["LU", "QR"])
-def test_gpu_full_size_config_B_residual(internal):
-    """n=16, nblock=100000, qr=qx=2, nr=nx=4: FP64 bar rel. residual <= 1e-13."""
+def test_gpu_full_size_config_B_vs_reference(internal):
+    """n=16, nblock=100000, qr=qx=2, nr=nx=4, the same seeded system as the
+    benchmark: forward error against the reference BorderedCR's solution
+    <= 1e-10 and relative residual with the reference's Mv <= 1e-13 (FP64)."""
+    if not po.ref_available():
+        pytest.skip("oracle/_ref not built")
     s = synth.collocation(**synth.CONFIGS["B"], seed=0)
     b = synth.rhs(s, nrhs=1, seed=1)[0]
+    xr, src = _reference_solution(s, b, internal)
     h = gpu_solver(s, internal, "LU")
     assert h.factorize(), h.last_error()
     x = gpu_solve(h, b)
-    r = h.mv(x[:s.ncols]) - b[:s.nrows]
-    rel = np.abs(r).max() / (block_norm_inf(s) * np.abs(x[:s.ncols]).max() + np.abs(b[:s.nrows]).max())
-    assert rel < 1e-13, rel
+    assert fwd_err(x[:s.ncols], xr[:s.ncols]) < 1e-10
+    assert _ref_relres(src, s, x, b) < 1e-13
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gpu_full_size_config_E_vs_reference(precision):
+    """n=128, nblock=8192, qr=qx=4, nr=nx=16 (the tensor-core configuration):
+    the FP64 path to rel. residual <= 1e-13, the mixed path (tcgen05 FP32
+    products + FP64 refinement) to <= 1e-12, both with the reference's Mv, and
+    the forward error against the reference BorderedCR's solution (<= 1e-10
+    FP64; the mixed path's stays within cond(A) * 1e-12 of it: <= 1e-6)."""
+    if not po.ref_available():
+        pytest.skip("oracle/_ref not built")
+    s = synth.collocation(**synth.CONFIGS["E"], seed=0)
+    b = synth.rhs(s, nrhs=1, seed=1)[0]
+    xr, src = _reference_solution(s, b)
+    h = gpu_solver(s)
+    if precision == "mixed":
+        h.set_precision(B.PRECISION_MIXED)
+    assert h.factorize(), h.last_error()
+    x = gpu_solve(h, b)
+    rel = _ref_relres(src, s, x, b)
+    fe = fwd_err(x[:s.ncols], xr[:s.ncols])
+    if precision == "fp64":
+        assert rel < 1e-13 and fe < 1e-10, (rel, fe)
+    else:
+        assert rel < 1e-12 and fe < 1e-6, (rel, fe)
 
 
 @pytest.mark.parametrize("dims,internal,nrhs", [
