@@ -132,11 +132,13 @@ _SIGS = [
     ("bcr_batch_synchronize", [ct.c_void_p], ct.c_int),
     ("bcr_batch_last_error", [ct.c_void_p], ct.c_char_p),
     ("bcr_batch_set_precision", [ct.c_void_p, ct.c_int], ct.c_int),
+    ("bcr_batch_set_schedule", [ct.c_void_p, ct.c_int], ct.c_int),
     ("bcr_batch_set_refinement", [ct.c_void_p, ct.c_double, ct.c_int], ct.c_int),
     ("bcr_batch_refinement_info", [ct.c_void_p, ct.POINTER(ct.c_int), _dp], ct.c_int),
 ]
 
 GRAPH_FACTORIZE, GRAPH_SOLVE, GRAPH_STEP = 1, 2, 3
+BATCH_PERSISTENT, BATCH_LEVELS = 0, 1
 
 _lib = None
 
@@ -528,6 +530,11 @@ class Batch:
 
     def set_refinement(self, tol: float = 1e-12, max_iter: int = 10):
         self._check(self.L.bcr_batch_set_refinement(self.b, float(tol), int(max_iter)))
+
+    def set_schedule(self, schedule: int):
+        """BATCH_LEVELS (default: one launch per level) or BATCH_PERSISTENT (one
+        persistent launch per class with a per-system level schedule); before prepare()."""
+        self._check(self.L.bcr_batch_set_schedule(self.b, int(schedule)))
 
     def refinement_info(self):
         """(corrections applied, worst |b-Ax|/(|A||x|+|b|) over the batch) of the last mixed solve."""

@@ -1294,6 +1294,7 @@ struct bcr_batch_s {
   bcr::StatusWords* d_st = nullptr;
   std::vector<bcr::StatusWords> h_st;
   // mixed path: FP32 working arrays, refined solutions, per-system norms
+  int schedule = BCR_BATCH_LEVELS;  // factorization: one launch per level, or one persistent launch
   int precision = BCR_PRECISION_FP64;
   double ir_tol = 1e-12;
   int ir_max = 30;  // converged systems drop out, so a slow one costs little
@@ -1608,6 +1609,7 @@ int bcr_batch_s::prepare(int autotune) {
     int nrm = 0, nxm = 0;
     for (int i : members[c]) { nrm = std::max(nrm, dims[i].nr); nxm = std::max(nxm, dims[i].nx); }
     cls[c].mixed = mixed() ? 1 : 0;
+    cls[c].persist = schedule == BCR_BATCH_PERSISTENT ? 1 : 0;
     for (const auto& t : g_batch_tuning)
       if (t.n == d0.n && t.nrm == nrm && t.nxm == nxm && t.mixed == cls[c].mixed) { cls[c].fam = t.fam; cls[c].chunk = t.chunk; }
     if (bcr::batch_build(cls[c], v, 1)) {
@@ -1943,6 +1945,15 @@ int bcr_batch_set_precision(bcr_batch b, int precision) {
     return b->fail(BCR_BAD_ARGUMENT, fmt("bcr_batch_set_precision: unknown precision %d\n", precision));
   b->release();
   b->precision = precision;
+  return BCR_OK;
+}
+
+int bcr_batch_set_schedule(bcr_batch b, int schedule) {
+  B_CHECK(b);
+  if (schedule != BCR_BATCH_PERSISTENT && schedule != BCR_BATCH_LEVELS)
+    return b->fail(BCR_BAD_ARGUMENT, fmt("bcr_batch_set_schedule: unknown schedule %d\n", schedule));
+  b->release();
+  b->schedule = schedule;
   return BCR_OK;
 }
 

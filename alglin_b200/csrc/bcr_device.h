@@ -95,8 +95,11 @@ struct BatchClass {
   void* sb = nullptr;    // device SweepArgs<double>[nsys], backward layout
   void* ld = nullptr;    // device last-block descriptors [nsys]
   void* rd = nullptr;    // device residual descriptors [nsys] (mixed path)
-  BatchCta* fmap = nullptr;  // device: factorization chunks of every level
+  BatchCta* fmap = nullptr;  // device: factorization chunks of every level (level order)
   BatchCta* smap = nullptr;  // device: sweep chunks of every level
+  int persist = 1;           // factorization: one persistent launch with a per-system level schedule
+  long items = 0;            // factorization chunks in fmap
+  int* qbuf = nullptr;       // device: item counter, per-system pair counters, published levels
   std::vector<long> foff, fcnt, soff, scnt;
 };
 

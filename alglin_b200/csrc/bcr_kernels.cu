@@ -21,6 +21,7 @@
 // C_jp); dC_jpp goes to a per-block scratch slot and is added to C_jpp by
 // k_border_fix after the level, because C_jpp is also C_jp of pair j+2k.
 // The F updates dF go to a per-block slot and are summed in a fixed order.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 
@@ -56,6 +57,19 @@ struct FactorArgs {
 template <typename T>
 __device__ __forceinline__ T ldsrc(bool first, const double* orig, const T* work, size_t i) {
   return first ? T(orig[i]) : work[i];
+}
+
+// the same where another CTA of the same launch may have written the element
+// (persistent batch launches): served by L2, never by a stale L1 line
+template <bool COH, typename T>
+__device__ __forceinline__ T ldsrc_c(bool first, const double* orig, const T* work, size_t i) {
+  if constexpr (COH) return first ? T(__ldcg(orig + i)) : __ldcg(work + i);
+  else return ldsrc(first, orig, work, i);
+}
+template <bool COH, typename T>
+__device__ __forceinline__ T ldro(const T* p) {
+  if constexpr (COH) return __ldcg(p);
+  else return __ldg(p);
 }
 
 // Pair range of one worker (warp or CTA).  Single system: a grid-stride loop
@@ -381,19 +395,15 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_factor_level(FactorArgs<T>
 // the lanes by column (lane c holds column c, and c+32) and are eliminated with
 // the same pivot rows, which yields C_j U^-1 and the C/F Schur updates.
 // ---------------------------------------------------------------------------
-template <typename T, int N, int NXM, int NRM, bool BATCH = false>
-__global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<T> a0, const FactorArgs<T>* tab,
-                                                         const BatchCta* cmap) {
+// pairs [q0, q1) step qs of one system and level, one per warp
+template <typename T, int N, int NXM, int NRM, bool COH>
+__device__ __forceinline__ void rows_body(const FactorArgs<T>& a, long q0, long q1, long qs) {
   constexpr int NC = 3 * N + NXM;
   constexpr int NCP = (NC + 1) & ~1;
   constexpr int SLOTS = (NC + 31) / 32;
   constexpr unsigned FULL = 0xffffffffu;
   __shared__ __align__(16) T ubuf[4][NCP];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  FactorArgs<T> ab;  // this CTA's system (batch only)
-  long q0, q1, qs;
-  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
-  const FactorArgs<T>& a = BATCH ? ab : a0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const Dims d = a.d;
   const int n = d.n, nr = d.nr, nx = d.nx, n2 = 2 * n;
   const size_t nn = (size_t)n * n, nnx = (size_t)n * nx, nrn = (size_t)nr * n, nrnx = (size_t)nr * nx;
@@ -415,8 +425,8 @@ __global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<T> a0, const 
         T pv = T(0), xv = T(0);
         if (act && c < n) {
           const size_t o = op + (size_t)c * n + ri;
-          pv = top ? ldsrc(first, a.E0, a.E, o) : ldsrc(first, a.D0, a.D, o);
-          xv = top ? ldsrc(first, a.D0, a.D, o) : ldsrc(first, a.E0, a.E, o);
+          pv = top ? ldsrc_c<COH>(first, a.E0, a.E, o) : ldsrc_c<COH>(first, a.D0, a.D, o);
+          xv = top ? ldsrc_c<COH>(first, a.D0, a.D, o) : ldsrc_c<COH>(first, a.E0, a.E, o);
         }
         row[c] = pv;
         row[N + c] = top ? xv : T(0);
@@ -424,7 +434,7 @@ __global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<T> a0, const 
       }
 #pragma unroll
       for (int c = 0; c < NXM; ++c)
-        row[3 * N + c] = (act && c < nx) ? ldsrc(first, a.B0, a.B, ob + (size_t)c * n + ri) : T(0);
+        row[3 * N + c] = (act && c < nx) ? ldsrc_c<COH>(first, a.B0, a.B, ob + (size_t)c * n + ri) : T(0);
     }
     T cr[NRM][SLOTS];
 #pragma unroll
@@ -435,7 +445,7 @@ __global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<T> a0, const 
       const size_t oc = (size_t)j * nrn + (size_t)lane * nr;
 #pragma unroll
       for (int r = 0; r < NRM; ++r)
-        if (r < nr) cr[r][0] = ldsrc(first, a.C0, a.C, oc + r);
+        if (r < nr) cr[r][0] = ldsrc_c<COH>(first, a.C0, a.C, oc + r);
     }
 
     int mypos = lane, mykey = 0, info = 0;
@@ -526,7 +536,7 @@ __global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<T> a0, const 
           const int c = col - N;
           if (c < n) {
             const size_t o = (size_t)jp * nrn + (size_t)c * nr + r;
-            a.C[o] = ldsrc(first, a.C0, a.C, o) + v;
+            a.C[o] = ldsrc_c<COH>(first, a.C0, a.C, o) + v;
           }
         } else if (col < 3 * N) {
           const int c = col - 2 * N;
@@ -538,6 +548,16 @@ __global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<T> a0, const 
       }
     }
   }
+}
+
+template <typename T, int N, int NXM, int NRM, bool BATCH = false>
+__global__ void __launch_bounds__(128) k_factor_lu_rows(FactorArgs<T> a0, const FactorArgs<T>* tab,
+                                                         const BatchCta* cmap) {
+  const int warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  FactorArgs<T> ab;  // this CTA's system (batch only)
+  long q0, q1, qs;
+  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
+  rows_body<T, N, NXM, NRM, false>(BATCH ? ab : a0, q0, q1, qs);
 }
 
 // ---------------------------------------------------------------------------
@@ -1288,9 +1308,9 @@ struct GrpProduct<float, N> {
 template <typename T, int N>
 constexpr int grp_min_blocks() { return N == 32 ? (sizeof(T) == 8 ? 5 : 6) : 4; }
 
-template <typename T, int N, bool BATCH = false>
-__global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
-    k_factor_lu_grp(FactorArgs<T> a0, const FactorArgs<T>* tab, const BatchCta* cmap) {
+// pairs [q0, q1) step qs of one system and level, one per CTA
+template <typename T, int N, bool COH>
+__device__ __forceinline__ void grp_body(const FactorArgs<T>& a, long q0, long q1, long qs) {
   using S = GrpShape<T, N>;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1300,10 +1320,6 @@ __global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
   int* hdr = reinterpret_cast<int*>(slot + 2 * S::NWP * S::LDS);  // [2][NWP][4] hi, lo, position, thread
   int* rowof = hdr + 2 * S::NWP * 4;               // position -> original row
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  FactorArgs<T> ab;  // this CTA's system (batch only)
-  long q0, q1, qs;
-  pair_range<BATCH>(a0, tab, cmap, 1, 0, ab, q0, q1, qs);
-  const FactorArgs<T>& a = BATCH ? ab : a0;
   const Dims d = a.d;
   const int nr = d.nr, nx = d.nx;
   constexpr int n = N, n2 = 2 * N;
@@ -1330,29 +1346,30 @@ __global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
         const size_t base = top ? (size_t)jp * nn : (size_t)j * nn;
         const auto* P = top ? E : D;
 #pragma unroll
-        for (int c = 0; c < N; ++c) row[c] = T(__ldg(P + base + (size_t)c * n + ri));
+        for (int c = 0; c < N; ++c) row[c] = T(ldro<COH>(P + base + (size_t)c * n + ri));
       } else {
 #pragma unroll
         for (int c = 0; c < N; ++c)
-          row[c] = brow ? T(__ldg(C + (size_t)j * nrn + (size_t)c * nr + (t - n2))) : T(0);
+          row[c] = brow ? T(ldro<COH>(C + (size_t)j * nrn + (size_t)c * nr + (t - n2))) : T(0);
       }
 #pragma unroll
       for (int it = 0; it < IT; ++it) {
         const int idx = t + S::NTH * it;
         const bool in = idx < (int)nn;
-        vd[it] = in ? T(__ldg(D + (size_t)jp * nn + idx)) : T(0);
-        ve[it] = in ? T(__ldg(E + (size_t)j * nn + idx)) : T(0);
+        vd[it] = in ? T(ldro<COH>(D + (size_t)jp * nn + idx)) : T(0);
+        ve[it] = in ? T(ldro<COH>(E + (size_t)j * nn + idx)) : T(0);
       }
 #pragma unroll
       for (int it = 0; it < IB; ++it) {
         const int idx = t + S::NTH * it;
         const bool in = idx < nx * n;
-        vbt[it] = in ? T(__ldg(Bm + (size_t)jp * nnx + idx)) : T(0);
-        vbb[it] = in ? T(__ldg(Bm + (size_t)j * nnx + idx)) : T(0);
+        vbt[it] = in ? T(ldro<COH>(Bm + (size_t)jp * nnx + idx)) : T(0);
+        vbb[it] = in ? T(ldro<COH>(Bm + (size_t)j * nnx + idx)) : T(0);
       }
     };
     if (first) load(a.D0, a.E0, a.B0, a.C0);
     else load(a.D, a.E, a.B, a.C);
+
     // trailing columns, compact: TOP rows [D_jp B_jp], BOTTOM rows [E_j B_j]
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
@@ -1505,7 +1522,7 @@ __global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
         if (rr < nr) {
           if (col < n) {
             const size_t o = (size_t)jp * nrn + (size_t)col * nr + rr;
-            a.C[o] = ldsrc(first, a.C0, a.C, o) + v;
+            a.C[o] = ldsrc_c<COH>(first, a.C0, a.C, o) + v;
           } else if (col < n2) {
             a.Rbuf[(size_t)j * nrn + (size_t)(col - n) * nr + rr] = v;
           } else if (col < n2 + nx) {
@@ -1515,6 +1532,15 @@ __global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
       }
     });
   }
+}
+
+template <typename T, int N, bool BATCH = false>
+__global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
+    k_factor_lu_grp(FactorArgs<T> a0, const FactorArgs<T>* tab, const BatchCta* cmap) {
+  FactorArgs<T> ab;  // this CTA's system (batch only)
+  long q0, q1, qs;
+  pair_range<BATCH>(a0, tab, cmap, 1, 0, ab, q0, q1, qs);
+  grp_body<T, N, false>(BATCH ? ab : a0, q0, q1, qs);
 }
 
 // ---------------------------------------------------------------------------
@@ -4046,6 +4072,229 @@ __global__ void __launch_bounds__(128) kb_border_fix(const FactorArgs<T>* tab, c
   }
 }
 
+// ---------------------------------------------------------------------------
+// Persistent batch factorization: one launch per class works through the
+// (system, level, pair range) items of every level, in level order, with a
+// per-system level schedule.  A CTA takes the next item from a counter and
+// waits (bounded) until that system's previous level is complete; systems
+// advance independently, so a deep system does not hold up shallow ones and
+// no level ever waits for the whole batch.  The worker that finishes the last
+// item of a (system, level) applies that level's C_jpp updates (the work of
+// kb_border_fix) and then publishes the level.  Items are taken in level order,
+// so every item an item waits for was taken earlier by a running CTA: the
+// waits always end.  A wait that exceeds its limit (about a second) reports
+// DEV_TIMEOUT for the system and skips the item's pairs.
+// ---------------------------------------------------------------------------
+struct BatchQueue {
+  int* next;         // next item (zero at launch)
+  int* done_pairs;   // per system: pairs finished, cumulative over levels
+  int* level_done;   // per system: levels published (border fix-up included)
+  long items;
+};
+
+// pairs of levels 0..L of a system of nb blocks
+__device__ __forceinline__ long pairs_through_level(int nb, int L) {
+  long s = 0;
+  for (int l = 0; l <= L; ++l) s += pairs_at_level(nb, 1 << l);
+  return s;
+}
+
+// CTA-wide: the next item; false when the queue is empty
+template <typename T>
+__device__ bool queue_next(const BatchQueue& qu, const BatchCta* items, const FactorArgs<T>* tab,
+                           FactorArgs<T>& a, BatchCta& c, bool& ok) {
+  __shared__ long s_it;
+  __shared__ int s_ok;
+  __syncthreads();  // the previous item's readers of s_it / s_ok are done
+  if (threadIdx.x == 0) {
+    const long it = atomicAdd(qu.next, 1);
+    int good = 1;
+    if (it < qu.items) {
+      const BatchCta ci = items[it];
+      if (ci.pad > 0) {
+        const volatile int* flag = qu.level_done + ci.sys;
+        unsigned spins = 0;
+        while (*flag < ci.pad) {
+          if (++spins > (1u << 23)) { good = 0; break; }
+          __nanosleep(100);
+        }
+        __threadfence();
+      }
+    }
+    s_it = it;
+    s_ok = good;
+  }
+  __syncthreads();
+  const long it = s_it;
+  if (it >= qu.items) return false;
+  __threadfence();  // acquire: the system's previous level is visible to every thread
+  c = items[it];
+  ok = s_ok != 0;
+  a = tab[c.sys];
+  a.k = 1 << c.pad;
+  a.first = c.pad == 0;
+  if (!ok && threadIdx.x == 0) report(a.st, DEV_TIMEOUT, -1, 0, a.k);
+  return true;
+}
+
+// CTA-wide: count the item's pairs; the CTA completing the (system, level)
+// applies the level's C_jpp updates and publishes the level
+// the C_jpp updates of every pair of (system, level): C_jpp += Rbuf[j], four
+// elements per thread and round with their loads in flight together
+template <typename T>
+__device__ void level_fixup(const FactorArgs<T>& a, const BatchCta& c, int tid, int nthr) {
+  const Dims d = a.d;
+  const int k = 1 << c.pad;
+  const size_t nrn = (size_t)d.nr * d.n;
+  const long np = pairs_at_level(d.nblock, k);
+  const size_t tot = (size_t)np * nrn;
+  for (size_t e0 = tid; e0 < tot; e0 += 4 * (size_t)nthr) {
+    size_t oc[4];
+    T cv[4], rv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const size_t e = e0 + u * (size_t)nthr;
+      oc[u] = 0;
+      cv[u] = rv[u] = T(0);
+      if (e < tot) {
+        const long q = (long)(e / nrn);
+        const size_t idx = e % nrn;
+        const int j = k + (int)(2L * k * q), jpp = min(j + k, d.nblock);
+        oc[u] = (size_t)jpp * nrn + idx;
+        cv[u] = __ldcg(a.C + oc[u]);
+        rv[u] = __ldcg(a.Rbuf + (size_t)j * nrn + idx);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (e0 + u * (size_t)nthr < tot) a.C[oc[u]] = cv[u] + rv[u];
+  }
+}
+
+// CTA-wide: count the item's pairs; the CTA completing the (system, level)
+// applies the level's C_jpp updates and publishes the level
+template <typename T>
+__device__ void queue_done(const BatchQueue& qu, const FactorArgs<T>& a, const BatchCta& c) {
+  __shared__ int s_last;
+  __threadfence();  // release: this thread's results of the item
+  __syncthreads();  // every pair of the item is finished
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const long cnt = c.q1 - c.q0;
+    const int old = atomicAdd(qu.done_pairs + c.sys, (int)cnt);
+    s_last = (long)old + cnt == pairs_through_level(a.d.nblock, c.pad);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  level_fixup<T>(a, c, threadIdx.x, blockDim.x);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicExch(qu.level_done + c.sys, c.pad + 1);
+  }
+}
+
+// The same per warp, for the warp-per-pair families: each warp takes, waits
+// for and publishes its own items, so no warp ever waits at a CTA barrier for
+// another warp's item.
+template <typename T>
+__device__ bool queue_next_warp(const BatchQueue& qu, const BatchCta* items, const FactorArgs<T>* tab,
+                                FactorArgs<T>& a, BatchCta& c, bool& ok) {
+  const int lane = threadIdx.x & 31;
+  long it = 0;
+  int good = 1;
+  if (lane == 0) {
+    it = atomicAdd(qu.next, 1);
+    if (it < qu.items) {
+      const BatchCta ci = items[it];
+      if (ci.pad > 0) {
+        const volatile int* flag = qu.level_done + ci.sys;
+        unsigned spins = 0;
+        while (*flag < ci.pad) {
+          if (++spins > (1u << 23)) { good = 0; break; }
+          __nanosleep(100);
+        }
+        __threadfence();
+      }
+    }
+  }
+  it = __shfl_sync(0xffffffffu, it, 0);
+  good = __shfl_sync(0xffffffffu, good, 0);
+  if (it >= qu.items) return false;
+  __threadfence();
+  c = items[it];
+  ok = good != 0;
+  a = tab[c.sys];
+  a.k = 1 << c.pad;
+  a.first = c.pad == 0;
+  if (!ok && lane == 0) report(a.st, DEV_TIMEOUT, -1, 0, a.k);
+  return true;
+}
+
+template <typename T>
+__device__ void queue_done_warp(const BatchQueue& qu, const FactorArgs<T>& a, const BatchCta& c) {
+  const int lane = threadIdx.x & 31;
+  __threadfence();
+  __syncwarp();
+  int last = 0;
+  if (lane == 0) {
+    const long cnt = c.q1 - c.q0;
+    const int old = atomicAdd(qu.done_pairs + c.sys, (int)cnt);
+    last = (long)old + cnt == pairs_through_level(a.d.nblock, c.pad);
+  }
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (!last) return;
+  __threadfence();
+  level_fixup<T>(a, c, lane, 32);
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) atomicExch(qu.level_done + c.sys, c.pad + 1);
+}
+
+template <typename T, int N, int NXM, int NRM>
+__global__ void __launch_bounds__(128) kp_factor_rows(const FactorArgs<T>* tab, const BatchCta* items, BatchQueue qu) {
+  FactorArgs<T> a;
+  BatchCta c;
+  bool ok;
+  while (queue_next_warp(qu, items, tab, a, c, ok)) {
+    if (ok) rows_body<T, N, NXM, NRM, true>(a, c.q0, c.q1, 1);
+    queue_done_warp(qu, a, c);
+  }
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
+    kp_factor_grp(const FactorArgs<T>* tab, const BatchCta* items, BatchQueue qu) {
+  FactorArgs<T> a;
+  BatchCta c;
+  bool ok;
+  while (queue_next(qu, items, tab, a, c, ok)) {
+    if (ok) grp_body<T, N, true>(a, c.q0, c.q1, 1);
+    queue_done(qu, a, c);
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(128, 4) kp_factor_tc(const FactorArgs<double>* tab, const BatchCta* items,
+                                                       BatchQueue qu) {
+  using S = TcShape<N>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double* Wt = reinterpret_cast<double*>(smem_raw + (size_t)warp * S::BYTES);
+  FactorArgs<double> a;
+  BatchCta c;
+  bool ok;
+  while (queue_next_warp(qu, items, tab, a, c, ok)) {
+    const TcTree tr{0, 0, 0};
+    if (ok)
+      for (long q = c.q0; q < c.q1; ++q)
+        tc_pair<N, 8>(a, a.k + (int)(2L * a.k * q), a.k, a.first != 0, Wt, lane, tr);
+    queue_done_warp(qu, a, c);
+  }
+}
+
 // F = F0 + sum of the Schur updates, one CTA per system (fixed order)
 __global__ void __launch_bounds__(256) kb_reduce_F(const LastDesc* t) {
   const LastDesc& L = t[blockIdx.x];
@@ -4253,15 +4502,21 @@ static void build_map(const std::vector<DevState>& sys, int levels, int chunk, s
                       std::vector<long>& off, std::vector<long>& cnt) {
   off.assign(levels, 0);
   cnt.assign(levels, 0);
+  // within a level the deepest systems come first: their chains of levels are
+  // the longest, so the persistent launch starts them first
+  std::vector<size_t> order(sys.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](size_t x, size_t y) { return sys[x].d.nblock > sys[y].d.nblock; });
   for (int L = 0; L < levels; ++L) {
     const int k = 1 << L;
     off[L] = (long)map.size();
-    for (size_t i = 0; i < sys.size(); ++i) {
+    for (size_t i : order) {
       const long np = pairs_at_level(sys[i].d.nblock, k);
       for (long q0 = 0; q0 < np; q0 += chunk) {
         BatchCta c;
         c.sys = (int)i;
-        c.pad = 0;
+        c.pad = L;  // the level (the persistent launch reads it)
         c.q0 = q0;
         c.q1 = q0 + chunk < np ? q0 + chunk : np;
         map.push_back(c);
@@ -4279,6 +4534,8 @@ static int upload_table(void*& dst, const std::vector<X>& v) {
 }
 
 void batch_free(BatchClass& c) {
+  if (c.qbuf) cudaFree(c.qbuf);
+  c.qbuf = nullptr;
   for (void** p : {&c.fa, &c.sf, &c.sb, &c.ld, &c.rd})
     if (*p) { cudaFree(*p); *p = nullptr; }
   if (c.fmap) { cudaFree(c.fmap); c.fmap = nullptr; }
@@ -4353,6 +4610,8 @@ static int batch_build_t(BatchClass& c, const std::vector<DevState>& sys, int nr
   bad |= upload_table(m1, fmap) | upload_table(m2, smap);
   c.fmap = static_cast<BatchCta*>(m1);
   c.smap = static_cast<BatchCta*>(m2);
+  c.items = (long)fmap.size();
+  if (cudaMalloc(&c.qbuf, (1 + 2 * (size_t)c.nsys) * sizeof(int)) != cudaSuccess) bad = 1;
   return bad;
 }
 
@@ -4406,12 +4665,58 @@ static void batch_pairs(BatchClass& c, int L, cudaStream_t st) {
   }
 }
 
+// every level of every system of the class in one persistent launch
+template <typename T>
+static void batch_pairs_persistent(BatchClass& c, cudaStream_t st) {
+  if (c.items == 0) return;
+  cudaMemsetAsync(c.qbuf, 0, (1 + 2 * (size_t)c.nsys) * sizeof(int), st);
+  BatchQueue qu{c.qbuf, c.qbuf + 1, c.qbuf + 1 + c.nsys, c.items};
+  const FactorArgs<T>* tab = static_cast<const FactorArgs<T>*>(c.fa);
+  auto grid = [&](auto* kern, int threads, size_t smem) {
+    return grid_for(c.items, 1, 148 * resident_ctas(kern, threads, smem));
+  };
+  if constexpr (sizeof(T) == 8) {
+    if (c.fam == PAIR_TC) {
+      const size_t sm = tc_smem_per_warp(c.n) * 4;
+      if (c.n == 16) {
+        smem_limit_once(kp_factor_tc<16>, sm);
+        kp_factor_tc<16><<<grid(kp_factor_tc<16>, 128, sm), 128, sm, st>>>(tab, c.fmap, qu);
+      } else {
+        smem_limit_once(kp_factor_tc<8>, sm);
+        kp_factor_tc<8><<<grid(kp_factor_tc<8>, 128, sm), 128, sm, st>>>(tab, c.fmap, qu);
+      }
+      check_launch("kp_factor_tc");
+      return;
+    }
+  }
+  if (c.fam == PAIR_GRP) {
+    if (c.n == 32) {
+      auto* kern = kp_factor_grp<T, 32>;
+      smem_limit_once(kern, GrpShape<T, 32>::BYTES);
+      kern<<<grid(kern, 96, GrpShape<T, 32>::BYTES), 96, GrpShape<T, 32>::BYTES, st>>>(tab, c.fmap, qu);
+    } else {
+      auto* kern = kp_factor_grp<T, 16>;
+      smem_limit_once(kern, GrpShape<T, 16>::BYTES);
+      kern<<<grid(kern, 64, GrpShape<T, 16>::BYTES), 64, GrpShape<T, 16>::BYTES, st>>>(tab, c.fmap, qu);
+    }
+  } else if (c.fam == PAIR_ROWS) {
+    auto* kern = c.n <= 4 ? kp_factor_rows<T, 4, 4, 4> : c.n <= 8 ? kp_factor_rows<T, 8, 4, 4>
+                                                                   : kp_factor_rows<T, 16, 4, 4>;
+    kern<<<grid(kern, 128, 0), 128, 0, st>>>(tab, c.fmap, qu);
+  }
+  check_launch("persistent batched pair kernel");
+}
+
 template <typename T>
 static void batch_factorize_t(BatchClass& c, cudaStream_t st) {
   const LastDesc* ld = static_cast<const LastDesc*>(c.ld);
   kb_begin<T><<<c.nsys, 256, 0, st>>>(ld);
   check_launch("kb_begin");
-  for (int L = 0; L < c.levels; ++L) batch_pairs<T>(c, L, st);
+  if (c.persist) {
+    batch_pairs_persistent<T>(c, st);
+  } else {
+    for (int L = 0; L < c.levels; ++L) batch_pairs<T>(c, L, st);
+  }
   kb_reduce_F<<<c.nsys, 256, 0, st>>>(ld);
   kb_last_assemble<T><<<c.nsys, 256, 0, st>>>(ld);
   kb_last_factor<<<c.nsys, 512, 0, st>>>(ld);

@@ -17,8 +17,10 @@ Workload (one "step" = factorize + solve of one system):
           and mixed on n=32, nblock=65536, nr=nx=8 at kappa = 1, 10, 100 and on
           n=128, nblock=8192, qr=qx=4, nr=nx=16 (the mixed pair kernel there
           runs its products on the tcgen05 tensor cores); a batch of 4096
-          uneven systems (systems/s, p50/p99 of the batch latency); and the
-          reference's own BorderedCR<float> (unrefined FP32) on this workload.
+          uneven systems (systems/s, p50/p99 of the batch latency; one launch
+          per level, and for comparison one persistent launch per class with a
+          per-system level schedule); and the reference's own
+          BorderedCR<float> (unrefined FP32) on this workload.
 
   accuracy: every entry carries its relative residual
           ||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf), with A x taken by
@@ -493,16 +495,18 @@ def variants(torch, bcr, synth, steps, warmup, rank, threads, sB, bB, refB, hB):
     out["E_mixed"] = _entry(mix, sE, xmx, bE, refE, workload=wl, pair_kernel="FP32 LU, tcgen05 3xTF32 products")
     out["E_mixed_over_fp64"] = mix["value"] / f64["value"]
     del sE, refE
-    for name, prec in (("D_batched_fp64", bcr.PRECISION_FP64), ("D_batched_mixed", bcr.PRECISION_MIXED)):
+    for name, prec, sched, ref in (("D_batched_fp64", bcr.PRECISION_FP64, bcr.BATCH_LEVELS, True),
+                                   ("D_batched_mixed", bcr.PRECISION_MIXED, bcr.BATCH_LEVELS, True),
+                                   ("D_batched_fp64_persistent", bcr.PRECISION_FP64, bcr.BATCH_PERSISTENT, False)):
         try:
-            out[name] = batched(torch, bcr, synth, rank, prec, threads)
+            out[name] = batched(torch, bcr, synth, rank, prec, threads, schedule=sched, reference=ref)
         except Exception as e:  # e.g. not enough device memory on a shared GPU
             out[name] = {"unavailable": str(e)[:200]}
         torch.cuda.empty_cache()
     return out
 
 
-def batched(torch, bcr, synth, rank, prec, threads, nsys=4096, sample_every=32):
+def batched(torch, bcr, synth, rank, prec, threads, nsys=4096, sample_every=32, schedule=None, reference=True):
     """4096 independent systems, nblock ~ U{64..4096}, n in {4,8,16,32},
     nr = nx in {0,2,4}: one CUDA graph per factorize + solve of the whole batch.
     Every 32nd system (128 in all) is also copied to the host: its GPU solution
@@ -519,6 +523,7 @@ def batched(torch, bcr, synth, rank, prec, threads, nsys=4096, sample_every=32):
     for d in dims:
         bt.add_device(*d)
     bt.set_precision(prec)
+    bt.set_schedule(bcr.BATCH_LEVELS if schedule is None else schedule)
     bt.prepare()
     g = torch.Generator(device="cuda")
     g.manual_seed(7 + rank)
@@ -568,7 +573,9 @@ def batched(torch, bcr, synth, rank, prec, threads, nsys=4096, sample_every=32):
         xh = np.zeros(max(s.nrows, s.ncols))
         rt.cudaMemcpy(xh.ctypes.data, bt.device_x(i), xh.nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
         xs[i] = xh
-    if po.ref_available():
+    out["schedule"] = "persistent (one launch per class, per-system level schedule)" \
+        if schedule == bcr.BATCH_PERSISTENT else "one launch per level"
+    if reference and po.ref_available():
         def ref_one(i):
             s, rhs = kept[i]
             src = po.RefBCR(s, "LU", "LU", "NONE", nthreads=0)
@@ -618,10 +625,35 @@ def cpu_baseline(s, b, steps, warmup):
              "sample": "full workload, one factorize+solve of the C oracle"}, None)
 
 
+def run_once_batch(args):
+    """One factorize + solve of a batch of --nsys-once uneven systems (the
+    batch workload's distribution) through the persistent schedule, for
+    profilers."""
+    import torch
+    from alglin_b200 import bcr, synth
+    dims = synth.batch_dims(args.nsys_once, 64, 4096, seed=0)
+    bt = bcr.Batch()
+    for d in dims:
+        bt.add_device(*d)
+    bt.set_precision(bcr.PRECISION_MIXED if args.precision == "mixed" else bcr.PRECISION_FP64)
+    bt.prepare()
+    for i, d in enumerate(dims):
+        ts = synth.collocation_torch(torch, *d, seed=i)
+        torch.cuda.synchronize()
+        bt.load_device(i, *[t.data_ptr() if t.numel() else 0 for t in ts])
+    xs = [np.ones(max(bt.system_size(i))) for i in range(len(dims))]
+    assert bt.factorize_solve(xs), bt.last_error()
+    print(json.dumps({"once": "D", "nsys": len(dims), "precision": args.precision,
+                      "classes": bt.classes()}))
+    return 0
+
+
 def run_once(args):
     """One factorize + solve of a named workload through the C ABI, for profilers."""
     import torch
     from alglin_b200 import bcr, synth
+    if args.once == "D":
+        return run_once_batch(args)
     cfg = dict(synth.CONFIGS[args.once])
     if args.nblock_once:
         cfg["nblock"] = args.nblock_once
@@ -654,7 +686,8 @@ def main():
                     help="skip the mixed-path, n=32 and batched measurements")
     ap.add_argument("--nblock", type=int, default=CFG["nblock"],
                     help="smaller systems for profiling runs (the reported workload is 100000)")
-    ap.add_argument("--once", choices=["A", "B", "C", "E"],
+    ap.add_argument("--nsys-once", type=int, default=64, help="systems of the --once D batch")
+    ap.add_argument("--once", choices=["A", "B", "C", "D", "E"],
                     help="run one factorize+solve of that workload and exit (for profilers)")
     ap.add_argument("--nblock-once", type=int, default=0, help="nblock of the --once workload")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="path of --once")

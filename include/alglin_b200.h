@@ -283,6 +283,17 @@ const char *bcr_batch_last_error(bcr_batch b);
    of the later corrections; the systems must be square */
 int bcr_batch_set_precision(bcr_batch b, int precision);
 int bcr_batch_set_refinement(bcr_batch b, double tol, int max_iter);
+/* Schedule of the batched factorization (set before prepare; extension, no
+   reference counterpart).  LEVELS (the default): one launch per level for all
+   systems of a class.  PERSISTENT: one launch per class works through every
+   (system, level, pair range) item in level order with a per-system level
+   schedule -- a worker waits (bounded, about a second, then
+   BCR_DEVICE_TIMEOUT for that system) only for its own system's previous
+   level, and the worker completing a level applies its border updates; the
+   results are bit-identical to LEVELS. */
+#define BCR_BATCH_PERSISTENT 0
+#define BCR_BATCH_LEVELS 1
+int bcr_batch_set_schedule(bcr_batch b, int schedule);
 int bcr_batch_refinement_info(bcr_batch b, int *iters, double *worst);
 
 #ifdef __cplusplus

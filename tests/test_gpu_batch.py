@@ -48,10 +48,12 @@ def check_against_oracle(systems, rhs, xs):
 
 
 @pytest.mark.parametrize("autotune", [False, True])
-def test_batch_matches_oracle(autotune):
+@pytest.mark.parametrize("schedule", [B.BATCH_PERSISTENT, B.BATCH_LEVELS])
+def test_batch_matches_oracle(autotune, schedule):
     systems, rhs = make_systems(28, 1, 300, seed=5)
     hs = handles_for(systems)
     bt = B.Batch(hs)
+    bt.set_schedule(schedule)
     bt.prepare(autotune=autotune)
     assert len(bt) == 28
     cls = bt.classes()
@@ -237,3 +239,29 @@ def test_batch_mixed_rejects_non_square():
     bt.set_precision(B.PRECISION_MIXED)
     with pytest.raises(B.BCRError, match="square"):
         bt.prepare()
+
+
+@pytest.mark.parametrize("precision", [B.PRECISION_FP64, B.PRECISION_MIXED])
+def test_batch_persistent_schedule_matches_level_launches(precision):
+    """The persistent launch (per-system level schedule, systems of very
+    different depths side by side: 1 to 2000 blocks) gives the same
+    factorization as one launch per level, bit for bit, for every family."""
+    dims = [(1, 8, 0, 0, 2, 2), (2, 16, 0, 0, 4, 4), (2000, 4, 0, 0, 0, 0), (3, 32, 0, 0, 2, 2),
+            (1500, 16, 0, 0, 4, 4), (777, 8, 0, 0, 2, 2), (1024, 32, 0, 0, 4, 4), (5, 4, 0, 0, 2, 2),
+            (1025, 16, 0, 0, 0, 0), (64, 32, 0, 0, 0, 0)]
+    systems = [synth.collocation(*d, seed=300 + i) for i, d in enumerate(dims)]
+    rhs = [synth.rhs(s, 1, seed=400 + i)[0] for i, s in enumerate(systems)]
+    out = []
+    for schedule in (B.BATCH_PERSISTENT, B.BATCH_LEVELS):
+        hs = handles_for(systems)
+        bt = B.Batch(hs)
+        bt.set_precision(precision)
+        bt.set_schedule(schedule)
+        bt.prepare()
+        xs = [b.copy() for b in rhs]
+        assert bt.factorize_solve(xs), bt.last_error()
+        out.append(xs)
+    for x1, x2 in zip(out[0], out[1]):
+        assert np.array_equal(x1, x2)
+    if precision == B.PRECISION_FP64:
+        check_against_oracle(systems, rhs, out[0])
