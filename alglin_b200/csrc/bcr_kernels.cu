@@ -2879,63 +2879,70 @@ __device__ void last_svd(Dims d, const double* A, LastBufs b, StatusWords* st) {
 // solvers: LU (getrf), LUPQ (complete pivoting), QR (geqrf), QRP (geqp3: the
 // column of largest remaining 2-norm first), and the SVD family
 // Last blocks of order <= LAST_SMALL (configs with n <= 16 and small borders):
-// LU and the LU solves run in shared memory on one warp (lane = rows lane and
-// lane + 32) instead of the CTA-wide loops over global memory, which cost a few
-// barriers and a global round trip per column.  Same pivot rule (largest |a|,
-// first row on ties, NaN never chosen), same operation order.
+// the LU runs out of shared memory (the general loop below works in global
+// memory, a round trip per column) and the LU solves run on one warp with the
+// values in registers.  Same pivot rule (largest |a|, first row on ties, NaN
+// never chosen), same operation order.
 constexpr int LAST_SMALL = 64;
 
 template <typename T>
 __device__ void last_lu_small(Dims d, LastBufs b, StatusWords* st) {
   __shared__ T As[LAST_SMALL * (LAST_SMALL + 1)];
-  __shared__ int s_bad;
+  __shared__ T s_pv;
+  __shared__ int s_p;
   const int N = d.Nc, ld = N + 1, tid = threadIdx.x, bs = blockDim.x;
   T* A = b.A;
-  for (int e = tid; e < N * N; e += bs) As[(e / N) * ld + e % N] = A[e];
-  if (tid == 0) s_bad = 0;
+  for (int c = tid / 32; c < N; c += bs / 32)  // one column per warp: coalesced, all loads in flight
+    for (int r = tid & 31; r < N; r += 32) As[c * ld + r] = A[(size_t)c * N + r];
   __syncthreads();
-  if (tid < 32) {
-    const int lane = tid, r0 = lane, r1 = lane + 32;
-    const bool in0 = r0 < N, in1 = r1 < N;
-    for (int i = 0; i < N; ++i) {
-      // pivot of column i: rows >= i, |a| (NaN counts as -1: never chosen)
-      T v0 = T(-2), v1 = T(-2);
-      int i0 = 0x7fffffff, i1 = 0x7fffffff;
-      if (in0 && r0 >= i) { const T v = dev_abs(As[i * ld + r0]); v0 = v > T(-1) ? v : T(-1); i0 = r0; }
-      if (in1 && r1 >= i) { const T v = dev_abs(As[i * ld + r1]); v1 = v > T(-1) ? v : T(-1); i1 = r1; }
-      T best = v0;
-      int p = i0;
-      if (v1 > v0) { best = v1; p = i1; }
-      warp_argmax(best, p);
-      const T pv = As[i * ld + p];
-      if (pv == T(0)) {
-        if (lane == 0) { report(st, DEV_LAST_SINGULAR, -1, i + 1, -1); s_bad = 1; }
-        break;
+  for (int i = 0; i < N; ++i) {
+    if (tid < 32) {  // pivot of column i: largest |a| over rows >= i, first row on ties, NaN never
+      T best = T(-2);
+      int bi = 0x7fffffff;
+      for (int r = i + tid; r < N; r += 32) {
+        T v = dev_abs(As[i * ld + r]);
+        if (!(v == v)) v = T(-1);
+        if (v > best) { best = v; bi = r; }
       }
-      if (lane == 0) b.piv[i] = p;
-      if (p != i)
-        for (int c = lane; c < N; c += 32) {
-          const T t = As[c * ld + i]; As[c * ld + i] = As[c * ld + p]; As[c * ld + p] = t;
-        }
-      __syncwarp();
-      const T rinv = T(1) / pv;
-      const bool u0 = in0 && r0 > i, u1 = in1 && r1 > i;
-      if (u0) As[i * ld + r0] *= rinv;
-      if (u1) As[i * ld + r1] *= rinv;
-      __syncwarp();
-      const T m0 = u0 ? As[i * ld + r0] : T(0), m1 = u1 ? As[i * ld + r1] : T(0);
-#pragma unroll 8
-      for (int c = i + 1; c < N; ++c) {
-        const T a = As[c * ld + i];
-        if (u0) As[c * ld + r0] = fma(-m0, a, As[c * ld + r0]);
-        if (u1) As[c * ld + r1] = fma(-m1, a, As[c * ld + r1]);
+      // upper words of |a| first (one reduction); the exact argmax only on a tie
+      const unsigned key = best < T(0) ? 0u : (unsigned)((unsigned long long)__double_as_longlong((double)best) >> 32) + 1u;
+      const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
+      const unsigned m = __ballot_sync(0xffffffffu, key == kmax);
+      if (__popc(m) == 1 && kmax > 0) {
+        bi = __shfl_sync(0xffffffffu, bi, __ffs(m) - 1);
+      } else {
+        warp_argmax(best, bi);
       }
-      __syncwarp();
+      if (tid == 0) { s_p = bi; s_pv = As[i * ld + bi]; }
     }
+    __syncthreads();
+    const int p = s_p;
+    const T pv = s_pv;
+    if (pv == T(0)) {
+      if (tid == 0) report(st, DEV_LAST_SINGULAR, -1, i + 1, -1);
+      return;
+    }
+    if (tid == 0) b.piv[i] = p;
+    if (p != i)
+      for (int c = tid; c < N; c += bs) {
+        const T t = As[c * ld + i]; As[c * ld + i] = As[c * ld + p]; As[c * ld + p] = t;
+      }
+    __syncthreads();
+    const T rinv = T(1) / pv;
+    for (int r = i + 1 + tid; r < N; r += bs) As[i * ld + r] *= rinv;
+    __syncthreads();
+    {  // trailing update: thread -> row (tid % 64), columns every bs/64
+      const int r = i + 1 + (tid & 63), cs = bs >> 6;
+      if (r < N) {
+        const T m = As[i * ld + r];
+        for (int c = i + 1 + (tid >> 6); c < N; c += cs)
+          As[c * ld + r] = fma(-m, As[c * ld + i], As[c * ld + r]);
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  if (s_bad) return;
-  for (int e = tid; e < N * N; e += bs) A[e] = As[(e / N) * ld + e % N];
+  for (int c = tid / 32; c < N; c += bs / 32)
+    for (int r = tid & 31; r < N; r += 32) A[(size_t)c * N + r] = As[c * ld + r];
   if (tid == 0) st->kind = FACT_LU;
 }
 
@@ -3355,6 +3362,11 @@ __global__ void __launch_bounds__(256, 1) k_last_lu_blocked(Dims d, LastBufs b, 
 }
 
 __global__ void k_last_fallback(Dims d, LastBufs b, StatusWords* st) { last_fallback_body(d, b, st); }
+
+// LU of a last block of order <= LAST_SMALL on its own (one CTA)
+__global__ void __launch_bounds__(256) k_last_lu_small(Dims d, LastBufs b, StatusWords* st) {
+  last_lu_small<double>(d, b, st);
+}
 
 template <typename T>
 __global__ void k_last_solve(Dims d, LastBufs b, const StatusWords* st, T* x, int ldx, int nrhs) {
@@ -3778,6 +3790,9 @@ static void factor_last(DevState& s, const WorkSet<T>& w, cudaStream_t st, bool 
     smem_limit_once(k_last_lu_blocked, sm);
     k_last_lu_blocked<<<1, 256, sm, st>>>(d, lb, s.st);
     check_launch("k_last_lu_blocked");
+  } else if (s.sel_last == LAST_LU && d.Nr == d.Nc && d.Nc <= LAST_SMALL) {
+    k_last_lu_small<<<1, 256, 0, st>>>(d, lb, s.st);
+    check_launch("k_last_lu_small");
   } else {
     k_last_factor<double><<<1, 512, 0, st>>>(d, lb, s.sel_last, s.st);
     check_launch("k_last_factor");
