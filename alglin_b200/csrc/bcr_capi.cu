@@ -86,6 +86,11 @@ struct bcr_handle_s {
   bcr::DevState s{};
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // chunked uploads of factorize_solve from host buffers: a copy stream and
+  // the events that order its chunks (created on first use)
+  static constexpr int NCHUNK_EV = 8;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t chunk_ev[NCHUNK_EV] = {};
   double* dX = nullptr;
   size_t dX_cap = 0;
   double* dY = nullptr;
@@ -144,6 +149,12 @@ struct bcr_handle_s {
     if (own_stream && stream) cudaStreamDestroy(stream);
     if (own_stream) stream = nullptr;
     own_stream = false;
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    copy_stream = nullptr;
+    for (auto& e : chunk_ev) {
+      if (e) cudaEventDestroy(e);
+      e = nullptr;
+    }
     dev_ready = false;
     dirty = true;
     factorized = false;
@@ -1097,10 +1108,44 @@ int bcr_factorize_solve(bcr_handle h, int nrhs, double* rhs, int ldRhs) {
     int rc = h->check_matrix();
     if (rc) return rc;
   }
-  int rc = h->upload();
-  if (rc) return rc;
   if (nrhs < 0 || ldRhs < h->L()) return h->fail(BCR_BAD_ARGUMENT, fmt("BorderedCR::solve: bad ldRhs = %d\n", ldRhs));
+  int rc = h->ensure_device();
+  if (rc) return rc;
   const size_t Lx = (size_t)h->L();
+  // the FP64 n = 8/16 path overlaps the upload of the matrix with the
+  // factorization of the chunks already on the device
+  if (nrhs > 0 && h->precision == BCR_PRECISION_FP64) {
+    if ((rc = h->ensure_buffer(h->dX, h->dX_cap, Lx * nrhs))) return rc;
+    if ((rc = h->prepare_launch())) return rc;
+    if (!h->copy_stream) {
+      if (cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess) h->copy_stream = nullptr;
+      for (auto& e : h->chunk_ev)
+        if (h->copy_stream && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) e = nullptr;
+    }
+    bool evs = h->copy_stream != nullptr;
+    for (auto e : h->chunk_ev) evs = evs && e;
+    if (evs) {
+      cudaMemcpy2DAsync(h->dX, Lx * 8, rhs, (size_t)ldRhs * 8, Lx * 8, nrhs, cudaMemcpyHostToDevice, h->stream);
+      // the copy stream starts after the previous use of the matrix arrays
+      cudaEventRecord(h->chunk_ev[0], h->stream);
+      cudaStreamWaitEvent(h->copy_stream, h->chunk_ev[0], 0);
+      const bcr::HostMatrix hm{h->hD.data(), h->hE.data(), h->hB.data(), h->hC.data(), h->hCq.data(),
+                               h->hF.data(), h->hH.data()};
+      h->factorized = false;
+      if (bcr::launch_upload_factorize_solve(h->s, hm, h->dX, (int)Lx, nrhs, h->stream, h->copy_stream,
+                                             h->chunk_ev, bcr_handle_s::NCHUNK_EV)) {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return h->cuda_fail(e, "factorize_solve launch");
+        h->dirty = false;
+        h->pending_status = true;
+        h->factorized = true;
+        cudaMemcpy2DAsync(rhs, (size_t)ldRhs * 8, h->dX, Lx * 8, Lx * 8, nrhs, cudaMemcpyDeviceToHost, h->stream);
+        return h->factorize_status();
+      }
+    }
+  }
+  rc = h->upload();
+  if (rc) return rc;
   if (nrhs > 0) {
     if ((rc = h->ensure_buffer(h->dX, h->dX_cap, Lx * nrhs))) return rc;
     cudaMemcpy2DAsync(h->dX, Lx * 8, rhs, (size_t)ldRhs * 8, Lx * 8, nrhs, cudaMemcpyHostToDevice, h->stream);

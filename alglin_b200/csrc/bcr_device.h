@@ -64,6 +64,17 @@ void launch_solve(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st);
 // can carry them
 void launch_factorize_solve(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st);
 bool factorize_solve_fuses(const DevState& s, int nrhs);
+// host copies of the loaded matrix (reference layout, pinned for full-rate copies)
+struct HostMatrix {
+  const double *D, *E, *B, *C, *Cq, *F, *H;
+};
+// factorize + solve with the matrix uploaded from hm in chunks on the copy
+// stream cst (events ev[0..nev) order the chunks), overlapped with the
+// factorization of the chunks already on the device; false (nothing enqueued)
+// when the shape does not take this path (FP64 n = 8/16 LU with fused
+// right-hand sides, at least 2048 blocks)
+bool launch_upload_factorize_solve(DevState& s, const HostMatrix& hm, double* x, int ldx, int nrhs,
+                                   cudaStream_t st, cudaStream_t cst, cudaEvent_t* ev, int nev);
 // res = alpha * A * x + beta * res with the loaded (unfactored) matrix
 void launch_mv(DevState& s, double alpha, const double* x, double beta, double* res,
                cudaStream_t st);

@@ -50,6 +50,8 @@ struct FactorArgs {
   double* x;
   int ldx, nrf;
   double* XB;
+  // pair range of a single-system launch, [qb, qe) of the level (qe == 0: all)
+  long qb, qe;
 };
 
 // element of a block: the loaded FP64 matrix at the first level, the working
@@ -83,6 +85,12 @@ __device__ __forceinline__ void take_level(FactorArgs<double>& a, const FactorAr
 template <typename A>
 __device__ __forceinline__ bool system_active(const A&) { return true; }
 
+// the pair range a single-system factorization launch is limited to (sweeps: all)
+template <typename T>
+__device__ __forceinline__ void launch_pair_range(const FactorArgs<T>& a, long& qb, long& qe) { qb = a.qb; qe = a.qe; }
+template <typename A>
+__device__ __forceinline__ void launch_pair_range(const A&, long&, long&) {}
+
 template <bool BATCH, typename A>
 __device__ __forceinline__ void pair_range(const A& a0, const A* tab, const BatchCta* cmap, int workers, int worker,
                                            A& a, long& q0, long& q1, long& qs) {
@@ -97,6 +105,9 @@ __device__ __forceinline__ void pair_range(const A& a0, const A* tab, const Batc
     q0 = (long)blockIdx.x * workers + worker;
     q1 = pairs_at_level(a0.d.nblock, a0.k);
     qs = (long)gridDim.x * workers;
+    long qb = 0, qe = 0;
+    launch_pair_range(a0, qb, qe);
+    if (qe > 0) { q0 += qb; q1 = qe; }
   }
 }
 
@@ -3909,6 +3920,7 @@ static bool factor_levels(DevState& s, const FactorPlan<T>& p, const WorkSet<T>&
   a.Tm = w.Tm; a.P = s.P; a.Rbuf = w.Rbuf; a.Fbuf = s.Fbuf; a.st = s.st;
   a.ldw = odd_ld(2 * n + d.nr);
   a.x = x; a.ldx = ldx; a.nrf = nrf; a.XB = s.XB;
+  a.qb = a.qe = 0;
   if constexpr (sizeof(T) == 8) {
     if (p.tree || p.tcb) {
       a.F0 = s.F0;
@@ -4192,6 +4204,105 @@ void launch_factorize_solve(DevState& s, double* x, int ldx, int nrhs, cudaStrea
   if (!tree) reduce_xb(s, x, ldx, nrf, st);
   factor_last(s, w, st, tree);
   last_and_backward(s, plan_sweeps<double>(s), w, x, ldx, nrf, st);
+}
+
+// Factorize + solve with the matrix uploaded from host memory in chunks of
+// 2^m consecutive blocks on the copy stream cst, each chunk's own CR levels
+// (the pairs lying inside it) launched on st as soon as it has arrived: the
+// tc pair kernels with the tree's border bookkeeping write nothing outside a
+// chunk but their own Rbuf/Fbuf/XB slots, so chunks need no fix-up and the
+// upload overlaps the factorization.  The levels spanning chunks, the root,
+// the last block and the backward sweep follow.  Returns false (nothing
+// enqueued) when the shape does not take this path.
+bool launch_upload_factorize_solve(DevState& s, const HostMatrix& hm, double* x, int ldx, int nrhs,
+                                   cudaStream_t st, cudaStream_t cst, cudaEvent_t* ev, int nev) {
+  if (s.mixed || !s.tree_cnt) return false;
+  const Dims d = s.d;
+  const int n = d.n, nb = d.nblock;
+  if (nb < 2048 || nev < 2) return false;
+  PairKernel saved = (PairKernel)s.pair_kernel;
+  if (saved != PAIR_AUTO && saved != PAIR_TC_GATHER) return false;
+  s.pair_kernel = PAIR_TC_GATHER;
+  const FactorPlan<double> p = plan_factor<double>(s);
+  s.pair_kernel = saved;
+  if (!p.tc || !p.tcb || !p.root) return false;
+  const int nrf = fusable_rhs(s, p, nrhs);
+  if (nrf != nrhs) return false;
+  // chunks: a power of two of blocks, at most nev of them
+  int chunk = 1024;
+  while ((long)chunk * nev < nb) chunk *= 2;
+  const int nchunks = (nb + chunk - 1) / chunk;
+  double* tag = nullptr;
+  const WorkSet<double> w = work_set(s, tag);
+  const size_t nn = (size_t)n * n, nnx = (size_t)n * d.nx, nrn = (size_t)d.nr * n;
+  // the small arrays first, then the chunks
+  auto up = [&](double* dst, const double* src, size_t cnt) {
+    if (cnt) cudaMemcpyAsync(dst, src, cnt * 8, cudaMemcpyHostToDevice, cst);
+  };
+  up(s.Cq, hm.Cq, (size_t)d.nr * d.qx);
+  up(s.F0, hm.F, (size_t)d.nr * d.nx);
+  up(s.H, hm.H, (size_t)(n + d.qr) * d.Nc);
+  FactorArgs<double> a;
+  a.d = d;
+  a.D0 = s.D0; a.E0 = s.E0; a.B0 = s.B0; a.C0 = s.C0;
+  a.D = w.D; a.E = w.E; a.B = w.B; a.C = w.C;
+  a.Tm = w.Tm; a.P = s.P; a.Rbuf = w.Rbuf; a.Fbuf = s.Fbuf; a.st = s.st;
+  a.ldw = odd_ld(2 * n + d.nr);
+  a.x = x; a.ldx = ldx; a.nrf = nrf; a.XB = s.XB;
+  a.F0 = s.F0;
+  cudaMemsetAsync(s.st, 0, sizeof(StatusWords), st);
+  for (int c = 0; c < nchunks; ++c) {
+    const long b0 = (long)c * chunk, b1 = std::min<long>(b0 + chunk, nb);
+    up(s.D0 + b0 * nn, hm.D + b0 * nn, (size_t)(b1 - b0) * nn);
+    up(s.E0 + b0 * nn, hm.E + b0 * nn, (size_t)(b1 - b0) * nn);
+    up(s.B0 + b0 * nnx, hm.B + b0 * nnx, (size_t)(b1 - b0) * nnx);
+    const long c1 = c == nchunks - 1 ? nb + 1 : b1;  // the last chunk also brings C_nblock
+    up(s.C0 + b0 * nrn, hm.C + b0 * nrn, (size_t)(c1 - b0) * nrn);
+    cudaEventRecord(ev[c % nev], cst);
+    cudaStreamWaitEvent(st, ev[c % nev], 0);
+    if (c == nchunks - 1) {  // blocks no pair of the first level touches: the odd tail and C_nblock
+      if (nb % 2 == 1) {
+        const size_t t = (size_t)(nb - 1);
+        k_convert_blocks<double><<<1, 256, 0, st>>>(s.D0 + t * nn, w.D + t * nn, nn);
+        k_convert_blocks<double><<<1, 256, 0, st>>>(s.E0 + t * nn, w.E + t * nn, nn);
+        if (nnx) k_convert_blocks<double><<<1, 256, 0, st>>>(s.B0 + t * nnx, w.B + t * nnx, nnx);
+        if (nrn) k_convert_blocks<double><<<1, 256, 0, st>>>(s.C0 + t * nrn, w.C + t * nrn, nrn);
+      }
+      if (nrn) k_convert_blocks<double><<<1, 256, 0, st>>>(s.C0 + (size_t)nb * nrn, w.C + (size_t)nb * nrn, nrn);
+    }
+    // the levels whose pairs lie inside [b0, b1): j = k (2q + 1) with b0 < j < b1
+    for (int k = 1; k < chunk; k *= 2) {
+      const long qb = b0 / (2L * k), np = pairs_at_level(nb, k);
+      const long qe = std::min<long>(np, (b1 + k - 1) / (2L * k));  // j < b1
+      if (qe <= qb) continue;
+      a.k = k;
+      a.first = k == 1;
+      a.qb = qb;
+      a.qe = qe;
+      (k == 1 ? p.tc : p.tcb)<<<grid_for(qe - qb, 4, 148 * 16), 128, p.tc_smem, st>>>(a, nullptr, nullptr);
+      check_launch("k_factor_lu_tc (chunk)");
+    }
+  }
+  a.qb = a.qe = 0;
+  TreeArgs ta;
+  ta.cnt = s.tree_cnt;
+  ta.leaf = s.tree_cnt + nb;
+  ta.Ffin = s.Ffin;
+  ta.xb = (nrf > 0 && d.nr > 0) ? x + (size_t)(nb + 1) * n + d.qr : nullptr;
+  int root = 1;
+  for (int k = 1; k < nb; k *= 2) {
+    root = k;
+    if (k < chunk) continue;
+    a.k = k;
+    a.first = 0;
+    p.tcb<<<grid_for(pairs_at_level(nb, k), 4, 148 * 16), 128, p.tc_smem, st>>>(a, nullptr, nullptr);
+    check_launch("k_factor_lu_tc");
+  }
+  p.root<<<1, 32, 0, st>>>(a, ta, root);
+  check_launch("k_tree_root");
+  factor_last(s, w, st, true);
+  last_and_backward(s, plan_sweeps<double>(s), w, x, ldx, nrf, st);
+  return true;
 }
 
 bool factorize_solve_fuses(const DevState& s, int nrhs) {

@@ -105,3 +105,27 @@ def test_tree_singular_panel_reports_like_reference():
     s2 = synth.collocation(64, 16, 0, 0, 2, 2, seed=2)
     h2 = _solver(s2, B.PAIR_TREE)
     assert h2.factorize(), h2.last_error()
+
+
+@pytest.mark.parametrize("dims", [(2048, 16, 2, 2, 4, 4), (5000, 8, 0, 0, 2, 2), (10001, 16, 1, 1, 3, 3),
+                                  (33000, 16, 0, 0, 0, 0)])
+@pytest.mark.parametrize("nrhs", [1, 2])
+def test_chunked_upload_factorize_solve(dims, nrhs):
+    """factorize_solve from host buffers uploads the matrix in chunks and
+    factors each chunk's own levels while the next chunk is in flight: the
+    oracle's answer, a second call on the same handle, the loaded matrix on the
+    device afterwards (Mv), and a later plain solve with the stored factors."""
+    s = synth.collocation(*dims, seed=sum(dims))
+    b = synth.rhs(s, nrhs=nrhs, seed=4)
+    o = po.Oracle(s, "LU", _last(s))
+    assert o.factorize(), o.last_error()
+    xo = o.solve(b)
+    h = _solver(s, B.PAIR_AUTO)
+    for _ in range(2):
+        X = b.copy()
+        assert h.factorize_solve(nrhs, X, X.shape[1]), h.last_error()
+        assert fwd_err(X[:, :s.ncols], xo[:, :s.ncols]) < 1e-10
+    xr = np.random.default_rng(1).standard_normal(s.ncols)
+    assert np.abs(h.mv(xr)[:s.nrows] - o.mv(xr)).max() < 1e-12 * max(1.0, np.abs(o.mv(xr)).max())
+    Y = _solve(h, b)
+    assert fwd_err(Y[:, :s.ncols], xo[:, :s.ncols]) < 1e-10
