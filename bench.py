@@ -53,8 +53,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "BABD factor+solve unknowns/s at rel. residual ≤1e-12: mixed vs plain FP64 GPU"
 # DRAM bytes per block moved by the factorization kernels of this workload,
-# from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum)
-FACT_DRAM_BYTES_PER_BLOCK = 23963
+# from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# same workload at nblock=40000 (the traffic grows with the blocks)
+FACT_DRAM_BYTES_PER_BLOCK = 21542
 CFG = dict(nblock=100000, n=16, qr=2, qx=2, nr=4, nx=4)
 
 
@@ -351,13 +352,14 @@ def run_ours(args):
             "data": "synthetic", "impl": "ours",
             "config": workload_config(), "parallelism": f"replicas x{world}",
             "phases_ms": {"factorize": fact_ms, "solve": solve_ms},
-            "roofline": {"bound": "hbm", "kernel": "factorize (tree-scheduled CR launch + last block)",
+            "roofline": {"bound": "hbm", "kernel": "factorize (every CR level launch, the top-level CTA, "
+                                                   "the F/xb sums and the last block)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": FACT_DRAM_BYTES_PER_BLOCK * CFG["nblock"],
                          "traffic_source": "ncu dram__bytes_read+write of one factorization of this "
-                                           "workload (nblock=100000; "
-                                           "profiles/dram_factor_solve_n16_nblock100000.md)",
+                                           "workload at nblock=40000, 21,542 B per block, scaled to "
+                                           "100000 blocks (profiles/dram_factor_solve_n16_nblock40000.md)",
                          "algorithmic_bytes": fact_b},
             "e2e": {"value": world * s.ncols / e2e_t, "unit": "unknowns/s",
                     "h2d_bytes_per_step": nbytes_mat + 8 * L, "d2h_bytes_per_step": 8 * L},
