@@ -155,13 +155,19 @@ def algorithmic_bytes(d, nrhs=1):
 
 
 def launches_per_step(nblock, nr, nx):
-    levels = 0
-    k = 1
+    """Kernel launches of one factorize+solve step of the FP64 n=16 path
+    (forward elimination fused into the pair kernel)."""
+    def pairs(k):
+        return (nblock - k - 1) // (2 * k) + 1 if nblock > k else 0
+    levels, k = [], 1
     while k < nblock:
-        levels += 1
+        levels.append(k)
         k *= 2
-    fact = levels * (2 if nr else 1) + (2 if nr * nx else 0) + 2
-    solve = levels * 2 + (2 if nr else 0) + 1
+    big = [k for k in levels if pairs(k) > 16]   # one pair-kernel launch (+ border fix-up) each
+    top = 1 if len(big) < len(levels) else 0     # the remaining top levels: one CTA
+    fact = (1 if nr else 0) + (4 if nblock % 2 else 0) + len(big) * (2 if nr else 1) + top
+    fact += (2 if nr * nx else 0) + (2 if nr else 0) + 2  # F and xb sums, assemble, last-block LU
+    solve = 1 + top + len(big)                   # last-block solve, backward top, backward levels
     return fact + solve
 
 
