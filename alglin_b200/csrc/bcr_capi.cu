@@ -1468,7 +1468,9 @@ struct bcr_batch_s {
       } else if (it >= fixed) {
         break;
       }
-      enqueue_solve();  // converged systems skip their sweeps
+      // the correction solve covers only the systems still refining
+      for (auto& c : cls) bcr::batch_compact(c, stream);
+      for (auto& c : cls) bcr::batch_solve(c, stream, true);
       for (auto& c : cls) bcr::batch_correct(c, stream);
       ++it;
     }

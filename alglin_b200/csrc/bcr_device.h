@@ -108,6 +108,8 @@ struct BatchClass {
   void* rd = nullptr;    // device residual descriptors [nsys] (mixed path)
   BatchCta* fmap = nullptr;  // device: factorization chunks of every level (level order)
   BatchCta* smap = nullptr;  // device: sweep chunks of every level
+  BatchCta* cmap = nullptr;  // device, mixed path: smap entries of the systems still refining
+  long* ccnt = nullptr;      // device, mixed path: cmap entries per level
   int persist = 1;           // factorization: one persistent launch with a per-system level schedule
   long items = 0;            // factorization chunks in fmap
   int* qbuf = nullptr;       // device: item counter, per-system pair counters, published levels
@@ -121,7 +123,11 @@ bool batch_family_ok(int fam, const Dims& d, bool mixed);
 int batch_build(BatchClass& c, const std::vector<DevState>& sys, int nrhs);
 void batch_free(BatchClass& c);
 void batch_factorize(BatchClass& c, cudaStream_t st);
-void batch_solve(BatchClass& c, cudaStream_t st);
+// compact: the sweeps walk the compacted maps of the last batch_compact
+void batch_solve(BatchClass& c, cudaStream_t st, bool compact = false);
+// mixed path: the sweep-map entries of the systems not yet converged, per
+// level, for the next correction solve
+void batch_compact(BatchClass& c, cudaStream_t st);
 // mixed path: r = b - A x_sol into the rhs slots, per-system norms and
 // converged flags (relative residual <= tol), batch-worst relative residual
 // (|A| is measured when with_A)

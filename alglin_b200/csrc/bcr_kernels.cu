@@ -32,6 +32,7 @@ namespace bcr {
 static constexpr int WARPS_PANEL = 4;
 static constexpr size_t SMEM_MAX = 227 * 1024;
 static constexpr int CTA_KERNEL_MIN_N = 24;  // n above this: one CTA per pair
+static constexpr long COMPACT_GRID = 148 * 8;  // CTAs of a sweep over a compacted batch map
 
 template <typename T>
 struct FactorArgs {
@@ -75,8 +76,9 @@ __device__ __forceinline__ T ldro(const T* p) {
 }
 
 // Pair range of one worker (warp or CTA).  Single system: a grid-stride loop
-// over the level's pairs.  Batch: CTA b works on pairs [q0, q1) of system
-// cmap[b].sys, whose arguments come from the table; the level is the batch's.
+// over the level's pairs.  Batch: map entry e (by default the CTA's index)
+// holds pairs [q0, q1) of system cmap[e].sys, whose arguments come from the
+// table; the level is the batch's.
 __device__ __forceinline__ void take_level(FactorArgs<float>& a, const FactorArgs<float>& a0) { a.k = a0.k; a.first = a0.first; }
 __device__ __forceinline__ void take_level(FactorArgs<double>& a, const FactorArgs<double>& a0) { a.k = a0.k; a.first = a0.first; }
 
@@ -93,9 +95,9 @@ __device__ __forceinline__ void launch_pair_range(const A&, long&, long&) {}
 
 template <bool BATCH, typename A>
 __device__ __forceinline__ void pair_range(const A& a0, const A* tab, const BatchCta* cmap, int workers, int worker,
-                                           A& a, long& q0, long& q1, long& qs) {
+                                           A& a, long& q0, long& q1, long& qs, long entry = -1) {
   if constexpr (BATCH) {
-    const BatchCta c = cmap[blockIdx.x];
+    const BatchCta c = cmap[entry < 0 ? (long)blockIdx.x : entry];
     a = tab[c.sys];
     take_level(a, a0);
     q0 = c.q0 + worker;
@@ -108,6 +110,20 @@ __device__ __forceinline__ void pair_range(const A& a0, const A* tab, const Batc
     long qb = 0, qe = 0;
     launch_pair_range(a0, qb, qe);
     if (qe > 0) { q0 += qb; q1 = qe; }
+  }
+}
+
+// Map entries of one CTA of a batched sweep: entry b alone (one CTA per
+// entry), or, when ecnt is given (the compacted maps of the refinement
+// passes, whose length the device wrote), entries b, b + grid, ... below
+// *ecnt.  Single systems: the body once.
+template <bool BATCH, typename F>
+__device__ __forceinline__ void for_entries(const long* ecnt, F&& body) {
+  if constexpr (BATCH) {
+    const long cnt = ecnt ? *ecnt : (long)gridDim.x;
+    for (long e = blockIdx.x; e < cnt; e += gridDim.x) body(e);
+  } else {
+    body(-1L);
   }
 }
 
@@ -2172,112 +2188,116 @@ __device__ __forceinline__ void take_level(SweepArgs<double>& a, const SweepArgs
 
 template <typename T, bool BATCH = false>
 __global__ void __launch_bounds__(WARPS_PANEL * 32) k_forward_level(SweepArgs<T> a0, const SweepArgs<T>* tab,
-                                                                const BatchCta* cmap) {
+                                                                const BatchCta* cmap, const long* ecnt) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  SweepArgs<T> ab;  // this CTA's system (batch only)
-  long q0, q1, qs;
-  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
-  const SweepArgs<T>& a = BATCH ? ab : a0;
-  const Dims d = a.d;
-  const int n = d.n, nr = d.nr, n2 = 2 * n, nrhs = a.nrhs, ldw = a.ldw, k = a.k;
-  double* W = reinterpret_cast<double*>(smem_raw) + (size_t)warp * ldw * nrhs;
-  for (long q = q0; q < q1; q += qs) {
-    const int j = k + (int)(2L * k * q), jp = j - k;
-    const T* Tj = a.Tm + (size_t)j * szT(d);
-    const unsigned char* Pj = a.P + (size_t)j * szP(d);
-    for (int idx = lane; idx < n2 * nrhs; idx += 32) {
-      const int pos = idx % n2, c = idx / n2;
-      const int r = a.sel == SEL_LU ? Pj[pos] : pos;  // original row at this position
-      const size_t o = (size_t)c * a.ldx + (r < n ? (size_t)jp * n + r : (size_t)j * n + (r - n));
-      W[(size_t)c * ldw + pos] = a.x[o];
-    }
-    __syncwarp();
-    if (a.sel == SEL_LU) {
-      for (int i = 0; i < n; ++i) {
-        for (int r = i + 1 + lane; r < n2; r += 32) {
-          const double l = Tj[(size_t)i * n2 + r];
-          for (int c = 0; c < nrhs; ++c) W[(size_t)c * ldw + r] -= l * W[(size_t)c * ldw + i];
-        }
-        __syncwarp();
+  for_entries<BATCH>(ecnt, [&](long entry) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    SweepArgs<T> ab;  // this CTA's system (batch only)
+    long q0, q1, qs;
+    pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs, entry);
+    const SweepArgs<T>& a = BATCH ? ab : a0;
+    const Dims d = a.d;
+    const int n = d.n, nr = d.nr, n2 = 2 * n, nrhs = a.nrhs, ldw = a.ldw, k = a.k;
+    double* W = reinterpret_cast<double*>(smem_raw) + (size_t)warp * ldw * nrhs;
+    for (long q = q0; q < q1; q += qs) {
+      const int j = k + (int)(2L * k * q), jp = j - k;
+      const T* Tj = a.Tm + (size_t)j * szT(d);
+      const unsigned char* Pj = a.P + (size_t)j * szP(d);
+      for (int idx = lane; idx < n2 * nrhs; idx += 32) {
+        const int pos = idx % n2, c = idx / n2;
+        const int r = a.sel == SEL_LU ? Pj[pos] : pos;  // original row at this position
+        const size_t o = (size_t)c * a.ldx + (r < n ? (size_t)jp * n + r : (size_t)j * n + (r - n));
+        W[(size_t)c * ldw + pos] = a.x[o];
       }
-    } else {
-      for (int i = 0; i < n; ++i) {
-        const double t = Tj[2 * (size_t)n * n + i];
-        const T* v = Tj + (size_t)i * n2;
-        for (int c = 0; c < nrhs; ++c) {
-          double* w = W + (size_t)c * ldw;
+      __syncwarp();
+      if (a.sel == SEL_LU) {
+        for (int i = 0; i < n; ++i) {
+          for (int r = i + 1 + lane; r < n2; r += 32) {
+            const double l = Tj[(size_t)i * n2 + r];
+            for (int c = 0; c < nrhs; ++c) W[(size_t)c * ldw + r] -= l * W[(size_t)c * ldw + i];
+          }
+          __syncwarp();
+        }
+      } else {
+        for (int i = 0; i < n; ++i) {
+          const double t = Tj[2 * (size_t)n * n + i];
+          const T* v = Tj + (size_t)i * n2;
+          for (int c = 0; c < nrhs; ++c) {
+            double* w = W + (size_t)c * ldw;
+            double s = 0.0;
+            for (int r = i + 1 + lane; r < n2; r += 32) s += double(v[r]) * w[r];
+            s = warp_sum(s);
+            s = (s + w[i]) * t;
+            __syncwarp();
+            if (lane == 0) w[i] -= s;
+            for (int r = i + 1 + lane; r < n2; r += 32) w[r] -= s * double(v[r]);
+            __syncwarp();
+          }
+        }
+      }
+      __syncwarp();
+      for (int idx = lane; idx < n * nrhs; idx += 32) {
+        const int i = idx % n, c = idx / n;
+        a.x[(size_t)c * a.ldx + (size_t)jp * n + i] = W[(size_t)c * ldw + n + i];
+        a.x[(size_t)c * a.ldx + (size_t)j * n + i] = W[(size_t)c * ldw + i];
+      }
+      if (nr > 0) {
+        const T* Cj = a.C + (size_t)j * nr * n;
+        for (int idx = lane; idx < nr * nrhs; idx += 32) {
+          const int r = idx % nr, c = idx / nr;
           double s = 0.0;
-          for (int r = i + 1 + lane; r < n2; r += 32) s += double(v[r]) * w[r];
-          s = warp_sum(s);
-          s = (s + w[i]) * t;
-          __syncwarp();
-          if (lane == 0) w[i] -= s;
-          for (int r = i + 1 + lane; r < n2; r += 32) w[r] -= s * double(v[r]);
-          __syncwarp();
+          for (int i = 0; i < n; ++i) s += double(Cj[(size_t)i * nr + r]) * W[(size_t)c * ldw + i];
+          a.XB[(size_t)j * nr * nrhs + idx] = -s;
         }
       }
+      __syncwarp();
     }
-    __syncwarp();
-    for (int idx = lane; idx < n * nrhs; idx += 32) {
-      const int i = idx % n, c = idx / n;
-      a.x[(size_t)c * a.ldx + (size_t)jp * n + i] = W[(size_t)c * ldw + n + i];
-      a.x[(size_t)c * a.ldx + (size_t)j * n + i] = W[(size_t)c * ldw + i];
-    }
-    if (nr > 0) {
-      const T* Cj = a.C + (size_t)j * nr * n;
-      for (int idx = lane; idx < nr * nrhs; idx += 32) {
-        const int r = idx % nr, c = idx / nr;
-        double s = 0.0;
-        for (int i = 0; i < n; ++i) s += double(Cj[(size_t)i * nr + r]) * W[(size_t)c * ldw + i];
-        a.XB[(size_t)j * nr * nrhs + idx] = -s;
-      }
-    }
-    __syncwarp();
-  }
+  });
 }
 
 template <typename T, bool BATCH = false>
 __global__ void __launch_bounds__(WARPS_PANEL * 32) k_backward_level(SweepArgs<T> a0, const SweepArgs<T>* tab,
-                                                                 const BatchCta* cmap) {
+                                                                 const BatchCta* cmap, const long* ecnt) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  SweepArgs<T> ab;  // this CTA's system (batch only)
-  long q0, q1, qs;
-  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
-  const SweepArgs<T>& a = BATCH ? ab : a0;
-  const Dims d = a.d;
-  const int n = d.n, nx = d.nx, n2 = 2 * n, nrhs = a.nrhs, k = a.k, nb = d.nblock;
-  double* Y = reinterpret_cast<double*>(smem_raw) + (size_t)warp * a.ldw;
-  const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
-  for (long q = q0; q < q1; q += qs) {
-    const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
-    const T* Dj = a.D + (size_t)j * n * n;
-    const T* Ej = a.E + (size_t)j * n * n;
-    const T* Bj = a.B + (size_t)j * n * nx;
-    const T* Tj = a.Tm + (size_t)j * szT(d);
-    for (int c = 0; c < nrhs; ++c) {
-      double* xc = a.x + (size_t)c * a.ldx;
-      for (int i = lane; i < n; i += 32) {
-        double s = xc[(size_t)j * n + i];
-        for (int m = 0; m < n; ++m) s -= Dj[(size_t)m * n + i] * xc[(size_t)jp * n + m];
-        for (int m = 0; m < n; ++m) s -= Ej[(size_t)m * n + i] * xc[(size_t)jpp * n + m];
-        for (int m = 0; m < nx; ++m) s -= Bj[(size_t)m * n + i] * xc[xb_off + m];
-        Y[i] = s;
-      }
-      __syncwarp();
-      for (int i = n - 1; i >= 0; --i) {
-        const double xi = Y[i] / double(Tj[(size_t)i * n2 + i]);
+  for_entries<BATCH>(ecnt, [&](long entry) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    SweepArgs<T> ab;  // this CTA's system (batch only)
+    long q0, q1, qs;
+    pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs, entry);
+    const SweepArgs<T>& a = BATCH ? ab : a0;
+    const Dims d = a.d;
+    const int n = d.n, nx = d.nx, n2 = 2 * n, nrhs = a.nrhs, k = a.k, nb = d.nblock;
+    double* Y = reinterpret_cast<double*>(smem_raw) + (size_t)warp * a.ldw;
+    const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
+    for (long q = q0; q < q1; q += qs) {
+      const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
+      const T* Dj = a.D + (size_t)j * n * n;
+      const T* Ej = a.E + (size_t)j * n * n;
+      const T* Bj = a.B + (size_t)j * n * nx;
+      const T* Tj = a.Tm + (size_t)j * szT(d);
+      for (int c = 0; c < nrhs; ++c) {
+        double* xc = a.x + (size_t)c * a.ldx;
+        for (int i = lane; i < n; i += 32) {
+          double s = xc[(size_t)j * n + i];
+          for (int m = 0; m < n; ++m) s -= Dj[(size_t)m * n + i] * xc[(size_t)jp * n + m];
+          for (int m = 0; m < n; ++m) s -= Ej[(size_t)m * n + i] * xc[(size_t)jpp * n + m];
+          for (int m = 0; m < nx; ++m) s -= Bj[(size_t)m * n + i] * xc[xb_off + m];
+          Y[i] = s;
+        }
         __syncwarp();
-        if (lane == 0) Y[i] = xi;
-        for (int r = lane; r < i; r += 32) Y[r] -= Tj[(size_t)i * n2 + r] * xi;
+        for (int i = n - 1; i >= 0; --i) {
+          const double xi = Y[i] / double(Tj[(size_t)i * n2 + i]);
+          __syncwarp();
+          if (lane == 0) Y[i] = xi;
+          for (int r = lane; r < i; r += 32) Y[r] -= Tj[(size_t)i * n2 + r] * xi;
+          __syncwarp();
+        }
+        const unsigned char* cmap = a.P + (size_t)j * szP(d) + 2 * n;
+        for (int i = lane; i < n; i += 32) xc[(size_t)j * n + (a.sel == SEL_QRP ? cmap[i] : i)] = Y[i];
         __syncwarp();
       }
-      const unsigned char* cmap = a.P + (size_t)j * szP(d) + 2 * n;
-      for (int i = lane; i < n; i += 32) xc[(size_t)j * n + (a.sel == SEL_QRP ? cmap[i] : i)] = Y[i];
-      __syncwarp();
     }
-  }
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -2294,133 +2314,137 @@ __global__ void __launch_bounds__(WARPS_PANEL * 32) k_backward_level(SweepArgs<T
 // ---------------------------------------------------------------------------
 template <typename TF, int N, int NRM, bool LU, bool BATCH = false>
 __global__ void __launch_bounds__(256, 2) k_forward_rows(SweepArgs<TF> a0, const SweepArgs<TF>* tab,
-                                                         const BatchCta* cmap) {
-  constexpr unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  SweepArgs<TF> ab;  // this CTA's system (batch only)
-  long q0, q1, qs;
-  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
-  const SweepArgs<TF>& a = BATCH ? ab : a0;
-  const Dims d = a.d;
-  const int n = d.n, nr = d.nr, n2 = 2 * n, nrhs = a.nrhs, k = a.k;
-  const bool act = lane < n2;
-  constexpr bool lu = LU;
-  for (long q = q0; q < q1; q += qs) {
-    const int j = k + (int)(2L * k * q), jp = j - k;
-    const TF* Tj = a.Tm + (size_t)j * szT(d);
-    double t[N];
-#pragma unroll
-    for (int c = 0; c < N; ++c) t[c] = (act && c < n) ? double(Tj[(size_t)c * n2 + lane]) : 0.0;
-    double tau[LU ? 1 : N];
-#pragma unroll
-    for (int c = 0; c < (LU ? 1 : N); ++c) tau[c] = (!lu && c < n) ? Tj[2 * (size_t)n * n + c] : 0.0;
-    const int src = (act && lu) ? (int)a.P[(size_t)j * szP(d) + lane] : lane;
-    double cp[NRM];
-    const TF* Cj = a.C + (size_t)j * nr * n;
-#pragma unroll
-    for (int r = 0; r < NRM; ++r) cp[r] = (lane < n && r < nr) ? Cj[(size_t)lane * nr + r] : 0.0;
-    for (int col = 0; col < nrhs; ++col) {
-      double* xc = a.x + (size_t)col * a.ldx;
-      const double orig = act ? (lane < n ? xc[(size_t)jp * n + lane] : xc[(size_t)j * n + lane - n]) : 0.0;
-      double w = __shfl_sync(FULL, orig, src);
-      if (lu) {
-#pragma unroll
-        for (int i = 0; i < N; ++i) {
-          if (i < n) {
-            const double wi = __shfl_sync(FULL, w, i);
-            if (lane > i && act) w = fma(-t[i], wi, w);
+                                                         const BatchCta* cmap, const long* ecnt) {
+  for_entries<BATCH>(ecnt, [&](long entry) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    SweepArgs<TF> ab;  // this CTA's system (batch only)
+    long q0, q1, qs;
+    pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs, entry);
+    const SweepArgs<TF>& a = BATCH ? ab : a0;
+    const Dims d = a.d;
+    const int n = d.n, nr = d.nr, n2 = 2 * n, nrhs = a.nrhs, k = a.k;
+    const bool act = lane < n2;
+    constexpr bool lu = LU;
+    for (long q = q0; q < q1; q += qs) {
+      const int j = k + (int)(2L * k * q), jp = j - k;
+      const TF* Tj = a.Tm + (size_t)j * szT(d);
+      double t[N];
+  #pragma unroll
+      for (int c = 0; c < N; ++c) t[c] = (act && c < n) ? double(Tj[(size_t)c * n2 + lane]) : 0.0;
+      double tau[LU ? 1 : N];
+  #pragma unroll
+      for (int c = 0; c < (LU ? 1 : N); ++c) tau[c] = (!lu && c < n) ? Tj[2 * (size_t)n * n + c] : 0.0;
+      const int src = (act && lu) ? (int)a.P[(size_t)j * szP(d) + lane] : lane;
+      double cp[NRM];
+      const TF* Cj = a.C + (size_t)j * nr * n;
+  #pragma unroll
+      for (int r = 0; r < NRM; ++r) cp[r] = (lane < n && r < nr) ? Cj[(size_t)lane * nr + r] : 0.0;
+      for (int col = 0; col < nrhs; ++col) {
+        double* xc = a.x + (size_t)col * a.ldx;
+        const double orig = act ? (lane < n ? xc[(size_t)jp * n + lane] : xc[(size_t)j * n + lane - n]) : 0.0;
+        double w = __shfl_sync(FULL, orig, src);
+        if (lu) {
+  #pragma unroll
+          for (int i = 0; i < N; ++i) {
+            if (i < n) {
+              const double wi = __shfl_sync(FULL, w, i);
+              if (lane > i && act) w = fma(-t[i], wi, w);
+            }
+          }
+        } else {
+  #pragma unroll
+          for (int i = 0; i < N; ++i) {
+            if (i < n) {
+              const double v = (lane > i && act) ? t[i] : (lane == i ? 1.0 : 0.0);
+              double sdot = warp_sum(v * w);
+              w = fma(-tau[LU ? 0 : i] * sdot, v, w);
+            }
           }
         }
-      } else {
-#pragma unroll
-        for (int i = 0; i < N; ++i) {
-          if (i < n) {
-            const double v = (lane > i && act) ? t[i] : (lane == i ? 1.0 : 0.0);
-            double sdot = warp_sum(v * w);
-            w = fma(-tau[LU ? 0 : i] * sdot, v, w);
-          }
+        if (act) {
+          if (lane < n) xc[(size_t)j * n + lane] = w;
+          else xc[(size_t)jp * n + lane - n] = w;
         }
-      }
-      if (act) {
-        if (lane < n) xc[(size_t)j * n + lane] = w;
-        else xc[(size_t)jp * n + lane - n] = w;
-      }
-      const double wt = lane < n ? w : 0.0;
-#pragma unroll
-      for (int r = 0; r < NRM; ++r) {
-        if (r < nr) {
-          const double sr = warp_sum(cp[r] * wt);
-          if (lane == 0) a.XB[(size_t)j * nr * nrhs + (size_t)col * nr + r] = -sr;
+        const double wt = lane < n ? w : 0.0;
+  #pragma unroll
+        for (int r = 0; r < NRM; ++r) {
+          if (r < nr) {
+            const double sr = warp_sum(cp[r] * wt);
+            if (lane == 0) a.XB[(size_t)j * nr * nrhs + (size_t)col * nr + r] = -sr;
+          }
         }
       }
     }
-  }
+  });
 }
 
 template <typename TF, int N, int NXM, bool BATCH = false>
 __global__ void __launch_bounds__(256, 2) k_backward_rows(SweepArgs<TF> a0, const SweepArgs<TF>* tab,
-                                                          const BatchCta* cmap) {
-  constexpr unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  SweepArgs<TF> ab;  // this CTA's system (batch only)
-  long q0, q1, qs;
-  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
-  const SweepArgs<TF>& a = BATCH ? ab : a0;
-  const Dims d = a.d;
-  const int n = d.n, nx = d.nx, nb = d.nblock, n2 = 2 * n, nrhs = a.nrhs, k = a.k;
-  const int i = lane & 15;
-  const bool hi = lane >= 16, rowok = i < n;
-  const bool qrp = a.sel == SEL_QRP;
-  const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
-  for (long q = q0; q < q1; q += qs) {
-    const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
-    const TF* Mt = (hi ? a.E : a.D) + (size_t)j * n * n;
-    const TF* Tj = a.Tm + (size_t)j * szT(d);
-    const TF* Bj = a.B + (size_t)j * n * nx;
-    double m[N], u[N], bb[NXM];
-#pragma unroll
-    for (int c = 0; c < N; ++c) m[c] = (rowok && c < n) ? Mt[(size_t)c * n + i] : 0.0;
-#pragma unroll
-    for (int c = 0; c < N; ++c) u[c] = (!hi && rowok && c < n) ? Tj[(size_t)c * n2 + i] : 0.0;
-#pragma unroll
-    for (int c = 0; c < NXM; ++c) bb[c] = (!hi && rowok && c < nx) ? Bj[(size_t)c * n + i] : 0.0;
-    // 1 / U(i,i): pick the diagonal element first, then one division per lane
-    double ud = 1.0;
-#pragma unroll
-    for (int c = 0; c < N; ++c)
-      if (c == i) ud = u[c];
-    const double rdi = (!hi && rowok) ? 1.0 / ud : 0.0;
-    const int dst = (qrp && !hi && rowok) ? (int)a.P[(size_t)j * szP(d) + n2 + i] : i;
-    for (int col = 0; col < nrhs; ++col) {
-      double* xc = a.x + (size_t)col * a.ldx;
-      const double xv = rowok ? (hi ? xc[(size_t)jpp * n + i] : xc[(size_t)jp * n + i]) : 0.0;
-      const double xj = (!hi && rowok) ? xc[(size_t)j * n + i] : 0.0;
-      double xbv[NXM];
-#pragma unroll
-      for (int c = 0; c < NXM; ++c) xbv[c] = c < nx ? xc[xb_off + c] : 0.0;
-      double s = 0.0;
-#pragma unroll
-      for (int c = 0; c < N; ++c) {
-        if (c < n) {
-          const double xcv = __shfl_sync(FULL, xv, (lane & 16) | c);
-          s = fma(m[c], xcv, s);
+                                                          const BatchCta* cmap, const long* ecnt) {
+  for_entries<BATCH>(ecnt, [&](long entry) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    SweepArgs<TF> ab;  // this CTA's system (batch only)
+    long q0, q1, qs;
+    pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs, entry);
+    const SweepArgs<TF>& a = BATCH ? ab : a0;
+    const Dims d = a.d;
+    const int n = d.n, nx = d.nx, nb = d.nblock, n2 = 2 * n, nrhs = a.nrhs, k = a.k;
+    const int i = lane & 15;
+    const bool hi = lane >= 16, rowok = i < n;
+    const bool qrp = a.sel == SEL_QRP;
+    const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
+    for (long q = q0; q < q1; q += qs) {
+      const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
+      const TF* Mt = (hi ? a.E : a.D) + (size_t)j * n * n;
+      const TF* Tj = a.Tm + (size_t)j * szT(d);
+      const TF* Bj = a.B + (size_t)j * n * nx;
+      double m[N], u[N], bb[NXM];
+  #pragma unroll
+      for (int c = 0; c < N; ++c) m[c] = (rowok && c < n) ? Mt[(size_t)c * n + i] : 0.0;
+  #pragma unroll
+      for (int c = 0; c < N; ++c) u[c] = (!hi && rowok && c < n) ? Tj[(size_t)c * n2 + i] : 0.0;
+  #pragma unroll
+      for (int c = 0; c < NXM; ++c) bb[c] = (!hi && rowok && c < nx) ? Bj[(size_t)c * n + i] : 0.0;
+      // 1 / U(i,i): pick the diagonal element first, then one division per lane
+      double ud = 1.0;
+  #pragma unroll
+      for (int c = 0; c < N; ++c)
+        if (c == i) ud = u[c];
+      const double rdi = (!hi && rowok) ? 1.0 / ud : 0.0;
+      const int dst = (qrp && !hi && rowok) ? (int)a.P[(size_t)j * szP(d) + n2 + i] : i;
+      for (int col = 0; col < nrhs; ++col) {
+        double* xc = a.x + (size_t)col * a.ldx;
+        const double xv = rowok ? (hi ? xc[(size_t)jpp * n + i] : xc[(size_t)jp * n + i]) : 0.0;
+        const double xj = (!hi && rowok) ? xc[(size_t)j * n + i] : 0.0;
+        double xbv[NXM];
+  #pragma unroll
+        for (int c = 0; c < NXM; ++c) xbv[c] = c < nx ? xc[xb_off + c] : 0.0;
+        double s = 0.0;
+  #pragma unroll
+        for (int c = 0; c < N; ++c) {
+          if (c < n) {
+            const double xcv = __shfl_sync(FULL, xv, (lane & 16) | c);
+            s = fma(m[c], xcv, s);
+          }
         }
-      }
-      s += __shfl_xor_sync(FULL, s, 16);
-#pragma unroll
-      for (int c = 0; c < NXM; ++c) s = fma(bb[c], xbv[c], s);
-      double y = xj - s;
-#pragma unroll
-      for (int ii = N - 1; ii >= 0; --ii) {
-        if (ii < n) {
-          const double xi = __shfl_sync(FULL, y * rdi, ii);
-          if (i == ii) y = xi;
-          else if (i < ii) y = fma(-u[ii], xi, y);
+        s += __shfl_xor_sync(FULL, s, 16);
+  #pragma unroll
+        for (int c = 0; c < NXM; ++c) s = fma(bb[c], xbv[c], s);
+        double y = xj - s;
+  #pragma unroll
+        for (int ii = N - 1; ii >= 0; --ii) {
+          if (ii < n) {
+            const double xi = __shfl_sync(FULL, y * rdi, ii);
+            if (i == ii) y = xi;
+            else if (i < ii) y = fma(-u[ii], xi, y);
+          }
         }
+        if (!hi && rowok) xc[(size_t)j * n + dst] = y;
       }
-      if (!hi && rowok) xc[(size_t)j * n + dst] = y;
     }
-  }
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -2626,97 +2650,101 @@ __global__ void __launch_bounds__(512, 1) k_backward_top(SweepArgs<double> a, in
 // ---------------------------------------------------------------------------
 template <typename TF, int NRM, bool BATCH = false>
 __global__ void __launch_bounds__(256, 2) k_forward_rows32(SweepArgs<TF> a0, const SweepArgs<TF>* tab,
-                                                           const BatchCta* cmap) {
-  constexpr unsigned FULL = 0xffffffffu;
-  constexpr int n = 32, n2 = 64;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  SweepArgs<TF> ab;  // this CTA's system (batch only)
-  long q0, q1, qs;
-  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
-  const SweepArgs<TF>& a = BATCH ? ab : a0;
-  const Dims d = a.d;
-  const int nr = d.nr, nrhs = a.nrhs, k = a.k;
-  for (long q = q0; q < q1; q += qs) {
-    const int j = k + (int)(2L * k * q), jp = j - k;
-    const TF* Tj = a.Tm + (size_t)j * szT(d);
-    const unsigned char* Pj = a.P + (size_t)j * szP(d);
-    const int s0 = Pj[lane], s1 = Pj[n + lane];  // original rows at positions lane, 32 + lane
-    double cp[NRM];
-    const TF* Cj = a.C + (size_t)j * nr * n;
-#pragma unroll
-    for (int r = 0; r < NRM; ++r) cp[r] = r < nr ? double(Cj[(size_t)lane * nr + r]) : 0.0;
-    for (int col = 0; col < nrhs; ++col) {
-      double* xc = a.x + (size_t)col * a.ldx;
-      const double ot = xc[(size_t)jp * n + lane], ob = xc[(size_t)j * n + lane];
-      const double a0t = __shfl_sync(FULL, ot, s0 & 31), a0b = __shfl_sync(FULL, ob, s0 & 31);
-      const double a1t = __shfl_sync(FULL, ot, s1 & 31), a1b = __shfl_sync(FULL, ob, s1 & 31);
-      double w0 = s0 < n ? a0t : a0b, w1 = s1 < n ? a1t : a1b;
-#pragma unroll
-      for (int i = 0; i < n; ++i) {
-        const double wi = __shfl_sync(FULL, w0, i);
-        const double t0 = double(Tj[(size_t)i * n2 + lane]), t1 = double(Tj[(size_t)i * n2 + n + lane]);
-        if (lane > i) w0 = fma(-t0, wi, w0);
-        w1 = fma(-t1, wi, w1);
-      }
-      xc[(size_t)j * n + lane] = w0;
-      xc[(size_t)jp * n + lane] = w1;
-#pragma unroll
-      for (int r = 0; r < NRM; ++r) {
-        if (r < nr) {
-          const double sr = warp_sum(cp[r] * w0);
-          if (lane == 0) a.XB[(size_t)j * nr * nrhs + (size_t)col * nr + r] = -sr;
+                                                           const BatchCta* cmap, const long* ecnt) {
+  for_entries<BATCH>(ecnt, [&](long entry) {
+    constexpr unsigned FULL = 0xffffffffu;
+    constexpr int n = 32, n2 = 64;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    SweepArgs<TF> ab;  // this CTA's system (batch only)
+    long q0, q1, qs;
+    pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs, entry);
+    const SweepArgs<TF>& a = BATCH ? ab : a0;
+    const Dims d = a.d;
+    const int nr = d.nr, nrhs = a.nrhs, k = a.k;
+    for (long q = q0; q < q1; q += qs) {
+      const int j = k + (int)(2L * k * q), jp = j - k;
+      const TF* Tj = a.Tm + (size_t)j * szT(d);
+      const unsigned char* Pj = a.P + (size_t)j * szP(d);
+      const int s0 = Pj[lane], s1 = Pj[n + lane];  // original rows at positions lane, 32 + lane
+      double cp[NRM];
+      const TF* Cj = a.C + (size_t)j * nr * n;
+  #pragma unroll
+      for (int r = 0; r < NRM; ++r) cp[r] = r < nr ? double(Cj[(size_t)lane * nr + r]) : 0.0;
+      for (int col = 0; col < nrhs; ++col) {
+        double* xc = a.x + (size_t)col * a.ldx;
+        const double ot = xc[(size_t)jp * n + lane], ob = xc[(size_t)j * n + lane];
+        const double a0t = __shfl_sync(FULL, ot, s0 & 31), a0b = __shfl_sync(FULL, ob, s0 & 31);
+        const double a1t = __shfl_sync(FULL, ot, s1 & 31), a1b = __shfl_sync(FULL, ob, s1 & 31);
+        double w0 = s0 < n ? a0t : a0b, w1 = s1 < n ? a1t : a1b;
+  #pragma unroll
+        for (int i = 0; i < n; ++i) {
+          const double wi = __shfl_sync(FULL, w0, i);
+          const double t0 = double(Tj[(size_t)i * n2 + lane]), t1 = double(Tj[(size_t)i * n2 + n + lane]);
+          if (lane > i) w0 = fma(-t0, wi, w0);
+          w1 = fma(-t1, wi, w1);
+        }
+        xc[(size_t)j * n + lane] = w0;
+        xc[(size_t)jp * n + lane] = w1;
+  #pragma unroll
+        for (int r = 0; r < NRM; ++r) {
+          if (r < nr) {
+            const double sr = warp_sum(cp[r] * w0);
+            if (lane == 0) a.XB[(size_t)j * nr * nrhs + (size_t)col * nr + r] = -sr;
+          }
         }
       }
     }
-  }
+  });
 }
 
 template <typename TF, int NXM, bool BATCH = false>
 __global__ void __launch_bounds__(256, 2) k_backward_rows32(SweepArgs<TF> a0, const SweepArgs<TF>* tab,
-                                                            const BatchCta* cmap) {
-  constexpr unsigned FULL = 0xffffffffu;
-  constexpr int n = 32, n2 = 64;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  SweepArgs<TF> ab;  // this CTA's system (batch only)
-  long q0, q1, qs;
-  pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
-  const SweepArgs<TF>& a = BATCH ? ab : a0;
-  const Dims d = a.d;
-  const int nx = d.nx, nb = d.nblock, nrhs = a.nrhs, k = a.k;
-  const bool qrp = a.sel == SEL_QRP;
-  const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
-  constexpr size_t nn = (size_t)n * n;
-  for (long q = q0; q < q1; q += qs) {
-    const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
-    const TF* Dj = a.D + (size_t)j * nn;
-    const TF* Ej = a.E + (size_t)j * nn;
-    const TF* Bj = a.B + (size_t)j * n * nx;
-    const TF* Tj = a.Tm + (size_t)j * szT(d);
-    const double rdi = 1.0 / double(Tj[(size_t)lane * n2 + lane]);
-    const int dst = qrp ? (int)a.P[(size_t)j * szP(d) + n2 + lane] : lane;
-    for (int col = 0; col < nrhs; ++col) {
-      double* xc = a.x + (size_t)col * a.ldx;
-      const double xjp = xc[(size_t)jp * n + lane], xjpp = xc[(size_t)jpp * n + lane];
-      const double xj = xc[(size_t)j * n + lane];
-      double s0 = 0.0, s1 = 0.0;
-#pragma unroll
-      for (int c = 0; c < n; ++c) {
-        s0 = fma(double(Dj[(size_t)c * n + lane]), __shfl_sync(FULL, xjp, c), s0);
-        s1 = fma(double(Ej[(size_t)c * n + lane]), __shfl_sync(FULL, xjpp, c), s1);
+                                                            const BatchCta* cmap, const long* ecnt) {
+  for_entries<BATCH>(ecnt, [&](long entry) {
+    constexpr unsigned FULL = 0xffffffffu;
+    constexpr int n = 32, n2 = 64;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    SweepArgs<TF> ab;  // this CTA's system (batch only)
+    long q0, q1, qs;
+    pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs, entry);
+    const SweepArgs<TF>& a = BATCH ? ab : a0;
+    const Dims d = a.d;
+    const int nx = d.nx, nb = d.nblock, nrhs = a.nrhs, k = a.k;
+    const bool qrp = a.sel == SEL_QRP;
+    const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
+    constexpr size_t nn = (size_t)n * n;
+    for (long q = q0; q < q1; q += qs) {
+      const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
+      const TF* Dj = a.D + (size_t)j * nn;
+      const TF* Ej = a.E + (size_t)j * nn;
+      const TF* Bj = a.B + (size_t)j * n * nx;
+      const TF* Tj = a.Tm + (size_t)j * szT(d);
+      const double rdi = 1.0 / double(Tj[(size_t)lane * n2 + lane]);
+      const int dst = qrp ? (int)a.P[(size_t)j * szP(d) + n2 + lane] : lane;
+      for (int col = 0; col < nrhs; ++col) {
+        double* xc = a.x + (size_t)col * a.ldx;
+        const double xjp = xc[(size_t)jp * n + lane], xjpp = xc[(size_t)jpp * n + lane];
+        const double xj = xc[(size_t)j * n + lane];
+        double s0 = 0.0, s1 = 0.0;
+  #pragma unroll
+        for (int c = 0; c < n; ++c) {
+          s0 = fma(double(Dj[(size_t)c * n + lane]), __shfl_sync(FULL, xjp, c), s0);
+          s1 = fma(double(Ej[(size_t)c * n + lane]), __shfl_sync(FULL, xjpp, c), s1);
+        }
+  #pragma unroll
+        for (int c = 0; c < NXM; ++c)
+          if (c < nx) s0 = fma(double(Bj[(size_t)c * n + lane]), xc[xb_off + c], s0);
+        double y = xj - (s0 + s1);
+  #pragma unroll
+        for (int ii = n - 1; ii >= 0; --ii) {
+          const double xi = __shfl_sync(FULL, y * rdi, ii);
+          if (lane == ii) y = xi;
+          else if (lane < ii) y = fma(-double(Tj[(size_t)ii * n2 + lane]), xi, y);
+        }
+        xc[(size_t)j * n + dst] = y;
       }
-#pragma unroll
-      for (int c = 0; c < NXM; ++c)
-        if (c < nx) s0 = fma(double(Bj[(size_t)c * n + lane]), xc[xb_off + c], s0);
-      double y = xj - (s0 + s1);
-#pragma unroll
-      for (int ii = n - 1; ii >= 0; --ii) {
-        const double xi = __shfl_sync(FULL, y * rdi, ii);
-        if (lane == ii) y = xi;
-        else if (lane < ii) y = fma(-double(Tj[(size_t)ii * n2 + lane]), xi, y);
-      }
-      xc[(size_t)j * n + dst] = y;
     }
-  }
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -4028,8 +4056,8 @@ void launch_factorize(DevState& s, cudaStream_t st) {
 // sweep kernels for one chunk of right-hand sides
 template <typename T>
 struct SweepPlan {
-  void (*fwd)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*) = nullptr;
-  void (*bwd)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*) = nullptr;
+  void (*fwd)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*, const long*) = nullptr;
+  void (*bwd)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*, const long*) = nullptr;
   // FP64 n = 8, 16 single systems: pipelined backward levels, the top in one CTA
   void (*bwd_pipe)(SweepArgs<double>) = nullptr;
   size_t bwd_pipe_smem = 0;
@@ -4116,8 +4144,8 @@ static void forward_levels(DevState& s, const SweepPlan<T>& p, const WorkSet<T>&
     a.k = K;
     const long np = pairs_at_level(d.nblock, K);
     if (p.fwd_cta) p.fwd_cta<<<grid_for(np, 1, 148 * 8), 256, 0, st>>>(a, nullptr, nullptr);
-    else if (p.fwd) p.fwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a, nullptr, nullptr);
-    else k_forward_level<T><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_f, st>>>(a, nullptr, nullptr);
+    else if (p.fwd) p.fwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a, nullptr, nullptr, nullptr);
+    else k_forward_level<T><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_f, st>>>(a, nullptr, nullptr, nullptr);
     check_launch("k_forward_level");
   }
   reduce_xb(s, x, ldx, nrhs, st);
@@ -4157,8 +4185,8 @@ static void last_and_backward(DevState& s, const SweepPlan<T>& p, const WorkSet<
     a.k = k;
     const long np = pairs_at_level(d.nblock, k);
     if (p.bwd_cta) p.bwd_cta<<<grid_for(np, 1, 148 * 8), 256, 0, st>>>(a, nullptr, nullptr);
-    else if (p.bwd) p.bwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a, nullptr, nullptr);
-    else k_backward_level<T><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_b, st>>>(a, nullptr, nullptr);
+    else if (p.bwd) p.bwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a, nullptr, nullptr, nullptr);
+    else k_backward_level<T><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_b, st>>>(a, nullptr, nullptr, nullptr);
     check_launch("k_backward_level");
   }
 }
@@ -4901,6 +4929,8 @@ void batch_free(BatchClass& c) {
     if (*p) { cudaFree(*p); *p = nullptr; }
   if (c.fmap) { cudaFree(c.fmap); c.fmap = nullptr; }
   if (c.smap) { cudaFree(c.smap); c.smap = nullptr; }
+  if (c.cmap) { cudaFree(c.cmap); c.cmap = nullptr; }
+  if (c.ccnt) { cudaFree(c.ccnt); c.ccnt = nullptr; }
   c.foff.clear(); c.fcnt.clear(); c.soff.clear(); c.scnt.clear();
 }
 
@@ -4973,6 +5003,10 @@ static int batch_build_t(BatchClass& c, const std::vector<DevState>& sys, int nr
   c.smap = static_cast<BatchCta*>(m2);
   c.items = (long)fmap.size();
   if (cudaMalloc(&c.qbuf, (1 + 2 * (size_t)c.nsys) * sizeof(int)) != cudaSuccess) bad = 1;
+  if (c.mixed && c.levels > 0) {  // compacted maps of the refinement passes
+    if (cudaMalloc(&c.cmap, std::max<size_t>(smap.size(), 1) * sizeof(BatchCta)) != cudaSuccess) bad = 1;
+    if (cudaMalloc(&c.ccnt, (size_t)c.levels * sizeof(long)) != cudaSuccess) bad = 1;
+  }
   return bad;
 }
 
@@ -5090,75 +5124,130 @@ void batch_factorize(BatchClass& c, cudaStream_t st) {
   else batch_factorize_t<double>(c, st);
 }
 
+// the sweep map of level L: the full map (one CTA per entry), or on the
+// refinement passes the compacted map of the systems still refining, walked by
+// a fixed grid (the launch is captured before the length is known)
+struct SweepMap {
+  const BatchCta* map;
+  const long* ecnt;
+  unsigned grid;
+};
+
+static SweepMap sweep_map(const BatchClass& c, int L, bool compact) {
+  if (!compact) return {c.smap + c.soff[L], nullptr, (unsigned)c.scnt[L]};
+  return {c.cmap + c.soff[L], c.ccnt + L, (unsigned)std::min<long>(c.scnt[L], COMPACT_GRID)};
+}
+
 template <typename T, int N>
-static void batch_sweeps_rows(BatchClass& c, cudaStream_t st, bool forward, int L) {
+static void batch_sweeps_rows(BatchClass& c, cudaStream_t st, bool forward, int L, const SweepMap& m) {
   const bool r4 = c.nrm <= 4, x4 = c.nxm <= 4;
-  const BatchCta* map = c.smap + c.soff[L];
-  const unsigned g = (unsigned)c.scnt[L];
   SweepArgs<T> a0{};
   a0.k = 1 << L;
   if (forward) {
     const SweepArgs<T>* tab = static_cast<const SweepArgs<T>*>(c.sf);
-    if (r4) k_forward_rows<T, N, 4, true, true><<<g, 256, 0, st>>>(a0, tab, map);
-    else k_forward_rows<T, N, 8, true, true><<<g, 256, 0, st>>>(a0, tab, map);
+    if (r4) k_forward_rows<T, N, 4, true, true><<<m.grid, 256, 0, st>>>(a0, tab, m.map, m.ecnt);
+    else k_forward_rows<T, N, 8, true, true><<<m.grid, 256, 0, st>>>(a0, tab, m.map, m.ecnt);
   } else {
     const SweepArgs<T>* tab = static_cast<const SweepArgs<T>*>(c.sb);
-    if (x4) k_backward_rows<T, N, 4, true><<<g, 256, 0, st>>>(a0, tab, map);
-    else k_backward_rows<T, N, 8, true><<<g, 256, 0, st>>>(a0, tab, map);
+    if (x4) k_backward_rows<T, N, 4, true><<<m.grid, 256, 0, st>>>(a0, tab, m.map, m.ecnt);
+    else k_backward_rows<T, N, 8, true><<<m.grid, 256, 0, st>>>(a0, tab, m.map, m.ecnt);
   }
 }
 
 template <typename T>
-static void batch_sweep_level(BatchClass& c, cudaStream_t st, bool forward, int L) {
+static void batch_sweep_level(BatchClass& c, cudaStream_t st, bool forward, int L, bool compact) {
   if (c.scnt[L] == 0) return;
-  if (c.n <= 4) batch_sweeps_rows<T, 4>(c, st, forward, L);
-  else if (c.n <= 8) batch_sweeps_rows<T, 8>(c, st, forward, L);
-  else if (c.n <= 16) batch_sweeps_rows<T, 16>(c, st, forward, L);
+  const SweepMap m = sweep_map(c, L, compact);
+  if (c.n <= 4) batch_sweeps_rows<T, 4>(c, st, forward, L, m);
+  else if (c.n <= 8) batch_sweeps_rows<T, 8>(c, st, forward, L, m);
+  else if (c.n <= 16) batch_sweeps_rows<T, 16>(c, st, forward, L, m);
   else if (c.n == 32) {
-    const BatchCta* map = c.smap + c.soff[L];
-    const unsigned g = (unsigned)c.scnt[L];
     SweepArgs<T> a0{};
     a0.k = 1 << L;
     if (forward) {
       const SweepArgs<T>* tab = static_cast<const SweepArgs<T>*>(c.sf);
-      if (c.nrm <= 4) k_forward_rows32<T, 4, true><<<g, 256, 0, st>>>(a0, tab, map);
-      else k_forward_rows32<T, 8, true><<<g, 256, 0, st>>>(a0, tab, map);
+      if (c.nrm <= 4) k_forward_rows32<T, 4, true><<<m.grid, 256, 0, st>>>(a0, tab, m.map, m.ecnt);
+      else k_forward_rows32<T, 8, true><<<m.grid, 256, 0, st>>>(a0, tab, m.map, m.ecnt);
     } else {
       const SweepArgs<T>* tab = static_cast<const SweepArgs<T>*>(c.sb);
-      if (c.nxm <= 4) k_backward_rows32<T, 4, true><<<g, 256, 0, st>>>(a0, tab, map);
-      else k_backward_rows32<T, 8, true><<<g, 256, 0, st>>>(a0, tab, map);
+      if (c.nxm <= 4) k_backward_rows32<T, 4, true><<<m.grid, 256, 0, st>>>(a0, tab, m.map, m.ecnt);
+      else k_backward_rows32<T, 8, true><<<m.grid, 256, 0, st>>>(a0, tab, m.map, m.ecnt);
     }
   } else {
-    const BatchCta* map = c.smap + c.soff[L];
-    const unsigned g = (unsigned)c.scnt[L];
     SweepArgs<T> a0{};
     a0.k = 1 << L;
     if (forward) {
       const size_t sm = (size_t)odd_ld(2 * c.n) * c.nrhs * 8 * WARPS_PANEL;
       smem_limit_once(k_forward_level<T, true>, sm);
-      k_forward_level<T, true><<<g, WARPS_PANEL * 32, sm, st>>>(a0, static_cast<const SweepArgs<T>*>(c.sf), map);
+      k_forward_level<T, true><<<m.grid, WARPS_PANEL * 32, sm, st>>>(a0, static_cast<const SweepArgs<T>*>(c.sf),
+                                                                     m.map, m.ecnt);
     } else {
       const size_t sm = (size_t)c.n * 8 * WARPS_PANEL;
-      k_backward_level<T, true><<<g, WARPS_PANEL * 32, sm, st>>>(a0, static_cast<const SweepArgs<T>*>(c.sb), map);
+      k_backward_level<T, true><<<m.grid, WARPS_PANEL * 32, sm, st>>>(a0, static_cast<const SweepArgs<T>*>(c.sb),
+                                                                      m.map, m.ecnt);
     }
   }
   check_launch(forward ? "batched forward sweep" : "batched backward sweep");
 }
 
 template <typename T>
-static void batch_solve_t(BatchClass& c, cudaStream_t st) {
+static void batch_solve_t(BatchClass& c, cudaStream_t st, bool compact) {
   const LastDesc* ld = static_cast<const LastDesc*>(c.ld);
-  for (int L = 0; L < c.levels; ++L) batch_sweep_level<T>(c, st, true, L);
+  for (int L = 0; L < c.levels; ++L) batch_sweep_level<T>(c, st, true, L, compact);
   kb_reduce_xb<<<c.nsys, 256, 0, st>>>(ld, c.nrhs);
   kb_last_solve<<<c.nsys, 256, c.last_smem, st>>>(ld, c.nrhs);
-  for (int L = c.levels - 1; L >= 0; --L) batch_sweep_level<T>(c, st, false, L);
+  for (int L = c.levels - 1; L >= 0; --L) batch_sweep_level<T>(c, st, false, L, compact);
   check_launch("batched solve");
 }
 
-void batch_solve(BatchClass& c, cudaStream_t st) {
+void batch_solve(BatchClass& c, cudaStream_t st, bool compact) {
   if (c.nsys == 0) return;
-  if (c.mixed) batch_solve_t<float>(c, st);
-  else batch_solve_t<double>(c, st);
+  compact = compact && c.cmap != nullptr;
+  if (c.mixed) batch_solve_t<float>(c, st, compact);
+  else batch_solve_t<double>(c, st, compact);
+}
+
+// Compacted sweep maps of the systems still refining: entry e of the full map
+// is kept when its system has not converged, at a free position of its level
+// (one atomic per warp and level; the pairs of a level are independent, so
+// the order within a level does not change any result)
+struct LevelOffsets {
+  long off[32];
+};
+
+__global__ void __launch_bounds__(256) kb_compact_map(const LastDesc* ld, const BatchCta* smap, long nent,
+                                                      LevelOffsets lo, BatchCta* cmap, long* ccnt) {
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  BatchCta c{};
+  bool keep = false;
+  if (e < nent) {
+    c = smap[e];
+    const int* dn = ld[c.sys].done;
+    keep = !(dn && *dn);
+  }
+  const unsigned act = __ballot_sync(0xffffffffu, keep);
+  if (!keep) return;
+  const int L = c.pad;  // the entry's level
+  const unsigned grp = __match_any_sync(act, L);
+  const int leader = __ffs(grp) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(reinterpret_cast<unsigned long long*>(ccnt + L), (unsigned long long)__popc(grp));
+  base = __shfl_sync(grp, base, leader);
+  const long pos = (long)base + __popc(grp & ((1u << lane) - 1u));
+  cmap[lo.off[L] + pos] = c;
+}
+
+void batch_compact(BatchClass& c, cudaStream_t st) {
+  if (c.nsys == 0 || !c.cmap || c.levels == 0) return;
+  const long nent = c.soff[c.levels - 1] + c.scnt[c.levels - 1];
+  LevelOffsets lo{};
+  for (int L = 0; L < c.levels; ++L) lo.off[L] = c.soff[L];
+  cudaMemsetAsync(c.ccnt, 0, sizeof(long) * c.levels, st);
+  if (nent > 0)
+    kb_compact_map<<<(unsigned)((nent + 255) / 256), 256, 0, st>>>(static_cast<const LastDesc*>(c.ld), c.smap, nent,
+                                                                    lo, c.cmap, c.ccnt);
+  check_launch("kb_compact_map");
 }
 
 }  // namespace bcr

@@ -265,3 +265,45 @@ def test_batch_persistent_schedule_matches_level_launches(precision):
         assert np.array_equal(x1, x2)
     if precision == B.PRECISION_FP64:
         check_against_oracle(systems, rhs, out[0])
+
+
+def test_batch_mixed_correction_passes_cover_the_unconverged_systems():
+    """Correction solves after the first walk compacted sweep maps of the
+    systems still refining.  A batch whose systems converge after different
+    numbers of corrections (two systems of the 4096-system workload, nblock
+    3787 and n=16, generated on the device as the benchmark does, beside
+    small ones) gives every system the same refined solution, bit for bit, as
+    a batch holding that system alone, and every system meets the mixed bar."""
+    torch = pytest.importorskip("torch")
+    slow = [(3320, (3787, 16, 0, 0, 4, 4)), (3755, (3787, 16, 0, 0, 2, 2))]
+    systems = []
+    for seed, d in slow:
+        ts = synth.collocation_torch(torch, *d, seed=seed)
+        arr = [t.cpu().numpy() for t in ts]
+        systems.append(synth.BABD(*d, D=arr[0], E=arr[1], B=arr[2], C=arr[3], Cq=arr[4], F=arr[5], H=arr[6]))
+    dims = [(50, 8, 0, 0, 2, 2), (300, 4, 0, 0, 0, 0), (120, 16, 0, 0, 4, 4), (700, 32, 0, 0, 2, 2),
+            (1, 8, 0, 0, 2, 2), (900, 16, 0, 0, 2, 2)]
+    systems += [synth.collocation(*d, seed=500 + i) for i, d in enumerate(dims)]
+    rhs = [synth.rhs(s, 1, seed=600 + i)[0] for i, s in enumerate(systems)]
+
+    def run(idx):
+        bt = B.Batch(handles_for([systems[i] for i in idx]))
+        bt.set_precision(B.PRECISION_MIXED)
+        bt.set_refinement(1e-12, 30)
+        bt.prepare()
+        xs = [rhs[i].copy() for i in idx]
+        assert bt.factorize_solve(xs), bt.last_error()
+        return xs, bt.refinement_info()
+
+    xs, (it, worst) = run(range(len(systems)))
+    assert worst <= 1e-12, (it, worst)
+    its = []
+    for i in range(len(systems)):
+        xi, (iti, wi) = run([i])
+        its.append(iti)
+        assert wi <= 1e-12, (i, iti, wi)
+        assert np.array_equal(xi[0], xs[i]), i
+    print("corrections per system", its)
+    assert it == max(its) >= 2 and min(its) < it, (it, its)
+    for i, rr in enumerate(relres_each(systems, rhs, xs)):
+        assert rr <= 1e-12, (i, rr)
