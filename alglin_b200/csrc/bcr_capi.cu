@@ -1294,6 +1294,10 @@ int bcr_synchronize(bcr_handle h) {
 // level of every system of a group in one launch.
 namespace {
 
+// per-system norm slots of the mixed batch (see kb_residual): |A|, |r|, |x|,
+// |b|, the relative residual, two block-row maxima, one spare
+constexpr int NRM_SLOTS = 8;
+
 struct BatchTune {
   int n, nrm, nxm, mixed, fam, chunk;
 };
@@ -1347,7 +1351,7 @@ struct bcr_batch_s {
   double ir_worst = 0.0;
   bool ir_pending = false;
   double* d_sol = nullptr;             // refined solutions, same packing as d_x
-  double* d_nrm = nullptr;             // 5 per system: |A|, |r|, |x|, |b|, relative residual
+  double* d_nrm = nullptr;             // NRM_SLOTS per system: |A|, |r|, |x|, |b|, relative residual, block-row maxima
   int* d_done = nullptr;               // per system: refinement converged
   unsigned long long* d_worst = nullptr;
   cudaStream_t stream = nullptr;
@@ -1454,12 +1458,14 @@ struct bcr_batch_s {
   // the refined solutions end in the rhs region
   int solve_mixed(int fixed, bool with_A) {
     cudaMemsetAsync(d_done, 0, hs.size() * sizeof(int), stream);  // every system solves x0
+    cudaMemsetAsync(d_nrm, 0, hs.size() * NRM_SLOTS * sizeof(double), stream);
     enqueue_solve();
     cudaMemcpyAsync(d_sol, d_x, x_elems * 8, cudaMemcpyDeviceToDevice, stream);
     int it = 0;
     for (;;) {
       cudaMemsetAsync(d_worst, 0, 8, stream);
-      for (auto& c : cls) bcr::batch_residual(c, with_A && it == 0 ? 1 : 0, ir_tol, d_worst, stream);
+      // after the first, the residual covers the systems just corrected
+      for (auto& c : cls) bcr::batch_residual(c, with_A && it == 0 ? 1 : 0, ir_tol, d_worst, stream, it > 0);
       ir_pending = true;
       if (fixed < 0) {
         int rc = read_worst();
@@ -1580,7 +1586,7 @@ int bcr_batch_s::prepare(int autotune) {
   if (e == cudaSuccess) e = cudaMalloc(&d_b, std::max<size_t>(x_elems, 1) * 8);
   if (e == cudaSuccess) e = cudaMalloc(&d_st, ns * sizeof(bcr::StatusWords));
   if (e == cudaSuccess && mixed()) e = cudaMalloc(&d_sol, std::max<size_t>(x_elems, 1) * 8);
-  if (e == cudaSuccess && mixed()) e = cudaMalloc(&d_nrm, ns * 5 * sizeof(double));
+  if (e == cudaSuccess && mixed()) e = cudaMalloc(&d_nrm, ns * NRM_SLOTS * sizeof(double));
   if (e == cudaSuccess && mixed()) e = cudaMalloc(&d_done, ns * sizeof(int));
   if (e == cudaSuccess && mixed()) e = cudaMalloc(&d_worst, 8);
   if (e == cudaSuccess && any_handle) e = cudaMallocHost(&h_in, in_bytes);
@@ -1611,7 +1617,7 @@ int bcr_batch_s::prepare(int autotune) {
       s.Df = F(o.D); s.Ef = F(o.E); s.Bf = F(o.B); s.Cf = F(o.C); s.Tf = F(o.T); s.Rbuff = F(o.Rbuf);
       s.bsol = d_sol + x_off[i];
       s.bb = d_b + x_off[i];
-      s.bnrm = d_nrm + 5 * i;
+      s.bnrm = d_nrm + NRM_SLOTS * i;
       s.bdone = d_done + i;
     } else {
       s.D = W(o.D); s.E = W(o.E); s.B = W(o.B); s.C = W(o.C); s.T = W(o.T);

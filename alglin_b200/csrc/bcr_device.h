@@ -19,7 +19,7 @@ struct DevState {
   int bldx;         // batch: its leading dimension
   double* bsol;     // batch, mixed path: the refined solution
   const double* bb; // batch, mixed path: the right-hand side
-  double* bnrm;     // batch, mixed path: |A|, |r|, |x|, |b|, relative residual
+  double* bnrm;     // batch, mixed path: |A|, |r|, |x|, |b|, relative residual, then two block-row maxima
   int* bdone;       // batch, mixed path: refinement converged (null otherwise)
   // loaded matrix (reference layout), never modified on the device
   double *D0, *E0, *B0, *C0, *Cq, *F0, *H;
@@ -131,7 +131,10 @@ void batch_compact(BatchClass& c, cudaStream_t st);
 // mixed path: r = b - A x_sol into the rhs slots, per-system norms and
 // converged flags (relative residual <= tol), batch-worst relative residual
 // (|A| is measured when with_A)
-void batch_residual(BatchClass& c, int with_A, double tol, unsigned long long* worst, cudaStream_t st);
+// (compact: the block rows of the systems in the compacted maps only, i.e. the
+// systems corrected since the last residual)
+void batch_residual(BatchClass& c, int with_A, double tol, unsigned long long* worst, cudaStream_t st,
+                    bool compact = false);
 // x_sol += d for the systems that have not converged
 void batch_correct(BatchClass& c, cudaStream_t st);
 

@@ -4759,23 +4759,25 @@ __device__ double block_max(double v, double* sv) {
   return sv[0];
 }
 
-__global__ void __launch_bounds__(256) kb_residual(const ResDesc* t, int with_A, double tol,
-                                                   unsigned long long* worst) {
-  __shared__ double sv[32];
-  const ResDesc& R = t[blockIdx.x];
-  if (*R.done) {  // converged earlier: its last figure still counts for the batch
-    if (threadIdx.x == 0) atomicMax(worst, (unsigned long long)__double_as_longlong(R.nrm[4]));
-    return;
-  }
+// a batch map with its launch shape: one CTA per entry, or a fixed grid over
+// a compacted map whose length (ecnt) the device wrote
+struct SweepMap {
+  const BatchCta* map;
+  const long* ecnt;
+  unsigned grid;
+};
+
+// r = b - (D_k x_k + E_k x_{k+1} + B_k xb) on block rows [k0, k1) of one
+// system, written into the rhs slot; the largest |r| and (with_A) the largest
+// row sum of |A| over this thread's rows
+__device__ __forceinline__ void res_block_rows(const ResDesc& R, long k0, long k1, int with_A, double& mr,
+                                               double& ma) {
   const Dims d = R.d;
-  const int n = d.n, nb = d.nblock, nr = d.nr, nx = d.nx, qx = d.qx, m = n + d.qr, Nc = d.Nc;
-  const int tid = threadIdx.x, bs = blockDim.x;
-  const size_t nn = (size_t)n * n, nnx = (size_t)n * nx, nrn = (size_t)nr * n;
-  const size_t xN = (size_t)nb * n, xq = (size_t)(nb + 1) * n, xb = xq + qx;
+  const int n = d.n, nx = d.nx;
+  const size_t nn = (size_t)n * n, nnx = (size_t)n * nx;
+  const size_t xb = (size_t)(d.nblock + 1) * n + d.qx;
   const double* xs = R.xs;
-  double mr = 0.0, ma = 0.0;
-  // block rows
-  for (long e = tid; e < (long)nb * n; e += bs) {
+  for (long e = k0 * n + threadIdx.x; e < k1 * n; e += blockDim.x) {
     const size_t k = (size_t)(e / n);
     const int i = (int)(e % n);
     const double* Dk = R.D0 + k * nn;
@@ -4796,6 +4798,60 @@ __global__ void __launch_bounds__(256) kb_residual(const ResDesc* t, int with_A,
     mr = fmax(mr, fabs(r));
     ma = fmax(ma, sa);
   }
+}
+
+// non-negative doubles order like their bit patterns
+__device__ __forceinline__ void atomic_max_nonneg(double* p, double v) {
+  atomicMax(reinterpret_cast<unsigned long long*>(p), (unsigned long long)__double_as_longlong(v));
+}
+
+// Block rows covered by the level-1 pairs [q0, q1) of each map entry
+// (rows 2 q0 .. 2 q1 - 1), spread over many CTAs: the full sweep map on the
+// first residual of a solve, the compacted map of the systems just corrected
+// afterwards (ecnt: its length).  The largest |r| and |A| row sum of each
+// entry go to nrm[5], nrm[6] of its system.
+__global__ void __launch_bounds__(128) kb_residual_rows(const ResDesc* t, const BatchCta* map, const long* ecnt,
+                                                        int with_A) {
+  __shared__ double sv[32];
+  const long cnt = ecnt ? *ecnt : (long)gridDim.x;
+  for (long e = blockIdx.x; e < cnt; e += gridDim.x) {
+    const BatchCta c = map[e];
+    const ResDesc& R = t[c.sys];
+    if (*R.done) continue;  // uniform over the CTA
+    double mr = 0.0, ma = 0.0;
+    res_block_rows(R, 2 * c.q0, 2 * c.q1, with_A, mr, ma);
+    mr = block_max(mr, sv);
+    ma = block_max(ma, sv);
+    if (threadIdx.x == 0) {
+      atomic_max_nonneg(R.nrm + 5, mr);
+      if (with_A) atomic_max_nonneg(R.nrm + 6, ma);
+    }
+  }
+}
+
+// The rest of the residual, one CTA per system still refining: block rows
+// from 2 * (level-1 pairs) on (the odd tail; every row when nblock = 1), the
+// boundary rows (H), the border rows (a CTA-wide sum over every block
+// column), |x| and |b|; then the norms with kb_residual_rows' maxima,
+// |r|/(|A||x|+|b|), the converged flag and the batch-worst figure (bits of a
+// non-negative double, so an integer max orders them).  Bit for bit the
+// residual of add_Mv (cc:2118-2166) on the loaded FP64 matrix.
+__global__ void __launch_bounds__(256) kb_residual(const ResDesc* t, int with_A, double tol,
+                                                   unsigned long long* worst) {
+  __shared__ double sv[32];
+  const ResDesc& R = t[blockIdx.x];
+  if (*R.done) {  // converged earlier: its last figure still counts for the batch
+    if (threadIdx.x == 0) atomicMax(worst, (unsigned long long)__double_as_longlong(R.nrm[4]));
+    return;
+  }
+  const Dims d = R.d;
+  const int n = d.n, nb = d.nblock, nr = d.nr, nx = d.nx, qx = d.qx, m = n + d.qr, Nc = d.Nc;
+  const int tid = threadIdx.x, bs = blockDim.x;
+  const size_t nrn = (size_t)nr * n;
+  const size_t xN = (size_t)nb * n, xq = (size_t)(nb + 1) * n, xb = xq + qx;
+  const double* xs = R.xs;
+  double mr = 0.0, ma = 0.0;
+  res_block_rows(R, 2 * pairs_at_level(nb, 1), nb, with_A, mr, ma);
   // boundary rows (H)
   for (int row = tid; row < m; row += bs) {
     double s = 0.0, sa = 0.0;
@@ -4843,7 +4899,10 @@ __global__ void __launch_bounds__(256) kb_residual(const ResDesc* t, int with_A,
   mb = block_max(mb, sv);
   if (with_A) ma = block_max(ma, sv);
   if (tid == 0) {
-    if (with_A) R.nrm[0] = ma;
+    mr = fmax(mr, R.nrm[5]);  // the block rows of kb_residual_rows
+    if (with_A) R.nrm[0] = fmax(ma, R.nrm[6]);
+    R.nrm[5] = 0.0;           // ready for the next residual
+    R.nrm[6] = 0.0;
     R.nrm[1] = mr;
     R.nrm[2] = mx;
     R.nrm[3] = mb;
@@ -4856,23 +4915,56 @@ __global__ void __launch_bounds__(256) kb_residual(const ResDesc* t, int with_A,
   }
 }
 
-// x_sol += d for the systems still refining (d was solved in place of r)
+// x_sol += d for the systems still refining (d was solved in place of r):
+// the x blocks of each map entry's level-1 pairs (2 q0 .. 2 q1 - 1) ...
+__global__ void __launch_bounds__(128) kb_correct_rows(const ResDesc* t, const BatchCta* map, const long* ecnt) {
+  const long cnt = ecnt ? *ecnt : (long)gridDim.x;
+  for (long e = blockIdx.x; e < cnt; e += gridDim.x) {
+    const BatchCta c = map[e];
+    const ResDesc& R = t[c.sys];
+    if (*R.done) continue;
+    const long n = R.d.n;
+    for (long i = 2 * c.q0 * n + threadIdx.x; i < 2 * c.q1 * n; i += blockDim.x) R.xs[i] += R.r[i];
+  }
+}
+
+// ... and the rest of x, one CTA per system
 __global__ void __launch_bounds__(256) kb_correct(const ResDesc* t) {
   const ResDesc& R = t[blockIdx.x];
   if (*R.done) return;
   const Dims d = R.d;
   const long ncols = (long)d.n * (d.nblock + 1) + d.qx + d.nx;
-  for (long i = threadIdx.x; i < ncols; i += blockDim.x) R.xs[i] += R.r[i];
+  for (long i = 2 * pairs_at_level(d.nblock, 1) * d.n + threadIdx.x; i < ncols; i += blockDim.x)
+    R.xs[i] += R.r[i];
 }
 
-void batch_residual(BatchClass& c, int with_A, double tol, unsigned long long* worst, cudaStream_t st) {
+// the level-1 entries of the sweep map: all of them, or the compacted ones
+static SweepMap level1_map(const BatchClass& c, bool compact) {
+  if (!compact) return {c.smap, nullptr, (unsigned)c.scnt[0]};
+  return {c.cmap, c.ccnt, (unsigned)std::min<long>(c.scnt[0], COMPACT_GRID)};
+}
+
+void batch_residual(BatchClass& c, int with_A, double tol, unsigned long long* worst, cudaStream_t st,
+                    bool compact) {
   if (c.nsys == 0) return;
+  compact = compact && c.cmap != nullptr;
+  if (c.levels > 0 && c.scnt[0] > 0) {
+    const SweepMap m = level1_map(c, compact);
+    kb_residual_rows<<<m.grid, 128, 0, st>>>(static_cast<const ResDesc*>(c.rd), m.map, m.ecnt, with_A);
+    check_launch("kb_residual_rows");
+  }
   kb_residual<<<c.nsys, 256, 0, st>>>(static_cast<const ResDesc*>(c.rd), with_A, tol, worst);
   check_launch("kb_residual");
 }
 
 void batch_correct(BatchClass& c, cudaStream_t st) {
   if (c.nsys == 0) return;
+  const bool compact = c.cmap != nullptr;
+  if (c.levels > 0 && c.scnt[0] > 0) {
+    const SweepMap m = level1_map(c, compact);
+    kb_correct_rows<<<m.grid, 128, 0, st>>>(static_cast<const ResDesc*>(c.rd), m.map, m.ecnt);
+    check_launch("kb_correct_rows");
+  }
   kb_correct<<<c.nsys, 256, 0, st>>>(static_cast<const ResDesc*>(c.rd));
   check_launch("kb_correct");
 }
@@ -5127,12 +5219,6 @@ void batch_factorize(BatchClass& c, cudaStream_t st) {
 // the sweep map of level L: the full map (one CTA per entry), or on the
 // refinement passes the compacted map of the systems still refining, walked by
 // a fixed grid (the launch is captured before the length is known)
-struct SweepMap {
-  const BatchCta* map;
-  const long* ecnt;
-  unsigned grid;
-};
-
 static SweepMap sweep_map(const BatchClass& c, int L, bool compact) {
   if (!compact) return {c.smap + c.soff[L], nullptr, (unsigned)c.scnt[L]};
   return {c.cmap + c.soff[L], c.ccnt + L, (unsigned)std::min<long>(c.scnt[L], COMPACT_GRID)};
