@@ -1346,7 +1346,9 @@ struct bcr_batch_s {
   int schedule = BCR_BATCH_LEVELS;  // factorization: one launch per level, or one persistent launch
   int precision = BCR_PRECISION_FP64;
   double ir_tol = 1e-12;
-  int ir_max = 30;  // converged systems drop out, so a slow one costs little
+  // corrections after the first sweep compacted maps of the systems still
+  // refining, so each extra pass costs about one solve of those systems
+  int ir_max = 30;
   int ir_iters = 0;
   double ir_worst = 0.0;
   bool ir_pending = false;

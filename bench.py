@@ -324,8 +324,11 @@ def run_ours(args):
                           "nblock": CFG["nblock"], "clocks": clocks, **acc}))
         return 0
     # end to end through the C ABI with host buffers: factorize + solve in one
-    # call (the matrix is uploaded from the pinned host copy every step)
-    xh = b.copy()
+    # call; every step uploads the matrix from the handle's page-locked host
+    # copy and the right-hand side from a page-locked buffer, into which the
+    # solution comes back
+    xh = torch.empty(b.shape, dtype=torch.float64, pin_memory=True).numpy()
+    xh[:] = b
     for _ in range(2):
         assert h.factorize_solve(1, xh, L), h.last_error()
         xh[:] = b
