@@ -638,8 +638,8 @@ def cpu_baseline(s, b, steps, warmup):
 
 def run_once_batch(args):
     """One factorize + solve of a batch of --nsys-once uneven systems (the
-    batch workload's distribution) through the persistent schedule, for
-    profilers."""
+    batch workload's systems, right-hand sides of ones) with the default
+    per-level schedule, for profilers."""
     import torch
     from alglin_b200 import bcr, synth
     dims = synth.batch_dims(args.nsys_once, 64, 4096, seed=0)
@@ -655,7 +655,7 @@ def run_once_batch(args):
     xs = [np.ones(max(bt.system_size(i))) for i in range(len(dims))]
     assert bt.factorize_solve(xs), bt.last_error()
     print(json.dumps({"once": "D", "nsys": len(dims), "precision": args.precision,
-                      "classes": bt.classes()}))
+                      "classes": bt.classes(), "refinement": bt.refinement_info()}))
     return 0
 
 
