@@ -4767,6 +4767,9 @@ struct SweepMap {
   unsigned grid;
 };
 
+// border rows of a batched system (batch_family_ok admits nr <= 8 only)
+constexpr int BATCH_NR_MAX = 8;
+
 // r = b - (D_k x_k + E_k x_{k+1} + B_k xb) on block rows [k0, k1) of one
 // system, written into the rhs slot; the largest |r| and (with_A) the largest
 // row sum of |A| over this thread's rows
@@ -4867,16 +4870,32 @@ __global__ void __launch_bounds__(256) kb_residual(const ResDesc* t, int with_A,
     mr = fmax(mr, fabs(r));
     ma = fmax(ma, with_A ? sa : 0.0);
   }
-  // border rows: every block column, reduced over the CTA
-  for (int rr = 0; rr < nr; ++rr) {
-    double s = 0.0, sa = 0.0;
+  // border rows (nr <= BATCH_NR_MAX in a batch): one walk over every block
+  // column accumulates all of them, each row's terms in the same order as a
+  // walk of its own; then one CTA reduction per row
+  double bs_s[BATCH_NR_MAX], bs_a[BATCH_NR_MAX];
+#pragma unroll
+  for (int rr = 0; rr < BATCH_NR_MAX; ++rr) bs_s[rr] = bs_a[rr] = 0.0;
+  if (nr > 0) {
     for (long e = tid; e < (long)(nb + 1) * n; e += bs) {
       const size_t k = (size_t)(e / n);
       const int c = (int)(e % n);
-      const double cv = R.C0[k * nrn + (size_t)c * nr + rr];
-      s = fma(cv, xs[k * n + c], s);
-      sa += fabs(cv);
+      const double xv = xs[k * n + c];
+      const double* cp = R.C0 + k * nrn + (size_t)c * nr;
+#pragma unroll
+      for (int rr = 0; rr < BATCH_NR_MAX; ++rr) {
+        if (rr < nr) {
+          const double cv = cp[rr];
+          bs_s[rr] = fma(cv, xv, bs_s[rr]);
+          bs_a[rr] += fabs(cv);
+        }
+      }
     }
+  }
+#pragma unroll
+  for (int rr = 0; rr < BATCH_NR_MAX; ++rr) {
+    if (rr >= nr) break;
+    double s = bs_s[rr], sa = bs_a[rr];
     for (int c = tid; c < qx; c += bs) { s = fma(R.Cq[(size_t)c * nr + rr], xs[xq + c], s); sa += fabs(R.Cq[(size_t)c * nr + rr]); }
     for (int c = tid; c < nx; c += bs) { s = fma(R.F0[(size_t)c * nr + rr], xs[xb + c], s); sa += fabs(R.F0[(size_t)c * nr + rr]); }
     s = block_sum(s, sv);
