@@ -1357,6 +1357,13 @@ struct bcr_batch_s {
   int* d_done = nullptr;               // per system: refinement converged
   unsigned long long* d_worst = nullptr;
   cudaStream_t stream = nullptr;
+  // one stream per class: a phase of the step (factorize, solve, a
+  // refinement pass) forks from `stream` into the classes and joins back, so
+  // the classes' launches overlap (they share no device memory but the
+  // batch-worst word, which they update atomically)
+  std::vector<cudaStream_t> cls_stream;
+  std::vector<cudaEvent_t> cls_done;
+  cudaEvent_t fork_ev = nullptr;
   cudaGraphExec_t graph = nullptr;
   bool prepared = false, factorized = false;
   std::string err = "no error";
@@ -1372,6 +1379,12 @@ struct bcr_batch_s {
   void release() {
     if (stream) cudaStreamSynchronize(stream);
     if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    for (cudaStream_t q : cls_stream) cudaStreamDestroy(q);
+    for (cudaEvent_t ev : cls_done) cudaEventDestroy(ev);
+    if (fork_ev) cudaEventDestroy(fork_ev);
+    cls_stream.clear();
+    cls_done.clear();
+    fork_ev = nullptr;
     for (auto& c : cls) bcr::batch_free(c);
     cls.clear();
     members.clear();
@@ -1435,11 +1448,39 @@ struct bcr_batch_s {
 
   int prepare(int autotune);
   int tune_class(size_t c);
+  // fn(class, its stream) for every class: forked from `stream` and joined
+  // back into it (all on `stream` when there is one class or no class streams)
+  template <typename F>
+  void per_class(F&& fn) {
+    if (cls.size() < 2 || cls_stream.size() != cls.size()) {
+      for (auto& c : cls) fn(c, stream);
+      return;
+    }
+    cudaEventRecord(fork_ev, stream);
+    for (size_t c = 0; c < cls.size(); ++c) {
+      cudaStreamWaitEvent(cls_stream[c], fork_ev, 0);
+      fn(cls[c], cls_stream[c]);
+      cudaEventRecord(cls_done[c], cls_stream[c]);
+    }
+    for (size_t c = 0; c < cls.size(); ++c) cudaStreamWaitEvent(stream, cls_done[c], 0);
+  }
+  int make_class_streams() {
+    for (size_t c = 0; c < cls.size() && cls.size() > 1; ++c) {
+      cudaStream_t q = nullptr;
+      cudaEvent_t ev = nullptr;
+      if (cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking) != cudaSuccess) return 1;
+      cls_stream.push_back(q);
+      if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) return 1;
+      cls_done.push_back(ev);
+    }
+    if (cls.size() > 1 && cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming) != cudaSuccess) return 1;
+    return 0;
+  }
   void enqueue_factorize() {
-    for (auto& c : cls) bcr::batch_factorize(c, stream);
+    per_class([](bcr::BatchClass& c, cudaStream_t q) { bcr::batch_factorize(c, q); });
   }
   void enqueue_solve() {
-    for (auto& c : cls) bcr::batch_solve(c, stream);
+    per_class([](bcr::BatchClass& c, cudaStream_t q) { bcr::batch_solve(c, q); });
   }
   bool mixed() const { return precision == BCR_PRECISION_MIXED; }
   // the worst relative residual of the last mixed solve
@@ -1467,7 +1508,8 @@ struct bcr_batch_s {
     for (;;) {
       cudaMemsetAsync(d_worst, 0, 8, stream);
       // after the first, the residual covers the systems just corrected
-      for (auto& c : cls) bcr::batch_residual(c, with_A && it == 0 ? 1 : 0, ir_tol, d_worst, stream, it > 0);
+      const int wa = with_A && it == 0 ? 1 : 0;
+      per_class([&](bcr::BatchClass& c, cudaStream_t q) { bcr::batch_residual(c, wa, ir_tol, d_worst, q, it > 0); });
       ir_pending = true;
       if (fixed < 0) {
         int rc = read_worst();
@@ -1477,9 +1519,11 @@ struct bcr_batch_s {
         break;
       }
       // the correction solve covers only the systems still refining
-      for (auto& c : cls) bcr::batch_compact(c, stream);
-      for (auto& c : cls) bcr::batch_solve(c, stream, true);
-      for (auto& c : cls) bcr::batch_correct(c, stream);
+      per_class([](bcr::BatchClass& c, cudaStream_t q) {
+        bcr::batch_compact(c, q);
+        bcr::batch_solve(c, q, true);
+        bcr::batch_correct(c, q);
+      });
       ++it;
     }
     cudaMemcpyAsync(d_x, d_sol, x_elems * 8, cudaMemcpyDeviceToDevice, stream);
@@ -1671,6 +1715,10 @@ int bcr_batch_s::prepare(int autotune) {
       release();
       return fail(BCR_CUDA_ERROR, "alglin_b200 batch: table upload failed\n");
     }
+  }
+  if (make_class_streams()) {
+    release();
+    return fail(BCR_CUDA_ERROR, "alglin_b200 batch: stream creation failed\n");
   }
   e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) return cuda_fail(e, "batch prepare");
