@@ -1299,7 +1299,7 @@ namespace {
 constexpr int NRM_SLOTS = 8;
 
 struct BatchTune {
-  int n, nrm, nxm, mixed, fam, chunk;
+  int n, nrm, nxm, mixed, persist, fam, chunk;  // shape, precision, schedule -> choice
 };
 std::vector<BatchTune> g_batch_tuning;  // in-process autotuner cache
 
@@ -1710,7 +1710,10 @@ int bcr_batch_s::prepare(int autotune) {
     cls[c].mixed = mixed() ? 1 : 0;
     cls[c].persist = schedule == BCR_BATCH_PERSISTENT ? 1 : 0;
     for (const auto& t : g_batch_tuning)
-      if (t.n == d0.n && t.nrm == nrm && t.nxm == nxm && t.mixed == cls[c].mixed) { cls[c].fam = t.fam; cls[c].chunk = t.chunk; }
+      if (t.n == d0.n && t.nrm == nrm && t.nxm == nxm && t.mixed == cls[c].mixed && t.persist == cls[c].persist) {
+        cls[c].fam = t.fam;
+        cls[c].chunk = t.chunk;
+      }
     if (bcr::batch_build(cls[c], v, 1)) {
       release();
       return fail(BCR_CUDA_ERROR, "alglin_b200 batch: table upload failed\n");
@@ -1772,8 +1775,12 @@ int bcr_batch_s::tune_class(size_t ci) {
   if (bcr::batch_build(c, v, 1)) return fail(BCR_CUDA_ERROR, "alglin_b200 batch: table upload failed\n");
   bool found = false;
   for (auto& t : g_batch_tuning)
-    if (t.n == dm.n && t.nrm == nrm && t.nxm == nxm && t.mixed == c.mixed) { t.fam = bf; t.chunk = bc; found = true; }
-  if (!found) g_batch_tuning.push_back({dm.n, nrm, nxm, c.mixed, bf, bc});
+    if (t.n == dm.n && t.nrm == nrm && t.nxm == nxm && t.mixed == c.mixed && t.persist == c.persist) {
+      t.fam = bf;
+      t.chunk = bc;
+      found = true;
+    }
+  if (!found) g_batch_tuning.push_back({dm.n, nrm, nxm, c.mixed, c.persist, bf, bc});
   return BCR_OK;
 }
 

@@ -24,6 +24,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <type_traits>
 
 #include "bcr_device.h"
 
@@ -610,7 +611,7 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
                : "d"(a), "d"(b));
 }
 
-template <int N>
+template <int N, typename T = double>
 struct TcShape {
   static constexpr int MT = 2 * N + 8;             // GEMM rows: U-row, reduced row, border (padded)
   static constexpr int NTILES = (2 * N + 8 + 7) / 8;  // trailing columns 2N + nx, nx <= 8
@@ -624,21 +625,25 @@ struct TcShape {
   static constexpr int MTILES = MT / 8;
   static constexpr int WS = 2 * N * LDW;            // doubles: the 2N panel rows' trailing part
   static constexpr int GS = MT * LDG;
-  static constexpr size_t BYTES = (size_t)(WS + GS + N + 2) * 8 + 2 * N * sizeof(int);
+  static constexpr size_t BYTES = (size_t)(WS + GS + N + 2) * sizeof(T) + 2 * N * sizeof(int);
 };
 
 // element (row, col) of the trailing part from the compact rows
-template <int N>
-__device__ __forceinline__ double tc_w(const double* Wt, int row, int col) {
+template <int N, typename T>
+__device__ __forceinline__ T tc_w(const T* Wt, int row, int col) {
   constexpr int LDW = TcShape<N>::LDW;
   const bool top = row < N;
-  if (col < N) return top ? Wt[row * LDW + col] : 0.0;
-  if (col < 2 * N) return top ? 0.0 : Wt[row * LDW + col - N];
+  if (col < N) return top ? Wt[row * LDW + col] : T(0);
+  if (col < 2 * N) return top ? T(0) : Wt[row * LDW + col - N];
   return Wt[row * LDW + col - N];
 }
 
 size_t tc_smem_per_warp(int n) {
   return n == 16 ? TcShape<16>::BYTES : n == 8 ? TcShape<8>::BYTES : 0;
+}
+template <typename T>
+static size_t tc_smem_per_warp_t(int n) {
+  return n == 16 ? TcShape<16, T>::BYTES : n == 8 ? TcShape<8, T>::BYTES : 0;
 }
 
 __host__ __device__ inline int lowbit(int v) { return v & -v; }
@@ -665,13 +670,13 @@ __device__ __forceinline__ double ldw(const double* p) { return __ldcg(p); }
 // cg holds columns cg*CPL .. cg*CPL + CPL - 1 of border row r (LPR = 32 / NRM
 // lanes per row), so their eliminations (C_j U^-1, then -C' L^-1) run in the
 // same instructions as everyone else instead of on nr lanes alone.
-template <int N, int NRM>
-__device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int k, bool first, double* Wt,
-                                        int lane, const TcTree& tr) {
-  using S = TcShape<N>;
+template <int N, int NRM, typename T = double>
+__device__ __forceinline__ bool tc_pair(const FactorArgs<T>& a, int j, int k, bool first, T* Wt, int lane,
+                                        const TcTree& tr) {
+  using S = TcShape<N, T>;
   constexpr unsigned FULL = 0xffffffffu;
-  double* Gs = Wt + S::WS;
-  double* bc = Gs + S::GS;                        // pivot row + its reciprocal
+  T* Gs = Wt + S::WS;
+  T* bc = Gs + S::GS;                             // pivot row + its reciprocal
   int* rowof = reinterpret_cast<int*>(bc + N + 2);
   const Dims d = a.d;
   const int nr = d.nr, nx = d.nx;
@@ -684,34 +689,44 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
   const int ri = top ? lane : lane - n;
   const int g = lane >> 2, t = lane & 3;
   const int jp = j - k;
-  const double* srcD = first ? a.D0 : a.D;
-  const double* srcE = first ? a.E0 : a.E;
-  const double* srcB = first ? a.B0 : a.B;
-  const double* srcC = first ? a.C0 : a.C;
+  // block elements: the loaded FP64 matrix at the first level, the working
+  // copy (type T) after it; always through L2 (see ldw)
+  using SrcT = typename std::conditional<sizeof(T) == 8, double, T>::type;
+  const SrcT* srcD = first ? (const SrcT*)a.D0 : (const SrcT*)a.D;
+  const SrcT* srcE = first ? (const SrcT*)a.E0 : (const SrcT*)a.E;
+  const SrcT* srcB = first ? (const SrcT*)a.B0 : (const SrcT*)a.B;
+  const SrcT* srcC = first ? (const SrcT*)a.C0 : (const SrcT*)a.C;
+  auto lds = [&](const SrcT* base, const double* orig, size_t i) -> T {
+    if constexpr (sizeof(T) == 8) return ldw(base + i);
+    else return first ? T(ldw(orig + i)) : __ldcg(base + i);
+  };
   // ------------------------------------------------------------ load
   constexpr int LPR = 32 / NRM, CPL = N / LPR;   // border layout (see above)
   const int br = lane / LPR, bc0 = (lane % LPR) * CPL;
   const bool blive = br < nr;
-  double rowA[N], cb[CPL];
+  T rowA[N], cb[CPL];
   double cs1[2] = {0.0, 0.0}, cs2[2] = {0.0, 0.0};  // children's F / xb sums (tree)
   {
-    const double* Pm = top ? srcE + (size_t)jp * nn : srcD + (size_t)j * nn;
+    const size_t po = top ? (size_t)jp * nn : (size_t)j * nn;
+    const SrcT* Pm = (top ? srcE : srcD) + po;
+    const double* Po = (top ? a.E0 : a.D0) + po;
 #pragma unroll
-    for (int c = 0; c < N; ++c) rowA[c] = act ? ldw(Pm + (size_t)c * n + ri) : 0.0;
+    for (int c = 0; c < N; ++c) rowA[c] = act ? lds(Pm, Po, (size_t)c * n + ri) : T(0);
 #pragma unroll
-    for (int q = 0; q < CPL; ++q) cb[q] = blive ? ldw(srcC + (size_t)j * nrn + (size_t)(bc0 + q) * nr + br) : 0.0;
+    for (int q = 0; q < CPL; ++q)
+      cb[q] = blive ? lds(srcC, a.C0, (size_t)j * nrn + (size_t)(bc0 + q) * nr + br) : T(0);
     // C_jpp contributions of the pairs (j - 2K', j - K') of earlier levels,
     // K' = 1, 2, ..., gather: loaded eight levels at a time so that their
     // latencies overlap, then added in level order
     for (int e0 = 0; e0 < 31 && (1 << e0) <= tr.gather; e0 += 8) {
-      double v[8][CPL];
+      T v[8][CPL];
 #pragma unroll
       for (int e = 0; e < 8; ++e) {
         const int kk = e0 + e < 31 ? 1 << (e0 + e) : 0;
         const bool on = blive && kk != 0 && kk <= tr.gather;
 #pragma unroll
         for (int q = 0; q < CPL; ++q)
-          v[e][q] = on ? ldw(a.Rbuf + (size_t)(j - kk) * nrn + (size_t)(bc0 + q) * nr + br) : 0.0;
+          v[e][q] = on ? T(__ldcg(a.Rbuf + (size_t)(j - kk) * nrn + (size_t)(bc0 + q) * nr + br)) : T(0);
       }
 #pragma unroll
       for (int e = 0; e < 8; ++e)
@@ -737,37 +752,41 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
     // trailing columns in the original row order: TOP [D_jp 0 B_jp], BOTTOM [0 E_j B_j]
     // compile-time trip counts: every load of the pair is issued before the
     // first one is consumed, so a lone pair pays one memory latency
-    const double* Djp = srcD + (size_t)jp * nn;
-    const double* Ej = srcE + (size_t)j * nn;
+    const SrcT* Djp = srcD + (size_t)jp * nn;
+    const SrcT* Ej = srcE + (size_t)j * nn;
+    const double* Djp0 = a.D0 + (size_t)jp * nn;
+    const double* Ej0 = a.E0 + (size_t)j * nn;
 #pragma unroll
     for (int it = 0; it < (int)(nn / 32); ++it) {
       const int idx = lane + 32 * it;
       const int r = idx % n, c = idx / n;
-      Wt[r * S::LDW + c] = ldw(Djp + idx);
-      Wt[(n + r) * S::LDW + c] = ldw(Ej + idx);
+      Wt[r * S::LDW + c] = lds(Djp, Djp0, idx);
+      Wt[(n + r) * S::LDW + c] = lds(Ej, Ej0, idx);
     }
-    const double* Bjp = srcB + (size_t)jp * nnx;
-    const double* Bj = srcB + (size_t)j * nnx;
+    const SrcT* Bjp = srcB + (size_t)jp * nnx;
+    const SrcT* Bj = srcB + (size_t)j * nnx;
+    const double* Bjp0 = a.B0 + (size_t)jp * nnx;
+    const double* Bj0 = a.B0 + (size_t)j * nnx;
 #pragma unroll
     for (int it = 0; it < (8 * N + 31) / 32; ++it) {
       const int idx = lane + 32 * it;
       if (idx < (int)nnx) {
         const int r = idx % n, c = idx / n;
-        Wt[r * S::LDW + n + c] = ldw(Bjp + idx);
-        Wt[(n + r) * S::LDW + n + c] = ldw(Bj + idx);
+        Wt[r * S::LDW + n + c] = lds(Bjp, Bjp0, idx);
+        Wt[(n + r) * S::LDW + n + c] = lds(Bj, Bj0, idx);
       }
     }
     // fused right-hand sides: TOP rows hold x_jp, BOTTOM rows x_j
     for (int idx = lane; idx < n2 * nrf; idx += 32) {
       const int r = idx % n2, c = idx / n2;
       const double* xc = a.x + (size_t)c * a.ldx;
-      Wt[r * S::LDW + n + nx + c] = r < n ? ldw(xc + (size_t)jp * n + r) : ldw(xc + (size_t)j * n + r - n);
+      Wt[r * S::LDW + n + nx + c] = T(r < n ? ldw(xc + (size_t)jp * n + r) : ldw(xc + (size_t)j * n + r - n));
     }
     // zero the padding columns of the live rows (they feed padding outputs only,
     // but keep them finite)
     for (int idx = lane; idx < n2 * (S::NTP - NT); idx += 32) {
       const int r = idx % n2, c = NT + idx / n2;
-      Wt[r * S::LDW + c - n] = 0.0;
+      Wt[r * S::LDW + c - n] = T(0);
     }
   }
   // --------------------------------------------------- phase 1: panel LU
@@ -777,20 +796,33 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
   for (int i = 0; i < N; ++i) {
     // every lane forms the reciprocal of its own candidate while the pivot is
     // searched; the pivot lane publishes its value with the pivot row
-    const double rc = __drcp_rn(rowA[i]);
     // pivot: max |a| over rows not yet used, ties to the smaller position
-    const double av = fabs(rowA[i]);
-    const unsigned long long bits = (unsigned long long)__double_as_longlong(av);
-    unsigned hi = (unsigned)(bits >> 32) + 1u;
-    if (done) hi = 0u;
-    else if (av != av) hi = 1u;  // NaN loses against every number
+    // (FP64: upper word of |a|, then the lower word; FP32: the whole word)
+    T rc;
+    unsigned hi, lob;
+    if constexpr (sizeof(T) == 8) {
+      rc = __drcp_rn(rowA[i]);
+      const double av = fabs(rowA[i]);
+      const unsigned long long bits = (unsigned long long)__double_as_longlong(av);
+      hi = (unsigned)(bits >> 32) + 1u;
+      if (done) hi = 0u;
+      else if (av != av) hi = 1u;  // NaN loses against every number
+      lob = (unsigned)bits;
+    } else {
+      rc = __frcp_rn(rowA[i]);
+      const float av = fabsf(rowA[i]);
+      hi = __float_as_uint(av) + 1u;
+      if (done) hi = 0u;
+      else if (av != av) hi = 1u;
+      lob = 0u;
+    }
     const unsigned hmax = __reduce_max_sync(FULL, hi);
     unsigned m = __ballot_sync(FULL, hi == hmax && !done);
     unsigned pmin;
     if (__popc(m) == 1) {  // unique maximum in the upper word: the usual case
       pmin = (unsigned)__shfl_sync(FULL, mypos, __ffs(m) - 1);
     } else {               // exact tie handling: lower word, then smallest position
-      const unsigned lo = (hi == hmax) ? (unsigned)bits : 0u;
+      const unsigned lo = (hi == hmax) ? lob : 0u;
       const unsigned lmax = __reduce_max_sync(FULL, lo);
       const bool cand = (hi == hmax) && (lo == lmax) && !done;
       pmin = __reduce_min_sync(FULL, cand ? (unsigned)mypos : 0xffffffffu);
@@ -801,30 +833,25 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
     if (lane == p) {
       mypos = i;
 #pragma unroll
-      for (int c = (i & ~1); c < N; c += 2)
-        *reinterpret_cast<double2*>(&bc[c]) = make_double2(rowA[c], rowA[c + 1]);
+      for (int c = (i & ~1); c < N; c += 2) store2(&bc[c], rowA[c], rowA[c + 1]);
       bc[N] = rc;
     }
     __syncwarp();
-    const double piv = bc[i];
-    if (piv == 0.0 && info == 0) info = i + 1;
-    const double rinv = piv != 0.0 ? bc[N] : 0.0;
-    double u[N];
+    const T piv = bc[i];
+    if (piv == T(0) && info == 0) info = i + 1;
+    const T rinv = piv != T(0) ? bc[N] : T(0);
+    T u[N];
 #pragma unroll
-    for (int c = (i + 1) & ~1; c < N; c += 2) {
-      const double2 v2 = *reinterpret_cast<const double2*>(&bc[c]);
-      u[c] = v2.x;
-      u[c + 1] = v2.y;
-    }
+    for (int c = (i + 1) & ~1; c < N; c += 2) load2(&bc[c], u[c], u[c + 1]);
     if (!done && lane != p) {
-      const double l = rowA[i] * rinv;
+      const T l = rowA[i] * rinv;
       rowA[i] = l;
 #pragma unroll
       for (int c = i + 1; c < N; ++c) rowA[c] = fma(-l, u[c], rowA[c]);
     }
     {  // border rows: multiplier from the lane holding column i of the row
-      const double ci = __shfl_sync(FULL, cb[i % CPL], (lane & ~(LPR - 1)) | (i / CPL));
-      const double l = ci * rinv;
+      const T ci = __shfl_sync(FULL, cb[i % CPL], (lane & ~(LPR - 1)) | (i / CPL));
+      const T l = ci * rinv;
 #pragma unroll
       for (int q = 0; q < CPL; ++q) {
         const int c = bc0 + q;
@@ -841,7 +868,7 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
   }
   // panel factors T_j (L\U and M in getrf row order), pivots, C_j U^-1
   {
-    double* Tj = a.Tm + (size_t)j * szT(d);
+    T* Tj = a.Tm + (size_t)j * szT(d);
     if (act) {
 #pragma unroll
       for (int c = 0; c < N; ++c) Tj[(size_t)mypos + (size_t)c * n2] = rowA[c];
@@ -855,31 +882,31 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
     // rows of L (row m contiguous) for the triangular solve
     if (act && mypos < n) {
 #pragma unroll
-      for (int c = 0; c < N; c += 2)
-        *reinterpret_cast<double2*>(&Gs[mypos * S::LDG + c]) = make_double2(rowA[c], rowA[c + 1]);
+      for (int c = 0; c < N; c += 2) store2(&Gs[mypos * S::LDG + c], rowA[c], rowA[c + 1]);
     }
   }
   __syncwarp();
   // ------------------------------------ phase 2: operator G (X L = R)
   // R rows: identity for U-row positions, -M for reduced positions, -C' for border rows
   {
-    double x[N];
+    T x[N];
 #pragma unroll
-    for (int c = 0; c < N; ++c) x[c] = (mypos < n) ? (c == mypos ? 1.0 : 0.0) : -rowA[c];
+    for (int c = 0; c < N; ++c) x[c] = (mypos < n) ? (c == mypos ? T(1) : T(0)) : -rowA[c];
 #pragma unroll
     for (int q = 0; q < CPL; ++q) cb[q] = -cb[q];
     // right-looking: once x[mm] is final, update every x[c], c < mm (the
     // updates of one step are independent, so the dependent chain is N long)
 #pragma unroll
     for (int mm = N - 1; mm > 0; --mm) {
-      const double xm = x[mm];
-      const double cm = __shfl_sync(FULL, cb[mm % CPL], (lane & ~(LPR - 1)) | (mm / CPL));
-      const double* Lrow = Gs + mm * S::LDG;  // L(mm, 0..mm-1)
+      const T xm = x[mm];
+      const T cm = __shfl_sync(FULL, cb[mm % CPL], (lane & ~(LPR - 1)) | (mm / CPL));
+      const T* Lrow = Gs + mm * S::LDG;  // L(mm, 0..mm-1)
 #pragma unroll
       for (int c = 0; c < mm; c += 2) {
-        const double2 l2 = *reinterpret_cast<const double2*>(&Lrow[c]);
-        x[c] = fma(-xm, l2.x, x[c]);
-        if (c + 1 < mm) x[c + 1] = fma(-xm, l2.y, x[c + 1]);
+        T l0, l1;
+        load2(&Lrow[c], l0, l1);
+        x[c] = fma(-xm, l0, x[c]);
+        if (c + 1 < mm) x[c + 1] = fma(-xm, l1, x[c + 1]);
       }
 #pragma unroll
       for (int q = 0; q < CPL; ++q)
@@ -888,30 +915,31 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
     __syncwarp();
     if (act) {
 #pragma unroll
-      for (int c = 0; c < N; c += 2)
-        *reinterpret_cast<double2*>(&Gs[mypos * S::LDG + c]) = make_double2(x[c], x[c + 1]);
+      for (int c = 0; c < N; c += 2) store2(&Gs[mypos * S::LDG + c], x[c], x[c + 1]);
     }
     // border rows of G (zero for rows >= nr, and rows NRM..7 of the tile)
 #pragma unroll
     for (int q = 0; q < CPL; ++q) {
-      Gs[(n2 + br) * S::LDG + bc0 + q] = blive ? cb[q] : 0.0;
-      if constexpr (NRM < 8) Gs[(n2 + NRM + br) * S::LDG + bc0 + q] = 0.0;
+      Gs[(n2 + br) * S::LDG + bc0 + q] = blive ? cb[q] : T(0);
+      if constexpr (NRM < 8) Gs[(n2 + NRM + br) * S::LDG + bc0 + q] = T(0);
     }
   }
   __syncwarp();
-  // ----------------------------------------- phase 3: tensor-core GEMM
-  // two passes over the column tiles keep the accumulators within budget
+  // ----------------------------------------- phase 3: the product
+  // FP64 tensor cores (DMMA 8x8x4) for double, the FP32 pipe for float, with
+  // the same accumulator layout; two passes over the column tiles keep the
+  // accumulators within budget
 #pragma unroll
   for (int pass = 0; pass < 2; ++pass) {
     constexpr int PC = S::PC;
-    double acc[S::MTILES][PC][2];
+    T acc[S::MTILES][PC][2];
 #pragma unroll
     for (int mt = 0; mt < S::MTILES; ++mt)
 #pragma unroll
       for (int ni = 0; ni < PC; ++ni) {
         const int nt = pass * PC + ni;
         const int row = mt * 8 + g;
-        double c0 = 0.0, c1 = 0.0;
+        T c0 = T(0), c1 = T(0);
         if (nt < S::NTILES && row >= n && row < n2) {  // (PW)_bot
           const int orow = rowof[row];
           c0 = tc_w<N>(Wt, orow, nt * 8 + 2 * t);
@@ -920,21 +948,45 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
         acc[mt][ni][0] = c0;
         acc[mt][ni][1] = c1;
       }
+    if constexpr (sizeof(T) == 8) {
 #pragma unroll
-    for (int ks = 0; ks < S::KSTEPS; ++ks) {
-      double bfr[PC];
-      const int orow = rowof[ks * 4 + t];
+      for (int ks = 0; ks < S::KSTEPS; ++ks) {
+        double bfr[PC];
+        const int orow = rowof[ks * 4 + t];
 #pragma unroll
-      for (int ni = 0; ni < PC; ++ni) {
-        const int nt = pass * PC + ni;
-        bfr[ni] = nt < S::NTILES ? tc_w<N>(Wt, orow, nt * 8 + g) : 0.0;
+        for (int ni = 0; ni < PC; ++ni) {
+          const int nt = pass * PC + ni;
+          bfr[ni] = nt < S::NTILES ? tc_w<N>(Wt, orow, nt * 8 + g) : 0.0;
+        }
+#pragma unroll
+        for (int mt = 0; mt < S::MTILES; ++mt) {
+          const double afr = Gs[(mt * 8 + g) * S::LDG + ks * 4 + t];
+#pragma unroll
+          for (int ni = 0; ni < PC; ++ni)
+            if (pass * PC + ni < S::NTILES) dmma_8x8x4(acc[mt][ni][0], acc[mt][ni][1], afr, bfr[ni]);
+        }
       }
+    } else {
+      // element (8mt+g, 8nt+2t+h) += sum over kk of G(8mt+g, kk) (PW)_top(kk, 8nt+2t+h)
+#pragma unroll 4
+      for (int kk = 0; kk < N; ++kk) {
+        const int orow = rowof[kk];
+        T bv[PC][2];
 #pragma unroll
-      for (int mt = 0; mt < S::MTILES; ++mt) {
-        const double afr = Gs[(mt * 8 + g) * S::LDG + ks * 4 + t];
+        for (int ni = 0; ni < PC; ++ni) {
+          const int nt = pass * PC + ni;
+          bv[ni][0] = nt < S::NTILES ? tc_w<N>(Wt, orow, nt * 8 + 2 * t) : T(0);
+          bv[ni][1] = nt < S::NTILES ? tc_w<N>(Wt, orow, nt * 8 + 2 * t + 1) : T(0);
+        }
 #pragma unroll
-        for (int ni = 0; ni < PC; ++ni)
-          if (pass * PC + ni < S::NTILES) dmma_8x8x4(acc[mt][ni][0], acc[mt][ni][1], afr, bfr[ni]);
+        for (int mt = 0; mt < S::MTILES; ++mt) {
+          const T av = Gs[(mt * 8 + g) * S::LDG + kk];
+#pragma unroll
+          for (int ni = 0; ni < PC; ++ni) {
+            acc[mt][ni][0] = fma(av, bv[ni][0], acc[mt][ni][0]);
+            acc[mt][ni][1] = fma(av, bv[ni][1], acc[mt][ni][1]);
+          }
+        }
       }
     }
     // ------------------------------------------------------------ store
@@ -952,7 +1004,7 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
             const int nt = pass * PC + ni;
             if (nt >= S::NTILES) continue;
             const int col = nt * 8 + 2 * t + hh;
-            const double v = acc[mt][ni][hh];
+            const T v = acc[mt][ni][hh];
             if (mt * 8 < n2) {  // panel rows (compile-time per mt)
               const bool ur = row < n;
               const int rr = ur ? row : row - n;
@@ -960,22 +1012,22 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
               if (col < n) a.D[blk * nn + (size_t)col * n + rr] = v;
               else if (col < n2) a.E[blk * nn + (size_t)(col - n) * n + rr] = v;
               else if (col < n2 + nx) a.B[blk * nnx + (size_t)(col - n2) * n + rr] = v;
-              else if (col < NT) a.x[(size_t)(col - n2 - nx) * a.ldx + blk * n + rr] = v;
+              else if (col < NT) a.x[(size_t)(col - n2 - nx) * a.ldx + blk * n + rr] = (double)v;
             } else {
               const int rr = row - n2;
               if (rr < nr) {
                 if (col < n) {
                   const size_t o = (size_t)jp * nrn + (size_t)col * nr + rr;
-                  a.C[o] = ldw(srcC + o) + v;
+                  a.C[o] = lds(srcC, a.C0, o) + v;
                 } else if (col < n2) {
                   a.Rbuf[(size_t)j * nrn + (size_t)(col - n) * nr + rr] = v;
                 } else if (col < n2 + nx) {
                   // own F update plus the partial sums of the child nodes (tree)
                   const size_t e = (size_t)(col - n2) * nr + rr;
-                  a.Fbuf[(size_t)j * nrnx + e] = v + cs1[hh] + cs2[hh];
+                  a.Fbuf[(size_t)j * nrnx + e] = (double)v + cs1[hh] + cs2[hh];
                 } else if (col < NT) {
                   const size_t e = (size_t)(col - n2 - nx) * nr + rr, nrr = (size_t)nr * nrf;
-                  a.XB[(size_t)j * nrr + e] = v + cs1[hh] + cs2[hh];
+                  a.XB[(size_t)j * nrr + e] = (double)v + cs1[hh] + cs2[hh];
                 }
               }
             }
@@ -992,17 +1044,22 @@ __device__ __forceinline__ bool tc_pair(const FactorArgs<double>& a, int j, int 
 // levels and adds its children's F / xb partial sums, so no border fix-up or
 // reduction launch is needed between or after the levels (k_tree_root
 // finishes C_nblock, F and xb after the last level).
-template <int N, bool BATCH = false, bool BOOK = false, int NRM = 8>
-__global__ void __launch_bounds__(128, 4) k_factor_lu_tc(FactorArgs<double> a0, const FactorArgs<double>* tab,
-                                                       const BatchCta* cmap) {
-  using S = TcShape<N>;
+// resident CTAs of 4 warps the register budget is sized for: FP32 pairs take
+// half the shared memory and fewer registers, so more of them fit on an SM
+template <typename T>
+constexpr int tc_min_blocks() { return sizeof(T) == 8 ? 4 : 6; }
+
+template <int N, bool BATCH = false, bool BOOK = false, int NRM = 8, typename T = double>
+__global__ void __launch_bounds__(128, tc_min_blocks<T>())
+    k_factor_lu_tc(FactorArgs<T> a0, const FactorArgs<T>* tab, const BatchCta* cmap) {
+  using S = TcShape<N, T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  FactorArgs<double> ab;  // this CTA's system (batch only)
+  FactorArgs<T> ab;  // this CTA's system (batch only)
   long q0, q1, qs;
   pair_range<BATCH>(a0, tab, cmap, wpb, warp, ab, q0, q1, qs);
-  const FactorArgs<double>& a = BATCH ? ab : a0;
-  double* Wt = reinterpret_cast<double*>(smem_raw + (size_t)warp * S::BYTES);
+  const FactorArgs<T>& a = BATCH ? ab : a0;
+  T* Wt = reinterpret_cast<T*>(smem_raw + (size_t)warp * S::BYTES);
   TcTree tr{0, 0, 0};
   for (long q = q0; q < q1; q += qs) {
     const int j = a.k + (int)(2L * a.k * q);
@@ -1010,7 +1067,7 @@ __global__ void __launch_bounds__(128, 4) k_factor_lu_tc(FactorArgs<double> a0, 
       tr.gather = a.k / 2;
       tree_children(j, a.d.nblock, tr.c1, tr.c2);
     }
-    tc_pair<N, NRM>(a, j, a.k, a.first != 0, Wt, lane, tr);
+    tc_pair<N, NRM, T>(a, j, a.k, a.first != 0, Wt, lane, tr);
   }
 }
 
@@ -3871,6 +3928,18 @@ static FactorPlan<T> plan_factor(const DevState& s) {
         p.tree_ctas = 148 * resident_ctas(p.tree, 128, p.tc_smem);
       }
     }
+  } else {
+    // FP32 factors (mixed path): the same warp-per-pair kernel with FP32
+    // products, level by level, no fused right-hand sides
+    if (s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 && (n == 16 || n == 8) && s.use_tc &&
+        (s.pair_kernel == PAIR_AUTO || s.pair_kernel == PAIR_TC)) {
+      p.tc_smem = tc_smem_per_warp_t<T>(n) * 4;
+      const bool r4 = d.nr <= 4;
+      if (n == 16) p.tc = r4 ? k_factor_lu_tc<16, false, false, 4, T> : k_factor_lu_tc<16, false, false, 8, T>;
+      else p.tc = r4 ? k_factor_lu_tc<8, false, false, 4, T> : k_factor_lu_tc<8, false, false, 8, T>;
+      smem_limit_once(p.tc, p.tc_smem);
+      p.tc_cols = 0;
+    }
   }
   const bool grp_ok = s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 &&
                       (n == 32 || (n == 16 && (sizeof(T) == 4 || s.pair_kernel == PAIR_GRP)));
@@ -4665,21 +4734,21 @@ __global__ void __launch_bounds__(2 * N + 32, grp_min_blocks<T, N>())
   }
 }
 
-template <int N>
-__global__ void __launch_bounds__(128, 4) kp_factor_tc(const FactorArgs<double>* tab, const BatchCta* items,
-                                                       BatchQueue qu) {
-  using S = TcShape<N>;
+template <int N, typename T = double>
+__global__ void __launch_bounds__(128, tc_min_blocks<T>())
+    kp_factor_tc(const FactorArgs<T>* tab, const BatchCta* items, BatchQueue qu) {
+  using S = TcShape<N, T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double* Wt = reinterpret_cast<double*>(smem_raw + (size_t)warp * S::BYTES);
-  FactorArgs<double> a;
+  T* Wt = reinterpret_cast<T*>(smem_raw + (size_t)warp * S::BYTES);
+  FactorArgs<T> a;
   BatchCta c;
   bool ok;
   while (queue_next_warp(qu, items, tab, a, c, ok)) {
     const TcTree tr{0, 0, 0};
     if (ok)
       for (long q = c.q0; q < c.q1; ++q)
-        tc_pair<N, 8>(a, a.k + (int)(2L * a.k * q), a.k, a.first != 0, Wt, lane, tr);
+        tc_pair<N, 8, T>(a, a.k + (int)(2L * a.k * q), a.k, a.first != 0, Wt, lane, tr);
     queue_done_warp(qu, a, c);
   }
 }
@@ -4991,7 +5060,7 @@ void batch_correct(BatchClass& c, cudaStream_t st) {
 bool batch_family_ok(int fam, const Dims& d, bool mixed) {
   if (d.nr > 8 || d.nx > 8) return false;
   switch (fam) {
-    case PAIR_TC: return !mixed && (d.n == 8 || d.n == 16);
+    case PAIR_TC: return d.n == 8 || d.n == 16;
     case PAIR_GRP: return d.n == 16 || d.n == 32;
     case PAIR_ROWS: return d.n <= 16 && d.nr <= 4 && d.nx <= 4;
     default: return false;
@@ -5137,19 +5206,16 @@ static void batch_pairs(BatchClass& c, int L, cudaStream_t st) {
   const FactorArgs<T>* tab = static_cast<const FactorArgs<T>*>(c.fa);
   const BatchCta* map = c.fmap + c.foff[L];
   const unsigned g = (unsigned)cnt;
-  if constexpr (sizeof(T) == 8) {
-    if (c.fam == PAIR_TC) {
-      if (c.n == 16) {
-        const size_t sm = tc_smem_per_warp(16) * 4;
-        smem_limit_once(k_factor_lu_tc<16, true>, sm);
-        k_factor_lu_tc<16, true><<<g, 128, sm, st>>>(a0, tab, map);
-      } else {
-        const size_t sm = tc_smem_per_warp(8) * 4;
-        smem_limit_once(k_factor_lu_tc<8, true>, sm);
-        k_factor_lu_tc<8, true><<<g, 128, sm, st>>>(a0, tab, map);
-      }
-      check_launch("batched pair kernel");
+  if (c.fam == PAIR_TC) {
+    const size_t sm = tc_smem_per_warp_t<T>(c.n) * 4;
+    if (c.n == 16) {
+      smem_limit_once(k_factor_lu_tc<16, true, false, 8, T>, sm);
+      k_factor_lu_tc<16, true, false, 8, T><<<g, 128, sm, st>>>(a0, tab, map);
+    } else {
+      smem_limit_once(k_factor_lu_tc<8, true, false, 8, T>, sm);
+      k_factor_lu_tc<8, true, false, 8, T><<<g, 128, sm, st>>>(a0, tab, map);
     }
+    check_launch("batched pair kernel");
   }
   if (c.fam == PAIR_GRP) {
     if (c.n == 32) {
@@ -5181,19 +5247,17 @@ static void batch_pairs_persistent(BatchClass& c, cudaStream_t st) {
   auto grid = [&](auto* kern, int threads, size_t smem) {
     return grid_for(c.items, 1, 148 * resident_ctas(kern, threads, smem));
   };
-  if constexpr (sizeof(T) == 8) {
-    if (c.fam == PAIR_TC) {
-      const size_t sm = tc_smem_per_warp(c.n) * 4;
-      if (c.n == 16) {
-        smem_limit_once(kp_factor_tc<16>, sm);
-        kp_factor_tc<16><<<grid(kp_factor_tc<16>, 128, sm), 128, sm, st>>>(tab, c.fmap, qu);
-      } else {
-        smem_limit_once(kp_factor_tc<8>, sm);
-        kp_factor_tc<8><<<grid(kp_factor_tc<8>, 128, sm), 128, sm, st>>>(tab, c.fmap, qu);
-      }
-      check_launch("kp_factor_tc");
-      return;
+  if (c.fam == PAIR_TC) {
+    const size_t sm = tc_smem_per_warp_t<T>(c.n) * 4;
+    if (c.n == 16) {
+      smem_limit_once(kp_factor_tc<16, T>, sm);
+      kp_factor_tc<16, T><<<grid(kp_factor_tc<16, T>, 128, sm), 128, sm, st>>>(tab, c.fmap, qu);
+    } else {
+      smem_limit_once(kp_factor_tc<8, T>, sm);
+      kp_factor_tc<8, T><<<grid(kp_factor_tc<8, T>, 128, sm), 128, sm, st>>>(tab, c.fmap, qu);
     }
+    check_launch("kp_factor_tc");
+    return;
   }
   if (c.fam == PAIR_GRP) {
     if (c.n == 32) {
