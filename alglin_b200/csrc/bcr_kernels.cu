@@ -2513,11 +2513,11 @@ __global__ void __launch_bounds__(256, 2) k_backward_rows(SweepArgs<TF> a0, cons
 // while the current pair is computed, so every warp keeps a pair's worth of
 // loads in flight.  Two buffers per warp.
 // ---------------------------------------------------------------------------
-template <int N, int NXM>
+template <int N, int NXM, typename T = double>
 struct BwdBuf {
   static constexpr int DE = N * N, BB = N * NXM, U = N * N;
   static constexpr int WORDS = 2 * DE + BB + U;  // D', E', B', U (rows 0..N-1 of T)
-  static constexpr size_t BYTES = (size_t)2 * WORDS * 8;  // two buffers
+  static constexpr size_t BYTES = (size_t)2 * WORDS * sizeof(T);  // two buffers
 };
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -2528,37 +2528,40 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int K>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
 
-// the factors of pair q into one buffer (every lane issues its share)
-template <int N, int NXM>
-__device__ __forceinline__ void bwd_stage(const SweepArgs<double>& a, long q, double* buf, int lane) {
-  using Bf = BwdBuf<N, NXM>;
+// the factors of pair q into one buffer (every lane issues its share), in
+// 16-byte chunks of V elements; for n = 8, 16 every block (D', E', B', the U
+// columns of T) starts and ends on a 16-byte boundary in FP64 and FP32
+template <int N, int NXM, typename T>
+__device__ __forceinline__ void bwd_stage(const SweepArgs<T>& a, long q, T* buf, int lane) {
+  using Bf = BwdBuf<N, NXM, T>;
+  constexpr int V = 16 / (int)sizeof(T);
   const Dims d = a.d;
   const int n = d.n, nx = d.nx, k = a.k;
   const int j = k + (int)(2L * k * q);
-  const double* Dj = a.D + (size_t)j * n * n;
-  const double* Ej = a.E + (size_t)j * n * n;
-  const double* Bj = a.B + (size_t)j * n * nx;
-  const double* Tj = a.Tm + (size_t)j * szT(d);
-  // D', E': n*n doubles each, n*n/2 chunks
-  for (int c = lane; c < n * n / 2; c += 32) {
-    cp_async16(buf + 2 * c, Dj + 2 * c);
-    cp_async16(buf + Bf::DE + 2 * c, Ej + 2 * c);
+  const T* Dj = a.D + (size_t)j * n * n;
+  const T* Ej = a.E + (size_t)j * n * n;
+  const T* Bj = a.B + (size_t)j * n * nx;
+  const T* Tj = a.Tm + (size_t)j * szT(d);
+  // D', E': n*n elements each
+  for (int c = lane; c < n * n / V; c += 32) {
+    cp_async16(buf + V * c, Dj + V * c);
+    cp_async16(buf + Bf::DE + V * c, Ej + V * c);
   }
-  for (int c = lane; c < n * nx / 2; c += 32) cp_async16(buf + 2 * Bf::DE + 2 * c, Bj + 2 * c);
+  for (int c = lane; c < n * nx / V; c += 32) cp_async16(buf + 2 * Bf::DE + V * c, Bj + V * c);
   // U: column col of T holds rows 0..n-1 of U at Tj + col * 2n
-  for (int c = lane; c < n * n / 2; c += 32) {
-    const int col = (2 * c) / n, r = (2 * c) % n;
+  for (int c = lane; c < n * n / V; c += 32) {
+    const int col = (V * c) / n, r = (V * c) % n;
     cp_async16(buf + 2 * Bf::DE + Bf::BB + col * n + r, Tj + (size_t)col * 2 * n + r);
   }
 }
 
-template <int N, int NXM>
-__global__ void __launch_bounds__(256, 2) k_backward_pipe(SweepArgs<double> a) {
-  using Bf = BwdBuf<N, NXM>;
+template <int N, int NXM, typename T = double>
+__global__ void __launch_bounds__(256, 2) k_backward_pipe(SweepArgs<T> a) {
+  using Bf = BwdBuf<N, NXM, T>;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  double* bufs = reinterpret_cast<double*>(smem_raw) + (size_t)warp * 2 * Bf::WORDS;
+  T* bufs = reinterpret_cast<T*>(smem_raw) + (size_t)warp * 2 * Bf::WORDS;
   const Dims d = a.d;
   const int n = d.n, nx = d.nx, nb = d.nblock, nrhs = a.nrhs, k = a.k;
   const int i = lane & 15;
@@ -2568,12 +2571,12 @@ __global__ void __launch_bounds__(256, 2) k_backward_pipe(SweepArgs<double> a) {
   const long np = pairs_at_level(nb, k);
   const long qs = (long)gridDim.x * wpb;
   long q = (long)blockIdx.x * wpb + warp;
-  if (q < np) bwd_stage<N, NXM>(a, q, bufs, lane);
+  if (q < np) bwd_stage<N, NXM, T>(a, q, bufs, lane);
   cp_async_commit();
   int cur = 0;
   for (; q < np; q += qs) {
     const bool more = q + qs < np;
-    if (more) bwd_stage<N, NXM>(a, q + qs, bufs + (cur ^ 1) * Bf::WORDS, lane);
+    if (more) bwd_stage<N, NXM, T>(a, q + qs, bufs + (cur ^ 1) * Bf::WORDS, lane);
     cp_async_commit();
     const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
     // the right-hand side values, loaded while the factors arrive
@@ -2585,7 +2588,7 @@ __global__ void __launch_bounds__(256, 2) k_backward_pipe(SweepArgs<double> a) {
     const int dst = (qrp && !hi && rowok) ? (int)a.P[(size_t)j * szP(d) + 2 * n + i] : i;
     cp_async_wait<1>();  // this pair's factors (the next pair's may still be in flight)
     __syncwarp();
-    const double* buf = bufs + cur * Bf::WORDS;
+    const T* buf = bufs + cur * Bf::WORDS;
     double m[N], u[N], bb[NXM];
 #pragma unroll
     for (int c = 0; c < N; ++c) m[c] = (rowok && c < n) ? buf[(hi ? Bf::DE : 0) + c * n + i] : 0.0;
@@ -2636,8 +2639,8 @@ __global__ void __launch_bounds__(256, 2) k_backward_pipe(SweepArgs<double> a) {
 // The top levels of the backward sweep (at most 16 pairs each) in one launch
 // of one CTA of 16 warps, levels in order with a barrier between them; the
 // pair arithmetic is k_backward_rows'.
-template <int N, int NXM>
-__global__ void __launch_bounds__(512, 1) k_backward_top(SweepArgs<double> a, int k_top, int k_min) {
+template <int N, int NXM, typename T = double>
+__global__ void __launch_bounds__(512, 1) k_backward_top(SweepArgs<T> a, int k_top, int k_min) {
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const Dims d = a.d;
@@ -2650,9 +2653,9 @@ __global__ void __launch_bounds__(512, 1) k_backward_top(SweepArgs<double> a, in
     const long np = pairs_at_level(nb, k);
     for (long q = warp; q < np; q += 16) {
       const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
-      const double* Mt = (hi ? a.E : a.D) + (size_t)j * n * n;
-      const double* Tj = a.Tm + (size_t)j * szT(d);
-      const double* Bj = a.B + (size_t)j * n * nx;
+      const T* Mt = (hi ? a.E : a.D) + (size_t)j * n * n;
+      const T* Tj = a.Tm + (size_t)j * szT(d);
+      const T* Bj = a.B + (size_t)j * n * nx;
       double m[N], u[N], bb[NXM];
 #pragma unroll
       for (int c = 0; c < N; ++c) m[c] = (rowok && c < n) ? Mt[(size_t)c * n + i] : 0.0;
@@ -4128,9 +4131,9 @@ struct SweepPlan {
   void (*fwd)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*, const long*) = nullptr;
   void (*bwd)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*, const long*) = nullptr;
   // FP64 n = 8, 16 single systems: pipelined backward levels, the top in one CTA
-  void (*bwd_pipe)(SweepArgs<double>) = nullptr;
+  void (*bwd_pipe)(SweepArgs<T>) = nullptr;
   size_t bwd_pipe_smem = 0;
-  void (*bwd_top)(SweepArgs<double>, int, int) = nullptr;
+  void (*bwd_top)(SweepArgs<T>, int, int) = nullptr;
   void (*fwd_cta)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*) = nullptr;  // CTA per pair (large n)
   void (*bwd_cta)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*) = nullptr;
 };
@@ -4151,20 +4154,18 @@ static SweepPlan<T> plan_sweeps(const DevState& s) {
 #undef BCR_FWD
 #undef BCR_BWD
   }
-  if constexpr (sizeof(T) == 8) {
-    if ((n == 16 || n == 8) && d.nx <= 8) {
-      const bool x4 = d.nx <= 4;
-      if (n == 16) {
-        p.bwd_pipe = x4 ? k_backward_pipe<16, 4> : k_backward_pipe<16, 8>;
-        p.bwd_pipe_smem = 8 * (x4 ? BwdBuf<16, 4>::BYTES : BwdBuf<16, 8>::BYTES);
-        p.bwd_top = x4 ? k_backward_top<16, 4> : k_backward_top<16, 8>;
-      } else {
-        p.bwd_pipe = x4 ? k_backward_pipe<8, 4> : k_backward_pipe<8, 8>;
-        p.bwd_pipe_smem = 8 * (x4 ? BwdBuf<8, 4>::BYTES : BwdBuf<8, 8>::BYTES);
-        p.bwd_top = x4 ? k_backward_top<8, 4> : k_backward_top<8, 8>;
-      }
-      smem_limit_once(p.bwd_pipe, p.bwd_pipe_smem);
+  if ((n == 16 || n == 8) && d.nx <= 8) {  // both precisions
+    const bool x4 = d.nx <= 4;
+    if (n == 16) {
+      p.bwd_pipe = x4 ? k_backward_pipe<16, 4, T> : k_backward_pipe<16, 8, T>;
+      p.bwd_pipe_smem = 8 * (x4 ? BwdBuf<16, 4, T>::BYTES : BwdBuf<16, 8, T>::BYTES);
+      p.bwd_top = x4 ? k_backward_top<16, 4, T> : k_backward_top<16, 8, T>;
+    } else {
+      p.bwd_pipe = x4 ? k_backward_pipe<8, 4, T> : k_backward_pipe<8, 8, T>;
+      p.bwd_pipe_smem = 8 * (x4 ? BwdBuf<8, 4, T>::BYTES : BwdBuf<8, 8, T>::BYTES);
+      p.bwd_top = x4 ? k_backward_top<8, 4, T> : k_backward_top<8, 8, T>;
     }
+    smem_limit_once(p.bwd_pipe, p.bwd_pipe_smem);
   }
   if (n == 32) {
     if (s.sel == SEL_LU && d.nr <= 8) p.fwd = d.nr <= 4 ? k_forward_rows32<T, 4> : k_forward_rows32<T, 8>;
@@ -4230,25 +4231,23 @@ static void last_and_backward(DevState& s, const SweepPlan<T>& p, const WorkSet<
   SweepArgs<T> a = sweep_args(s, w, x, ldx, nrhs);
   a.ldw = d.n;
   const size_t smem_b = (size_t)d.n * 8 * WARPS_PANEL;
-  if constexpr (sizeof(T) == 8) {
-    if (p.bwd_pipe) {
-      // the levels with at most 16 pairs (the top) in one CTA, then one
-      // pipelined launch per level below
-      int k = top_level(d.nblock) / 2, k_split = 0;
-      for (int kk = k; kk > 0; kk /= 2)
-        if (pairs_at_level(d.nblock, kk) > 16) { k_split = kk; break; }
-      if (k > k_split) {
-        p.bwd_top<<<1, 512, 0, st>>>(a, k, k_split * 2 > 0 ? k_split * 2 : 1);
-        check_launch("k_backward_top");
-      }
-      for (int kk = k_split; kk > 0; kk /= 2) {
-        a.k = kk;
-        const long np = pairs_at_level(d.nblock, kk);
-        p.bwd_pipe<<<grid_for(np, 8, 148 * 2), 256, p.bwd_pipe_smem, st>>>(a);
-        check_launch("k_backward_pipe");
-      }
-      return;
+  if (p.bwd_pipe) {
+    // the levels with at most 16 pairs (the top) in one CTA, then one
+    // pipelined launch per level below
+    int k = top_level(d.nblock) / 2, k_split = 0;
+    for (int kk = k; kk > 0; kk /= 2)
+      if (pairs_at_level(d.nblock, kk) > 16) { k_split = kk; break; }
+    if (k > k_split) {
+      p.bwd_top<<<1, 512, 0, st>>>(a, k, k_split * 2 > 0 ? k_split * 2 : 1);
+      check_launch("k_backward_top");
     }
+    for (int kk = k_split; kk > 0; kk /= 2) {
+      a.k = kk;
+      const long np = pairs_at_level(d.nblock, kk);
+      p.bwd_pipe<<<grid_for(np, 8, 148 * 2), 256, p.bwd_pipe_smem, st>>>(a);
+      check_launch("k_backward_pipe");
+    }
+    return;
   }
   for (int k = top_level(d.nblock); (k /= 2) > 0;) {
     a.k = k;
