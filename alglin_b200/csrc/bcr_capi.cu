@@ -321,13 +321,15 @@ struct bcr_handle_s {
     if (rc) return rc;
     if (s.mixed) {
       // adaptive refinement needs the factorization's status first
-      enqueue_factorize();
+      if (nrhs > 0 && (rc = save_rhs(nrhs, dx, ld))) return rc;
+      if (nrhs > 0) bcr::launch_factorize_solve(s, dx, ld, nrhs, stream);  // x0 with the factors
+      else enqueue_factorize();
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return cuda_fail(e, "factorize launch");
       pending_status = true;
       factorized = true;
       if ((rc = factorize_status())) return rc;
-      return nrhs > 0 ? solve_mixed(nrhs, dx, ld, -1) : BCR_OK;
+      return nrhs > 0 ? solve_mixed(nrhs, dx, ld, -1, true) : BCR_OK;
     }
     if (nrhs == 0) bcr::launch_factorize(s, stream);
     else bcr::launch_factorize_solve(s, dx, ld, nrhs, stream);
@@ -389,19 +391,37 @@ struct bcr_handle_s {
     return BCR_OK;
   }
 
-  // mixed path: x = A^-1 b with FP32 factors, then corrections d = A^-1 r from
-  // FP64 residuals r = b - Ax until |r|/(|A||x|+|b|) <= ir_tol (adaptive: the
-  // host reads the norms after every residual) or for exactly `fixed` steps
-  // (graph capture: no host synchronisation)
-  int solve_mixed(int nrhs, double* dx, int ld, int fixed) {
-    const size_t Lx = (size_t)L(), nrw = (size_t)nrows(), ncl = (size_t)ncols();
+  // mixed path: the right-hand sides b kept in dB while x0 = A^-1 b is formed
+  // in place
+  int save_rhs(int nrhs, double* dx, int ld) {
+    const size_t Lx = (size_t)L(), nrw = (size_t)nrows();
+    int rc = ensure_buffer(dB, dB_cap, Lx * nrhs);
+    if (rc) return rc;
+    cudaMemcpy2DAsync(dB, Lx * 8, dx, (size_t)ld * 8, nrw * 8, nrhs, cudaMemcpyDeviceToDevice, stream);
+    return BCR_OK;
+  }
+  // mixed factorize + solve on the device: b saved, x0 from the factorization
+  // (which carries the first forward elimination where the pair kernel can),
+  // then the refinement for exactly `fixed` steps (graph capture)
+  int factorize_solve_mixed(int nrhs, double* dx, int ld, int fixed) {
+    int rc = save_rhs(nrhs, dx, ld);
+    if (rc) return rc;
+    bcr::launch_factorize_solve(s, dx, ld, nrhs, stream);
+    return solve_mixed(nrhs, dx, ld, fixed, true);
+  }
+  // mixed path: x = A^-1 b with FP32 factors (unless x0_done: x holds it and
+  // dB holds b), then corrections d = A^-1 r from FP64 residuals r = b - Ax
+  // until |r|/(|A||x|+|b|) <= ir_tol (adaptive: the host reads the norms after
+  // every residual) or for exactly `fixed` steps (graph capture: no host
+  // synchronisation)
+  int solve_mixed(int nrhs, double* dx, int ld, int fixed, bool x0_done = false) {
+    const size_t Lx = (size_t)L(), ncl = (size_t)ncols();
     int rc;
-    if ((rc = ensure_buffer(dB, dB_cap, Lx * nrhs))) return rc;
+    if (!x0_done && (rc = save_rhs(nrhs, dx, ld))) return rc;
     if ((rc = ensure_buffer(dR, dR_cap, Lx * nrhs))) return rc;
     if ((rc = ensure_buffer(dNorm, dNorm_cap, 1 + 3 * (size_t)nrhs))) return rc;
     auto* norms = reinterpret_cast<unsigned long long*>(dNorm);
-    cudaMemcpy2DAsync(dB, Lx * 8, dx, (size_t)ld * 8, nrw * 8, nrhs, cudaMemcpyDeviceToDevice, stream);
-    bcr::launch_solve(s, dx, ld, nrhs, stream);
+    if (!x0_done) bcr::launch_solve(s, dx, ld, nrhs, stream);
     ir_nrhs = nrhs;
     int it = 0;
     for (;;) {
@@ -1195,14 +1215,21 @@ int bcr_graph_capture(bcr_handle h, int what, int nrhs, double* d_x, int ld, con
   if ((what & BCR_GRAPH_SOLVE) && (nrhs < 1 || ld < h->L() || !d_x))
     return h->fail(BCR_BAD_ARGUMENT, "bcr_graph_capture: bad right-hand-side buffer\n");
   // one eager run first: it validates the selection and sets kernel attributes
-  if (what & BCR_GRAPH_FACTORIZE) {
-    if ((rc = h->factorize_device())) return rc;
-  } else if (!h->factorized) {
-    return h->fail(BCR_NUMERICAL, "bcr_graph_capture: factorize before capturing a solve\n");
-  }
-  if (what & BCR_GRAPH_SOLVE) {
+  // (a mixed step runs exactly what the graph will, so that the graph replays
+  // the number of corrections this run needed)
+  if (what == BCR_GRAPH_STEP && h->s.mixed) {
     if (d_rhs) cudaMemcpyAsync(d_x, d_rhs, (size_t)ld * nrhs * 8, cudaMemcpyDeviceToDevice, h->stream);
-    if ((rc = h->solve_device(nrhs, d_x, ld))) return rc;
+    if ((rc = h->factorize_solve_launch(nrhs, d_x, ld))) return rc;
+  } else {
+    if (what & BCR_GRAPH_FACTORIZE) {
+      if ((rc = h->factorize_device())) return rc;
+    } else if (!h->factorized) {
+      return h->fail(BCR_NUMERICAL, "bcr_graph_capture: factorize before capturing a solve\n");
+    }
+    if (what & BCR_GRAPH_SOLVE) {
+      if (d_rhs) cudaMemcpyAsync(d_x, d_rhs, (size_t)ld * nrhs * 8, cudaMemcpyDeviceToDevice, h->stream);
+      if ((rc = h->solve_device(nrhs, d_x, ld))) return rc;
+    }
   }
   // the mixed path's graph replays the refinement steps the eager run needed
   const int ir_steps = h->ir_iters;
@@ -1215,8 +1242,7 @@ int bcr_graph_capture(bcr_handle h, int what, int nrhs, double* d_x, int ld, con
   if (what == BCR_GRAPH_STEP) {
     if (d_rhs) cudaMemcpyAsync(d_x, d_rhs, (size_t)ld * nrhs * 8, cudaMemcpyDeviceToDevice, h->stream);
     if (mixed) {
-      h->enqueue_factorize();
-      rc = h->solve_mixed(nrhs, d_x, ld, ir_steps);
+      rc = h->factorize_solve_mixed(nrhs, d_x, ld, ir_steps);
     } else {
       bcr::launch_factorize_solve(h->s, d_x, ld, nrhs, h->stream);
     }

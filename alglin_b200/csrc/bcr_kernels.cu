@@ -3941,7 +3941,7 @@ static FactorPlan<T> plan_factor(const DevState& s) {
       if (n == 16) p.tc = r4 ? k_factor_lu_tc<16, false, false, 4, T> : k_factor_lu_tc<16, false, false, 8, T>;
       else p.tc = r4 ? k_factor_lu_tc<8, false, false, 4, T> : k_factor_lu_tc<8, false, false, 8, T>;
       smem_limit_once(p.tc, p.tc_smem);
-      p.tc_cols = 0;
+      p.tc_cols = n == 16 ? TcShape<16, T>::NTP : TcShape<8, T>::NTP;
     }
   }
   const bool grp_ok = s.sel == SEL_LU && d.nr <= 8 && d.nx <= 8 &&
@@ -4281,15 +4281,11 @@ void launch_solve(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st) {
 // factorize and solve in one pass: when the pair kernel can carry the right-
 // hand sides, their forward elimination rides in the factorization's GEMM and
 // the separate forward sweep disappears
-void launch_factorize_solve(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st) {
-  if (s.mixed) {
-    launch_factorize(s, st);
-    launch_solve(s, x, ldx, nrhs, st);
-    return;
-  }
-  double* tag = nullptr;
-  const WorkSet<double> w = work_set(s, tag);
-  const FactorPlan<double> fp = plan_factor<double>(s);
+template <typename T>
+static void factorize_solve_t(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st) {
+  T* tag = nullptr;
+  const WorkSet<T> w = work_set(s, tag);
+  const FactorPlan<T> fp = plan_factor<T>(s);
   const int nrf = fusable_rhs(s, fp, nrhs);
   if (nrf == 0) {
     launch_factorize(s, st);
@@ -4299,7 +4295,15 @@ void launch_factorize_solve(DevState& s, double* x, int ldx, int nrhs, cudaStrea
   const bool tree = factor_levels(s, fp, w, x, ldx, nrf, st);
   if (!tree) reduce_xb(s, x, ldx, nrf, st);
   factor_last(s, w, st, tree);
-  last_and_backward(s, plan_sweeps<double>(s), w, x, ldx, nrf, st);
+  last_and_backward(s, plan_sweeps<T>(s), w, x, ldx, nrf, st);
+}
+
+void launch_factorize_solve(DevState& s, double* x, int ldx, int nrhs, cudaStream_t st) {
+  // FP32 factors (mixed path): the right-hand sides are eliminated in FP32,
+  // which is the accuracy of the solve with those factors anyway; the caller
+  // refines the result
+  if (s.mixed) factorize_solve_t<float>(s, x, ldx, nrhs, st);
+  else factorize_solve_t<double>(s, x, ldx, nrhs, st);
 }
 
 // Factorize + solve with the matrix uploaded from host memory in chunks of

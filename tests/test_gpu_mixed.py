@@ -197,3 +197,28 @@ def test_mixed_tensor_core_large_blocks(dims):
     assert it <= 3 and rr <= RELRES_BAR, (dims, it, rr)
     assert relres(o, s, x, b[0]) <= RELRES_BAR
     assert fwd_err(x[:s.ncols], xo[0, :s.ncols]) <= FWD_BAR
+
+
+@pytest.mark.parametrize("n", [8, 16])
+@pytest.mark.parametrize("nrhs", [1, 3, 5])
+def test_mixed_factorize_solve_fused_first_solve(n, nrhs):
+    """factorize_solve on the mixed path forms x0 with the FP32 factorization
+    carrying the right-hand sides (at most 2n + nx + nrhs <= the pair kernel's
+    trailing columns; 5 right-hand sides at n=16 take the separate solve), then
+    refines every column to the bar."""
+    s = synth.collocation(3001, n, 0, 0, 4, 4, seed=n + nrhs)
+    b = synth.rhs(s, nrhs=nrhs, seed=7)
+    o, xo = oracle_solution(s, b)
+    h = mixed_solver(s)
+    x = np.array(b, copy=True)
+    assert h.factorize_solve(nrhs, x, x.shape[1]), h.last_error()
+    it, rr = h.refinement_info()
+    assert 1 <= it <= 10 and rr <= RELRES_BAR, (it, rr)
+    for c in range(nrhs):
+        assert relres(o, s, x[c], b[c]) <= RELRES_BAR
+        assert fwd_err(x[c, :s.ncols], xo[c, :s.ncols]) <= FWD_BAR
+    # the factors again, with a plain solve
+    y = np.array(b, copy=True)
+    assert h.solve_n(nrhs, y, y.shape[1]), h.last_error()
+    for c in range(nrhs):
+        assert relres(o, s, y[c], b[c]) <= RELRES_BAR
