@@ -2704,6 +2704,108 @@ __global__ void __launch_bounds__(512, 1) k_backward_top(SweepArgs<T> a, int k_t
 }
 
 // ---------------------------------------------------------------------------
+// Forward sweep for LU factors, n = 8 or 16, single systems: the pair
+// arithmetic of k_forward_rows (lane = position r < 2n of the stacked
+// [x_jp; x_j], row map gathered by one shuffle, n broadcast steps of L and M,
+// xb partial -C'_j x_j), with the factors of the warp's NEXT pair (the 2n x n
+// L\U and M block of T, and C_j) copied into shared memory by cp.async while
+// the current pair is computed, and the next pair's row-map entry read into a
+// register one pair ahead.  Two buffers per warp.
+// ---------------------------------------------------------------------------
+template <int N, int NRM, typename T = double>
+struct FwdBuf {
+  static constexpr int TT = 2 * N * N, CC = N * NRM;
+  static constexpr int WORDS = TT + CC;                        // T_j (2n x n), C_j (n x nr)
+  static constexpr size_t BYTES = (size_t)2 * WORDS * sizeof(T);  // two buffers
+};
+
+// the factors of pair q into one buffer, in 16-byte chunks of V elements (for
+// n = 8, 16 both blocks are multiples of 16 bytes in FP64 and FP32)
+template <int N, int NRM, typename T>
+__device__ __forceinline__ void fwd_stage(const SweepArgs<T>& a, long q, T* buf, int lane) {
+  using Bf = FwdBuf<N, NRM, T>;
+  constexpr int V = 16 / (int)sizeof(T);
+  const Dims d = a.d;
+  const int n = d.n, nr = d.nr, k = a.k;
+  const int j = k + (int)(2L * k * q);
+  const T* Tj = a.Tm + (size_t)j * szT(d);
+  const T* Cj = a.C + (size_t)j * nr * n;
+  for (int c = lane; c < 2 * n * n / V; c += 32) cp_async16(buf + V * c, Tj + V * c);
+  for (int c = lane; c < n * nr / V; c += 32) cp_async16(buf + Bf::TT + V * c, Cj + V * c);
+}
+
+template <int N, int NRM, typename T = double>
+__global__ void __launch_bounds__(256, 2) k_forward_pipe(SweepArgs<T> a) {
+  using Bf = FwdBuf<N, NRM, T>;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  T* bufs = reinterpret_cast<T*>(smem_raw) + (size_t)warp * 2 * Bf::WORDS;
+  const Dims d = a.d;
+  const int n = d.n, nr = d.nr, n2 = 2 * n, nb = d.nblock, nrhs = a.nrhs, k = a.k;
+  const bool act = lane < n2;
+  const long np = pairs_at_level(nb, k);
+  const long qs = (long)gridDim.x * wpb;
+  long q = (long)blockIdx.x * wpb + warp;
+  int src_next = lane;
+  if (q < np) {
+    fwd_stage<N, NRM, T>(a, q, bufs, lane);
+    const int j0 = k + (int)(2L * k * q);
+    if (act) src_next = (int)a.P[(size_t)j0 * szP(d) + lane];
+  }
+  cp_async_commit();
+  int cur = 0;
+  for (; q < np; q += qs) {
+    const int src = src_next;
+    if (q + qs < np) {
+      fwd_stage<N, NRM, T>(a, q + qs, bufs + (cur ^ 1) * Bf::WORDS, lane);
+      const int jn = k + (int)(2L * k * (q + qs));
+      if (act) src_next = (int)a.P[(size_t)jn * szP(d) + lane];
+    }
+    cp_async_commit();
+    const int j = k + (int)(2L * k * q), jp = j - k;
+    // the first right-hand side's values, loaded while the factors arrive
+    const double orig0 = act ? (lane < n ? a.x[(size_t)jp * n + lane] : a.x[(size_t)j * n + lane - n]) : 0.0;
+    cp_async_wait<1>();  // this pair's factors (the next pair's may still be in flight)
+    __syncwarp();
+    const T* buf = bufs + cur * Bf::WORDS;
+    double t[N], cp[NRM];
+#pragma unroll
+    for (int c = 0; c < N; ++c) t[c] = (act && c < n) ? double(buf[c * n2 + lane]) : 0.0;
+#pragma unroll
+    for (int r = 0; r < NRM; ++r) cp[r] = (lane < n && r < nr) ? double(buf[Bf::TT + lane * nr + r]) : 0.0;
+    for (int col = 0; col < nrhs; ++col) {
+      double* xc = a.x + (size_t)col * a.ldx;
+      const double orig =
+          col == 0 ? orig0 : (act ? (lane < n ? xc[(size_t)jp * n + lane] : xc[(size_t)j * n + lane - n]) : 0.0);
+      double w = __shfl_sync(FULL, orig, src);
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        if (i < n) {
+          const double wi = __shfl_sync(FULL, w, i);
+          if (lane > i && act) w = fma(-t[i], wi, w);
+        }
+      }
+      if (act) {
+        if (lane < n) xc[(size_t)j * n + lane] = w;
+        else xc[(size_t)jp * n + lane - n] = w;
+      }
+      const double wt = lane < n ? w : 0.0;
+#pragma unroll
+      for (int r = 0; r < NRM; ++r) {
+        if (r < nr) {
+          const double sr = warp_sum(cp[r] * wt);
+          if (lane == 0) a.XB[(size_t)j * nr * nrhs + (size_t)col * nr + r] = -sr;
+        }
+      }
+    }
+    __syncwarp();  // every lane is done with this buffer before it is refilled
+    cur ^= 1;
+  }
+  cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
 // sweeps for n = 32: one warp per pair, lane i holds panel positions i and
 // 32 + i (forward) or U-row i (backward); x values are exchanged by shuffles
 // and every factor element is read once, coalesced
@@ -4130,7 +4232,10 @@ template <typename T>
 struct SweepPlan {
   void (*fwd)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*, const long*) = nullptr;
   void (*bwd)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*, const long*) = nullptr;
-  // FP64 n = 8, 16 single systems: pipelined backward levels, the top in one CTA
+  // n = 8, 16 single systems: pipelined forward (LU) and backward levels,
+  // the backward top in one CTA
+  void (*fwd_pipe)(SweepArgs<T>) = nullptr;
+  size_t fwd_pipe_smem = 0;
   void (*bwd_pipe)(SweepArgs<T>) = nullptr;
   size_t bwd_pipe_smem = 0;
   void (*bwd_top)(SweepArgs<T>, int, int) = nullptr;
@@ -4153,6 +4258,17 @@ static SweepPlan<T> plan_sweeps(const DevState& s) {
     else { p.fwd = BCR_FWD(16); p.bwd = BCR_BWD(16); }
 #undef BCR_FWD
 #undef BCR_BWD
+  }
+  if ((n == 16 || n == 8) && s.sel == SEL_LU && d.nr <= 8) {  // both precisions
+    const bool r4 = d.nr <= 4;
+    if (n == 16) {
+      p.fwd_pipe = r4 ? k_forward_pipe<16, 4, T> : k_forward_pipe<16, 8, T>;
+      p.fwd_pipe_smem = 8 * (r4 ? FwdBuf<16, 4, T>::BYTES : FwdBuf<16, 8, T>::BYTES);
+    } else {
+      p.fwd_pipe = r4 ? k_forward_pipe<8, 4, T> : k_forward_pipe<8, 8, T>;
+      p.fwd_pipe_smem = 8 * (r4 ? FwdBuf<8, 4, T>::BYTES : FwdBuf<8, 8, T>::BYTES);
+    }
+    smem_limit_once(p.fwd_pipe, p.fwd_pipe_smem);
   }
   if ((n == 16 || n == 8) && d.nx <= 8) {  // both precisions
     const bool x4 = d.nx <= 4;
@@ -4213,7 +4329,8 @@ static void forward_levels(DevState& s, const SweepPlan<T>& p, const WorkSet<T>&
   for (int K = 1; K < d.nblock; K *= 2) {
     a.k = K;
     const long np = pairs_at_level(d.nblock, K);
-    if (p.fwd_cta) p.fwd_cta<<<grid_for(np, 1, 148 * 8), 256, 0, st>>>(a, nullptr, nullptr);
+    if (p.fwd_pipe) p.fwd_pipe<<<grid_for(np, 8, 148 * 2), 256, p.fwd_pipe_smem, st>>>(a);
+    else if (p.fwd_cta) p.fwd_cta<<<grid_for(np, 1, 148 * 8), 256, 0, st>>>(a, nullptr, nullptr);
     else if (p.fwd) p.fwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a, nullptr, nullptr, nullptr);
     else k_forward_level<T><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_f, st>>>(a, nullptr, nullptr, nullptr);
     check_launch("k_forward_level");
