@@ -2528,15 +2528,16 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int K>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
 
-// the factors of pair q into one buffer (every lane issues its share), in
-// 16-byte chunks of V elements; for n = 8, 16 every block (D', E', B', the U
-// columns of T) starts and ends on a 16-byte boundary in FP64 and FP32
+// the factors of pair q (level stride k) into one buffer (every lane issues
+// its share), in 16-byte chunks of V elements; for n = 8, 16 every block (D',
+// E', B', the U columns of T) starts and ends on a 16-byte boundary in FP64
+// and FP32
 template <int N, int NXM, typename T>
-__device__ __forceinline__ void bwd_stage(const SweepArgs<T>& a, long q, T* buf, int lane) {
+__device__ __forceinline__ void bwd_stage(const SweepArgs<T>& a, int k, long q, T* buf, int lane) {
   using Bf = BwdBuf<N, NXM, T>;
   constexpr int V = 16 / (int)sizeof(T);
   const Dims d = a.d;
-  const int n = d.n, nx = d.nx, k = a.k;
+  const int n = d.n, nx = d.nx;
   const int j = k + (int)(2L * k * q);
   const T* Dj = a.D + (size_t)j * n * n;
   const T* Ej = a.E + (size_t)j * n * n;
@@ -2555,83 +2556,141 @@ __device__ __forceinline__ void bwd_stage(const SweepArgs<T>& a, long q, T* buf,
   }
 }
 
-template <int N, int NXM, typename T = double>
-__global__ void __launch_bounds__(256, 2) k_backward_pipe(SweepArgs<T> a) {
+// Work items of a warp in the pipelined sweeps.  Single system: pair q =
+// item, items first, first + step, ... below the level's pair count.  Batch:
+// item = entry of the level's sweep map (the full map: nent entries; or the
+// compacted map of the systems still refining: *ecnt entries), the warp's
+// pair is entry.q0 + warp, and the system's arguments come from the table.
+template <bool BATCH, typename T>
+struct PipeItems {
+  SweepArgs<T> a0;
+  const SweepArgs<T>* tab;
+  const BatchCta* map;
+  long cnt, first, step;
+  int warp;
+  __device__ PipeItems(const SweepArgs<T>& a, const SweepArgs<T>* t, const BatchCta* m, const long* ecnt,
+                       long nent, int wpb, int w)
+      : a0(a), tab(t), map(m), warp(w) {
+    if constexpr (BATCH) {
+      cnt = ecnt ? *ecnt : nent;
+      first = blockIdx.x;
+      step = gridDim.x;
+    } else {
+      cnt = pairs_at_level(a.d.nblock, a.k);
+      first = (long)blockIdx.x * wpb + w;
+      step = (long)gridDim.x * wpb;
+    }
+  }
+  // the warp's pair of item it (false: none for this warp)
+  __device__ bool pair(long it, int& sys, long& q) const {
+    if constexpr (BATCH) {
+      const BatchCta c = map[it];
+      sys = c.sys;
+      q = c.q0 + warp;
+      if (q >= c.q1) return false;
+      const int* dn = tab[sys].done;
+      return !(dn && *dn);
+    } else {
+      sys = 0;
+      q = it;
+      return true;
+    }
+  }
+  __device__ const SweepArgs<T>& args(int sys) const {
+    if constexpr (BATCH) return tab[sys];
+    else return a0;
+  }
+};
+
+template <int N, int NXM, typename T = double, bool BATCH = false>
+__global__ void __launch_bounds__(256, 2) k_backward_pipe(SweepArgs<T> a0, const SweepArgs<T>* tab,
+                                                          const BatchCta* map, const long* ecnt, long nent) {
   using Bf = BwdBuf<N, NXM, T>;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   T* bufs = reinterpret_cast<T*>(smem_raw) + (size_t)warp * 2 * Bf::WORDS;
-  const Dims d = a.d;
-  const int n = d.n, nx = d.nx, nb = d.nblock, nrhs = a.nrhs, k = a.k;
+  const PipeItems<BATCH, T> items(a0, tab, map, ecnt, nent, wpb, warp);
+  const int k = a0.k;
   const int i = lane & 15;
-  const bool hi = lane >= 16, rowok = i < n;
-  const bool qrp = a.sel == SEL_QRP;
-  const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
-  const long np = pairs_at_level(nb, k);
-  const long qs = (long)gridDim.x * wpb;
-  long q = (long)blockIdx.x * wpb + warp;
-  if (q < np) bwd_stage<N, NXM, T>(a, q, bufs, lane);
+  long it = items.first;
+  int sys = 0;
+  long q = 0;
+  bool have = it < items.cnt && items.pair(it, sys, q);
+  if (have) bwd_stage<N, NXM, T>(items.args(sys), k, q, bufs, lane);
   cp_async_commit();
   int cur = 0;
-  for (; q < np; q += qs) {
-    const bool more = q + qs < np;
-    if (more) bwd_stage<N, NXM, T>(a, q + qs, bufs + (cur ^ 1) * Bf::WORDS, lane);
+  for (; it < items.cnt; it += items.step) {
+    int sysn = 0;
+    long qn = 0;
+    const bool haven = it + items.step < items.cnt && items.pair(it + items.step, sysn, qn);
+    if (haven) bwd_stage<N, NXM, T>(items.args(sysn), k, qn, bufs + (cur ^ 1) * Bf::WORDS, lane);
     cp_async_commit();
-    const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
-    // the right-hand side values, loaded while the factors arrive
-    double xv0 = 0.0, xj0 = 0.0;
-    if (nrhs >= 1) {
-      xv0 = rowok ? (hi ? a.x[(size_t)jpp * n + i] : a.x[(size_t)jp * n + i]) : 0.0;
-      xj0 = (!hi && rowok) ? a.x[(size_t)j * n + i] : 0.0;
-    }
-    const int dst = (qrp && !hi && rowok) ? (int)a.P[(size_t)j * szP(d) + 2 * n + i] : i;
-    cp_async_wait<1>();  // this pair's factors (the next pair's may still be in flight)
-    __syncwarp();
-    const T* buf = bufs + cur * Bf::WORDS;
-    double m[N], u[N], bb[NXM];
-#pragma unroll
-    for (int c = 0; c < N; ++c) m[c] = (rowok && c < n) ? buf[(hi ? Bf::DE : 0) + c * n + i] : 0.0;
-#pragma unroll
-    for (int c = 0; c < N; ++c) u[c] = (!hi && rowok && c < n) ? buf[2 * Bf::DE + Bf::BB + c * n + i] : 0.0;
-#pragma unroll
-    for (int c = 0; c < NXM; ++c) bb[c] = (!hi && rowok && c < nx) ? buf[2 * Bf::DE + c * n + i] : 0.0;
-    double ud = 1.0;
-#pragma unroll
-    for (int c = 0; c < N; ++c)
-      if (c == i) ud = u[c];
-    const double rdi = (!hi && rowok) ? 1.0 / ud : 0.0;
-    for (int col = 0; col < nrhs; ++col) {
-      double* xc = a.x + (size_t)col * a.ldx;
-      const double xv = col == 0 ? xv0 : (rowok ? (hi ? xc[(size_t)jpp * n + i] : xc[(size_t)jp * n + i]) : 0.0);
-      const double xj = col == 0 ? xj0 : ((!hi && rowok) ? xc[(size_t)j * n + i] : 0.0);
-      double xbv[NXM];
-#pragma unroll
-      for (int c = 0; c < NXM; ++c) xbv[c] = c < nx ? xc[xb_off + c] : 0.0;
-      double sacc = 0.0;
-#pragma unroll
-      for (int c = 0; c < N; ++c) {
-        if (c < n) {
-          const double xcv = __shfl_sync(FULL, xv, (lane & 16) | c);
-          sacc = fma(m[c], xcv, sacc);
-        }
+    if (have) {
+      const SweepArgs<T>& a = items.args(sys);
+      const Dims d = a.d;
+      const int n = d.n, nx = d.nx, nb = d.nblock, nrhs = a.nrhs;
+      const bool hi = lane >= 16, rowok = i < n;
+      const bool qrp = a.sel == SEL_QRP;
+      const size_t xb_off = (size_t)(nb + 1) * n + d.qx;
+      const int j = k + (int)(2L * k * q), jp = j - k, jpp = min(j + k, nb);
+      // the right-hand side values, loaded while the factors arrive
+      double xv0 = 0.0, xj0 = 0.0;
+      if (nrhs >= 1) {
+        xv0 = rowok ? (hi ? a.x[(size_t)jpp * n + i] : a.x[(size_t)jp * n + i]) : 0.0;
+        xj0 = (!hi && rowok) ? a.x[(size_t)j * n + i] : 0.0;
       }
-      sacc += __shfl_xor_sync(FULL, sacc, 16);
+      const int dst = (qrp && !hi && rowok) ? (int)a.P[(size_t)j * szP(d) + 2 * n + i] : i;
+      cp_async_wait<1>();  // this pair's factors (the next pair's may still be in flight)
+      __syncwarp();
+      const T* buf = bufs + cur * Bf::WORDS;
+      double m[N], u[N], bb[NXM];
 #pragma unroll
-      for (int c = 0; c < NXM; ++c) sacc = fma(bb[c], xbv[c], sacc);
-      double y = xj - sacc;
+      for (int c = 0; c < N; ++c) m[c] = (rowok && c < n) ? buf[(hi ? Bf::DE : 0) + c * n + i] : 0.0;
 #pragma unroll
-      for (int ii = N - 1; ii >= 0; --ii) {
-        if (ii < n) {
-          const double xi = __shfl_sync(FULL, y * rdi, ii);
-          if (i == ii) y = xi;
-          else if (i < ii) y = fma(-u[ii], xi, y);
+      for (int c = 0; c < N; ++c) u[c] = (!hi && rowok && c < n) ? buf[2 * Bf::DE + Bf::BB + c * n + i] : 0.0;
+#pragma unroll
+      for (int c = 0; c < NXM; ++c) bb[c] = (!hi && rowok && c < nx) ? buf[2 * Bf::DE + c * n + i] : 0.0;
+      double ud = 1.0;
+#pragma unroll
+      for (int c = 0; c < N; ++c)
+        if (c == i) ud = u[c];
+      const double rdi = (!hi && rowok) ? 1.0 / ud : 0.0;
+      for (int col = 0; col < nrhs; ++col) {
+        double* xc = a.x + (size_t)col * a.ldx;
+        const double xv = col == 0 ? xv0 : (rowok ? (hi ? xc[(size_t)jpp * n + i] : xc[(size_t)jp * n + i]) : 0.0);
+        const double xj = col == 0 ? xj0 : ((!hi && rowok) ? xc[(size_t)j * n + i] : 0.0);
+        double xbv[NXM];
+#pragma unroll
+        for (int c = 0; c < NXM; ++c) xbv[c] = c < nx ? xc[xb_off + c] : 0.0;
+        double sacc = 0.0;
+#pragma unroll
+        for (int c = 0; c < N; ++c) {
+          if (c < n) {
+            const double xcv = __shfl_sync(FULL, xv, (lane & 16) | c);
+            sacc = fma(m[c], xcv, sacc);
+          }
         }
+        sacc += __shfl_xor_sync(FULL, sacc, 16);
+#pragma unroll
+        for (int c = 0; c < NXM; ++c) sacc = fma(bb[c], xbv[c], sacc);
+        double y = xj - sacc;
+#pragma unroll
+        for (int ii = N - 1; ii >= 0; --ii) {
+          if (ii < n) {
+            const double xi = __shfl_sync(FULL, y * rdi, ii);
+            if (i == ii) y = xi;
+            else if (i < ii) y = fma(-u[ii], xi, y);
+          }
+        }
+        if (!hi && rowok) xc[(size_t)j * n + dst] = y;
       }
-      if (!hi && rowok) xc[(size_t)j * n + dst] = y;
     }
     __syncwarp();  // every lane is done with this buffer before it is refilled
     cur ^= 1;
+    have = haven;
+    sys = sysn;
+    q = qn;
   }
   cp_async_wait<0>();
 }
@@ -2719,14 +2778,15 @@ struct FwdBuf {
   static constexpr size_t BYTES = (size_t)2 * WORDS * sizeof(T);  // two buffers
 };
 
-// the factors of pair q into one buffer, in 16-byte chunks of V elements (for
-// n = 8, 16 both blocks are multiples of 16 bytes in FP64 and FP32)
+// the factors of pair q (level stride k) into one buffer, in 16-byte chunks
+// of V elements (for n = 8, 16 both blocks are multiples of 16 bytes in FP64
+// and FP32)
 template <int N, int NRM, typename T>
-__device__ __forceinline__ void fwd_stage(const SweepArgs<T>& a, long q, T* buf, int lane) {
+__device__ __forceinline__ void fwd_stage(const SweepArgs<T>& a, int k, long q, T* buf, int lane) {
   using Bf = FwdBuf<N, NRM, T>;
   constexpr int V = 16 / (int)sizeof(T);
   const Dims d = a.d;
-  const int n = d.n, nr = d.nr, k = a.k;
+  const int n = d.n, nr = d.nr;
   const int j = k + (int)(2L * k * q);
   const T* Tj = a.Tm + (size_t)j * szT(d);
   const T* Cj = a.C + (size_t)j * nr * n;
@@ -2734,73 +2794,88 @@ __device__ __forceinline__ void fwd_stage(const SweepArgs<T>& a, long q, T* buf,
   for (int c = lane; c < n * nr / V; c += 32) cp_async16(buf + Bf::TT + V * c, Cj + V * c);
 }
 
-template <int N, int NRM, typename T = double>
-__global__ void __launch_bounds__(256, 2) k_forward_pipe(SweepArgs<T> a) {
+template <int N, int NRM, typename T = double, bool BATCH = false>
+__global__ void __launch_bounds__(256, 2) k_forward_pipe(SweepArgs<T> a0, const SweepArgs<T>* tab,
+                                                         const BatchCta* map, const long* ecnt, long nent) {
   using Bf = FwdBuf<N, NRM, T>;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   T* bufs = reinterpret_cast<T*>(smem_raw) + (size_t)warp * 2 * Bf::WORDS;
-  const Dims d = a.d;
-  const int n = d.n, nr = d.nr, n2 = 2 * n, nb = d.nblock, nrhs = a.nrhs, k = a.k;
-  const bool act = lane < n2;
-  const long np = pairs_at_level(nb, k);
-  const long qs = (long)gridDim.x * wpb;
-  long q = (long)blockIdx.x * wpb + warp;
-  int src_next = lane;
-  if (q < np) {
-    fwd_stage<N, NRM, T>(a, q, bufs, lane);
-    const int j0 = k + (int)(2L * k * q);
-    if (act) src_next = (int)a.P[(size_t)j0 * szP(d) + lane];
+  const PipeItems<BATCH, T> items(a0, tab, map, ecnt, nent, wpb, warp);
+  const int k = a0.k;
+  // the row-map entry of a pair (read a pair ahead, into a register)
+  auto row_src = [&](const SweepArgs<T>& a, long q) -> int {
+    const int j = k + (int)(2L * k * q);
+    return lane < 2 * a.d.n ? (int)a.P[(size_t)j * szP(a.d) + lane] : lane;
+  };
+  long it = items.first;
+  int sys = 0, src_next = lane;
+  long q = 0;
+  bool have = it < items.cnt && items.pair(it, sys, q);
+  if (have) {
+    fwd_stage<N, NRM, T>(items.args(sys), k, q, bufs, lane);
+    src_next = row_src(items.args(sys), q);
   }
   cp_async_commit();
   int cur = 0;
-  for (; q < np; q += qs) {
+  for (; it < items.cnt; it += items.step) {
     const int src = src_next;
-    if (q + qs < np) {
-      fwd_stage<N, NRM, T>(a, q + qs, bufs + (cur ^ 1) * Bf::WORDS, lane);
-      const int jn = k + (int)(2L * k * (q + qs));
-      if (act) src_next = (int)a.P[(size_t)jn * szP(d) + lane];
+    int sysn = 0;
+    long qn = 0;
+    const bool haven = it + items.step < items.cnt && items.pair(it + items.step, sysn, qn);
+    if (haven) {
+      fwd_stage<N, NRM, T>(items.args(sysn), k, qn, bufs + (cur ^ 1) * Bf::WORDS, lane);
+      src_next = row_src(items.args(sysn), qn);
     }
     cp_async_commit();
-    const int j = k + (int)(2L * k * q), jp = j - k;
-    // the first right-hand side's values, loaded while the factors arrive
-    const double orig0 = act ? (lane < n ? a.x[(size_t)jp * n + lane] : a.x[(size_t)j * n + lane - n]) : 0.0;
-    cp_async_wait<1>();  // this pair's factors (the next pair's may still be in flight)
-    __syncwarp();
-    const T* buf = bufs + cur * Bf::WORDS;
-    double t[N], cp[NRM];
+    if (have) {
+      const SweepArgs<T>& a = items.args(sys);
+      const Dims d = a.d;
+      const int n = d.n, nr = d.nr, n2 = 2 * n, nrhs = a.nrhs;
+      const bool act = lane < n2;
+      const int j = k + (int)(2L * k * q), jp = j - k;
+      // the first right-hand side's values, loaded while the factors arrive
+      const double orig0 = act ? (lane < n ? a.x[(size_t)jp * n + lane] : a.x[(size_t)j * n + lane - n]) : 0.0;
+      cp_async_wait<1>();  // this pair's factors (the next pair's may still be in flight)
+      __syncwarp();
+      const T* buf = bufs + cur * Bf::WORDS;
+      double t[N], cp[NRM];
 #pragma unroll
-    for (int c = 0; c < N; ++c) t[c] = (act && c < n) ? double(buf[c * n2 + lane]) : 0.0;
+      for (int c = 0; c < N; ++c) t[c] = (act && c < n) ? double(buf[c * n2 + lane]) : 0.0;
 #pragma unroll
-    for (int r = 0; r < NRM; ++r) cp[r] = (lane < n && r < nr) ? double(buf[Bf::TT + lane * nr + r]) : 0.0;
-    for (int col = 0; col < nrhs; ++col) {
-      double* xc = a.x + (size_t)col * a.ldx;
-      const double orig =
-          col == 0 ? orig0 : (act ? (lane < n ? xc[(size_t)jp * n + lane] : xc[(size_t)j * n + lane - n]) : 0.0);
-      double w = __shfl_sync(FULL, orig, src);
+      for (int r = 0; r < NRM; ++r) cp[r] = (lane < n && r < nr) ? double(buf[Bf::TT + lane * nr + r]) : 0.0;
+      for (int col = 0; col < nrhs; ++col) {
+        double* xc = a.x + (size_t)col * a.ldx;
+        const double orig =
+            col == 0 ? orig0 : (act ? (lane < n ? xc[(size_t)jp * n + lane] : xc[(size_t)j * n + lane - n]) : 0.0);
+        double w = __shfl_sync(FULL, orig, src);
 #pragma unroll
-      for (int i = 0; i < N; ++i) {
-        if (i < n) {
-          const double wi = __shfl_sync(FULL, w, i);
-          if (lane > i && act) w = fma(-t[i], wi, w);
+        for (int i = 0; i < N; ++i) {
+          if (i < n) {
+            const double wi = __shfl_sync(FULL, w, i);
+            if (lane > i && act) w = fma(-t[i], wi, w);
+          }
         }
-      }
-      if (act) {
-        if (lane < n) xc[(size_t)j * n + lane] = w;
-        else xc[(size_t)jp * n + lane - n] = w;
-      }
-      const double wt = lane < n ? w : 0.0;
+        if (act) {
+          if (lane < n) xc[(size_t)j * n + lane] = w;
+          else xc[(size_t)jp * n + lane - n] = w;
+        }
+        const double wt = lane < n ? w : 0.0;
 #pragma unroll
-      for (int r = 0; r < NRM; ++r) {
-        if (r < nr) {
-          const double sr = warp_sum(cp[r] * wt);
-          if (lane == 0) a.XB[(size_t)j * nr * nrhs + (size_t)col * nr + r] = -sr;
+        for (int r = 0; r < NRM; ++r) {
+          if (r < nr) {
+            const double sr = warp_sum(cp[r] * wt);
+            if (lane == 0) a.XB[(size_t)j * nr * nrhs + (size_t)col * nr + r] = -sr;
+          }
         }
       }
     }
     __syncwarp();  // every lane is done with this buffer before it is refilled
     cur ^= 1;
+    have = haven;
+    sys = sysn;
+    q = qn;
   }
   cp_async_wait<0>();
 }
@@ -4234,9 +4309,9 @@ struct SweepPlan {
   void (*bwd)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*, const long*) = nullptr;
   // n = 8, 16 single systems: pipelined forward (LU) and backward levels,
   // the backward top in one CTA
-  void (*fwd_pipe)(SweepArgs<T>) = nullptr;
+  void (*fwd_pipe)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*, const long*, long) = nullptr;
   size_t fwd_pipe_smem = 0;
-  void (*bwd_pipe)(SweepArgs<T>) = nullptr;
+  void (*bwd_pipe)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*, const long*, long) = nullptr;
   size_t bwd_pipe_smem = 0;
   void (*bwd_top)(SweepArgs<T>, int, int) = nullptr;
   void (*fwd_cta)(SweepArgs<T>, const SweepArgs<T>*, const BatchCta*) = nullptr;  // CTA per pair (large n)
@@ -4329,7 +4404,8 @@ static void forward_levels(DevState& s, const SweepPlan<T>& p, const WorkSet<T>&
   for (int K = 1; K < d.nblock; K *= 2) {
     a.k = K;
     const long np = pairs_at_level(d.nblock, K);
-    if (p.fwd_pipe) p.fwd_pipe<<<grid_for(np, 8, 148 * 2), 256, p.fwd_pipe_smem, st>>>(a);
+    if (p.fwd_pipe)
+      p.fwd_pipe<<<grid_for(np, 8, 148 * 2), 256, p.fwd_pipe_smem, st>>>(a, nullptr, nullptr, nullptr, 0);
     else if (p.fwd_cta) p.fwd_cta<<<grid_for(np, 1, 148 * 8), 256, 0, st>>>(a, nullptr, nullptr);
     else if (p.fwd) p.fwd<<<grid_for(np, 8, 148 * 32), 256, 0, st>>>(a, nullptr, nullptr, nullptr);
     else k_forward_level<T><<<grid_for(np, WARPS_PANEL, 148 * 16), WARPS_PANEL * 32, smem_f, st>>>(a, nullptr, nullptr, nullptr);
@@ -4361,7 +4437,7 @@ static void last_and_backward(DevState& s, const SweepPlan<T>& p, const WorkSet<
     for (int kk = k_split; kk > 0; kk /= 2) {
       a.k = kk;
       const long np = pairs_at_level(d.nblock, kk);
-      p.bwd_pipe<<<grid_for(np, 8, 148 * 2), 256, p.bwd_pipe_smem, st>>>(a);
+      p.bwd_pipe<<<grid_for(np, 8, 148 * 2), 256, p.bwd_pipe_smem, st>>>(a, nullptr, nullptr, nullptr, 0);
       check_launch("k_backward_pipe");
     }
     return;
@@ -5432,6 +5508,26 @@ static void batch_sweeps_rows(BatchClass& c, cudaStream_t st, bool forward, int 
   const bool r4 = c.nrm <= 4, x4 = c.nxm <= 4;
   SweepArgs<T> a0{};
   a0.k = 1 << L;
+  if constexpr (N == 8 || N == 16) {
+    if (c.n == N) {  // pipelined: a fixed grid walks the level's map entries
+      const long nent = c.scnt[L];
+      const unsigned g = (unsigned)std::min<long>(nent, 148 * 2);
+      if (forward) {
+        const SweepArgs<T>* tab = static_cast<const SweepArgs<T>*>(c.sf);
+        auto* kern = r4 ? k_forward_pipe<N, 4, T, true> : k_forward_pipe<N, 8, T, true>;
+        const size_t sm = 8 * (r4 ? FwdBuf<N, 4, T>::BYTES : FwdBuf<N, 8, T>::BYTES);
+        smem_limit_once(kern, sm);
+        kern<<<g, 256, sm, st>>>(a0, tab, m.map, m.ecnt, nent);
+      } else {
+        const SweepArgs<T>* tab = static_cast<const SweepArgs<T>*>(c.sb);
+        auto* kern = x4 ? k_backward_pipe<N, 4, T, true> : k_backward_pipe<N, 8, T, true>;
+        const size_t sm = 8 * (x4 ? BwdBuf<N, 4, T>::BYTES : BwdBuf<N, 8, T>::BYTES);
+        smem_limit_once(kern, sm);
+        kern<<<g, 256, sm, st>>>(a0, tab, m.map, m.ecnt, nent);
+      }
+      return;
+    }
+  }
   if (forward) {
     const SweepArgs<T>* tab = static_cast<const SweepArgs<T>*>(c.sf);
     if (r4) k_forward_rows<T, N, 4, true, true><<<m.grid, 256, 0, st>>>(a0, tab, m.map, m.ecnt);
