@@ -2505,8 +2505,8 @@ __global__ void __launch_bounds__(256, 2) k_backward_rows(SweepArgs<TF> a0, cons
 }
 
 // ---------------------------------------------------------------------------
-// Backward sweep for FP64 factors, n = 8 or 16, single systems: the same pair
-// arithmetic as k_backward_rows (lane i < n: U-row i with D'_j, U and B'_j;
+// Backward sweep for n = 8 or 16 (FP64 or FP32 factors; single systems and
+// batch classes, see PipeItems): the same pair arithmetic as k_backward_rows (lane i < n: U-row i with D'_j, U and B'_j;
 // lane 16 + i: E'_j row i), with the factors of the warp's NEXT pair copied
 // into shared memory by cp.async (16-byte chunks, straight from the blocks'
 // column-major layout, which is also the conflict-free layout for lane = row)
@@ -2763,8 +2763,8 @@ __global__ void __launch_bounds__(512, 1) k_backward_top(SweepArgs<T> a, int k_t
 }
 
 // ---------------------------------------------------------------------------
-// Forward sweep for LU factors, n = 8 or 16, single systems: the pair
-// arithmetic of k_forward_rows (lane = position r < 2n of the stacked
+// Forward sweep for LU factors, n = 8 or 16 (FP64 or FP32; single systems and
+// batch classes, see PipeItems): the pair arithmetic of k_forward_rows (lane = position r < 2n of the stacked
 // [x_jp; x_j], row map gathered by one shuffle, n broadcast steps of L and M,
 // xb partial -C'_j x_j), with the factors of the warp's NEXT pair (the 2n x n
 // L\U and M block of T, and C_j) copied into shared memory by cp.async while
