@@ -1387,6 +1387,98 @@ struct GrpProduct<float, N> {
   }
 };
 
+// FP32 n=32: the product on the tensor cores as a 3xTF32 split
+// (mma.sync m16n8k8: a*b ~ a_small*b_big + a_big*b_small + a_big*b_big with
+// a_big = tf32(a), a_small = tf32(a - a_big), FP32 accumulators), close to
+// FP32 accuracy at a tenth of the FMA product's instructions.  Warp w owns
+// column tiles [3w, 3w+3) of all five 16-row tiles (rows >= 72 are padding).
+__device__ __forceinline__ unsigned to_tf32(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void split_tf32(float x, unsigned& big, unsigned& small) {
+  big = to_tf32(x);
+  small = to_tf32(x - __uint_as_float(big));
+}
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+template <>
+struct GrpProduct<float, 32> {
+  static constexpr int N = 32;
+  using S = GrpShape<float, N>;
+  static constexpr int M16 = (S::MT + 15) / 16, NPW = S::NTILES / S::NWA;
+  static_assert(S::NTILES % S::NWA == 0, "column tiles per warp");
+  template <typename Out>
+  __device__ static void run(const float* Wt, const float* Gs, const int* rowof, int t, Out out) {
+    const int w = t >> 5, lane = t & 31, g = lane >> 2, q = lane & 3;
+    float acc[M16][NPW][4];
+    // [0; (P W)_bot; 0]: accumulator element c0..c3 = (row r, col c), (r, c+1),
+    // (r+8, c), (r+8, c+1) with r = 16 mi + g, c = 8 nt + 2q
+#pragma unroll
+    for (int mi = 0; mi < M16; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < NPW; ++ni) {
+        const int col = (w * NPW + ni) * 8 + 2 * q;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int row = mi * 16 + g + 8 * h;
+          const bool bot = row >= N && row < 2 * N;
+          const int orow = bot ? rowof[row] : 0;
+          acc[mi][ni][2 * h] = bot ? w_at<float, N>(Wt, orow, col) : 0.0f;
+          acc[mi][ni][2 * h + 1] = bot ? w_at<float, N>(Wt, orow, col + 1) : 0.0f;
+        }
+      }
+#pragma unroll
+    for (int ks = 0; ks < N / 8; ++ks) {
+      // B fragment of (P W)_top: (k = 8 ks + q, col = 8 nt + g) and k + 4
+      const int o0 = rowof[ks * 8 + q], o1 = rowof[ks * 8 + q + 4];
+      unsigned bb[NPW][2], bs[NPW][2];
+#pragma unroll
+      for (int ni = 0; ni < NPW; ++ni) {
+        const int col = (w * NPW + ni) * 8 + g;
+        split_tf32(w_at<float, N>(Wt, o0, col), bb[ni][0], bs[ni][0]);
+        split_tf32(w_at<float, N>(Wt, o1, col), bb[ni][1], bs[ni][1]);
+      }
+#pragma unroll
+      for (int mi = 0; mi < M16; ++mi) {
+        // A fragment of G: (r, k), (r + 8, k), (r, k + 4), (r + 8, k + 4)
+        const int r0 = mi * 16 + g, r1 = r0 + 8, kk = ks * 8 + q;
+        const float av[4] = {r0 < S::MT ? Gs[r0 * S::LDG + kk] : 0.0f, r1 < S::MT ? Gs[r1 * S::LDG + kk] : 0.0f,
+                             r0 < S::MT ? Gs[r0 * S::LDG + kk + 4] : 0.0f,
+                             r1 < S::MT ? Gs[r1 * S::LDG + kk + 4] : 0.0f};
+        unsigned ab[4], as[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) split_tf32(av[e], ab[e], as[e]);
+#pragma unroll
+        for (int ni = 0; ni < NPW; ++ni) {
+          mma_tf32(acc[mi][ni], as, bb[ni][0], bb[ni][1]);
+          mma_tf32(acc[mi][ni], ab, bs[ni][0], bs[ni][1]);
+          mma_tf32(acc[mi][ni], ab, bb[ni][0], bb[ni][1]);
+        }
+      }
+    }
+#pragma unroll
+    for (int mi = 0; mi < M16; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < NPW; ++ni)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int row = mi * 16 + g + 8 * h, col = (w * NPW + ni) * 8 + 2 * q;
+          if (row < S::MT) {
+            out(row, col, acc[mi][ni][2 * h]);
+            out(row, col + 1, acc[mi][ni][2 * h + 1]);
+          }
+        }
+  }
+};
+
 // CTAs per SM the register budget is sized for (FP64 n=32 is shared-memory
 // bound at 5, FP32 n=32 register bound at 6)
 template <typename T, int N>
