@@ -1242,7 +1242,8 @@ __global__ void __launch_bounds__(128, 4) k_factor_tree_tc(FactorArgs<double> a,
 // search spans the panel warps: each publishes its best candidate row and its
 // reciprocal, one barrier per column, double-buffered by column parity); the
 // operator G = [L^-1; -M L^-1; -C' L^-1]; one product G * (P W)_top, on the
-// FP64 tensor cores (DMMA 8x8x4) for double and on the FP32 pipe for float.
+// FP64 tensor cores (DMMA 8x8x4) for double, as a 3xTF32 split on the tensor
+// cores for float at n = 32, on the FP32 pipe for float at n = 16.
 // ---------------------------------------------------------------------------
 template <typename T> __device__ __forceinline__ T rcp_rn(T x);
 template <> __device__ __forceinline__ double rcp_rn<double>(double x) { return __drcp_rn(x); }
