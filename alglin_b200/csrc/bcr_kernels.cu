@@ -5125,9 +5125,6 @@ struct SweepMap {
   unsigned grid;
 };
 
-// border rows of a batched system (batch_family_ok admits nr <= 8 only)
-constexpr int BATCH_NR_MAX = 8;
-
 // r = b - (D_k x_k + E_k x_{k+1} + B_k xb) on block rows [k0, k1) of one
 // system, written into the rhs slot; the largest |r| and (with_A) the largest
 // row sum of |A| over this thread's rows
@@ -5197,7 +5194,7 @@ __global__ void __launch_bounds__(128) kb_residual_rows(const ResDesc* t, const 
 // |r|/(|A||x|+|b|), the converged flag and the batch-worst figure (bits of a
 // non-negative double, so an integer max orders them).  Bit for bit the
 // residual of add_Mv (cc:2118-2166) on the loaded FP64 matrix.
-__global__ void __launch_bounds__(256) kb_residual(const ResDesc* t, int with_A, double tol,
+__global__ void __launch_bounds__(256, 2) kb_residual(const ResDesc* t, int with_A, double tol,
                                                    unsigned long long* worst) {
   __shared__ double sv[32];
   const ResDesc& R = t[blockIdx.x];
@@ -5228,49 +5225,81 @@ __global__ void __launch_bounds__(256) kb_residual(const ResDesc* t, int with_A,
     mr = fmax(mr, fabs(r));
     ma = fmax(ma, with_A ? sa : 0.0);
   }
-  // border rows (nr <= BATCH_NR_MAX in a batch): one walk over every block
-  // column accumulates all of them, each row's terms in the same order as a
-  // walk of its own; then one CTA reduction per row
-  double bs_s[BATCH_NR_MAX], bs_a[BATCH_NR_MAX];
+  // border rows, four at a time: one walk over every block column
+  // accumulates four rows, each row's terms in the same order as a walk of
+  // its own; then one CTA reduction per row.  A thread's columns e = tid,
+  // tid + bs, ... are loaded RES_U at a time before any is added, so a lone
+  // long system (the late refinement passes) pays one load latency per RES_U
+  // columns; the additions keep the column order.
+  constexpr int RES_U = 4;
+  const long tot = (long)(nb + 1) * n;
+  const long dk = bs / n;
+  const int dc = bs % n;
+  for (int r0 = 0; r0 < nr; r0 += 4) {
+    double s4[4] = {0.0, 0.0, 0.0, 0.0}, a4[4] = {0.0, 0.0, 0.0, 0.0};
+    size_t k = (size_t)(tid / n);  // block and column of element e
+    int c = tid % n;
+    for (long e0 = tid; e0 < tot; e0 += (long)RES_U * bs) {
+      double xv[RES_U], cv[RES_U][4];
 #pragma unroll
-  for (int rr = 0; rr < BATCH_NR_MAX; ++rr) bs_s[rr] = bs_a[rr] = 0.0;
-  if (nr > 0) {
-    for (long e = tid; e < (long)(nb + 1) * n; e += bs) {
-      const size_t k = (size_t)(e / n);
-      const int c = (int)(e % n);
-      const double xv = xs[k * n + c];
-      const double* cp = R.C0 + k * nrn + (size_t)c * nr;
+      for (int u = 0; u < RES_U; ++u) {
+        const bool on = e0 + (long)u * bs < tot;
+        const double* cp = R.C0 + k * nrn + (size_t)c * nr + r0;
+        xv[u] = on ? xs[k * n + c] : 0.0;
 #pragma unroll
-      for (int rr = 0; rr < BATCH_NR_MAX; ++rr) {
-        if (rr < nr) {
-          const double cv = cp[rr];
-          bs_s[rr] = fma(cv, xv, bs_s[rr]);
-          bs_a[rr] += fabs(cv);
+        for (int i = 0; i < 4; ++i) cv[u][i] = (on && r0 + i < nr) ? cp[i] : 0.0;
+        k += dk;
+        c += dc;
+        if (c >= n) { c -= n; ++k; }
+      }
+#pragma unroll
+      for (int u = 0; u < RES_U; ++u) {
+        if (e0 + (long)u * bs >= tot) break;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          if (r0 + i < nr) {
+            s4[i] = fma(cv[u][i], xv[u], s4[i]);
+            a4[i] += fabs(cv[u][i]);
+          }
         }
       }
     }
-  }
 #pragma unroll
-  for (int rr = 0; rr < BATCH_NR_MAX; ++rr) {
-    if (rr >= nr) break;
-    double s = bs_s[rr], sa = bs_a[rr];
-    for (int c = tid; c < qx; c += bs) { s = fma(R.Cq[(size_t)c * nr + rr], xs[xq + c], s); sa += fabs(R.Cq[(size_t)c * nr + rr]); }
-    for (int c = tid; c < nx; c += bs) { s = fma(R.F0[(size_t)c * nr + rr], xs[xb + c], s); sa += fabs(R.F0[(size_t)c * nr + rr]); }
-    s = block_sum(s, sv);
-    sa = block_sum(sa, sv);
-    if (tid == 0) {
-      const size_t o = xN + m + rr;
-      const double r = R.b[o] - s;
-      R.r[o] = r;
-      mr = fmax(mr, fabs(r));
-      ma = fmax(ma, with_A ? sa : 0.0);
+    for (int i = 0; i < 4; ++i) {
+      const int rr = r0 + i;
+      if (rr >= nr) break;
+      double s = s4[i], sa = a4[i];
+      for (int c = tid; c < qx; c += bs) { s = fma(R.Cq[(size_t)c * nr + rr], xs[xq + c], s); sa += fabs(R.Cq[(size_t)c * nr + rr]); }
+      for (int c = tid; c < nx; c += bs) { s = fma(R.F0[(size_t)c * nr + rr], xs[xb + c], s); sa += fabs(R.F0[(size_t)c * nr + rr]); }
+      s = block_sum(s, sv);
+      sa = block_sum(sa, sv);
+      if (tid == 0) {
+        const size_t o = xN + m + rr;
+        const double r = R.b[o] - s;
+        R.r[o] = r;
+        mr = fmax(mr, fabs(r));
+        ma = fmax(ma, with_A ? sa : 0.0);
+      }
     }
   }
   const long nrows = (long)n * (nb + 1) + d.qr + nr;
   const long ncols = (long)n * (nb + 1) + qx + nx;
+  // |x| and |b|: maxima are exact in any order, so eight loads per round
   double mx = 0.0, mb = 0.0;
-  for (long e = tid; e < ncols; e += bs) mx = fmax(mx, fabs(xs[e]));
-  for (long e = tid; e < nrows; e += bs) mb = fmax(mb, fabs(R.b[e]));
+  for (long e0 = tid; e0 < ncols; e0 += 8L * bs) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = e0 + (long)u * bs < ncols ? fabs(xs[e0 + (long)u * bs]) : 0.0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) mx = fmax(mx, v[u]);
+  }
+  for (long e0 = tid; e0 < nrows; e0 += 8L * bs) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = e0 + (long)u * bs < nrows ? fabs(R.b[e0 + (long)u * bs]) : 0.0;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) mb = fmax(mb, v[u]);
+  }
   mr = block_max(mr, sv);
   mx = block_max(mx, sv);
   mb = block_max(mb, sv);
