@@ -77,6 +77,30 @@ def dist_env():
     return rank, world, local
 
 
+def replica_seeds(rank):
+    """Seeds of the system and right-hand side that `rank` solves: each replica
+    factors its own independent system (no data crosses ranks)."""
+    return rank, 1 + rank
+
+
+def max_over_ranks(dist, v, device):
+    """The slowest rank's time, known to every rank (all ranks must call it in
+    the same order); `dist` is None for a single process.  `device` is "cuda"
+    under NCCL and "cpu" under gloo."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(world, ncols, seconds):
+    """Unknowns/s of the whole job: every replica solves `ncols` unknowns in
+    `seconds` (the slowest rank's time)."""
+    return world * ncols / seconds
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -269,8 +293,9 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from alglin_b200 import bcr, synth
 
-    s = synth.collocation(**CFG, seed=rank)
-    b = synth.rhs(s, 1, seed=1 + rank)[0]
+    seed_s, seed_b = replica_seeds(rank)
+    s = synth.collocation(**CFG, seed=seed_s)
+    b = synth.rhs(s, 1, seed=seed_b)[0]
     L = max(s.nrows, s.ncols)
     h = bcr.BorderedCR()
     h.load_system(s)
@@ -311,11 +336,8 @@ def run_ours(args):
         ms = timed(bcr.GRAPH_STEP, args.steps)
     clocks = clk.summary()
     assert h.factorize_status(), h.last_error()
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * s.ncols / (ms * 1e-3)
+    ms = max_over_ranks(dist, ms, "cuda")
+    value = whole_job_value(world, s.ncols, ms * 1e-3)
     x = x_dev.cpu().numpy()
 
     if args.no_e2e:
@@ -340,11 +362,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         assert h.factorize_solve(1, xh, L), h.last_error()
         te.append(time.perf_counter() - t0)
-    e2e_t = statistics.median(te)
-    if dist:
-        t = torch.tensor([e2e_t], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    e2e_t = max_over_ranks(dist, statistics.median(te), "cuda")
 
     fact_b, solve_b = algorithmic_bytes(CFG)
     peak, peak_kind = load_peaks()
@@ -370,7 +388,7 @@ def run_ours(args):
                                            "workload at nblock=40000, 21,542 B per block, scaled to "
                                            "100000 blocks (profiles/dram_factor_solve_n16_nblock40000.md)",
                          "algorithmic_bytes": fact_b},
-            "e2e": {"value": world * s.ncols / e2e_t, "unit": "unknowns/s",
+            "e2e": {"value": whole_job_value(world, s.ncols, e2e_t), "unit": "unknowns/s",
                     "h2d_bytes_per_step": nbytes_mat + 8 * L, "d2h_bytes_per_step": 8 * L},
             "gpu_launches": launches_per_step(CFG["nblock"], CFG["nr"], CFG["nx"]) * args.steps,
             "clocks": clocks,
